@@ -1,0 +1,138 @@
+// Stable LSD radix sort of (uint64 key, uint32 value) pairs, 8 bits per
+// pass: per-tile digit histograms -> one exclusive scan (digit-major, so the
+// result is stable across tiles) -> scatter with in-tile stable ranks from
+// warp match masks. HBM-bound: each pass reads 12 B and writes 12 B per
+// element plus the key read of the histogram pass.
+#include <algorithm>
+
+#include "amk_internal.cuh"
+
+namespace amk {
+namespace {
+
+constexpr int kSortThreads = 256;
+constexpr int kItems = 16;
+constexpr int kTile = kSortThreads * kItems;
+constexpr int kWarps = kSortThreads / 32;
+
+__global__ void __launch_bounds__(kSortThreads)
+hist_kernel(const uint64_t* __restrict__ keys, long n, int shift, int nb, uint32_t* __restrict__ hist) {
+  __shared__ uint32_t h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const long base = static_cast<long>(blockIdx.x) * kTile;
+#pragma unroll 4
+  for (int k = 0; k < kItems; ++k) {
+    const long i = base + k * kSortThreads + threadIdx.x;
+    if (i < n) atomicAdd(&h[(keys[i] >> shift) & 0xFF], 1u);
+  }
+  __syncthreads();
+  hist[static_cast<long>(threadIdx.x) * nb + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of `len` counters with one CTA of 1024 threads.
+__global__ void __launch_bounds__(1024) scan_kernel(uint32_t* __restrict__ data, long len) {
+  __shared__ uint32_t s[1024];
+  const long per = (len + 1023) / 1024;
+  const long b = threadIdx.x * per;
+  const long e = min(len, b + per);
+  uint32_t sum = 0;
+  for (long i = b; i < e; ++i) sum += data[i];
+  s[threadIdx.x] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    uint32_t v = threadIdx.x >= off ? s[threadIdx.x - off] : 0u;
+    __syncthreads();
+    s[threadIdx.x] += v;
+    __syncthreads();
+  }
+  uint32_t run = s[threadIdx.x] - sum;
+  for (long i = b; i < e; ++i) {
+    const uint32_t v = data[i];
+    data[i] = run;
+    run += v;
+  }
+}
+
+__global__ void __launch_bounds__(kSortThreads)
+scatter_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, long n, int shift, int nb,
+               const uint32_t* __restrict__ offs, uint64_t* __restrict__ kout, uint32_t* __restrict__ vout) {
+  __shared__ uint32_t cnt[kWarps][256];
+  __shared__ uint32_t running[256];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  running[threadIdx.x] = 0;
+  const uint32_t base_off = 0;
+  (void)base_off;
+  const long base = static_cast<long>(blockIdx.x) * kTile;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  for (int k = 0; k < kItems; ++k) {
+    const long i = base + k * kSortThreads + threadIdx.x;
+    const bool valid = i < n;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) cnt[w][threadIdx.x] = 0;
+    __syncthreads();
+    uint64_t key = 0;
+    uint32_t val = 0;
+    int d = 0;
+    uint32_t rank = 0;
+    const uint32_t active = __ballot_sync(0xffffffffu, valid);
+    if (valid) {
+      key = kin[i];
+      val = vin[i];
+      d = static_cast<int>((key >> shift) & 0xFF);
+      const uint32_t peers = __match_any_sync(active, d);
+      rank = __popc(peers & lt_mask);
+      if ((peers & lt_mask) == 0) cnt[warp][d] = __popc(peers);
+    }
+    __syncthreads();
+    if (valid) {
+      uint32_t pre = running[d] + rank;
+      for (int w = 0; w < warp; ++w) pre += cnt[w][d];
+      const long pos = static_cast<long>(offs[static_cast<long>(d) * nb + blockIdx.x]) + pre;
+      kout[pos] = key;
+      vout[pos] = val;
+    }
+    __syncthreads();
+    uint32_t add = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) add += cnt[w][threadIdx.x];
+    running[threadIdx.x] += add;
+    __syncthreads();
+  }
+}
+
+}  // namespace
+
+int radix_sort_pairs(amk_ctx* c, const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out,
+                     uint32_t* vals_out, long n, int key_bits) {
+  if (n <= 0) return AMK_OK;
+  if (n > 0xFFFFFFF0L) return fail(AMK_ERR_LIMIT, "radix sort of %ld elements exceeds 32-bit ranks", n);
+  const int passes = std::max(1, (key_bits + 7) / 8);
+  const int nb = static_cast<int>((n + kTile - 1) / kTile);
+  int rc = AMK_OK;
+  uint64_t* kt = slot<uint64_t>(c, kSlotKeysB, static_cast<size_t>(n), &rc);
+  AMK_TRY(rc);
+  uint32_t* vt = slot<uint32_t>(c, kSlotValsB, static_cast<size_t>(n), &rc);
+  AMK_TRY(rc);
+  uint32_t* hist = slot<uint32_t>(c, kSlotSortHist, static_cast<size_t>(256) * nb, &rc);
+  AMK_TRY(rc);
+  const uint64_t* ksrc = keys_in;
+  const uint32_t* vsrc = vals_in;
+  for (int p = 0; p < passes; ++p) {
+    const bool to_out = ((passes - 1 - p) % 2) == 0;
+    uint64_t* kdst = to_out ? keys_out : kt;
+    uint32_t* vdst = to_out ? vals_out : vt;
+    const int shift = 8 * p;
+    hist_kernel<<<nb, kSortThreads, 0, c->stream>>>(ksrc, n, shift, nb, hist);
+    AMK_TRY(check_launch(c, "hist_kernel"));
+    scan_kernel<<<1, 1024, 0, c->stream>>>(hist, static_cast<long>(256) * nb);
+    AMK_TRY(check_launch(c, "scan_kernel"));
+    scatter_kernel<<<nb, kSortThreads, 0, c->stream>>>(ksrc, vsrc, n, shift, nb, hist, kdst, vdst);
+    AMK_TRY(check_launch(c, "scatter_kernel"));
+    ksrc = kdst;
+    vsrc = vdst;
+  }
+  return AMK_OK;
+}
+
+}  // namespace amk

@@ -1,0 +1,388 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 particle path; prints ONE JSON line on rank 0.
+
+Workload (default ``direct65k``): the plain direct all-pairs Coulomb run --
+N = 65,536 (32,768 positrons + 32,768 antiprotons, real charges and masses),
+uniform ellipsoidal cloud with radii 2e-4 x 2e-4 x 5e-4 m drawn by the
+reference's own generator (seed 42), Maxwellian velocities at 10 K, b0 = 3 T,
+trap_voltage = 50 V, z0 = rho0 = 0.01 m, dt from the reference's rule
+(2.977e-12 s), FP32 pair arithmetic with compensated accumulation and FP64
+state, cooling and annihilation off. One bench step = one simulation step
+(all-pairs force -> Boris push) of the whole cloud.
+
+``value`` is particle-steps/s over all ranks with the state resident in HBM
+(device-timed with CUDA events on the library's stream, L2 flushed by a
+256 MiB write between steps, the flush outside the per-step events). ``e2e``
+is the same metric through the C ABI with host buffers: every step uploads
+x, v from pinned host memory (amk_update_state), steps, and reads x, v and
+the alive flags back (amk_get_particles).
+
+``--impl reference`` times the reference's own CPU code for the same step on
+the host cores (its Barnes-Hut tree at theta = 0, i.e. the exact all-pairs
+sum, compiled from the reference sources into oracle/_ref, plus the FP64
+push restatement), on a bounded sample of targets per step.
+
+Multi-GPU: the single-instance run does not shard (replicas only); under
+torchrun every rank runs its own replica and ``value`` sums them over the
+slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "antimatter-kernel_b200"))
+
+METRIC = "particle-steps/s at ≤1e-5 force err vs FP64 direct: learned/batched vs plain"
+UNIT = "particle-steps/s"
+E = 1.602176634e-19
+
+
+def workload_direct65k():
+    import amk
+    p = amk.make_params(
+        seed=42, b0=3.0, trap_voltage=50.0, z0=0.01, rho0=0.01, num_steps=1000,
+        populations={"antiproton": 32768, "positron": 32768},
+        temperatures={"antiproton": 10.0, "positron": 10.0},
+        cloud_radii=(2e-4, 2e-4, 5e-4), bath_temperature=0.0, cooling_scale=0.0,
+        cooling_enabled=0, coulomb_forces_enabled=1, coulomb_method="allpairs",
+        energy_method="allpairs", annihilation_enabled=0)
+    config = {"workload": "direct all-pairs Coulomb + Boris push, N=65,536 "
+                          "(32,768 e+ + 32,768 pbar), uniform ellipsoid 2e-4 x 2e-4 x 5e-4 m, "
+                          "10 K Maxwellian, b0=3 T, U=50 V, z0=rho0=0.01 m, dt=2.977e-12 s",
+              "n_particles": 65536, "solver": "allpairs (tiled FP32, double-float positions, "
+                                                  "compensated accumulation)",
+              "state_precision": "fp64 positions/velocities", "cooling": False,
+              "annihilation": False, "seed": 42,
+              "l2": "flushed between steps by a 256 MiB write (inputs 6.5 MB < L2)"}
+    return p, config
+
+
+WORKLOADS = {"direct65k": workload_direct65k}
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.rows = []
+        self.proc = None
+        self.device_index = device_index
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device_index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for k, name in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ helpers
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def max_over_ranks(value, world, device):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _dp(ptr):
+    return C.cast(C.c_void_p(ptr), C.POINTER(C.c_double))
+
+
+# ------------------------------------------------------------------ CPU legs
+def cpu_reference_step_time(x, y, z, q, m, n_sample, seed=0):
+    """Reference CPU step on a bounded sample: the reference's Barnes-Hut tree
+    at theta = 0 (exact all-pairs) over all N sources, walked for n_sample
+    targets and extrapolated to N, plus the FP64 push of all N particles.
+    Returns (seconds per full step, kind, sampled target ids, sampled forces)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_lib as O
+    n = len(x)
+    rng = np.random.default_rng(seed)
+    targets = np.sort(rng.choice(n, n_sample, replace=False))
+    if O.ref_available():
+        kind = "reference"
+        t0 = time.perf_counter()
+        O.ref_bh_forces_subset(x, y, z, q, 0.0, targets[:1], 8)
+        t_build = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        f = O.ref_bh_forces_subset(x, y, z, q, 0.0, targets, 8)
+        t_walk = max(time.perf_counter() - t0 - t_build, 1e-9)
+    else:
+        kind = "port"
+        t_build = 0.0
+        t0 = time.perf_counter()
+        f = O.allpairs_subset(x, y, z, q, targets)
+        t_walk = time.perf_counter() - t0
+    state = dict(x=x.copy(), y=y.copy(), z=z.copy(), vx=np.zeros(n), vy=np.zeros(n), vz=np.zeros(n),
+                 q=q, m=m, alive=np.ones(n, np.uint8))
+    t0 = time.perf_counter()
+    O.boris_push(state, np.zeros(n), np.zeros(n), np.zeros(n), 3.0, 50.0, 0.01, 0.01, 2.977e-12, True)
+    t_push = time.perf_counter() - t0
+    return t_build + t_walk * n / n_sample + t_push, kind, targets, f
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    import amk
+    p, config = WORKLOADS[args.workload]()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_lib as O
+    pops = {"antiproton": 32768, "positron": 32768}
+    pos = O.initial_positions(pops, [2e-4, 2e-4, 5e-4], 42)
+    sp = O.species_column(pops)
+    m, q = O.species_props(sp)
+    x, y, z = pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy()
+    sample = args.ref_sample
+    times = []
+    kind = "reference"
+    for k in range(args.warmup + args.steps):
+        t, kind, _, _ = cpu_reference_step_time(x, y, z, q, m, sample, seed=k)
+        if k >= args.warmup:
+            times.append(t)
+    t_step = float(np.mean(times))
+    value = len(x) / t_step
+    cores = os.cpu_count()
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (reference initial-condition generator, seed 42)", "config": config,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
+                             "sample": f"per step: tree over all {len(x)} sources, theta=0 walks for "
+                                       f"{sample} sampled targets extrapolated to {len(x)}, FP64 "
+                                       f"push of all {len(x)}"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_amk(args):
+    import torch
+    import amk
+    world, rank, local = dist_setup()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    p, config = WORKLOADS[args.workload]()
+    sim = amk.Simulation(p, device=local)
+    sim.init_particles()
+    n = sim.num_particles()
+    stream = torch.cuda.ExternalStream(sim.stream(), device=device)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    def flush_l2(k):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    # ---------------- warm-up
+    for k in range(args.warmup):
+        sim.step(1)
+        flush_l2(k)
+    sim.synchronize()
+
+    # ---------------- timed region (resident state)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = sim.kernel_launches()
+    for k in range(args.steps):
+        starts[k].record(stream)
+        sim.step(1)
+        ends[k].record(stream)
+        flush_l2(k)
+    torch.cuda.synchronize()
+    barrier()
+    launches = sim.kernel_launches() - launches0
+    clocks = sampler.stop()
+    total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    total_ms = max_over_ranks(total_ms, world, device)
+    value = world * n * args.steps / (total_ms * 1e-3)
+
+    # ---------------- roofline of the dominant kernel (live phase events)
+    prof_steps = min(args.steps, 50)
+    sim.set_profiling(True)
+    sim.reset_phase_times()
+    for k in range(prof_steps):
+        sim.step(1)
+        flush_l2(k)
+    sim.synchronize()
+    phases = sim.phase_times()
+    sim.set_profiling(False)
+    ap_ms, ap_launches = phases["allpairs"]
+    ap_avg_ms = ap_ms / max(ap_launches, 1)
+    flops_per_launch = 20.0 * n * (n - 1)
+    achieved = flops_per_launch / (ap_avg_ms * 1e-3) / 1e12
+    peak = sim.measure_fp32_peak()
+    roofline = {"bound": "fp32", "kernel": "allpairs_kernel", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": "measured in this run: FFMA probe kernel over all SMs "
+                               "(2 flop/FFMA); no FP32 figure in the driver's peak file",
+                "flops_per_launch": flops_per_launch,
+                "flop_convention": "20 flop per pair interaction x N(N-1) pairs",
+                "avg_launch_ms": ap_avg_ms,
+                "phase_ms_per_step": {k: v[0] / max(prof_steps, 1) for k, v in phases.items() if v[1]}}
+
+    # ---------------- end to end through the C ABI with host buffers
+    L = amk.lib()
+    host = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in
+            ("x", "y", "z", "vx", "vy", "vz")}
+    alive = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    ptr = {k: v.data_ptr() for k, v in host.items()}
+    order = ("x", "y", "z", "vx", "vy", "vz")
+    amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k]) for k in order],
+                                  C.cast(C.c_void_p(alive.data_ptr()), C.POINTER(C.c_uint8))))
+    e2e_steps = args.steps
+    barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for k in range(e2e_steps):
+        sim.update_state(*[ptr[k2] for k2 in order])
+        sim.step(1)
+        amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k2]) for k2 in order],
+                                      C.cast(C.c_void_p(alive.data_ptr()), C.POINTER(C.c_uint8))))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1), world, device)
+    e2e_value = world * n * e2e_steps / (e2e_ms * 1e-3)
+    e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 6 * 8 * n,
+           "d2h_bytes_per_step": 6 * 8 * n + n, "steps": e2e_steps,
+           "api": "amk_update_state + amk_step + amk_get_particles (pinned host buffers)"}
+
+    # ---------------- CPU baseline + force check (rank 0, one GPU only)
+    cpu = None
+    err = None
+    if rank == 0 and world == 1:
+        st = sim.get_particles()
+        sim.coulomb_allpairs()
+        fx, fy, fz = sim.get_forces()
+        q = np.where(np.asarray(_species(sim, p)) == 1, E, -E)
+        m = np.where(np.asarray(_species(sim, p)) == 1, 9.1093837015e-31, 1.67262192369e-27)
+        t_step, kind, targets, fref = cpu_reference_step_time(st["x"], st["y"], st["z"], q, m,
+                                                              args.cpu_sample)
+        cpu = {"value": n / t_step, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
+               "sample": f"reference Barnes-Hut theta=0 (exact all-pairs) tree over all {n} "
+                         f"sources walked for {args.cpu_sample} sampled targets, extrapolated to "
+                         f"{n}, + FP64 push of all {n}; OpenMP on all host cores"}
+        num = np.sqrt((fx[targets] - fref[0]) ** 2 + (fy[targets] - fref[1]) ** 2 +
+                      (fz[targets] - fref[2]) ** 2)
+        den = np.sqrt(fref[0] ** 2 + fref[1] ** 2 + fref[2] ** 2)
+        rel = num / den
+        err = {"rms_rel": float(np.sqrt(np.mean(rel ** 2))), "max_rel": float(np.max(rel)),
+               "targets": int(len(targets)), "against": f"{kind} FP64 exact sum"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+                "data": "synthetic (reference initial-condition generator, seed 42)",
+                "config": dict(config, parallelism=f"replicas x{world} (single instance does not shard)"),
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clocks, "force_error_vs_fp64": err}
+        print(json.dumps(line), flush=True)
+    sim.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def _species(sim, p):
+    # species in creation order: populations in enum order (antiproton, positron)
+    out = []
+    for i in sorted(range(p.n_species), key=lambda k: p.species[k]):
+        out += [p.species[i]] * p.populations[i]
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["amk", "reference"], default="amk")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="direct65k")
+    ap.add_argument("--cpu-sample", type=int, default=8192,
+                    help="targets walked by the CPU baseline leg")
+    ap.add_argument("--ref-sample", type=int, default=256,
+                    help="targets walked per step by the reference arm")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)  # at least three untimed warm-up steps
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_amk(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,293 @@
+/*
+ * amk.h -- C ABI of the B200-native antimatter-kernel particle path.
+ *
+ * One shared library (libamk.so, sm_100a) replaces the reference's per-step
+ * hot path: the three Coulomb solvers, the Boris push in the Penning-trap
+ * field with cyclotron cooling, the annihilation contact search and the
+ * energy diagnostics. Particle state lives in HBM as structure-of-arrays
+ * (positions and velocities FP64, trap-centred) for the life of a context.
+ *
+ * Conventions (all functions):
+ *   - return AMK_OK (0) or a negative AMK_ERR_* code; nothing throws across
+ *     the ABI; amk_last_error() gives a message for the calling thread;
+ *   - host buffers are caller-owned and only read/written during the call;
+ *   - device buffers are owned by the context; one CUDA stream per context;
+ *     a context is not re-entrant (one host thread at a time);
+ *   - SI units throughout (m, m/s, kg, C, N, J, s).
+ *
+ * Reference interfaces replaced (paths inside the antimatter-kernel tree):
+ *   ComputeStandardCoulombForces      src/interaction/coulomb_interaction.h:10
+ *   ComputeBarnesHutCoulombForces     src/interaction/barnes-hut.h:76
+ *   BarnesHutTree                     src/interaction/barnes-hut.h:28-74
+ *   ComputeFastMultipoleCoulombForces src/interaction/fast-multipole.h:73
+ *   FastMultipoleSolver               src/interaction/fast-multipole.h:46-71
+ *   LorentzForce::Run                 src/forces/lorentz.h:15-35
+ *   CyclotronCooling::Run             src/forces/cooling.h:16-40
+ *   AnnihilationInteraction::Run      src/interaction/annihilation.h:11-20
+ *   ComputeTotalEnergy                src/analysis/energy_analysis.h:35
+ *   PhysicsParams/InteractionParams/StochasticParams::LoadParams
+ *                                     src/params/*_params.h
+ */
+#ifndef AMK_H_
+#define AMK_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------ status codes */
+#define AMK_OK 0
+#define AMK_ERR_INVALID (-1)     /* bad argument or configuration            */
+#define AMK_ERR_CUDA (-2)        /* CUDA runtime error                       */
+#define AMK_ERR_NOMEM (-3)       /* device allocation failed                 */
+#define AMK_ERR_STATE (-4)       /* call made in the wrong state             */
+#define AMK_ERR_TIMEOUT (-5)     /* a bounded device-side wait gave up       */
+#define AMK_ERR_UNSUPPORTED (-6) /* option not built                         */
+#define AMK_ERR_LIMIT (-7)       /* size beyond a documented maximum         */
+#define AMK_ERR_IO (-8)          /* file could not be read                   */
+
+/* ------------------------------------------------------------ enumerations */
+/* Coulomb / energy methods: interaction_params.cc:14-28 ("standard",
+ * "barnes-hut", "fast-multipole") plus the tiled all-pairs direct sum. */
+#define AMK_METHOD_STANDARD 0
+#define AMK_METHOD_BARNES_HUT 1
+#define AMK_METHOD_FAST_MULTIPOLE 2
+#define AMK_METHOD_ALLPAIRS 3
+
+/* ParticleSpecies, src/agents/particle_species.h:9-17 (same values). */
+#define AMK_ANTIPROTON 0
+#define AMK_POSITRON 1
+#define AMK_ANTIHYDROGEN 2
+#define AMK_ELECTRON 3
+#define AMK_PROTON 4
+#define AMK_ANTIHELIUM 5
+#define AMK_MAX_SPECIES 6
+
+/* ------------------------------------------------------------ parameters */
+/* Mirrors the params.json keys read by physics_params.cc:42-100,
+ * interaction_params.cc:30-47 and stochastic_params.cc:13-24. */
+typedef struct amk_params {
+  int seed;                     /* "seed"                                  */
+  double b0;                    /* "b0" [T]                                */
+  double trap_voltage;          /* "trap_voltage" [V]                      */
+  double z0;                    /* "z0" [m]                                */
+  double rho0;                  /* "rho0" [m]                              */
+  double dt;                    /* derived, physics_params.cc:60-74 [s]    */
+  long num_steps;               /* "num_steps"                             */
+  double bath_temperature;      /* "bath_temperature" [K]                  */
+  double cooling_scale;         /* "cooling_scale"                         */
+  int cooling_enabled;          /* cooling behaviour attached (default 1)  */
+  int coulomb_forces_enabled;   /* "coulomb_forces_enabled"                */
+  int coulomb_method;           /* "coulomb_computation_method"            */
+  int energy_method;            /* "energy_computation_method"             */
+  double cutoff_radius;         /* "cutoff_radius" [m]                     */
+  double barnes_hut_theta;      /* "barnes_hut_theta"                      */
+  double fast_multipole_order;  /* "fast_multipole_order" (real, truncated) */
+  double fast_multipole_theta;  /* "fast_multipole_theta"                  */
+  int fmm_learned;              /* learned p=2 correction (no reference key) */
+  int annihilation_enabled;     /* "annihilation_enabled"                  */
+  double contact_radius;        /* "contact_radius" [m]                    */
+  double annihilation_probability; /* "annihilation_probability"          */
+  int n_species;                /* entries of "particle_populations"       */
+  int species[AMK_MAX_SPECIES];
+  long populations[AMK_MAX_SPECIES];
+  double temperatures[AMK_MAX_SPECIES]; /* "particle_temperatures" [K]    */
+  double cloud_radii[3];        /* "initial_cloud_radii" radius_x/y/z [m] */
+} amk_params;
+
+/* Defaults of the reference's ParamGroups (physics_params.h:21-46,
+ * interaction_params.h:28-55, stochastic_params.h:11-29). */
+int amk_params_default(amk_params* out);
+
+/* Reads a params.json file with the reference's keys. Missing keys keep the
+ * values already in *inout; dt is re-derived as physics_params.cc:60-74 does.
+ * Method strings accept "standard", "barnes-hut", "fast-multipole" (and the
+ * README spellings "barnes_hut", "fast_multipole", plus "allpairs"). */
+int amk_params_load_json(const char* path, amk_params* inout);
+
+/* Validation of physics_params.cc:126-160, interaction_params.cc:71-115 and
+ * stochastic_params.cc:35-46. `strict` = 1 keeps the reference's
+ * cooling_scale <= 1 rule (physics_params.cc:139). */
+int amk_params_validate(const amk_params* p, int strict);
+
+/* dt rule of physics_params.cc:60-74 for a species list. */
+double amk_dt_for_species(int n_species, const int* species, double b0);
+
+/* Default mass [kg] and charge [C], particle_species.h:27-46. */
+int amk_species_properties(int species, double* mass, double* charge);
+
+/* Characteristic dimension d = sqrt(z0^2/2 + rho0^2/4), penning_trap.cc:15-20. */
+double amk_trap_dimension(double z0, double rho0);
+
+/* Perpendicular-energy e-folding time, cooling.cc:16-22. */
+double amk_cooling_time(double charge, double mass, double b_mag);
+
+/* ------------------------------------------------------------ context */
+typedef struct amk_ctx amk_ctx;
+
+/* Creates a context on CUDA device `device` with its own stream. */
+int amk_create(const amk_params* params, int device, amk_ctx** out);
+int amk_destroy(amk_ctx* ctx);
+
+/* Last error message of the calling thread (never NULL). */
+const char* amk_last_error(void);
+
+/* Replaces the context's stream (a cudaStream_t; NULL = the context's own). */
+int amk_set_stream(amk_ctx* ctx, void* cuda_stream);
+int amk_get_stream(amk_ctx* ctx, void** cuda_stream);
+int amk_synchronize(amk_ctx* ctx);
+
+/* Updates the physics/interaction/stochastic parameters of a live context. */
+int amk_set_params(amk_ctx* ctx, const amk_params* params);
+int amk_get_params(const amk_ctx* ctx, amk_params* out);
+
+/* ------------------------------------------------------------ particles */
+/* Loads n particles from host arrays (positions trap-centred). Mass and
+ * charge come from the species defaults; all particles start alive; the
+ * first push back-staggers v by dt/2 (lorentz.cc:56-60). */
+int amk_set_particles(amk_ctx* ctx, long n, const double* x, const double* y,
+                      const double* z, const double* vx, const double* vy,
+                      const double* vz, const uint8_t* species);
+
+/* Same, from device pointers already resident on the context's device. */
+int amk_set_particles_device(amk_ctx* ctx, long n, const double* x, const double* y,
+                             const double* z, const double* vx, const double* vy,
+                             const double* vz, const uint8_t* species);
+
+/* Overwrites positions and velocities of the current particle set from host
+ * arrays (same n; species, alive flags, step counter and the half-step
+ * stagger are kept). For callers that keep the state on the host and hand
+ * it to the GPU each step. */
+int amk_update_state(amk_ctx* ctx, const double* x, const double* y, const double* z,
+                     const double* vx, const double* vy, const double* vz);
+
+/* Overrides per-particle charge and mass (ChargedAntiparticle::SetCharge /
+ * SetMass). Either pointer may be NULL. */
+int amk_set_charge_mass(amk_ctx* ctx, const double* charge, const double* mass);
+
+/* Builds the reference's initial cloud from the context's parameters
+ * (penning_trap.cc:51-160: uniform ellipsoid by rejection sampling with
+ * std::default_random_engine(seed), Maxwellian velocities with a fresh
+ * std::mt19937(seed) per species) and loads it. */
+int amk_init_particles(amk_ctx* ctx);
+
+/* Copies the state back. Any pointer may be NULL. alive[i] = 0 once
+ * annihilated. */
+int amk_get_particles(amk_ctx* ctx, double* x, double* y, double* z, double* vx,
+                      double* vy, double* vz, uint8_t* alive);
+int amk_get_particles_device(amk_ctx* ctx, double* x, double* y, double* z, double* vx,
+                             double* vy, double* vz, uint8_t* alive);
+long amk_num_particles(const amk_ctx* ctx);
+long amk_num_alive(amk_ctx* ctx);
+
+/* ------------------------------------------------------------ forces */
+/* Each solver writes the Coulomb force on every alive particle into the
+ * context's force slot (the agent's coulomb_force_), which the next push
+ * consumes and zeroes (lorentz.cc:53,70). Dead or neutral particles get 0. */
+
+/* Cutoff direct sum, coulomb_interaction.cc:23-80 (rc <= 0: zero forces). */
+int amk_coulomb_standard(amk_ctx* ctx, double cutoff_radius);
+/* Exact all-pairs direct sum (no cutoff), tiled on the GPU. */
+int amk_coulomb_allpairs(amk_ctx* ctx);
+/* Barnes-Hut, barnes-hut.cc:271-299 (leaf capacity 8). */
+int amk_coulomb_barnes_hut(amk_ctx* ctx, double theta);
+/* Cartesian FMM, fast-multipole.cc:684-713 (order clamped to [1,8], leaf
+ * capacity 32). learned != 0 selects the p=2 far field plus the learned
+ * correction (order is then ignored). */
+int amk_coulomb_fmm(amk_ctx* ctx, int order, double theta, int learned);
+/* Dispatches on the context's coulomb_method (antimatter-kernel.cc:155-160). */
+int amk_coulomb(amk_ctx* ctx);
+/* Copies the force slot back to the host. */
+int amk_get_forces(amk_ctx* ctx, double* fx, double* fy, double* fz);
+
+/* ------------------------------------------------------------ behaviours */
+/* LorentzForce::Run then CyclotronCooling::Run for every alive particle
+ * (lorentz.cc:37-71, cooling.cc:24-66), fused in one kernel. Cooling noise
+ * is Philox4x32-10 keyed by (seed, step, particle id). The push ends a step:
+ * it advances the step counter (steps are numbered from 1). */
+int amk_push(amk_ctx* ctx);
+/* AnnihilationInteraction::Run for every alive particle, deterministic:
+ * greedy matching in ascending (owner id, partner id) order over contacts
+ * r^2 < contact_radius^2 whose Philox draw u(owner->partner) < p, with the
+ * draws keyed by the step of the last push (1 before any push). Returns
+ * the number of particles annihilated this call in *marked (may be NULL). */
+int amk_annihilate(amk_ctx* ctx, long* marked);
+/* One or more full steps: Coulomb (context method) -> push+cooling ->
+ * annihilation, as antimatter-kernel.cc:153-162. */
+int amk_step(amk_ctx* ctx, int nsteps);
+long amk_step_count(const amk_ctx* ctx);
+
+/* ------------------------------------------------------------ energy */
+typedef struct amk_energy_out {
+  double kinetic;          /* sum 1/2 m v^2 over alive particles        */
+  double trap_potential;   /* sum q phi_trap(x)                          */
+  double coulomb_potential;/* per the energy method                      */
+  double total;
+  long num_active;
+} amk_energy_out;
+
+/* ComputeTotalEnergy, energy_analysis.cc:84-145. time_centre != 0 averages
+ * the potentials with the previous call's (EnergyHistory, :126-142). The
+ * Coulomb term uses the context's energy_method: standard = shifted-cutoff
+ * pair sum (:16-43), barnes-hut = BH potential walk (:45-69),
+ * fast-multipole = FMM energy (:71-81), allpairs = exact pair sum. All
+ * reductions are FP64. */
+int amk_energy(amk_ctx* ctx, int time_centre, amk_energy_out* out);
+
+/* ------------------------------------------------------------ solver mirrors */
+/* Stateless counterparts of the reference's solver classes, on caller
+ * buffers (host memory). They use the context only for its device, stream
+ * and scratch; the context's particle state is untouched.
+ *   BarnesHutTree(theta, leaf_capacity).Build + ComputeForce per source
+ *   (self excluded) / ComputePotential: barnes-hut.h:40-44.
+ *   FastMultipoleSolver(order, theta, leaf_capacity).Compute: fast-multipole.h:55-64
+ * phi / energy outputs may be NULL. phi_i = sum_j q_j / r_ij (no k). */
+int amk_solve_allpairs(amk_ctx* ctx, long n, const double* x, const double* y,
+                       const double* z, const double* q, double* fx, double* fy,
+                       double* fz, double* phi);
+int amk_solve_cutoff(amk_ctx* ctx, long n, const double* x, const double* y,
+                     const double* z, const double* q, double cutoff_radius, double* fx,
+                     double* fy, double* fz);
+int amk_solve_barnes_hut(amk_ctx* ctx, long n, const double* x, const double* y,
+                         const double* z, const double* q, double theta, long leaf_capacity,
+                         double* fx, double* fy, double* fz, double* phi);
+int amk_solve_fmm(amk_ctx* ctx, long n, const double* x, const double* y, const double* z,
+                  const double* q, int order, double theta, long leaf_capacity,
+                  double* fx, double* fy, double* fz, double* energy);
+
+/* ------------------------------------------------------------ profiling */
+/* Per-phase device time (CUDA events on the context stream) accumulated
+ * since the last reset, in ms. Phases: see AMK_PHASE_*. */
+#define AMK_PHASE_STAGE 0
+#define AMK_PHASE_ALLPAIRS 1
+#define AMK_PHASE_CUTOFF 2
+#define AMK_PHASE_SORT 3
+#define AMK_PHASE_TREE 4
+#define AMK_PHASE_BH_WALK 5
+#define AMK_PHASE_FMM_UP 6
+#define AMK_PHASE_FMM_LISTS 7
+#define AMK_PHASE_FMM_M2L 8
+#define AMK_PHASE_FMM_DOWN 9
+#define AMK_PHASE_FMM_P2P 10
+#define AMK_PHASE_MLP 11
+#define AMK_PHASE_PUSH 12
+#define AMK_PHASE_ANNIHILATION 13
+#define AMK_PHASE_ENERGY 14
+#define AMK_NUM_PHASES 15
+int amk_set_profiling(amk_ctx* ctx, int enabled);
+int amk_phase_times(amk_ctx* ctx, double* ms_out, long* launches_out, int n);
+int amk_reset_phase_times(amk_ctx* ctx);
+/* Number of kernels this library launched on the context since creation. */
+long amk_kernel_launches(const amk_ctx* ctx);
+/* FP32 FMA-pipe throughput of the context's device in TFLOP/s (2 flops per
+ * FFMA), measured by a short probe kernel on the context stream: the
+ * roofline denominator of the FP32-bound pair kernels. */
+int amk_measure_fp32_peak(amk_ctx* ctx, double* tflops, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AMK_H_ */

@@ -1,0 +1,146 @@
+"""GPU parity of the per-step behaviours (Boris push + cyclotron cooling,
+annihilation, energies) and of whole README-scale steps against the oracle."""
+import os
+
+import numpy as np
+import pytest
+
+import amk
+import oracle_lib as O
+from conftest import E, gaussian_cloud
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+NOTEBOOK_STEP0 = {"kinetic": 4.21895e-18, "trap_potential": -3.18438e-22,
+                  "coulomb_potential": 5.47464e-24}
+
+
+def readme_params(**over):
+    kw = dict(seed=42, b0=1.0, trap_voltage=10.0, z0=0.01, rho0=0.01, num_steps=100,
+              populations={"positron": 100, "electron": 100},
+              temperatures={"positron": 1e3, "electron": 1e3}, cloud_radii=(1e-4, 1e-4, 1e-4),
+              bath_temperature=4.0, cooling_scale=1.0, coulomb_forces_enabled=1,
+              coulomb_method="standard", energy_method="standard", cutoff_radius=1e-5,
+              annihilation_enabled=1, contact_radius=5e-6, annihilation_probability=1.0)
+    kw.update(over)
+    return amk.make_params(**kw)
+
+
+def oracle_state(pos, vel, sp):
+    m, q = O.species_props(sp)
+    return dict(x=pos[:, 0].copy(), y=pos[:, 1].copy(), z=pos[:, 2].copy(), vx=vel[:, 0].copy(),
+                vy=vel[:, 1].copy(), vz=vel[:, 2].copy(), q=q, m=m,
+                alive=np.ones(len(sp), np.uint8), species=np.asarray(sp, np.uint8))
+
+
+def test_init_particles_bit_exact_and_step0_energy():
+    g = np.load(os.path.join(GOLD, "readme_ic.npz"))
+    with amk.Simulation(readme_params()) as s:
+        s.init_particles()
+        st = s.get_particles()
+        assert np.array_equal(np.stack([st["x"], st["y"], st["z"]], 1), g["pos"])
+        assert np.array_equal(np.stack([st["vx"], st["vy"], st["vz"]], 1), g["vel"])
+        e = s.energy(time_centre=True)
+        for k, v in NOTEBOOK_STEP0.items():
+            assert float(f"{e[k]:.5e}") == v, (k, e[k])
+        assert e["num_active"] == 200
+
+
+def test_push_and_cooling_match_oracle():
+    g = np.load(os.path.join(GOLD, "readme_ic.npz"))
+    p = readme_params(annihilation_enabled=0)
+    with amk.Simulation(p) as s:
+        s.init_particles()
+        ref = oracle_state(g["pos"], g["vel"], g["species"])
+        for step in range(1, 6):
+            s.coulomb_standard(p.cutoff_radius)
+            fx, fy, fz = s.get_forces()
+            gx, gy, gz = O.cutoff(ref["x"], ref["y"], ref["z"], ref["q"], p.cutoff_radius, ref["alive"])
+            for a, b in zip((fx, fy, fz), (gx, gy, gz)):
+                assert np.max(np.abs(a - b)) <= 1e-10 * max(np.max(np.abs(b)), 1e-300)
+            s.push()
+            O.boris_push(ref, gx, gy, gz, p.b0, p.trap_voltage, p.z0, p.rho0, p.dt, step == 1)
+            O.cooling(ref, p.b0, p.dt, p.cooling_scale, p.bath_temperature, p.seed, step)
+        st = s.get_particles()
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            assert np.max(np.abs(st[k] - ref[k])) <= 1e-10 * np.max(np.abs(ref[k])), k
+
+
+def test_boris_only_multistep_matches_oracle():
+    x, y, z, _ = gaussian_cloud(1000, 3, sigma=(1e-4, 1e-4, 1e-4))
+    rng = np.random.default_rng(3)
+    vel = rng.normal(0, 1e4, (1000, 3))
+    sp = np.where(rng.random(1000) < 0.5, 1, 3).astype(np.uint8)
+    p = readme_params(coulomb_forces_enabled=0, annihilation_enabled=0, cooling_enabled=0)
+    with amk.Simulation(p) as s:
+        s.set_particles(x, y, z, vel[:, 0], vel[:, 1], vel[:, 2], sp)
+        ref = oracle_state(np.stack([x, y, z], 1), vel, sp)
+        zero = np.zeros(1000)
+        for step in range(1, 21):
+            s.step(1)
+            O.boris_push(ref, zero, zero, zero, p.b0, p.trap_voltage, p.z0, p.rho0, p.dt, step == 1)
+        st = s.get_particles()
+        for k in ("x", "y", "z", "vx", "vy", "vz"):
+            assert np.max(np.abs(st[k] - ref[k])) <= 1e-12 * np.max(np.abs(ref[k])), k
+
+
+def test_cooling_with_bath_matches_oracle_one_step():
+    x, y, z, _ = gaussian_cloud(2000, 8, sigma=(1e-4, 1e-4, 1e-4))
+    rng = np.random.default_rng(8)
+    vel = rng.normal(0, 1e5, (2000, 3))
+    sp = np.where(rng.random(2000) < 0.5, 1, 3).astype(np.uint8)
+    p = readme_params(coulomb_forces_enabled=0, annihilation_enabled=0, cooling_scale=1e-9,
+                      bath_temperature=300.0)
+    with amk.Simulation(p) as s:
+        s.set_particles(x, y, z, vel[:, 0], vel[:, 1], vel[:, 2], sp)
+        ref = oracle_state(np.stack([x, y, z], 1), vel, sp)
+        s.step(1)
+        zero = np.zeros(2000)
+        O.boris_push(ref, zero, zero, zero, p.b0, p.trap_voltage, p.z0, p.rho0, p.dt, True)
+        O.cooling(ref, p.b0, p.dt, p.cooling_scale, p.bath_temperature, p.seed, 1)
+        st = s.get_particles()
+        for k in ("vx", "vy", "vz"):
+            assert np.max(np.abs(st[k] - ref[k])) <= 1e-11 * np.max(np.abs(ref[k])), k
+        # strong damping: v_perp relaxes to the bath (sigma^2 = kT/m)
+        s.step(200)
+        st = s.get_particles()
+        m = 9.1093837015e-31
+        vperp2 = np.mean(st["vx"] ** 2 + st["vy"] ** 2) / 2
+        assert abs(vperp2 / (1.380649e-23 * 300.0 / m) - 1.0) < 0.1
+
+
+def test_annihilation_bit_exact_vs_oracle():
+    # dense two-species cloud so that many contacts compete for partners
+    n = 3000
+    rng = np.random.default_rng(12)
+    pos = rng.uniform(-2e-5, 2e-5, (n, 3))
+    sp = np.where(rng.random(n) < 0.5, 1, 3).astype(np.uint8)
+    for prob, seed in ((1.0, 42), (0.5, 42), (0.5, 7), (0.0, 1)):
+        p = readme_params(annihilation_probability=prob, contact_radius=1.5e-6, seed=seed,
+                          coulomb_forces_enabled=0)
+        with amk.Simulation(p) as s:
+            s.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], np.zeros(n), np.zeros(n), np.zeros(n), sp)
+            ref = oracle_state(pos, np.zeros((n, 3)), sp)
+            for _ in range(2):  # second call sees the survivors of the first
+                marked = s.annihilate()
+                mo = O.annihilation(ref, p.contact_radius, prob, seed, 1)
+                assert np.array_equal(s.get_particles()["alive"], ref["alive"]), (prob, seed)
+                assert marked == mo
+            if prob == 0.0:
+                assert ref["alive"].all()
+            else:
+                assert not ref["alive"].all()
+
+
+def test_readme_run_energy_and_population():
+    p = readme_params()
+    with amk.Simulation(p) as s:
+        s.init_particles()
+        e0 = s.energy()
+        s.step(100)
+        e1 = s.energy()
+        assert s.step_count() == 100
+        assert 0 < e1["num_active"] <= 200 and e1["num_active"] % 2 == 0
+        assert np.isfinite(e1["total"])
+        # annihilation removes kinetic energy; the total cannot grow much
+        assert e1["total"] < e0["total"] * 1.05
