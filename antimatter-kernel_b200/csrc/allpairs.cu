@@ -14,9 +14,10 @@
 //   * each 256-source tile is summed in FP32 and folded into a (hi, lo) float
 //     pair with TwoSum, so accumulated rounding stays O(eps) per tile rather
 //     than O(N eps) (compensated accumulation);
-//   * a persistent grid of (SM count x resident CTAs) walks (target block,
-//     source chunk) units; each unit writes its partial, and the finalize
-//     kernel sums the chunks in a fixed order in FP64 (deterministic).
+//   * a persistent grid of (SM count x resident CTAs) walks contiguous
+//     ranges of (target block, source chunk) units, keeping a target block's
+//     sums in registers across its chunks; the finalize kernel adds the
+//     partial runs in a fixed order in FP64 (deterministic).
 #include <algorithm>
 
 #include "amk_internal.cuh"
@@ -35,6 +36,13 @@ __device__ __forceinline__ void two_sum_fold(float& hi, float& lo, float p) {
   lo += e;
 }
 
+// Work decomposition: units = (target block tb, source chunk) in tb-major
+// order; CTA c owns the contiguous unit range [start(c), start(c+1)) with
+// start(c) = floor(c * units / grid). Consecutive units of one target block
+// accumulate in registers; a run is flushed to partial slot
+// (first chunk of the run, tb) when the target block changes.
+__device__ __forceinline__ long unit_start(long c, long units, long grid) { return (c * units) / grid; }
+
 template <bool kPhi>
 __global__ void __launch_bounds__(kThreads, 3)
 allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, int n, int n_tb,
@@ -42,28 +50,51 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, in
   __shared__ float4 sh[2][kThreads];
   __shared__ float4 sl[2][kThreads];
   const int tid = threadIdx.x;
-  const int units = n_tb * n_split;
-  for (int u = blockIdx.x; u < units; u += gridDim.x) {
-    const int tb = u / n_split;
-    const int split = u - tb * n_split;
-    const int src_begin = split * chunk;
-    const int src_end = min(n, src_begin + chunk);
+  const long units = static_cast<long>(n_tb) * n_split;
+  const long u_begin = unit_start(blockIdx.x, units, gridDim.x);
+  const long u_end = unit_start(blockIdx.x + 1, units, gridDim.x);
+  // the self pair (and pairs closer than 1e-15 m) have d2 < 2 eps2: they are
+  // left out of the potential (barnes-hut.cc:242-246)
+  const float self_cut = 2.0f * eps2;
 
-    float tx[kR], ty[kR], tz[kR], ux[kR], uy[kR], uz[kR];
-    float ahx[kR], ahy[kR], ahz[kR], ahp[kR], alx[kR], aly[kR], alz[kR], alp[kR];
+  float tx[kR], ty[kR], tz[kR], ux[kR], uy[kR], uz[kR];
+  float ahx[kR], ahy[kR], ahz[kR], ahp[kR], alx[kR], aly[kR], alz[kR], alp[kR];
+  int run_tb = -1, run_split = 0;
+
+  auto flush = [&]() {
 #pragma unroll
     for (int r = 0; r < kR; ++r) {
-      const int i = tb * (kThreads * kR) + r * kThreads + tid;
-      float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
+      const int i = run_tb * (kThreads * kR) + r * kThreads + tid;
       if (i < n) {
-        h = hq[i];
-        l = lo[i];
+        part[(static_cast<size_t>(run_split) * 2 + 0) * n + i] = make_float4(ahx[r], ahy[r], ahz[r], ahp[r]);
+        part[(static_cast<size_t>(run_split) * 2 + 1) * n + i] = make_float4(alx[r], aly[r], alz[r], alp[r]);
       }
-      tx[r] = h.x; ty[r] = h.y; tz[r] = h.z;
-      ux[r] = l.x; uy[r] = l.y; uz[r] = l.z;
-      ahx[r] = ahy[r] = ahz[r] = ahp[r] = 0.f;
-      alx[r] = aly[r] = alz[r] = alp[r] = 0.f;
     }
+  };
+
+  for (long u = u_begin; u < u_end; ++u) {
+    const int tb = static_cast<int>(u / n_split);
+    const int split = static_cast<int>(u - static_cast<long>(tb) * n_split);
+    if (tb != run_tb) {
+      if (run_tb >= 0) flush();
+      run_tb = tb;
+      run_split = split;
+#pragma unroll
+      for (int r = 0; r < kR; ++r) {
+        const int i = tb * (kThreads * kR) + r * kThreads + tid;
+        float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
+        if (i < n) {
+          h = hq[i];
+          l = lo[i];
+        }
+        tx[r] = h.x; ty[r] = h.y; tz[r] = h.z;
+        ux[r] = l.x; uy[r] = l.y; uz[r] = l.z;
+        ahx[r] = ahy[r] = ahz[r] = ahp[r] = 0.f;
+        alx[r] = aly[r] = alz[r] = alp[r] = 0.f;
+      }
+    }
+    const int src_begin = split * chunk;
+    const int src_end = min(n, src_begin + chunk);
 
     // prefetch the first tile into registers
     float4 nh = make_float4(0.f, 0.f, 0.f, 0.f), nl = nh;
@@ -75,7 +106,7 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, in
       }
     }
     int buf = 0;
-    __syncthreads();  // previous unit's readers are done with both buffers
+    __syncthreads();  // the previous unit's readers are done with both buffers
     sh[buf][tid] = nh;
     sl[buf][tid] = nl;
     __syncthreads();
@@ -107,7 +138,7 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, in
           px[r] = fmaf(w, dx, px[r]);
           py[r] = fmaf(w, dy, py[r]);
           pz[r] = fmaf(w, dz, pz[r]);
-          if (kPhi) pp[r] += qr;
+          if (kPhi) pp[r] += (d2 >= self_cut) ? qr : 0.0f;
         }
       }
 #pragma unroll
@@ -122,28 +153,32 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, in
       sl[buf][tid] = nl;
       __syncthreads();
     }
-#pragma unroll
-    for (int r = 0; r < kR; ++r) {
-      const int i = tb * (kThreads * kR) + r * kThreads + tid;
-      if (i < n) {
-        part[(static_cast<size_t>(split) * 2 + 0) * n + i] = make_float4(ahx[r], ahy[r], ahz[r], ahp[r]);
-        part[(static_cast<size_t>(split) * 2 + 1) * n + i] = make_float4(alx[r], aly[r], alz[r], alp[r]);
-      }
-    }
   }
+  if (run_tb >= 0) flush();
 }
 
-// Sums the chunk partials in chunk order (FP64) and converts to SI:
-// F_i = k e q_i / L^2 * sum, phi_i = e / L * sum_phi.
-__global__ void allpairs_finalize_kernel(int n, int n_split, const float4* __restrict__ part,
+// Sums the partial runs of each target in chunk order (FP64) and converts to
+// SI: F_i = k e q_i / L^2 * sum, phi_i = e / L * sum_phi. The runs of target
+// block tb start at chunk 0 and at every CTA boundary inside tb's units.
+__global__ void allpairs_finalize_kernel(int n, int n_tb, int n_split, int grid, const float4* __restrict__ part,
                                          const double* __restrict__ q, const uint8_t* __restrict__ alive,
                                          const float4* __restrict__ hq, double force_coef, double phi_coef,
                                          double* __restrict__ fx, double* __restrict__ fy,
                                          double* __restrict__ fz, double* __restrict__ phi) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
+  const long units = static_cast<long>(n_tb) * n_split;
+  const int tb = i / (kThreads * kR);
+  const long ub = static_cast<long>(tb) * n_split, ue = ub + n_split;
+  long c = (ub * grid) / units;
+  while (c + 1 < grid && unit_start(c + 1, units, grid) <= ub) ++c;
+  while (c > 0 && unit_start(c, units, grid) > ub) --c;
   double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0;
-  for (int s = 0; s < n_split; ++s) {
+  for (; c < grid; ++c) {
+    const long st = unit_start(c, units, grid);
+    if (st >= ue) break;
+    if (unit_start(c + 1, units, grid) <= st) continue;  // CTA without units
+    const int s = static_cast<int>((st > ub ? st : ub) - ub);
     const float4 h = part[(static_cast<size_t>(s) * 2 + 0) * n + i];
     const float4 l = part[(static_cast<size_t>(s) * 2 + 1) * n + i];
     sx += static_cast<double>(h.x) + static_cast<double>(l.x);
@@ -153,10 +188,10 @@ __global__ void allpairs_finalize_kernel(int n, int n_split, const float4* __res
   }
   // Targets that are dead, neutral or non-finite were staged with q_e = 0.
   const bool live = hq[i].w != 0.0f;
-  const double c = live ? force_coef * q[i] : 0.0;
-  fx[i] = c * sx;
-  fy[i] = c * sy;
-  fz[i] = c * sz;
+  const double cq = live ? force_coef * q[i] : 0.0;
+  fx[i] = cq * sx;
+  fy[i] = cq * sy;
+  fz[i] = cq * sz;
   if (phi) phi[i] = (alive == nullptr || alive[i]) ? phi_coef * sp : 0.0;
 }
 
@@ -177,13 +212,14 @@ int allpairs_forces(amk_ctx* c, const View& v) {
   const int grid_cap = g_num_sms * std::max(1, g_ctas_per_sm[want_phi ? 1 : 0]);
   const int per_tb = kThreads * kR;
   const int n_tb = (n + per_tb - 1) / per_tb;
-  // Source chunks: enough units for >= 4 per CTA, chunks a multiple of the tile.
-  int n_split = std::max(1, (4 * grid_cap + n_tb - 1) / n_tb);
-  int chunk = (n + n_split - 1) / n_split;
-  chunk = ((chunk + kThreads - 1) / kThreads) * kThreads;
+  // Source chunks of whole tiles; aim for >= 32 units per CTA so that the
+  // contiguous per-CTA ranges balance to within ~3%.
+  const int tiles = (n + kThreads - 1) / kThreads;
+  int n_split = std::min(tiles, std::max(1, (32 * grid_cap + n_tb - 1) / n_tb));
+  const int chunk = ((tiles + n_split - 1) / n_split) * kThreads;
   n_split = (n + chunk - 1) / chunk;
-  const int units = n_tb * n_split;
-  const int grid = std::min(units, grid_cap);
+  const long units = static_cast<long>(n_tb) * n_split;
+  const int grid = static_cast<int>(std::min<long>(units, grid_cap));
 
   int rc = AMK_OK;
   float4* part = slot<float4>(c, kSlotPartial, static_cast<size_t>(n_split) * 2 * n, &rc);
@@ -200,7 +236,7 @@ int allpairs_forces(amk_ctx* c, const View& v) {
   AMK_TRY(phase_end(c, AMK_PHASE_ALLPAIRS));
   AMK_TRY(phase_begin(c, AMK_PHASE_STAGE));
   allpairs_finalize_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(
-      n, n_split, part, v.q, v.alive, v.hq, kCoulombConstant * kElementaryCharge / (l * l),
+      n, n_tb, n_split, grid, part, v.q, v.alive, v.hq, kCoulombConstant * kElementaryCharge / (l * l),
       kElementaryCharge / l, v.fx, v.fy, v.fz, v.phi);
   AMK_TRY(check_launch(c, "allpairs_finalize_kernel"));
   AMK_TRY(phase_end(c, AMK_PHASE_STAGE));

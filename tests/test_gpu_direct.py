@@ -34,7 +34,8 @@ def test_allpairs_vs_reference_bh_theta0_fixture(sim):
     rel, _ = rel_errors((fx, fy, fz), ref.T)
     assert np.sqrt(np.mean(rel ** 2)) < DIRECT_RMS_TOL
     pref = g["phi_theta0.0"]
-    assert np.max(np.abs(phi - pref) / np.abs(pref)) < 1e-5
+    # phi sums +-q/r with ~100x cancellation: bound the error by the scale
+    assert np.max(np.abs(phi - pref)) < 2e-6 * np.max(np.abs(pref))
 
 
 def test_allpairs_ragged_sizes(sim):
