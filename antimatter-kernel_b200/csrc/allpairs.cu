@@ -2,31 +2,42 @@
 //
 // The reference's exact all-pairs force is Barnes-Hut at theta = 0
 // (barnes-hut.h:22-24, barnes-hut.cc:183-221): F_i = sum_{j != i} k q_i q_j
-// r_ij / r^3, skipping q_j = 0 and r^2 < 1e-30. Here:
-//   * positions are scaled by a power of two L and split into a float pair
-//     (hi, lo); the pair difference (xi_hi - xj_hi) + (xi_lo - xj_lo) is
-//     exact to FP32 rounding of |r_ij| even for close pairs (Sterbenz), so no
-//     absolute position rounding enters the 1/r^2 force;
-//   * the pair math is FP32 with one MUFU.RSQ; r^2 gets eps2 = 1e-30 m^2 / L^2
-//     added so that the self pair (r = 0, q_j r_ij = 0) contributes exactly 0
-//     without a per-pair branch (pairs closer than 1e-15 m are skipped by the
-//     reference and are not bit-compatible here);
+// r_ij / r^3, skipping q_j = 0 and r^2 < 1e-30. Design:
+//   * particles are ordered along a 30-bit Morton curve (radix sort; the
+//     order is reused for 16 calls on a context's own particle set -- tile
+//     boxes are rebuilt on every call, so a stale order costs speed only);
+//     tiles of 256 consecutive particles get an axis-aligned box;
+//   * positions are scaled by a power of two L. For tile pairs whose boxes
+//     are closer than their combined half-extents ("near"), positions are a
+//     float pair (hi, lo) and r_ij = (xi_hi - xj_hi) + (xi_lo - xj_lo) is
+//     exact to FP32 rounding of |r_ij| (Sterbenz) -- 18 FP32 ops per pair;
+//   * for separated tile pairs ("far", |r_ij| >= the boxes' gap >= their
+//     half-extents) each source carries its offset from its tile centre in
+//     FP32 and each target forms a_i = x_i - c_tile once per tile, so
+//     r_ij = a_i - u_j costs one FADD per component and stays within ~2 eps
+//     of |r_ij| -- 12 FP32 ops per pair;
+//   * r^2 gets eps2 = max(1e-30 m^2 / L^2, 1e-25) added so that the self pair
+//     (r = 0) contributes exactly 0 without a branch and rinv^3 cannot
+//     overflow (the reference skips pairs closer than 1e-15 m; such pairs,
+//     and pairs closer than 3e-13 L, are softened here instead);
 //   * each 256-source tile is summed in FP32 and folded into a (hi, lo) float
-//     pair with TwoSum, so accumulated rounding stays O(eps) per tile rather
-//     than O(N eps) (compensated accumulation);
+//     pair with TwoSum (compensated accumulation);
 //   * a persistent grid of (SM count x resident CTAs) walks contiguous
 //     ranges of (target block, source chunk) units, keeping a target block's
 //     sums in registers across its chunks; the finalize kernel adds the
 //     partial runs in a fixed order in FP64 (deterministic).
+// Compiled with -ftz=true: every operand is a normal float by construction.
 #include <algorithm>
 
 #include "amk_internal.cuh"
+#include "morton.cuh"
 
 namespace amk {
 namespace {
 
-constexpr int kThreads = 256;  // threads per CTA = sources per tile
-constexpr int kR = 2;          // targets per thread
+constexpr int kThreads = 256;  // threads per CTA = particles per tile
+constexpr int kR = 2;          // targets per thread (a target block = 2 tiles)
+constexpr int kResortEvery = 16;
 
 __device__ __forceinline__ void two_sum_fold(float& hi, float& lo, float p) {
   const float s = hi + p;
@@ -36,29 +47,161 @@ __device__ __forceinline__ void two_sum_fold(float& hi, float& lo, float p) {
   lo += e;
 }
 
-// Work decomposition: units = (target block tb, source chunk) in tb-major
-// order; CTA c owns the contiguous unit range [start(c), start(c+1)) with
-// start(c) = floor(c * units / grid). Consecutive units of one target block
-// accumulate in registers; a run is flushed to partial slot
-// (first chunk of the run, tb) when the target block changes.
+__device__ __forceinline__ bool usable(const View& v, long i) {
+  return (v.alive == nullptr || v.alive[i]) && v.q[i] != 0.0 && isfinite(v.x[i]) && isfinite(v.y[i]) &&
+         isfinite(v.z[i]);
+}
+
+// ------------------------------------------------------------ ordering
+__global__ void ap_bbox_kernel(View v, unsigned long long* bb) {
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x; i < v.n;
+       i += static_cast<long>(gridDim.x) * blockDim.x) {
+    if (!usable(v, i)) continue;
+    const double p[3] = {v.x[i], v.y[i], v.z[i]};
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = fmin(lo[d], p[d]);
+      hi[d] = fmax(hi[d], p[d]);
+    }
+  }
+  for (int d = 0; d < 3; ++d) {
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[d] = fmin(lo[d], __shfl_xor_sync(0xffffffffu, lo[d], o));
+      hi[d] = fmax(hi[d], __shfl_xor_sync(0xffffffffu, hi[d], o));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+    for (int d = 0; d < 3; ++d) {
+      atomicMin(&bb[d], double_order_bits(lo[d]));
+      atomicMin(&bb[3 + d], double_order_bits(-hi[d]));
+    }
+  }
+}
+
+// 30-bit Morton key (10 bits per axis) inside the live bounding box; unusable
+// particles sort last.
+__global__ void ap_key_kernel(View v, const unsigned long long* bb, uint64_t* keys, uint32_t* vals) {
+  const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (i >= v.n) return;
+  vals[i] = static_cast<uint32_t>(i);
+  if (!usable(v, i)) {
+    keys[i] = 0xFFFFFFFFull;
+    return;
+  }
+  const double p[3] = {v.x[i], v.y[i], v.z[i]};
+  uint32_t c[3];
+  for (int d = 0; d < 3; ++d) {
+    const double lo = double_from_order_bits(bb[d]);
+    const double hi = -double_from_order_bits(bb[3 + d]);
+    const double ext = hi - lo;
+    const double f = ext > 0.0 ? (p[d] - lo) / ext : 0.0;
+    c[d] = static_cast<uint32_t>(fmin(fmax(f * 1024.0, 0.0), 1023.0));
+  }
+  keys[i] = morton3_21(c[0], c[1], c[2]);
+}
+
+// ------------------------------------------------------------ staging
+struct TileBox {
+  float4 c;   // centre (scaled, float hi part); w = 1 when the tile has sources
+  float4 cl;  // centre low part
+  float4 h;   // half-extent per axis (rounded up); w = |h|
+};
+
+// One CTA per tile of 256 sorted particles: double-float positions, offsets
+// from the tile centre, and the tile box of its usable particles.
+__global__ void __launch_bounds__(kThreads)
+ap_stage_kernel(View v, const uint32_t* __restrict__ perm, double inv_l, float4* __restrict__ hq,
+                float4* __restrict__ lo, float4* __restrict__ rel, TileBox* __restrict__ boxes) {
+  __shared__ double red[6][kThreads / 32];
+  __shared__ double box[6];
+  const int t = blockIdx.x;
+  const long k = static_cast<long>(t) * kThreads + threadIdx.x;
+  double xs = 0.0, ys = 0.0, zs = 0.0, qe = 0.0;
+  bool ok = false;
+  if (k < v.n) {
+    const long i = perm[k];
+    ok = usable(v, i);
+    if (ok) {
+      xs = v.x[i] * inv_l;
+      ys = v.y[i] * inv_l;
+      zs = v.z[i] * inv_l;
+      qe = v.q[i] / kElementaryCharge;
+    }
+  }
+  double m[6] = {ok ? xs : INFINITY, ok ? ys : INFINITY, ok ? zs : INFINITY,
+                 ok ? -xs : INFINITY, ok ? -ys : INFINITY, ok ? -zs : INFINITY};
+  for (int d = 0; d < 6; ++d)
+    for (int o = 16; o > 0; o >>= 1) m[d] = fmin(m[d], __shfl_xor_sync(0xffffffffu, m[d], o));
+  if ((threadIdx.x & 31) == 0)
+    for (int d = 0; d < 6; ++d) red[d][threadIdx.x >> 5] = m[d];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double r = INFINITY;
+    for (int w = 0; w < kThreads / 32; ++w) r = fmin(r, red[threadIdx.x][w]);
+    box[threadIdx.x] = r;
+  }
+  __syncthreads();
+  const bool any = isfinite(box[0]);
+  const double cx = any ? 0.5 * (box[0] - box[3]) : 0.0;
+  const double cy = any ? 0.5 * (box[1] - box[4]) : 0.0;
+  const double cz = any ? 0.5 * (box[2] - box[5]) : 0.0;
+  float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h, u = h;
+  if (ok) {
+    h.x = __double2float_rn(xs);
+    h.y = __double2float_rn(ys);
+    h.z = __double2float_rn(zs);
+    h.w = __double2float_rn(qe);
+    l.x = __double2float_rn(xs - static_cast<double>(h.x));
+    l.y = __double2float_rn(ys - static_cast<double>(h.y));
+    l.z = __double2float_rn(zs - static_cast<double>(h.z));
+    u.x = __double2float_rn(xs - cx);
+    u.y = __double2float_rn(ys - cy);
+    u.z = __double2float_rn(zs - cz);
+    u.w = h.w;
+  }
+  if (k < v.n) {
+    hq[k] = h;
+    lo[k] = l;
+    rel[k] = u;
+  }
+  if (threadIdx.x == 0) {
+    TileBox b;
+    b.c = make_float4(__double2float_rn(cx), __double2float_rn(cy), __double2float_rn(cz), any ? 1.f : 0.f);
+    b.cl = make_float4(__double2float_rn(cx - static_cast<double>(b.c.x)),
+                       __double2float_rn(cy - static_cast<double>(b.c.y)),
+                       __double2float_rn(cz - static_cast<double>(b.c.z)), 0.f);
+    const double hx = any ? 0.5 * (-box[3] - box[0]) : 0.0;
+    const double hy = any ? 0.5 * (-box[4] - box[1]) : 0.0;
+    const double hz = any ? 0.5 * (-box[5] - box[2]) : 0.0;
+    b.h = make_float4(__double2float_ru(hx), __double2float_ru(hy), __double2float_ru(hz),
+                      __double2float_ru(sqrt(hx * hx + hy * hy + hz * hz)));
+    boxes[t] = b;
+  }
+}
+
+// ------------------------------------------------------------ pair kernel
 __device__ __forceinline__ long unit_start(long c, long units, long grid) { return (c * units) / grid; }
 
+// Work: units = (target block tb, chunk of source tiles), tb-major; CTA c owns
+// units [start(c), start(c+1)), start(c) = floor(c * units / grid). A target
+// block's sums stay in registers over its consecutive units; a run is
+// flushed to partial slot (first chunk of the run) when the block changes.
 template <bool kPhi>
 __global__ void __launch_bounds__(kThreads, 3)
-allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, int n, int n_tb,
-                int n_split, int chunk, float eps2, float4* __restrict__ part) {
-  __shared__ float4 sh[2][kThreads];
-  __shared__ float4 sl[2][kThreads];
+allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, const float4* __restrict__ rel,
+                const TileBox* __restrict__ boxes, int n, int n_tiles, int n_tb, int n_split,
+                int tiles_per_chunk, float eps2, float4* __restrict__ part) {
+  __shared__ float4 sa[kThreads];
+  __shared__ float4 sb[kThreads];
   const int tid = threadIdx.x;
   const long units = static_cast<long>(n_tb) * n_split;
   const long u_begin = unit_start(blockIdx.x, units, gridDim.x);
   const long u_end = unit_start(blockIdx.x + 1, units, gridDim.x);
-  // the self pair (and pairs closer than 1e-15 m) have d2 < 2 eps2: they are
-  // left out of the potential (barnes-hut.cc:242-246)
-  const float self_cut = 2.0f * eps2;
+  const float self_cut = 2.0f * eps2;  // self pair and r < 1e-15 m: not in phi
 
   float tx[kR], ty[kR], tz[kR], ux[kR], uy[kR], uz[kR];
   float ahx[kR], ahy[kR], ahz[kR], ahp[kR], alx[kR], aly[kR], alz[kR], alp[kR];
+  float4 bc = make_float4(0.f, 0.f, 0.f, 0.f), bh = bc;  // target block box
   int run_tb = -1, run_split = 0;
 
   auto flush = [&]() {
@@ -92,53 +235,92 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, in
         ahx[r] = ahy[r] = ahz[r] = ahp[r] = 0.f;
         alx[r] = aly[r] = alz[r] = alp[r] = 0.f;
       }
+      // union box of the block's (up to two) tiles
+      TileBox b0 = boxes[kR * tb];
+      TileBox b1 = (kR * tb + 1 < n_tiles) ? boxes[kR * tb + 1] : b0;
+      if (b1.c.w == 0.f) b1 = b0;
+      if (b0.c.w == 0.f) b0 = b1;
+      const float lx = fminf(b0.c.x - b0.h.x, b1.c.x - b1.h.x), hx = fmaxf(b0.c.x + b0.h.x, b1.c.x + b1.h.x);
+      const float ly = fminf(b0.c.y - b0.h.y, b1.c.y - b1.h.y), hy = fmaxf(b0.c.y + b0.h.y, b1.c.y + b1.h.y);
+      const float lz = fminf(b0.c.z - b0.h.z, b1.c.z - b1.h.z), hz = fmaxf(b0.c.z + b0.h.z, b1.c.z + b1.h.z);
+      bc = make_float4(0.5f * (lx + hx), 0.5f * (ly + hy), 0.5f * (lz + hz), 0.f);
+      bh = make_float4(0.5001f * (hx - lx), 0.5001f * (hy - ly), 0.5001f * (hz - lz), 0.f);
+      bh.w = 1.0001f * sqrtf(bh.x * bh.x + bh.y * bh.y + bh.z * bh.z);
     }
-    const int src_begin = split * chunk;
-    const int src_end = min(n, src_begin + chunk);
+    const int t_begin = split * tiles_per_chunk;
+    const int t_end = min(n_tiles, t_begin + tiles_per_chunk);
 
-    // prefetch the first tile into registers
-    float4 nh = make_float4(0.f, 0.f, 0.f, 0.f), nl = nh;
-    {
-      const int j = src_begin + tid;
-      if (j < src_end) {
-        nh = hq[j];
-        nl = lo[j];
+    for (int t = t_begin; t < t_end; ++t) {
+      const TileBox sbox = boxes[t];
+      if (sbox.c.w == 0.f) continue;  // no usable sources in this tile (uniform)
+      // near: the boxes' gap is below their summed half-extents
+      const float gx = fmaxf(fabsf(bc.x - sbox.c.x) - (bh.x + sbox.h.x), 0.f);
+      const float gy = fmaxf(fabsf(bc.y - sbox.c.y) - (bh.y + sbox.h.y), 0.f);
+      const float gz = fmaxf(fabsf(bc.z - sbox.c.z) - (bh.z + sbox.h.z), 0.f);
+      const float lim = 1.01f * (bh.w + sbox.h.w);
+      const bool near = gx * gx + gy * gy + gz * gz < lim * lim;
+      const int j = t * kThreads + tid;
+      __syncthreads();  // the previous tile's readers are done with the buffers
+      if (near) {
+        float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
+        if (j < n) {
+          h = hq[j];
+          l = lo[j];
+        }
+        sa[tid] = h;
+        sb[tid] = l;
+      } else {
+        sa[tid] = (j < n) ? rel[j] : make_float4(0.f, 0.f, 0.f, 0.f);
       }
-    }
-    int buf = 0;
-    __syncthreads();  // the previous unit's readers are done with both buffers
-    sh[buf][tid] = nh;
-    sl[buf][tid] = nl;
-    __syncthreads();
-    for (int t0 = src_begin; t0 < src_end; t0 += kThreads) {
-      // prefetch the next tile while this one is consumed
-      const int jn = t0 + kThreads + tid;
-      nh = make_float4(0.f, 0.f, 0.f, 0.f);
-      nl = nh;
-      if (jn < src_end) {
-        nh = hq[jn];
-        nl = lo[jn];
-      }
+      __syncthreads();
       float px[kR], py[kR], pz[kR], pp[kR];
 #pragma unroll
       for (int r = 0; r < kR; ++r) px[r] = py[r] = pz[r] = pp[r] = 0.f;
+      if (near) {
 #pragma unroll 8
-      for (int k = 0; k < kThreads; ++k) {
-        const float4 s = sh[buf][k];
-        const float4 l = sl[buf][k];
+        for (int k = 0; k < kThreads; ++k) {
+          const float4 s = sa[k];
+          const float4 l = sb[k];
+#pragma unroll
+          for (int r = 0; r < kR; ++r) {
+            const float dx = (tx[r] - s.x) + (ux[r] - l.x);
+            const float dy = (ty[r] - s.y) + (uy[r] - l.y);
+            const float dz = (tz[r] - s.z) + (uz[r] - l.z);
+            const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+            const float rinv = rsqrtf(d2);
+            const float qr = s.w * rinv;
+            const float w = qr * (rinv * rinv);
+            px[r] = fmaf(w, dx, px[r]);
+            py[r] = fmaf(w, dy, py[r]);
+            pz[r] = fmaf(w, dz, pz[r]);
+            if (kPhi) pp[r] += (d2 >= self_cut) ? qr : 0.0f;
+          }
+        }
+      } else {
+        float ax[kR], ay[kR], az[kR];
 #pragma unroll
         for (int r = 0; r < kR; ++r) {
-          const float dx = (tx[r] - s.x) + (ux[r] - l.x);
-          const float dy = (ty[r] - s.y) + (uy[r] - l.y);
-          const float dz = (tz[r] - s.z) + (uz[r] - l.z);
-          const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-          const float rinv = rsqrtf(d2);
-          const float qr = s.w * rinv;
-          const float w = qr * (rinv * rinv);
-          px[r] = fmaf(w, dx, px[r]);
-          py[r] = fmaf(w, dy, py[r]);
-          pz[r] = fmaf(w, dz, pz[r]);
-          if (kPhi) pp[r] += (d2 >= self_cut) ? qr : 0.0f;
+          ax[r] = (tx[r] - sbox.c.x) + (ux[r] - sbox.cl.x);
+          ay[r] = (ty[r] - sbox.c.y) + (uy[r] - sbox.cl.y);
+          az[r] = (tz[r] - sbox.c.z) + (uz[r] - sbox.cl.z);
+        }
+#pragma unroll 8
+        for (int k = 0; k < kThreads; ++k) {
+          const float4 s = sa[k];
+#pragma unroll
+          for (int r = 0; r < kR; ++r) {
+            const float dx = ax[r] - s.x;
+            const float dy = ay[r] - s.y;
+            const float dz = az[r] - s.z;
+            const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+            const float rinv = rsqrtf(d2);
+            const float qr = s.w * rinv;
+            const float w = qr * (rinv * rinv);
+            px[r] = fmaf(w, dx, px[r]);
+            py[r] = fmaf(w, dy, py[r]);
+            pz[r] = fmaf(w, dz, pz[r]);
+            if (kPhi) pp[r] += qr;
+          }
         }
       }
 #pragma unroll
@@ -148,27 +330,24 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, in
         two_sum_fold(ahz[r], alz[r], pz[r]);
         if (kPhi) two_sum_fold(ahp[r], alp[r], pp[r]);
       }
-      buf ^= 1;
-      sh[buf][tid] = nh;
-      sl[buf][tid] = nl;
-      __syncthreads();
     }
   }
   if (run_tb >= 0) flush();
 }
 
-// Sums the partial runs of each target in chunk order (FP64) and converts to
-// SI: F_i = k e q_i / L^2 * sum, phi_i = e / L * sum_phi. The runs of target
-// block tb start at chunk 0 and at every CTA boundary inside tb's units.
+// Sums the partial runs of each (sorted) target in chunk order in FP64 and
+// scatters to the caller's order: F_i = k e q_i / L^2 * sum,
+// phi_i = e / L * sum_phi. The runs of target block tb start at chunk 0 and
+// at every CTA boundary inside tb's units.
 __global__ void allpairs_finalize_kernel(int n, int n_tb, int n_split, int grid, const float4* __restrict__ part,
+                                         const uint32_t* __restrict__ perm, const float4* __restrict__ hq,
                                          const double* __restrict__ q, const uint8_t* __restrict__ alive,
-                                         const float4* __restrict__ hq, double force_coef, double phi_coef,
-                                         double* __restrict__ fx, double* __restrict__ fy,
-                                         double* __restrict__ fz, double* __restrict__ phi) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+                                         double force_coef, double phi_coef, double* __restrict__ fx,
+                                         double* __restrict__ fy, double* __restrict__ fz, double* __restrict__ phi) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
   const long units = static_cast<long>(n_tb) * n_split;
-  const int tb = i / (kThreads * kR);
+  const int tb = k / (kThreads * kR);
   const long ub = static_cast<long>(tb) * n_split, ue = ub + n_split;
   long c = (ub * grid) / units;
   while (c + 1 < grid && unit_start(c + 1, units, grid) <= ub) ++c;
@@ -179,15 +358,16 @@ __global__ void allpairs_finalize_kernel(int n, int n_tb, int n_split, int grid,
     if (st >= ue) break;
     if (unit_start(c + 1, units, grid) <= st) continue;  // CTA without units
     const int s = static_cast<int>((st > ub ? st : ub) - ub);
-    const float4 h = part[(static_cast<size_t>(s) * 2 + 0) * n + i];
-    const float4 l = part[(static_cast<size_t>(s) * 2 + 1) * n + i];
+    const float4 h = part[(static_cast<size_t>(s) * 2 + 0) * n + k];
+    const float4 l = part[(static_cast<size_t>(s) * 2 + 1) * n + k];
     sx += static_cast<double>(h.x) + static_cast<double>(l.x);
     sy += static_cast<double>(h.y) + static_cast<double>(l.y);
     sz += static_cast<double>(h.z) + static_cast<double>(l.z);
     sp += static_cast<double>(h.w) + static_cast<double>(l.w);
   }
+  const long i = perm[k];
   // Targets that are dead, neutral or non-finite were staged with q_e = 0.
-  const bool live = hq[i].w != 0.0f;
+  const bool live = hq[k].w != 0.0f;
   const double cq = live ? force_coef * q[i] : 0.0;
   fx[i] = cq * sx;
   fy[i] = cq * sy;
@@ -209,34 +389,84 @@ int allpairs_forces(amk_ctx* c, const View& v) {
     AMK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_ctas_per_sm[0], allpairs_kernel<false>, kThreads, 0));
     AMK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_ctas_per_sm[1], allpairs_kernel<true>, kThreads, 0));
   }
-  const int grid_cap = g_num_sms * std::max(1, g_ctas_per_sm[want_phi ? 1 : 0]);
-  const int per_tb = kThreads * kR;
-  const int n_tb = (n + per_tb - 1) / per_tb;
-  // Source chunks of whole tiles; aim for >= 32 units per CTA so that the
-  // contiguous per-CTA ranges balance to within ~3%.
-  const int tiles = (n + kThreads - 1) / kThreads;
-  int n_split = std::min(tiles, std::max(1, (32 * grid_cap + n_tb - 1) / n_tb));
-  const int chunk = ((tiles + n_split - 1) / n_split) * kThreads;
-  n_split = (n + chunk - 1) / chunk;
-  const long units = static_cast<long>(n_tb) * n_split;
-  const int grid = static_cast<int>(std::min<long>(units, grid_cap));
-
   int rc = AMK_OK;
-  float4* part = slot<float4>(c, kSlotPartial, static_cast<size_t>(n_split) * 2 * n, &rc);
+  const int n_tiles = (n + kThreads - 1) / kThreads;
+
+  // ---- Morton order (reused for kResortEvery calls on the context's own set)
+  const bool main_set = v.x == c->x.as<double>();
+  uint32_t* perm = nullptr;
+  bool resort = true;
+  if (main_set) {
+    AMK_TRY(c->ap_perm.reserve(static_cast<size_t>(n) * sizeof(uint32_t)));
+    perm = c->ap_perm.as<uint32_t>();
+    resort = c->ap_perm_n != n || c->ap_perm_age >= kResortEvery;
+  } else {
+    perm = slot<uint32_t>(c, kSlotSorted0, static_cast<size_t>(n), &rc);
+    AMK_TRY(rc);
+  }
+  AMK_TRY(phase_begin(c, AMK_PHASE_STAGE));
+  if (resort) {
+    unsigned long long* bb = slot<unsigned long long>(c, kSlotCellStart, 8, &rc);
+    AMK_TRY(rc);
+    uint64_t* keys = slot<uint64_t>(c, kSlotKeysA, n, &rc);
+    AMK_TRY(rc);
+    uint32_t* vals = slot<uint32_t>(c, kSlotValsA, n, &rc);
+    AMK_TRY(rc);
+    uint64_t* skeys = slot<uint64_t>(c, kSlotTreeKeys, n, &rc);
+    AMK_TRY(rc);
+    AMK_CUDA_TRY(cudaMemsetAsync(bb, 0xFF, 6 * sizeof(unsigned long long), c->stream));
+    ap_bbox_kernel<<<148, 256, 0, c->stream>>>(v, bb);
+    AMK_TRY(check_launch(c, "ap_bbox_kernel"));
+    ap_key_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(v, bb, keys, vals);
+    AMK_TRY(check_launch(c, "ap_key_kernel"));
+    AMK_TRY(radix_sort_pairs(c, keys, vals, skeys, perm, n, 32));
+    if (main_set) {
+      c->ap_perm_n = n;
+      c->ap_perm_age = 0;
+    }
+  }
+  if (main_set) c->ap_perm_age++;
+
+  // ---- sorted staging + tile boxes
+  float4* hq = slot<float4>(c, kSlotSorted1, n, &rc);
+  AMK_TRY(rc);
+  float4* lo = slot<float4>(c, kSlotSorted2, n, &rc);
+  AMK_TRY(rc);
+  float4* rel = slot<float4>(c, kSlotTreeAux0, n, &rc);
+  AMK_TRY(rc);
+  TileBox* boxes = slot<TileBox>(c, kSlotTreeAux1, n_tiles + 1, &rc);
   AMK_TRY(rc);
   const double l = v.length_scale;
-  const float eps2 = static_cast<float>(kMinSquaredDistance / (l * l));
+  ap_stage_kernel<<<n_tiles, kThreads, 0, c->stream>>>(v, perm, 1.0 / l, hq, lo, rel, boxes);
+  AMK_TRY(check_launch(c, "ap_stage_kernel"));
+  AMK_TRY(phase_end(c, AMK_PHASE_STAGE));
+
+  // ---- work split: chunks of whole tiles, >= 32 units per CTA
+  const int grid_cap = g_num_sms * std::max(1, g_ctas_per_sm[want_phi ? 1 : 0]);
+  const int n_tb = (n_tiles + kR - 1) / kR;
+  int n_split = std::min(n_tiles, std::max(1, (32 * grid_cap + n_tb - 1) / n_tb));
+  const int tiles_per_chunk = (n_tiles + n_split - 1) / n_split;
+  n_split = (n_tiles + tiles_per_chunk - 1) / tiles_per_chunk;
+  const long units = static_cast<long>(n_tb) * n_split;
+  const int grid = static_cast<int>(std::min<long>(units, grid_cap));
+  float4* part = slot<float4>(c, kSlotPartial, static_cast<size_t>(n_split) * 2 * n, &rc);
+  AMK_TRY(rc);
+  // r^2 floor: 1e-30 m^2 (the reference's skip radius), raised to 1e-25 in
+  // scaled units so that rinv^3 stays finite in FP32 for any length scale.
+  const float eps2 = static_cast<float>(std::max(kMinSquaredDistance / (l * l), 1e-25));
 
   AMK_TRY(phase_begin(c, AMK_PHASE_ALLPAIRS));
   if (want_phi)
-    allpairs_kernel<true><<<grid, kThreads, 0, c->stream>>>(v.hq, v.lo, n, n_tb, n_split, chunk, eps2, part);
+    allpairs_kernel<true><<<grid, kThreads, 0, c->stream>>>(hq, lo, rel, boxes, n, n_tiles, n_tb, n_split,
+                                                            tiles_per_chunk, eps2, part);
   else
-    allpairs_kernel<false><<<grid, kThreads, 0, c->stream>>>(v.hq, v.lo, n, n_tb, n_split, chunk, eps2, part);
+    allpairs_kernel<false><<<grid, kThreads, 0, c->stream>>>(hq, lo, rel, boxes, n, n_tiles, n_tb, n_split,
+                                                             tiles_per_chunk, eps2, part);
   AMK_TRY(check_launch(c, "allpairs_kernel"));
   AMK_TRY(phase_end(c, AMK_PHASE_ALLPAIRS));
   AMK_TRY(phase_begin(c, AMK_PHASE_STAGE));
   allpairs_finalize_kernel<<<(n + 255) / 256, 256, 0, c->stream>>>(
-      n, n_tb, n_split, grid, part, v.q, v.alive, v.hq, kCoulombConstant * kElementaryCharge / (l * l),
+      n, n_tb, n_split, grid, part, perm, hq, v.q, v.alive, kCoulombConstant * kElementaryCharge / (l * l),
       kElementaryCharge / l, v.fx, v.fy, v.fz, v.phi);
   AMK_TRY(check_launch(c, "allpairs_finalize_kernel"));
   AMK_TRY(phase_end(c, AMK_PHASE_STAGE));

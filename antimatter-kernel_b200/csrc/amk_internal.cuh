@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "amk.h"
+#include "morton.cuh"
 
 namespace amk {
 
@@ -179,6 +180,10 @@ struct amk_ctx {
   bool staggered = false;     // first push done (lorentz.h:34)
   long step = 0;              // completed steps
   bool stage_dirty = true;    // hq/lo must be rebuilt from x,y,z
+  // Morton order of the all-pairs kernel, reused for a few calls
+  amk::DevBuf ap_perm;
+  long ap_perm_n = -1;
+  int ap_perm_age = 0;
   // aux particle set for the stateless solver mirrors
   amk::DevBuf ax, ay, az, aq, ahq, alo, afx, afy, afz, aphi;
   long aux_capacity = 0;

@@ -415,6 +415,7 @@ __global__ void max_abs_kernel(long n, const double* __restrict__ x, const doubl
 
 static int finish_load(amk_ctx* c, long n) {
   c->n = n;
+  c->ap_perm_n = -1;
   c->staggered = false;
   c->step = 0;
   c->energy_has_previous = false;
@@ -661,14 +662,12 @@ static int ensure_staged(amk_ctx* c) {
 extern "C" int amk_coulomb_allpairs(amk_ctx* c) {
   if (!c) return fail(AMK_ERR_INVALID, "null context");
   if (c->n == 0) return AMK_OK;
-  AMK_TRY(ensure_staged(c));
   return allpairs_forces(c, main_view(c));
 }
 
 extern "C" int amk_coulomb_standard(amk_ctx* c, double cutoff) {
   if (!c) return fail(AMK_ERR_INVALID, "null context");
   if (c->n == 0) return AMK_OK;
-  AMK_TRY(ensure_staged(c));
   return cutoff_forces(c, main_view(c), cutoff, nullptr);
 }
 
@@ -722,7 +721,7 @@ extern "C" int amk_push(amk_ctx* c) {
   if (!c) return fail(AMK_ERR_INVALID, "null context");
   if (c->n > 0) {
     AMK_TRY(push_step(c, static_cast<uint64_t>(c->step + 1)));
-    c->stage_dirty = false;  // the push re-stages positions
+    c->stage_dirty = true;
   }
   c->step++;
   return AMK_OK;

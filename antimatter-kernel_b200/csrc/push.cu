@@ -1,9 +1,9 @@
 // Fused per-particle behaviours: LorentzForce::Run (Boris push in the ideal
 // Penning-trap field) followed by CyclotronCooling::Run (exact exponential
-// damping of v_perp plus Langevin noise), then re-staging of the new
-// position for the next force evaluation. All arithmetic is FP64 in the
+// damping of v_perp plus Langevin noise). All arithmetic is FP64 in the
 // reference's operation order; the kernel is HBM-bound (x, v read and
-// written, F read: ~110 B per particle-step).
+// written, F read and zeroed, q, m, alive, id read: ~133 B per
+// particle-step).
 #include "amk_internal.cuh"
 #include "philox.cuh"
 
@@ -21,7 +21,6 @@ struct PushParams {
   double bath_temp;  // bath_temperature
   uint32_t seed;
   uint64_t step;
-  double inv_l;      // 1 / L for re-staging
 };
 
 // BorisVelocity, lorentz.cc:18-35 (same operation order).
@@ -54,7 +53,7 @@ push_kernel(long n, double* __restrict__ x, double* __restrict__ y, double* __re
             double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
             double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
             const double* __restrict__ q, const double* __restrict__ m, const uint8_t* __restrict__ alive,
-            const uint32_t* __restrict__ ids, float4* __restrict__ hq, float4* __restrict__ lo, PushParams P) {
+            const uint32_t* __restrict__ ids, PushParams P) {
   const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
   if (i >= n) return;
   const bool live = alive[i] != 0;
@@ -118,21 +117,6 @@ push_kernel(long n, double* __restrict__ x, double* __restrict__ y, double* __re
     vy[i] = v[1];
     vz[i] = v[2];
   }
-  // ---- re-stage (same rule as stage_kernel)
-  const double xs = px * P.inv_l, ys = py * P.inv_l, zs = pz * P.inv_l;
-  const bool ok = live && qi != 0.0 && isfinite(xs) && isfinite(ys) && isfinite(zs);
-  float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
-  if (ok) {
-    h.x = __double2float_rn(xs);
-    h.y = __double2float_rn(ys);
-    h.z = __double2float_rn(zs);
-    h.w = __double2float_rn(qi / kElementaryCharge);
-    l.x = __double2float_rn(xs - static_cast<double>(h.x));
-    l.y = __double2float_rn(ys - static_cast<double>(h.y));
-    l.z = __double2float_rn(zs - static_cast<double>(h.z));
-  }
-  hq[i] = h;
-  lo[i] = l;
 }
 
 }  // namespace
@@ -152,13 +136,12 @@ int push_step(amk_ctx* c, uint64_t step_index) {
   P.bath_temp = p.bath_temperature;
   P.seed = static_cast<uint32_t>(p.seed);
   P.step = step_index;
-  P.inv_l = 1.0 / c->length_scale;
   AMK_TRY(phase_begin(c, AMK_PHASE_PUSH));
   const long n = c->n;
   push_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, c->stream>>>(
       n, c->x.as<double>(), c->y.as<double>(), c->z.as<double>(), c->vx.as<double>(), c->vy.as<double>(),
       c->vz.as<double>(), c->fx.as<double>(), c->fy.as<double>(), c->fz.as<double>(), c->q.as<double>(),
-      c->m.as<double>(), c->alive.as<uint8_t>(), c->ids.as<uint32_t>(), c->hq.as<float4>(), c->lo.as<float4>(), P);
+      c->m.as<double>(), c->alive.as<uint8_t>(), c->ids.as<uint32_t>(), P);
   AMK_TRY(check_launch(c, "push_kernel"));
   AMK_TRY(phase_end(c, AMK_PHASE_PUSH));
   c->staggered = true;

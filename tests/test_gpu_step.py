@@ -101,8 +101,12 @@ def test_cooling_with_bath_matches_oracle_one_step():
         st = s.get_particles()
         for k in ("vx", "vy", "vz"):
             assert np.max(np.abs(st[k] - ref[k])) <= 1e-11 * np.max(np.abs(ref[k])), k
-        # strong damping: v_perp relaxes to the bath (sigma^2 = kT/m)
-        s.step(200)
+        # strong damping (tau = 2.6e-11 s, ~10 e-folds of v_perp^2 per 60
+        # steps): v_perp relaxes to the bath, sigma^2 = kT/m per component
+        p2 = s.params
+        p2.cooling_scale = 1e-11
+        s.params = p2
+        s.step(300)
         st = s.get_particles()
         m = 9.1093837015e-31
         vperp2 = np.mean(st["vx"] ** 2 + st["vy"] ** 2) / 2
