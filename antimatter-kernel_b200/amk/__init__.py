@@ -130,6 +130,8 @@ def lib():
                                            _dp, _dp, _dp, _dp]),
         "amk_solve_fmm": (C.c_int, [vp, C.c_long, _dp, _dp, _dp, _dp, C.c_int, C.c_double, C.c_long,
                                     _dp, _dp, _dp, _dp]),
+        "amk_bh_tree_dump": (C.c_long, [vp, C.c_long, _dp, _dp, _dp, _dp, C.c_long, C.c_long, _dp,
+                                        C.POINTER(C.c_long)]),
         "amk_set_profiling": (C.c_int, [vp, C.c_int]),
         "amk_phase_times": (C.c_int, [vp, _dp, C.POINTER(C.c_long), C.c_int]),
         "amk_reset_phase_times": (C.c_int, [vp]),
@@ -402,6 +404,18 @@ class Simulation:
                                          int(leaf_capacity), _d(fx), _d(fy), _d(fz), _d(phi)),
               "amk_solve_barnes_hut")
         return (fx, fy, fz, phi) if want_phi else (fx, fy, fz)
+
+    def bh_tree(self, x, y, z, q, leaf_capacity=8):
+        """Barnes-Hut octree nodes in the reference's order (see amk_bh_tree_dump)."""
+        x, y, z, q = map(_f64, (x, y, z, q))
+        cap = 4 * len(x) + 64
+        f = np.zeros((cap, 12))
+        g = np.zeros((cap, 11), np.int64)
+        nn = lib().amk_bh_tree_dump(self._h, len(x), _d(x), _d(y), _d(z), _d(q), int(leaf_capacity), cap,
+                                    _d(f), g.ctypes.data_as(C.POINTER(C.c_long)))
+        if nn < 0:
+            check(int(nn), "amk_bh_tree_dump")
+        return f[:nn], g[:nn]
 
     def solve_fmm(self, x, y, z, q, order, theta, leaf_capacity=32, want_energy=False):
         x, y, z, q = map(_f64, (x, y, z, q))

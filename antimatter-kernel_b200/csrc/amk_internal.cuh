@@ -99,7 +99,7 @@ struct View {
 
 // ---------------------------------------------------------------- context
 struct Scratch {
-  DevBuf b[48];
+  DevBuf b[96];
 };
 
 enum ScratchSlot {
@@ -150,8 +150,33 @@ enum ScratchSlot {
   kSlotAuxState4,
   kSlotAuxState5,
   kSlotAuxState6,
+  kSlotScanSums,
+  kSlotTreeFrame,
+  kSlotTreeL,
+  kSlotTreeLeafDepth,
+  kSlotTreeCount,
+  kSlotTreeBase,
+  kSlotTreeCenter,
+  kSlotTreeChild,
+  kSlotTreeRange,
+  kSlotTreeMeta,
+  kSlotTreeParent,
+  kSlotTreeSrc,
+  kSlotTreeOrder,
+  kSlotTreeSortedKeys,
+  kSlotBhPos,
+  kSlotBhNeg,
+  kSlotWalkOut,
+  kSlotFmmRadius,
+  kSlotFmmWork0,
+  kSlotFmmWork1,
+  kSlotFmmWork2,
+  kSlotFmmWork3,
+  kSlotFmmWork4,
+  kSlotFmmWork5,
   kNumSlots
 };
+static_assert(kNumSlots <= 96, "scratch slots");
 
 struct PhaseClock {
   cudaEvent_t start[AMK_NUM_PHASES] = {};
@@ -240,6 +265,10 @@ int barnes_hut_forces(amk_ctx* c, const View& v, double theta, long leaf_capacit
 int fmm_forces(amk_ctx* c, const View& v, int order, double theta, long leaf_capacity,
                bool learned, double* energy_out);
 
+// Copies host sources into the context's auxiliary set (solver mirrors).
+int load_aux_view(amk_ctx* c, long n, const double* x, const double* y, const double* z, const double* q,
+                  View* out);
+
 // Power-of-two length scale for a set of host coordinates.
 double length_scale_for(double max_abs);
 
@@ -247,6 +276,43 @@ double length_scale_for(double max_abs);
 // 32-bit; sorts `n` elements on bits [0, key_bits); result in keys_out/vals_out.
 int radix_sort_pairs(amk_ctx* c, const uint64_t* keys_in, const uint32_t* vals_in,
                      uint64_t* keys_out, uint32_t* vals_out, long n, int key_bits);
+
+// Exclusive prefix sum of int32 values; *total_dev receives the sum.
+int exclusive_scan_int(amk_ctx* c, const int* in, long n, int* out, int* total_dev);
+
+// ---------------------------------------------------------------- octree
+// The reference's octrees (barnes-hut.cc:38-164, fast-multipole.cc:234-311,
+// :342-397) rebuilt from sorted Morton keys. Tree coordinates: Barnes-Hut
+// uses physical positions; the FMM rescales to a unit cube,
+// x' = (x - mid) / length (fast-multipole.cc:355-390).
+constexpr int kTreeLevels = 21;  // 63-bit keys: depth limit 21 (reference: 32)
+
+struct TreeFrame {
+  double mid[3];     // FMM: bbox centre (0 for Barnes-Hut)
+  double length;     // FMM: cube edge (1 for Barnes-Hut)
+  double root_c[3];  // root cube centre in tree coordinates
+  double root_h;     // root half edge in tree coordinates
+};
+
+struct Octree {
+  long m = 0;                  // sources in the tree, sorted positions [0, m)
+  long n_nodes = 0;
+  int leaf_cap = 8;
+  int max_depth = 0;           // deepest node
+  TreeFrame* frame = nullptr;  // device
+  uint32_t* order = nullptr;   // sorted position -> view index
+  uint64_t* keys = nullptr;    // sorted keys
+  double4* src = nullptr;      // sorted sources: tree coordinates + charge
+  double4* center = nullptr;   // node centre (tree coordinates) + half edge
+  int* child = nullptr;        // 8 per node, -1 = none (octant order)
+  int2* range = nullptr;       // node particle range [begin, end)
+  uchar2* meta = nullptr;      // (depth, is_leaf)
+  int* parent = nullptr;       // -1 for the root
+};
+
+// mode 0: Barnes-Hut (sources = live particles, physical coordinates);
+// mode 1: FMM (sources = live charged particles, unit-cube coordinates).
+int build_octree(amk_ctx* c, const View& v, int leaf_cap, int mode, Octree* out);
 
 // Deterministic FP64 sum of `n` doubles into *out_dev (device pointer).
 int reduce_sum(amk_ctx* c, const double* in, long n, double* out_dev);

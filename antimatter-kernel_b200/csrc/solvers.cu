@@ -8,7 +8,7 @@
 
 namespace amk {
 
-static int load_aux(amk_ctx* c, long n, const double* x, const double* y, const double* z, const double* q,
+int load_aux_view(amk_ctx* c, long n, const double* x, const double* y, const double* z, const double* q,
                     View* out) {
   if (n < 0 || n > 0x7fffffffL) return fail(AMK_ERR_LIMIT, "source count %ld outside [0, 2^31)", n);
   if (n > 0 && (!x || !y || !z || !q)) return fail(AMK_ERR_INVALID, "null source array");
@@ -71,7 +71,7 @@ extern "C" int amk_solve_allpairs(amk_ctx* c, long n, const double* x, const dou
                                   const double* q, double* fx, double* fy, double* fz, double* phi) {
   if (!c) return fail(AMK_ERR_INVALID, "null context");
   View v;
-  AMK_TRY(load_aux(c, n, x, y, z, q, &v));
+  AMK_TRY(load_aux_view(c, n, x, y, z, q, &v));
   if (n == 0) return AMK_OK;
   if (phi) v.phi = c->aphi.as<double>();
   AMK_TRY(allpairs_forces(c, v));
@@ -82,7 +82,7 @@ extern "C" int amk_solve_cutoff(amk_ctx* c, long n, const double* x, const doubl
                                 const double* q, double cutoff, double* fx, double* fy, double* fz) {
   if (!c) return fail(AMK_ERR_INVALID, "null context");
   View v;
-  AMK_TRY(load_aux(c, n, x, y, z, q, &v));
+  AMK_TRY(load_aux_view(c, n, x, y, z, q, &v));
   if (n == 0) return AMK_OK;
   AMK_TRY(cutoff_forces(c, v, cutoff, nullptr));
   return copy_out(c, v, fx, fy, fz, nullptr);
@@ -93,7 +93,7 @@ extern "C" int amk_solve_barnes_hut(amk_ctx* c, long n, const double* x, const d
                                     double* fz, double* phi) {
   if (!c) return fail(AMK_ERR_INVALID, "null context");
   View v;
-  AMK_TRY(load_aux(c, n, x, y, z, q, &v));
+  AMK_TRY(load_aux_view(c, n, x, y, z, q, &v));
   if (n == 0) return AMK_OK;
   if (phi) v.phi = c->aphi.as<double>();
   AMK_TRY(barnes_hut_forces(c, v, theta, leaf_capacity < 1 ? 1 : leaf_capacity));
@@ -106,7 +106,7 @@ extern "C" int amk_solve_fmm(amk_ctx* c, long n, const double* x, const double* 
   if (!c) return fail(AMK_ERR_INVALID, "null context");
   if (energy) *energy = 0.0;
   View v;
-  AMK_TRY(load_aux(c, n, x, y, z, q, &v));
+  AMK_TRY(load_aux_view(c, n, x, y, z, q, &v));
   if (n == 0) return AMK_OK;
   AMK_TRY(fmm_forces(c, v, order, theta, leaf_capacity < 1 ? 1 : leaf_capacity, false, energy));
   return copy_out(c, v, fx, fy, fz, nullptr);

@@ -3,10 +3,6 @@
 
 namespace amk {
 
-int barnes_hut_forces(amk_ctx*, const View&, double, long) {
-  return fail(AMK_ERR_UNSUPPORTED, "Barnes-Hut solver not built");
-}
-
 int fmm_forces(amk_ctx*, const View&, int, double, long, bool, double*) {
   return fail(AMK_ERR_UNSUPPORTED, "FMM solver not built");
 }

@@ -258,6 +258,16 @@ int amk_solve_fmm(amk_ctx* ctx, long n, const double* x, const double* y, const 
                   const double* q, int order, double theta, long leaf_capacity,
                   double* fx, double* fy, double* fz, double* energy);
 
+/* Builds the Barnes-Hut octree of the given sources (BarnesHutTree::Build,
+ * barnes-hut.cc:38-164) and copies its nodes out in the reference's order
+ * and layout: node_f64 holds 12 doubles per node (centre xyz, half size,
+ * positive charge, |negative| charge, positive centre xyz, negative centre
+ * xyz), node_i64 holds 11 per node (children[8] with -1 for none, begin, end,
+ * is_leaf). Returns the node count (BarnesHutTree::NumNodes) or an error. */
+long amk_bh_tree_dump(amk_ctx* ctx, long n, const double* x, const double* y, const double* z,
+                      const double* q, long leaf_capacity, long max_nodes, double* node_f64,
+                      long* node_i64);
+
 /* ------------------------------------------------------------ profiling */
 /* Per-phase device time (CUDA events on the context stream) accumulated
  * since the last reset, in ms. Phases: see AMK_PHASE_*. */

@@ -70,8 +70,12 @@ def test_allpairs_edge_cases(sim):
     q = np.array([E, -E, E, 0.0, -E])
     f = sim.solve_allpairs(x, y, z, q)
     g = O.allpairs(x, y, z, q)
+    # particle 2 feels a dipole whose two terms cancel to 4e-6 of each term:
+    # FP32 pair arithmetic resolves forces to ~1e-7 of the largest term
+    scale = max(np.max(np.abs(b)) for b in g)
     for a, b in zip(f, g):
-        assert np.allclose(a, b, rtol=1e-6, atol=1e-30)
+        assert np.all(np.isfinite(a))
+        assert np.max(np.abs(a - b)) < 1e-7 * scale
     assert f[0][3] == 0.0 and f[1][3] == 0.0  # neutral target gets no force
 
 
