@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "amk.h"
@@ -73,6 +74,13 @@ struct DevBuf {
   T* as() const {
     return static_cast<T*>(ptr);
   }
+  void swap(DevBuf& o) {
+    std::swap(ptr, o.ptr);
+    std::swap(bytes, o.bytes);
+  }
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
 };
 
 // ---------------------------------------------------------------- particle views

@@ -1,0 +1,757 @@
+// Cartesian fast multipole method on the GPU octree (fast-multipole.cc).
+//
+// Same mathematics as the reference (all in unit-cube coordinates,
+// fast-multipole.cc:91-113): multipoles M_a = sum q (y - c)^a / a!, local
+// expansions L_g = 1/g! sum_a (-1)^|a| M_a D_{a+g}(t - s) with D = d^a (1/r)
+// from the recurrence r^2 d_i f = -x_i f, L2L/M2M shifts by the binomial
+// tables, L2P as E = -grad phi, near field by direct sums. Order P in [1, 8],
+// leaf capacity 32, theta acceptance (r_T + r_S)^2 < theta^2 d^2.
+//
+// GPU mapping:
+//   radii, P2M      leaves in parallel (a thread per leaf / a warp per leaf)
+//   M2M, L2L        level-synchronous, a warp per node, lanes over coefficients
+//   lists           the reference's dual-tree recursion run breadth-first over
+//                   (target, source) pairs; M2L and P2P pairs are grouped per
+//                   target and each group sorted by source index, so every
+//                   sum has a fixed order (run-to-run deterministic)
+//   M2L             a warp per target cell; per source the derivative tensor
+//                   is built degree by degree in shared memory (lanes over the
+//                   multi-indices of one degree) and contracted with the
+//                   source's multipole, lanes over local coefficients
+//   L2P + P2P       a warp per target leaf, a lane per target particle,
+//                   source leaves broadcast through warp shuffles
+// Arithmetic is FP64 throughout, as in the reference.
+#include <algorithm>
+#include <array>
+#include <map>
+#include <memory>
+#include <vector>
+
+#include "amk_internal.cuh"
+
+namespace amk {
+
+// ------------------------------------------------------------ tables
+// FmmTables, fast-multipole.cc:41-178 (multi-indices sorted by degree,
+// within a degree by a then b descending).
+struct FmmHostTables {
+  int p = 0, n_m = 0, n_d = 0;
+  std::vector<int4> multi;  // a, b, c, degree
+  std::vector<double> fact, inv_fact, sign;
+  std::vector<int> deg_start;                // n_d entries grouped by degree
+  std::vector<int> rec_axis;                 // per k
+  std::vector<int> rec_delta, rec_m1, rec_m2;  // 3 per k
+  std::vector<int> m2l_index;                // [g * n_m + a]
+  std::vector<int> m2m_off, m2m_b, m2m_c;    // CSR by a
+  std::vector<int> l2l_off, l2l_b, l2l_c;    // CSR by a
+  std::vector<int> grad;                     // 3 per g, -1 none
+
+  explicit FmmHostTables(int order) : p(order) {
+    const int size = 2 * p + 1, maxdeg = 2 * p;
+    std::vector<int> lookup(static_cast<size_t>(size) * size * size, -1);
+    auto index = [&](int a, int b, int c) {
+      if (a < 0 || b < 0 || c < 0 || a >= size || b >= size || c >= size) return -1;
+      return lookup[(a * size + b) * size + c];
+    };
+    for (int deg = 0; deg <= maxdeg; ++deg) {
+      deg_start.push_back(static_cast<int>(multi.size()));
+      for (int a = deg; a >= 0; --a)
+        for (int b = deg - a; b >= 0; --b) {
+          const int c = deg - a - b;
+          lookup[(a * size + b) * size + c] = static_cast<int>(multi.size());
+          multi.push_back(make_int4(a, b, c, deg));
+        }
+    }
+    deg_start.push_back(static_cast<int>(multi.size()));
+    n_d = static_cast<int>(multi.size());
+    n_m = (p + 1) * (p + 2) * (p + 3) / 6;
+    std::vector<double> factorial(maxdeg + 1, 1.0);
+    for (int i = 1; i <= maxdeg; ++i) factorial[i] = factorial[i - 1] * i;
+    for (int k = 0; k < n_d; ++k) {
+      const int4 m = multi[k];
+      fact.push_back(factorial[m.x] * factorial[m.y] * factorial[m.z]);
+      inv_fact.push_back(1.0 / fact.back());
+      sign.push_back(((m.x + m.y + m.z) % 2 == 0) ? 1.0 : -1.0);
+    }
+    rec_axis.assign(n_d, 0);
+    rec_delta.assign(3 * n_d, 0);
+    rec_m1.assign(3 * n_d, -1);
+    rec_m2.assign(3 * n_d, -1);
+    for (int k = 1; k < n_d; ++k) {
+      const int m[3] = {multi[k].x, multi[k].y, multi[k].z};
+      rec_axis[k] = m[0] > 0 ? 0 : (m[1] > 0 ? 1 : 2);
+      for (int j = 0; j < 3; ++j) {
+        rec_delta[3 * k + j] = m[j];
+        int t[3] = {m[0], m[1], m[2]};
+        if (m[j] >= 1) {
+          t[j] -= 1;
+          rec_m1[3 * k + j] = index(t[0], t[1], t[2]);
+        }
+        if (m[j] >= 2) {
+          t[j] -= 1;
+          rec_m2[3 * k + j] = index(t[0], t[1], t[2]);
+        }
+      }
+    }
+    m2l_index.resize(static_cast<size_t>(n_m) * n_m);
+    for (int g = 0; g < n_m; ++g)
+      for (int a = 0; a < n_m; ++a)
+        m2l_index[static_cast<size_t>(g) * n_m + a] =
+            index(multi[a].x + multi[g].x, multi[a].y + multi[g].y, multi[a].z + multi[g].z);
+    m2m_off.push_back(0);
+    l2l_off.push_back(0);
+    for (int a = 0; a < n_m; ++a) {
+      for (int b = 0; b < n_m; ++b) {
+        if (multi[b].x <= multi[a].x && multi[b].y <= multi[a].y && multi[b].z <= multi[a].z) {
+          m2m_b.push_back(b);
+          m2m_c.push_back(index(multi[a].x - multi[b].x, multi[a].y - multi[b].y, multi[a].z - multi[b].z));
+        }
+        if (multi[a].x <= multi[b].x && multi[a].y <= multi[b].y && multi[a].z <= multi[b].z) {
+          l2l_b.push_back(b);
+          l2l_c.push_back(index(multi[b].x - multi[a].x, multi[b].y - multi[a].y, multi[b].z - multi[a].z));
+        }
+      }
+      m2m_off.push_back(static_cast<int>(m2m_b.size()));
+      l2l_off.push_back(static_cast<int>(l2l_b.size()));
+    }
+    grad.assign(3 * n_m, -1);
+    for (int g = 0; g < n_m; ++g) {
+      const int m[3] = {multi[g].x, multi[g].y, multi[g].z};
+      for (int k = 0; k < 3; ++k) {
+        int t[3] = {m[0], m[1], m[2]};
+        if (t[k] >= 1) {
+          t[k] -= 1;
+          grad[3 * g + k] = index(t[0], t[1], t[2]);
+        }
+      }
+    }
+  }
+};
+
+// Device copy of one order's tables.
+struct FmmDevTables {
+  int p, n_m, n_d;
+  const int4* multi;
+  const double* fact;
+  const double* inv_fact;
+  const double* sign;
+  const int* deg_start;
+  const int* rec_axis;
+  const int* rec_delta;
+  const int* rec_m1;
+  const int* rec_m2;
+  const int* m2l_index;
+  const int* m2m_off;
+  const int* m2m_b;
+  const int* m2m_c;
+  const int* l2l_off;
+  const int* l2l_b;
+  const int* l2l_c;
+  const int* grad;
+};
+
+struct FmmLists {
+  DevBuf cur, next, m2l, p2p;
+};
+
+struct Fmm {
+  std::map<int, std::pair<DevBuf*, FmmDevTables>> tables;
+  FmmLists lists;
+  ~Fmm() {
+    for (auto& kv : tables) delete kv.second.first;
+  }
+};
+
+namespace {
+
+constexpr int kMaxOrder = 8;
+constexpr int kMaxNm = 165;  // n_m(8)
+constexpr int kMaxNd = 969;  // n_d(8): degree <= 16
+constexpr int kFmmWarps = 4;
+
+template <typename T>
+size_t append(std::vector<char>& blob, const std::vector<T>& v) {
+  while (blob.size() % 16) blob.push_back(0);
+  const size_t off = blob.size();
+  const char* p = reinterpret_cast<const char*>(v.data());
+  blob.insert(blob.end(), p, p + v.size() * sizeof(T));
+  return off;
+}
+
+int get_tables(amk_ctx* c, int order, FmmDevTables* out) {
+  if (!c->fmm) c->fmm = new Fmm();
+  auto it = c->fmm->tables.find(order);
+  if (it != c->fmm->tables.end()) {
+    *out = it->second.second;
+    return AMK_OK;
+  }
+  FmmHostTables h(order);
+  std::vector<char> blob;
+  const size_t o_multi = append(blob, h.multi), o_fact = append(blob, h.fact), o_if = append(blob, h.inv_fact),
+               o_sign = append(blob, h.sign), o_ds = append(blob, h.deg_start), o_ax = append(blob, h.rec_axis),
+               o_de = append(blob, h.rec_delta), o_m1 = append(blob, h.rec_m1), o_m2 = append(blob, h.rec_m2),
+               o_idx = append(blob, h.m2l_index), o_mo = append(blob, h.m2m_off), o_mb = append(blob, h.m2m_b),
+               o_mc = append(blob, h.m2m_c), o_lo = append(blob, h.l2l_off), o_lb = append(blob, h.l2l_b),
+               o_lc = append(blob, h.l2l_c), o_g = append(blob, h.grad);
+  DevBuf* buf = new DevBuf();
+  int rc = buf->reserve(blob.size());
+  if (rc != AMK_OK) {
+    delete buf;
+    return rc;
+  }
+  AMK_CUDA_TRY(cudaMemcpy(buf->ptr, blob.data(), blob.size(), cudaMemcpyHostToDevice));
+  const char* b = static_cast<const char*>(buf->ptr);
+  FmmDevTables t;
+  t.p = h.p;
+  t.n_m = h.n_m;
+  t.n_d = h.n_d;
+  t.multi = reinterpret_cast<const int4*>(b + o_multi);
+  t.fact = reinterpret_cast<const double*>(b + o_fact);
+  t.inv_fact = reinterpret_cast<const double*>(b + o_if);
+  t.sign = reinterpret_cast<const double*>(b + o_sign);
+  t.deg_start = reinterpret_cast<const int*>(b + o_ds);
+  t.rec_axis = reinterpret_cast<const int*>(b + o_ax);
+  t.rec_delta = reinterpret_cast<const int*>(b + o_de);
+  t.rec_m1 = reinterpret_cast<const int*>(b + o_m1);
+  t.rec_m2 = reinterpret_cast<const int*>(b + o_m2);
+  t.m2l_index = reinterpret_cast<const int*>(b + o_idx);
+  t.m2m_off = reinterpret_cast<const int*>(b + o_mo);
+  t.m2m_b = reinterpret_cast<const int*>(b + o_mb);
+  t.m2m_c = reinterpret_cast<const int*>(b + o_mc);
+  t.l2l_off = reinterpret_cast<const int*>(b + o_lo);
+  t.l2l_b = reinterpret_cast<const int*>(b + o_lb);
+  t.l2l_c = reinterpret_cast<const int*>(b + o_lc);
+  t.grad = reinterpret_cast<const int*>(b + o_g);
+  c->fmm->tables[order] = {buf, t};
+  *out = t;
+  return AMK_OK;
+}
+
+// powers x^i, y^i, z^i for i <= p, then mono[k] = x^a y^b z^c (Monomials,
+// fast-multipole.cc:190-204)
+__device__ __forceinline__ void powers(int p, double x, double y, double z, double* px, double* py, double* pz) {
+  px[0] = py[0] = pz[0] = 1.0;
+  for (int i = 1; i <= p; ++i) {
+    px[i] = px[i - 1] * x;
+    py[i] = py[i - 1] * y;
+    pz[i] = pz[i - 1] * z;
+  }
+}
+
+// ------------------------------------------------------------ radii
+__global__ void fmm_leaf_radius_kernel(const Octree t, double* __restrict__ radius) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= t.n_nodes || !t.meta[id].y) return;
+  const double4 c = t.center[id];
+  const int2 r = t.range[id];
+  double r2 = 0.0;
+  for (int k = r.x; k < r.y; ++k) {
+    const double4 s = t.src[k];
+    const double dx = s.x - c.x, dy = s.y - c.y, dz = s.z - c.z;
+    r2 = fmax(r2, __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
+  }
+  radius[id] = sqrt(r2);
+}
+
+__global__ void fmm_parent_radius_kernel(const Octree t, int depth, double* __restrict__ radius) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= t.n_nodes) return;
+  const uchar2 mt = t.meta[id];
+  if (mt.y || mt.x != depth) return;
+  const double4 c = t.center[id];
+  double r = 0.0;
+  for (int o = 0; o < 8; ++o) {
+    const int ch = t.child[8 * id + o];
+    if (ch < 0) continue;
+    const double4 cc = t.center[ch];
+    const double dx = cc.x - c.x, dy = cc.y - c.y, dz = cc.z - c.z;
+    r = fmax(r, sqrt(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz))) + radius[ch]);
+  }
+  radius[id] = r;
+}
+
+// ------------------------------------------------------------ P2M, M2M
+// A warp per leaf; lanes over coefficients (fast-multipole.cc:443-461).
+__global__ void __launch_bounds__(32 * kFmmWarps)
+fmm_p2m_kernel(const Octree t, FmmDevTables T, double* __restrict__ M) {
+  const int lane = threadIdx.x & 31;
+  const int id = blockIdx.x * kFmmWarps + (threadIdx.x >> 5);
+  if (id >= t.n_nodes || !t.meta[id].y) return;
+  const double4 c = t.center[id];
+  const int2 r = t.range[id];
+  double acc[(kMaxNm + 31) / 32];
+  for (int u = 0; u < (kMaxNm + 31) / 32; ++u) acc[u] = 0.0;
+  double px[kMaxOrder + 1], py[kMaxOrder + 1], pz[kMaxOrder + 1];
+  for (int k = r.x; k < r.y; ++k) {
+    const double4 s = t.src[k];
+    if (s.w == 0.0) continue;
+    powers(T.p, s.x - c.x, s.y - c.y, s.z - c.z, px, py, pz);
+    for (int u = 0, a = lane; a < T.n_m; ++u, a += 32) {
+      const int4 m = T.multi[a];
+      acc[u] += s.w * (px[m.x] * py[m.y] * pz[m.z]) * T.inv_fact[a];
+    }
+  }
+  for (int u = 0, a = lane; a < T.n_m; ++u, a += 32) M[static_cast<size_t>(id) * T.n_m + a] = acc[u];
+}
+
+// M2M for parents at `depth` (fast-multipole.cc:463-482).
+__global__ void __launch_bounds__(32 * kFmmWarps)
+fmm_m2m_kernel(const Octree t, FmmDevTables T, int depth, double* __restrict__ M) {
+  const int lane = threadIdx.x & 31;
+  const int id = blockIdx.x * kFmmWarps + (threadIdx.x >> 5);
+  if (id >= t.n_nodes) return;
+  const uchar2 mt = t.meta[id];
+  if (mt.y || mt.x != depth) return;
+  const double4 c = t.center[id];
+  double acc[(kMaxNm + 31) / 32];
+  for (int u = 0; u < (kMaxNm + 31) / 32; ++u) acc[u] = 0.0;
+  double px[kMaxOrder + 1], py[kMaxOrder + 1], pz[kMaxOrder + 1];
+  for (int o = 0; o < 8; ++o) {
+    const int ch = t.child[8 * id + o];
+    if (ch < 0) continue;
+    const double4 cc = t.center[ch];
+    powers(T.p, cc.x - c.x, cc.y - c.y, cc.z - c.z, px, py, pz);
+    const double* mc = M + static_cast<size_t>(ch) * T.n_m;
+    for (int u = 0, a = lane; a < T.n_m; ++u, a += 32) {
+      double s = acc[u];
+      for (int e = T.m2m_off[a]; e < T.m2m_off[a + 1]; ++e) {
+        const int cidx = T.m2m_c[e];
+        const int4 m = T.multi[cidx];
+        s += mc[T.m2m_b[e]] * (px[m.x] * py[m.y] * pz[m.z]) * T.inv_fact[cidx];
+      }
+      acc[u] = s;
+    }
+  }
+  for (int u = 0, a = lane; a < T.n_m; ++u, a += 32) M[static_cast<size_t>(id) * T.n_m + a] = acc[u];
+}
+
+// ------------------------------------------------------------ dual traversal
+// One level of the reference's stack recursion (fast-multipole.cc:484-526)
+// for every pending (target, source) pair.
+__global__ void fmm_traverse_kernel(const Octree t, const double* __restrict__ radius, double theta2,
+                                    const int2* __restrict__ cur, int n_cur, int2* __restrict__ next,
+                                    int2* __restrict__ m2l, int2* __restrict__ p2p, int* counters) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n_cur) return;
+  const int2 pr = cur[i];
+  const int ti = pr.x, si = pr.y;
+  const double4 tc = t.center[ti], sc = t.center[si];
+  const double dx = tc.x - sc.x, dy = tc.y - sc.y, dz = tc.z - sc.z;
+  const double dist2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+  const double rt = radius[ti], rs = radius[si];
+  const double rsum = rt + rs;
+  if (__dmul_rn(rsum, rsum) < __dmul_rn(theta2, dist2)) {
+    m2l[atomicAdd(&counters[0], 1)] = pr;
+    return;
+  }
+  const bool tleaf = t.meta[ti].y, sleaf = t.meta[si].y;
+  if (tleaf && sleaf) {
+    p2p[atomicAdd(&counters[1], 1)] = pr;
+    return;
+  }
+  const bool split_target = sleaf || (!tleaf && rt >= rs);
+  const int node = split_target ? ti : si;
+  int kids[8], nk = 0;
+  for (int o = 0; o < 8; ++o) {
+    const int ch = t.child[8 * node + o];
+    if (ch >= 0) kids[nk++] = ch;
+  }
+  const int base = atomicAdd(&counters[2], nk);
+  for (int k = 0; k < nk; ++k) next[base + k] = split_target ? make_int2(kids[k], si) : make_int2(ti, kids[k]);
+}
+
+// Group pairs by target: count, scan (host side helper), scatter, then sort
+// each group by source so that every sum runs in a fixed order.
+__global__ void pair_count_kernel(const int2* __restrict__ pairs, int n, int* __restrict__ count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) atomicAdd(&count[pairs[i].x], 1);
+}
+
+__global__ void pair_scatter_kernel(const int2* __restrict__ pairs, int n, const int* __restrict__ off,
+                                    int* __restrict__ cursor, int* __restrict__ src) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int2 p = pairs[i];
+  src[off[p.x] + atomicAdd(&cursor[p.x], 1)] = p.y;
+}
+
+__global__ void segment_sort_kernel(const int* __restrict__ off, const int* __restrict__ count, int n_seg,
+                                    int* __restrict__ src) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_seg) return;
+  const int b = off[s], e = b + count[s];
+  for (int i = b + 1; i < e; ++i) {  // insertion sort (groups are short)
+    const int v = src[i];
+    int j = i - 1;
+    while (j >= b && src[j] > v) {
+      src[j + 1] = src[j];
+      --j;
+    }
+    src[j + 1] = v;
+  }
+}
+
+// ------------------------------------------------------------ M2L
+// A warp per target cell (fast-multipole.cc:528-555). Derivatives
+// (fast-multipole.cc:207-232) are built degree by degree in shared memory.
+__global__ void __launch_bounds__(32 * kFmmWarps)
+fmm_m2l_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, const int* __restrict__ count,
+               const int* __restrict__ src, const double* __restrict__ M, double* __restrict__ L) {
+  __shared__ double sD[kFmmWarps][kMaxNd];
+  __shared__ double sM[kFmmWarps][kMaxNm];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int ti = blockIdx.x * kFmmWarps + w;
+  if (ti >= t.n_nodes) return;
+  const int cnt = count[ti];
+  if (cnt == 0) return;
+  double* D = sD[w];
+  double* Ms = sM[w];
+  const double4 tc = t.center[ti];
+  double acc[(kMaxNm + 31) / 32];
+  for (int u = 0; u < (kMaxNm + 31) / 32; ++u) acc[u] = 0.0;
+  const int b = off[ti];
+  for (int e = b; e < b + cnt; ++e) {
+    const int si = src[e];
+    const double4 sc = t.center[si];
+    const double xs[3] = {tc.x - sc.x, tc.y - sc.y, tc.z - sc.z};
+    for (int a = lane; a < T.n_m; a += 32) Ms[a] = T.sign[a] * M[static_cast<size_t>(si) * T.n_m + a];
+    const double inv_r2 = 1.0 / (xs[0] * xs[0] + xs[1] * xs[1] + xs[2] * xs[2]);
+    if (lane == 0) D[0] = sqrt(inv_r2);
+    __syncwarp();
+    for (int deg = 1; deg <= 2 * T.p; ++deg) {
+      for (int k = T.deg_start[deg] + lane; k < T.deg_start[deg + 1]; k += 32) {
+        const int i = T.rec_axis[k];
+        const int di = T.rec_delta[3 * k + i];
+        double sum = (2 * di - 1) * xs[i] * D[T.rec_m1[3 * k + i]];
+        if (T.rec_m2[3 * k + i] >= 0) sum += (di - 1) * (di - 1) * D[T.rec_m2[3 * k + i]];
+        for (int j = 0; j < 3; ++j) {
+          const int dj = T.rec_delta[3 * k + j];
+          if (j == i || dj == 0) continue;
+          sum += 2.0 * dj * xs[j] * D[T.rec_m1[3 * k + j]];
+          if (T.rec_m2[3 * k + j] >= 0) sum += dj * (dj - 1) * D[T.rec_m2[3 * k + j]];
+        }
+        D[k] = -sum * inv_r2;
+      }
+      __syncwarp();
+    }
+    for (int u = 0, g = lane; g < T.n_m; ++u, g += 32) {
+      const int* idx = T.m2l_index + static_cast<size_t>(g) * T.n_m;
+      double s = 0.0;
+      for (int a = 0; a < T.n_m; ++a) s += Ms[a] * D[idx[a]];
+      acc[u] += s * T.inv_fact[g];
+    }
+    __syncwarp();
+  }
+  for (int u = 0, g = lane; g < T.n_m; ++u, g += 32) L[static_cast<size_t>(ti) * T.n_m + g] += acc[u];
+}
+
+// ------------------------------------------------------------ L2L
+// Children at `depth` receive their parent's expansion (fast-multipole.cc:557-578).
+__global__ void __launch_bounds__(32 * kFmmWarps)
+fmm_l2l_kernel(const Octree t, FmmDevTables T, int depth, double* __restrict__ L) {
+  const int lane = threadIdx.x & 31;
+  const int id = blockIdx.x * kFmmWarps + (threadIdx.x >> 5);
+  if (id >= t.n_nodes) return;
+  if (t.meta[id].x != depth) return;
+  const int par = t.parent[id];
+  if (par < 0) return;
+  const double4 c = t.center[id], pc = t.center[par];
+  double px[kMaxOrder + 1], py[kMaxOrder + 1], pz[kMaxOrder + 1];
+  powers(T.p, c.x - pc.x, c.y - pc.y, c.z - pc.z, px, py, pz);
+  const double* lp = L + static_cast<size_t>(par) * T.n_m;
+  double* lc = L + static_cast<size_t>(id) * T.n_m;
+  for (int a = lane; a < T.n_m; a += 32) {
+    double s = lc[a];
+    for (int e = T.l2l_off[a]; e < T.l2l_off[a + 1]; ++e) {
+      const int bb = T.l2l_b[e], cc = T.l2l_c[e];
+      const int4 m = T.multi[cc];
+      s += lp[bb] * T.fact[bb] * T.inv_fact[a] * T.inv_fact[cc] * (px[m.x] * py[m.y] * pz[m.z]);
+    }
+    lc[a] = s;
+  }
+}
+
+// ------------------------------------------------------------ L2P + P2P
+// A warp per target leaf, a lane per target particle (fast-multipole.cc:580-661).
+// Outputs in sorted order: ef = (Ex, Ey, Ez, phi) per unit target charge.
+__global__ void __launch_bounds__(32 * kFmmWarps)
+fmm_l2p_p2p_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, const int* __restrict__ count,
+                   const int* __restrict__ src, const double* __restrict__ L, double min_sq, bool want_phi,
+                   double4* __restrict__ ef) {
+  const int lane = threadIdx.x & 31;
+  const int ti = blockIdx.x * kFmmWarps + (threadIdx.x >> 5);
+  if (ti >= t.n_nodes || !t.meta[ti].y) return;
+  const double4 tc = t.center[ti];
+  const int2 tr = t.range[ti];
+  const double* l = L + static_cast<size_t>(ti) * T.n_m;
+  for (int base = tr.x; base < tr.y; base += 32) {
+    const int i = base + lane;
+    const bool valid = i < tr.y;
+    double4 me = make_double4(0.0, 0.0, 0.0, 0.0);
+    if (valid) me = t.src[i];
+    double pot = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
+    if (valid) {
+      double px[kMaxOrder + 1], py[kMaxOrder + 1], pz[kMaxOrder + 1];
+      powers(T.p, me.x - tc.x, me.y - tc.y, me.z - tc.z, px, py, pz);
+      if (want_phi)
+        for (int g = 0; g < T.n_m; ++g) {
+          const int4 m = T.multi[g];
+          pot += l[g] * (px[m.x] * py[m.y] * pz[m.z]);
+        }
+      double gx = 0.0, gy = 0.0, gz = 0.0;
+      for (int g = 1; g < T.n_m; ++g) {
+        const int4 m = T.multi[g];
+        const int g0 = T.grad[3 * g], g1 = T.grad[3 * g + 1], g2 = T.grad[3 * g + 2];
+        if (g0 >= 0) {
+          const int4 q = T.multi[g0];
+          gx += m.x * l[g] * (px[q.x] * py[q.y] * pz[q.z]);
+        }
+        if (g1 >= 0) {
+          const int4 q = T.multi[g1];
+          gy += m.y * l[g] * (px[q.x] * py[q.y] * pz[q.z]);
+        }
+        if (g2 >= 0) {
+          const int4 q = T.multi[g2];
+          gz += m.z * l[g] * (px[q.x] * py[q.y] * pz[q.z]);
+        }
+      }
+      fx = -gx;
+      fy = -gy;
+      fz = -gz;
+    }
+    const int sb = off[ti], se = sb + count[ti];
+    for (int e = sb; e < se; ++e) {
+      const int si = src[e];
+      const int2 sr = t.range[si];
+      for (int jb = sr.x; jb < sr.y; jb += 32) {
+        const int jn = min(32, sr.y - jb);
+        double4 sv = make_double4(0.0, 0.0, 0.0, 0.0);
+        if (lane < jn) sv = t.src[jb + lane];
+        for (int u = 0; u < jn; ++u) {
+          const double sx = __shfl_sync(0xffffffffu, sv.x, u);
+          const double sy = __shfl_sync(0xffffffffu, sv.y, u);
+          const double sz = __shfl_sync(0xffffffffu, sv.z, u);
+          const double sq = __shfl_sync(0xffffffffu, sv.w, u);
+          const int j = jb + u;
+          if (!valid || j == i || sq == 0.0) continue;
+          const double rx = me.x - sx, ry = me.y - sy, rz = me.z - sz;
+          const double r2 = rx * rx + ry * ry + rz * rz;
+          if (r2 < min_sq) continue;
+          const double inv_r = 1.0 / sqrt(r2);
+          const double f = sq * inv_r / r2;
+          fx += rx * f;
+          fy += ry * f;
+          fz += rz * f;
+          pot += sq * inv_r;
+        }
+      }
+    }
+    if (valid) ef[i] = make_double4(fx, fy, fz, pot);
+  }
+}
+
+__global__ void fmm_output_kernel(const Octree t, const double4* __restrict__ ef, double force_scale, View v,
+                                  double* __restrict__ qphi) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= t.m) return;
+  const double4 e = ef[k];
+  const double q = t.src[k].w;
+  const long i = t.order[k];
+  const double s = force_scale * q;  // fast-multipole.cc:663-673
+  v.fx[i] = s * e.x;
+  v.fy[i] = s * e.y;
+  v.fz[i] = s * e.z;
+  if (qphi) qphi[k] = q * e.w;
+}
+
+__global__ void zero_forces_kernel(View v) {
+  const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (i >= v.n) return;
+  v.fx[i] = 0.0;
+  v.fy[i] = 0.0;
+  v.fz[i] = 0.0;
+}
+
+// Growable int2 list that keeps its contents.
+int grow_keep(amk_ctx* c, DevBuf& b, size_t used_bytes, size_t want_bytes) {
+  if (want_bytes <= b.bytes) return AMK_OK;
+  DevBuf nb;
+  AMK_TRY(nb.reserve(want_bytes));
+  if (used_bytes) AMK_CUDA_TRY(cudaMemcpyAsync(nb.ptr, b.ptr, used_bytes, cudaMemcpyDeviceToDevice, c->stream));
+  AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  b.swap(nb);
+  return AMK_OK;
+}
+
+struct Grouped {
+  int* off = nullptr;
+  int* count = nullptr;
+  int* src = nullptr;
+};
+
+int group_pairs(amk_ctx* c, const int2* pairs, long n_pairs, long n_nodes, int slot_off, int slot_cnt, int slot_src,
+                int slot_cursor, Grouped* g) {
+  int rc = AMK_OK;
+  g->off = slot<int>(c, slot_off, n_nodes + 1, &rc);
+  AMK_TRY(rc);
+  g->count = slot<int>(c, slot_cnt, n_nodes + 1, &rc);
+  AMK_TRY(rc);
+  g->src = slot<int>(c, slot_src, std::max<long>(n_pairs, 1), &rc);
+  AMK_TRY(rc);
+  int* cursor = slot<int>(c, slot_cursor, n_nodes + 1, &rc);
+  AMK_TRY(rc);
+  int* total = slot<int>(c, kSlotStatus, 8, &rc) + 6;
+  AMK_TRY(rc);
+  AMK_CUDA_TRY(cudaMemsetAsync(g->count, 0, (n_nodes + 1) * sizeof(int), c->stream));
+  AMK_CUDA_TRY(cudaMemsetAsync(cursor, 0, (n_nodes + 1) * sizeof(int), c->stream));
+  if (n_pairs > 0) {
+    pair_count_kernel<<<static_cast<unsigned>((n_pairs + 255) / 256), 256, 0, c->stream>>>(pairs, static_cast<int>(n_pairs),
+                                                                                          g->count);
+    AMK_TRY(check_launch(c, "pair_count_kernel"));
+  }
+  AMK_TRY(exclusive_scan_int(c, g->count, n_nodes, g->off, total));
+  if (n_pairs > 0) {
+    pair_scatter_kernel<<<static_cast<unsigned>((n_pairs + 255) / 256), 256, 0, c->stream>>>(
+        pairs, static_cast<int>(n_pairs), g->off, cursor, g->src);
+    AMK_TRY(check_launch(c, "pair_scatter_kernel"));
+    segment_sort_kernel<<<static_cast<unsigned>((n_nodes + 255) / 256), 256, 0, c->stream>>>(
+        g->off, g->count, static_cast<int>(n_nodes), g->src);
+    AMK_TRY(check_launch(c, "segment_sort_kernel"));
+  }
+  return AMK_OK;
+}
+
+}  // namespace
+
+int fmm_forces(amk_ctx* c, const View& v, int order, double theta, long leaf_capacity, bool learned,
+               double* energy_out) {
+  if (energy_out) *energy_out = 0.0;
+  if (learned) return fail(AMK_ERR_UNSUPPORTED, "learned FMM correction not built");
+  const long n = v.n;
+  if (n == 0) return AMK_OK;
+  order = std::min(std::max(order, 1), kMaxOrder);  // fast-multipole.cc:324-328
+  zero_forces_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, c->stream>>>(v);
+  AMK_TRY(check_launch(c, "zero_forces_kernel"));
+  FmmDevTables T;
+  AMK_TRY(get_tables(c, order, &T));
+  Octree t;
+  AMK_TRY(phase_begin(c, AMK_PHASE_TREE));
+  AMK_TRY(build_octree(c, v, static_cast<int>(std::min<long>(leaf_capacity, 1 << 20)), 1, &t));
+  AMK_TRY(phase_end(c, AMK_PHASE_TREE));
+  if (t.m == 0) return AMK_OK;
+  const long nn = t.n_nodes;
+  int rc = AMK_OK;
+  double* radius = slot<double>(c, kSlotFmmRadius, nn, &rc);
+  AMK_TRY(rc);
+  double* M = slot<double>(c, kSlotFmmM, static_cast<size_t>(nn) * T.n_m, &rc);
+  AMK_TRY(rc);
+  double* Lx = slot<double>(c, kSlotFmmL, static_cast<size_t>(nn) * T.n_m, &rc);
+  AMK_TRY(rc);
+  const unsigned gn = static_cast<unsigned>((nn + 255) / 256);
+  const unsigned gw = static_cast<unsigned>((nn + kFmmWarps - 1) / kFmmWarps);
+
+  // ---- upward pass
+  AMK_TRY(phase_begin(c, AMK_PHASE_FMM_UP));
+  fmm_leaf_radius_kernel<<<gn, 256, 0, c->stream>>>(t, radius);
+  AMK_TRY(check_launch(c, "fmm_leaf_radius_kernel"));
+  for (int d = t.max_depth; d >= 0; --d) {
+    fmm_parent_radius_kernel<<<gn, 256, 0, c->stream>>>(t, d, radius);
+    AMK_TRY(check_launch(c, "fmm_parent_radius_kernel"));
+  }
+  fmm_p2m_kernel<<<gw, 32 * kFmmWarps, 0, c->stream>>>(t, T, M);
+  AMK_TRY(check_launch(c, "fmm_p2m_kernel"));
+  for (int d = t.max_depth; d >= 0; --d) {
+    fmm_m2m_kernel<<<gw, 32 * kFmmWarps, 0, c->stream>>>(t, T, d, M);
+    AMK_TRY(check_launch(c, "fmm_m2m_kernel"));
+  }
+  AMK_TRY(phase_end(c, AMK_PHASE_FMM_UP));
+
+  // ---- interaction lists
+  AMK_TRY(phase_begin(c, AMK_PHASE_FMM_LISTS));
+  FmmLists& lists = c->fmm->lists;
+  int* counters = slot<int>(c, kSlotFmmAux0, 4, &rc);
+  AMK_TRY(rc);
+  long n_cur = 1, n_m2l = 0, n_p2p = 0;
+  AMK_TRY(grow_keep(c, lists.cur, 0, 64 * sizeof(int2)));
+  const int2 root = make_int2(0, 0);
+  AMK_CUDA_TRY(cudaMemcpyAsync(lists.cur.ptr, &root, sizeof(int2), cudaMemcpyHostToDevice, c->stream));
+  const double theta2 = theta * theta;
+  for (int level = 0; n_cur > 0; ++level) {
+    if (level > 4 * kTreeLevels + 8) return fail(AMK_ERR_TIMEOUT, "FMM traversal did not terminate");
+    AMK_TRY(grow_keep(c, lists.next, 0, static_cast<size_t>(8 * n_cur + 8) * sizeof(int2)));
+    AMK_TRY(grow_keep(c, lists.m2l, n_m2l * sizeof(int2), static_cast<size_t>(n_m2l + n_cur + 8) * sizeof(int2)));
+    AMK_TRY(grow_keep(c, lists.p2p, n_p2p * sizeof(int2), static_cast<size_t>(n_p2p + n_cur + 8) * sizeof(int2)));
+    const int hc[4] = {static_cast<int>(n_m2l), static_cast<int>(n_p2p), 0, 0};
+    AMK_CUDA_TRY(cudaMemcpyAsync(counters, hc, sizeof(hc), cudaMemcpyHostToDevice, c->stream));
+    fmm_traverse_kernel<<<static_cast<unsigned>((n_cur + 255) / 256), 256, 0, c->stream>>>(
+        t, radius, theta2, lists.cur.as<int2>(), static_cast<int>(n_cur), lists.next.as<int2>(), lists.m2l.as<int2>(),
+        lists.p2p.as<int2>(), counters);
+    AMK_TRY(check_launch(c, "fmm_traverse_kernel"));
+    int out[4];
+    AMK_CUDA_TRY(cudaMemcpyAsync(out, counters, sizeof(out), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    n_m2l = out[0];
+    n_p2p = out[1];
+    n_cur = out[2];
+    lists.cur.swap(lists.next);
+  }
+  Grouped gm, gp;
+  AMK_TRY(group_pairs(c, lists.m2l.as<int2>(), n_m2l, nn, kSlotFmmLists0, kSlotFmmLists1, kSlotFmmWork0,
+                      kSlotFmmWork1, &gm));
+  AMK_TRY(group_pairs(c, lists.p2p.as<int2>(), n_p2p, nn, kSlotFmmLists2, kSlotFmmLists3, kSlotFmmWork2,
+                      kSlotFmmWork3, &gp));
+  AMK_TRY(phase_end(c, AMK_PHASE_FMM_LISTS));
+
+  // ---- M2L
+  AMK_CUDA_TRY(cudaMemsetAsync(Lx, 0, static_cast<size_t>(nn) * T.n_m * sizeof(double), c->stream));
+  AMK_TRY(phase_begin(c, AMK_PHASE_FMM_M2L));
+  fmm_m2l_kernel<<<gw, 32 * kFmmWarps, 0, c->stream>>>(t, T, gm.off, gm.count, gm.src, M, Lx);
+  AMK_TRY(check_launch(c, "fmm_m2l_kernel"));
+  AMK_TRY(phase_end(c, AMK_PHASE_FMM_M2L));
+
+  // ---- L2L
+  AMK_TRY(phase_begin(c, AMK_PHASE_FMM_DOWN));
+  for (int d = 1; d <= t.max_depth; ++d) {
+    fmm_l2l_kernel<<<gw, 32 * kFmmWarps, 0, c->stream>>>(t, T, d, Lx);
+    AMK_TRY(check_launch(c, "fmm_l2l_kernel"));
+  }
+  AMK_TRY(phase_end(c, AMK_PHASE_FMM_DOWN));
+
+  // ---- L2P + P2P
+  double4* ef = slot<double4>(c, kSlotFmmWork4, t.m, &rc);
+  AMK_TRY(rc);
+  TreeFrame hf;
+  AMK_CUDA_TRY(cudaMemcpyAsync(&hf, t.frame, sizeof(hf), cudaMemcpyDeviceToHost, c->stream));
+  AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const double min_sq = kMinSquaredDistance / (hf.length * hf.length);
+  AMK_TRY(phase_begin(c, AMK_PHASE_FMM_P2P));
+  fmm_l2p_p2p_kernel<<<gw, 32 * kFmmWarps, 0, c->stream>>>(t, T, gp.off, gp.count, gp.src, Lx, min_sq,
+                                                           energy_out != nullptr, ef);
+  AMK_TRY(check_launch(c, "fmm_l2p_p2p_kernel"));
+  AMK_TRY(phase_end(c, AMK_PHASE_FMM_P2P));
+  double* qphi = nullptr;
+  if (energy_out) {
+    qphi = slot<double>(c, kSlotFmmWork5, t.m, &rc);
+    AMK_TRY(rc);
+  }
+  const double force_scale = kCoulombConstant / (hf.length * hf.length);
+  fmm_output_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, c->stream>>>(t, ef, force_scale, v, qphi);
+  AMK_TRY(check_launch(c, "fmm_output_kernel"));
+  if (energy_out) {
+    double* res = slot<double>(c, kSlotAuxState4, 8, &rc);
+    AMK_TRY(rc);
+    AMK_TRY(reduce_sum(c, qphi, t.m, res));
+    double h = 0.0;
+    AMK_CUDA_TRY(cudaMemcpyAsync(&h, res, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    *energy_out = 0.5 * kCoulombConstant / hf.length * h;  // fast-multipole.cc:676-680
+  }
+  return AMK_OK;
+}
+
+}  // namespace amk
+
+void fmm_destroy(amk_ctx* c) {
+  delete c->fmm;
+  c->fmm = nullptr;
+}

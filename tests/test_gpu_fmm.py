@@ -1,0 +1,104 @@
+"""GPU Cartesian FMM against the reference's FastMultipoleSolver: forces and
+energies from the reference's own code (golden fixtures, N = 2,000), theta = 0
+equal to the exact sum, and accuracy against the exact sum no worse than the
+reference's at the same order and theta."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle_lib as O
+from conftest import E, gaussian_cloud, rel_errors
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+FMM_TOL = 1e-9  # FP64 expansions; only summation order differs from the reference
+
+
+@pytest.mark.parametrize("order,theta", [(2, 0.5), (4, 0.5), (6, 0.5), (4, 0.0)])
+def test_fmm_matches_reference_fixture(sim, order, theta):
+    g = np.load(os.path.join(GOLD, "fmm_n2000.npz"))
+    f, e = sim.solve_fmm(g["x"], g["y"], g["z"], g["q"], order, theta, want_energy=True)
+    ref = g[f"f_p{order}_theta{theta}"].T
+    rel, glob = rel_errors(f, ref)
+    assert np.max(rel) < FMM_TOL, np.max(rel)
+    eref = float(g[f"e_p{order}_theta{theta}"])
+    assert abs(e - eref) <= 1e-10 * abs(eref)
+
+
+def test_fmm_theta0_is_allpairs(sim):
+    x, y, z, q = gaussian_cloud(2500, 40)
+    f = sim.solve_fmm(x, y, z, q, 3, 0.0)
+    rel, _ = rel_errors(f, O.allpairs(x, y, z, q))
+    assert np.max(rel) < FMM_TOL
+
+
+def test_fmm_error_no_worse_than_reference():
+    import amk
+    err = json.load(open(os.path.join(GOLD, "fmm_n4000_err.json")))["errors"]
+    with amk.Simulation() as s:
+        for label, mixed in (("mixed", True), ("positive", False)):
+            x, y, z, q = gaussian_cloud(4000, 11)
+            if not mixed:
+                q = np.full(4000, E)
+            exact = O.allpairs(x, y, z, q)
+            for p in (2, 4, 6):
+                f = s.solve_fmm(x, y, z, q, p, 0.5)
+                rel, glob = rel_errors(f, exact)
+                ref = err[f"{label}_p{p}"]
+                assert np.sqrt(np.mean(rel ** 2)) <= ref["rms"] * (1 + 1e-6), (label, p)
+                assert glob <= ref["global"] * (1 + 1e-6), (label, p)
+
+
+def test_fmm_order_clamp_and_leaf_capacity(sim):
+    x, y, z, q = gaussian_cloud(1200, 41)
+    a = sim.solve_fmm(x, y, z, q, 0, 0.5)
+    b = sim.solve_fmm(x, y, z, q, 1, 0.5)
+    assert all(np.array_equal(u, v) for u, v in zip(a, b))   # order clamped to [1, 8]
+    a = sim.solve_fmm(x, y, z, q, 12, 0.5)
+    b = sim.solve_fmm(x, y, z, q, 8, 0.5)
+    assert all(np.array_equal(u, v) for u, v in zip(a, b))
+    if O.ref_available():
+        for cap in (4, 16, 100):
+            f = sim.solve_fmm(x, y, z, q, 3, 0.6, leaf_capacity=cap)
+            (rx, ry, rz), _ = O.ref_fmm(x, y, z, q, 3, 0.6, cap)
+            rel, _ = rel_errors(f, (rx, ry, rz))
+            assert np.max(rel) < FMM_TOL, cap
+
+
+def test_fmm_neutral_and_annihilated_particles():
+    import amk
+    x, y, z, q = gaussian_cloud(600, 42)
+    sp = np.where(q > 0, 1, 3).astype(np.uint8)
+    sp[::10] = 2  # antihydrogen: neutral, force 0 (fast-multipole.cc:690)
+    p = amk.make_params(populations={"positron": 300, "electron": 300}, annihilation_enabled=1,
+                        contact_radius=2e-5, annihilation_probability=1.0)
+    with amk.Simulation(p) as s:
+        s.set_particles(x, y, z, np.zeros(600), np.zeros(600), np.zeros(600), sp)
+        s.annihilate()
+        alive = s.get_particles()["alive"].astype(bool)
+        s.coulomb_fmm(4, 0.5)
+        f = s.get_forces()
+        charged = alive & (sp != 2)
+        assert np.all(f[0][~charged] == 0.0)
+        qq = np.where(sp == 1, E, -E)
+        if O.ref_available():
+            (rx, ry, rz), _ = O.ref_fmm(x[charged], y[charged], z[charged], qq[charged], 4, 0.5)
+            rel, _ = rel_errors(tuple(a[charged] for a in f), (rx, ry, rz))
+            assert np.max(rel) < FMM_TOL
+
+
+def test_fmm_energy_method_in_context():
+    import amk
+    g = np.load(os.path.join(GOLD, "fmm_n2000.npz"))
+    n = len(g["x"])
+    sp = np.where(g["q"] > 0, 1, 3).astype(np.uint8)
+    p = amk.make_params(populations={"positron": n // 2, "electron": n - n // 2},
+                        energy_method="fast-multipole", fast_multipole_order=4.0,
+                        fast_multipole_theta=0.5)
+    with amk.Simulation(p) as s:
+        s.set_particles(g["x"], g["y"], g["z"], np.zeros(n), np.zeros(n), np.zeros(n), sp)
+        e = s.energy(time_centre=False)
+        eref = float(g["e_p4_theta0.5"])
+        assert abs(e["coulomb_potential"] - eref) <= 1e-10 * abs(eref)
