@@ -2,8 +2,7 @@
 // Penning-trap field) followed by CyclotronCooling::Run (exact exponential
 // damping of v_perp plus Langevin noise). All arithmetic is FP64 in the
 // reference's operation order; the kernel is HBM-bound (x, v read and
-// written, F read and zeroed, q, m, alive, id read: ~133 B per
-// particle-step).
+// written, F read and zeroed, q, m and alive read: 161 B per particle-step).
 #include "amk_internal.cuh"
 #include "philox.cuh"
 
