@@ -438,3 +438,120 @@ int annihilate_step(amk_ctx* c, uint64_t step_index, long* marked) {
 }
 
 }  // namespace amk
+
+// ======================================================================
+// Allocation-free cutoff solver.
+//
+// Some callers cannot let a library allocate device memory: a host code
+// whose device memory is already owned by its own pool allocator (a
+// library cudaMalloc could fail there, or fragment the pool), or a
+// per-step loop that cannot take the implicit device-wide synchronisation
+// of cudaMalloc/cudaFree. For them this variant of the cutoff solver keeps
+// all of its scratch (cell keys, sort buffers, histograms: about 2.4 MB)
+// in one file-scope device array sized for kNoAllocMaxParticles. Every GPU
+// that loads this library holds that array until the process exits.
+//
+// Set-up: the first call on a device (with that device current) looks up
+// the array's device address with cudaGetSymbolAddress and caches it; make
+// that first call during set-up, before any stream capture. Later calls
+// allocate nothing and call no allocating routine.
+//
+// Every call uses the same array and it keeps the last call's contents:
+// only the bounding-box words must start cleared and they are reset at the
+// start of each call. Calls that overlap on the GPU (different streams, or
+// different host threads without ordering) race on the array.
+// ======================================================================
+#include <mutex>
+
+namespace amk {
+namespace {
+
+constexpr long kNoAllocMaxParticles = 65536;
+constexpr long kNoAllocSortTile = 4096;  // the sort's tile (256 threads x 16)
+constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+constexpr size_t kNaBbox = 0;
+constexpr size_t kNaKeys = align256(kNaBbox + 8 * sizeof(unsigned long long));
+constexpr size_t kNaVals = align256(kNaKeys + kNoAllocMaxParticles * sizeof(uint64_t));
+constexpr size_t kNaSKeys = align256(kNaVals + kNoAllocMaxParticles * sizeof(uint32_t));
+constexpr size_t kNaSIdx = align256(kNaSKeys + kNoAllocMaxParticles * sizeof(uint64_t));
+constexpr size_t kNaTKeys = align256(kNaSIdx + kNoAllocMaxParticles * sizeof(uint32_t));
+constexpr size_t kNaTVals = align256(kNaTKeys + kNoAllocMaxParticles * sizeof(uint64_t));
+constexpr size_t kNaHist = align256(kNaTVals + kNoAllocMaxParticles * sizeof(uint32_t));
+constexpr size_t kNaBytes =
+    align256(kNaHist + 256 * ((kNoAllocMaxParticles + kNoAllocSortTile - 1) / kNoAllocSortTile) * sizeof(uint32_t));
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {};
+
+}  // namespace
+
+cudaError_t radix_sort_pairs_buffers(cudaStream_t stream, const uint64_t* keys_in, const uint32_t* vals_in,
+                                     uint64_t* keys_out, uint32_t* vals_out, uint64_t* ktmp, uint32_t* vtmp,
+                                     uint32_t* hist, long n, int key_bits);
+
+}  // namespace amk
+
+extern "C" int amk_coulomb_standard_noalloc(const double* x, const double* y, const double* z, const double* q,
+                                            const uint8_t* alive, long n, double cutoff_radius, double* fx,
+                                            double* fy, double* fz, void* stream) {
+  using namespace amk;
+  if (n < 0) return fail(AMK_ERR_INVALID, "amk_coulomb_standard_noalloc: n < 0");
+  if (n > kNoAllocMaxParticles)
+    return fail(AMK_ERR_LIMIT,
+                "amk_coulomb_standard_noalloc: %ld particles exceed the allocation-free maximum of %ld", n,
+                kNoAllocMaxParticles);
+  if (n == 0) return AMK_OK;
+  if (!x || !y || !z || !q || !fx || !fy || !fz) return fail(AMK_ERR_INVALID, "amk_coulomb_standard_noalloc: null array");
+  int dev = 0;
+  AMK_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return fail(AMK_ERR_LIMIT, "device %d beyond the supported range", dev);
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+      if (e != cudaSuccess || p == nullptr)
+        return fail(AMK_ERR_CUDA, "cudaGetSymbolAddress of the allocation-free scratch failed: %s",
+                    cudaGetErrorString(e));
+      g_noalloc_addr[dev] = static_cast<unsigned char*>(p);
+    }
+    base = g_noalloc_addr[dev];
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  View v;
+  v.n = n;
+  v.x = const_cast<double*>(x);
+  v.y = const_cast<double*>(y);
+  v.z = const_cast<double*>(z);
+  v.q = const_cast<double*>(q);
+  v.alive = const_cast<uint8_t*>(alive);
+  v.fx = fx;
+  v.fy = fy;
+  v.fz = fz;
+  const unsigned blocks = static_cast<unsigned>((n + 255) / 256);
+  if (!(cutoff_radius > 0.0)) {  // coulomb_interaction.cc:33-37
+    zero_forces_kernel<<<blocks, 256, 0, s>>>(v);
+    AMK_CUDA_TRY(cudaGetLastError());
+    return AMK_OK;
+  }
+  unsigned long long* bb = reinterpret_cast<unsigned long long*>(base + kNaBbox);
+  uint64_t* keys = reinterpret_cast<uint64_t*>(base + kNaKeys);
+  uint32_t* vals = reinterpret_cast<uint32_t*>(base + kNaVals);
+  uint64_t* skeys = reinterpret_cast<uint64_t*>(base + kNaSKeys);
+  uint32_t* sidx = reinterpret_cast<uint32_t*>(base + kNaSIdx);
+  uint64_t* ktmp = reinterpret_cast<uint64_t*>(base + kNaTKeys);
+  uint32_t* vtmp = reinterpret_cast<uint32_t*>(base + kNaTVals);
+  uint32_t* hist = reinterpret_cast<uint32_t*>(base + kNaHist);
+  AMK_CUDA_TRY(cudaMemsetAsync(bb, 0xFF, 6 * sizeof(unsigned long long), s));
+  bbox_kernel<<<148, 256, 0, s>>>(v, bb);
+  cell_key_kernel<<<blocks, 256, 0, s>>>(v, bb, cutoff_radius, keys, vals);
+  AMK_CUDA_TRY(cudaGetLastError());
+  AMK_CUDA_TRY(radix_sort_pairs_buffers(s, keys, vals, skeys, sidx, ktmp, vtmp, hist, n, 64));
+  cutoff_kernel<<<static_cast<unsigned>((n + 127) / 128), 128, 0, s>>>(v, bb, cutoff_radius, skeys, sidx, nullptr);
+  AMK_CUDA_TRY(cudaGetLastError());
+  return AMK_OK;
+}

@@ -136,3 +136,31 @@ int radix_sort_pairs(amk_ctx* c, const uint64_t* keys_in, const uint32_t* vals_i
 }
 
 }  // namespace amk
+
+namespace amk {
+
+// The same sort on caller-provided buffers (no context, no allocation):
+// ktmp/vtmp hold n elements, hist holds 256 * ceil(n / 4096) counters.
+cudaError_t radix_sort_pairs_buffers(cudaStream_t stream, const uint64_t* keys_in, const uint32_t* vals_in,
+                                     uint64_t* keys_out, uint32_t* vals_out, uint64_t* ktmp, uint32_t* vtmp,
+                                     uint32_t* hist, long n, int key_bits) {
+  if (n <= 0) return cudaSuccess;
+  const int passes = std::max(1, (key_bits + 7) / 8);
+  const int nb = static_cast<int>((n + kTile - 1) / kTile);
+  const uint64_t* ksrc = keys_in;
+  const uint32_t* vsrc = vals_in;
+  for (int p = 0; p < passes; ++p) {
+    const bool to_out = ((passes - 1 - p) % 2) == 0;
+    uint64_t* kdst = to_out ? keys_out : ktmp;
+    uint32_t* vdst = to_out ? vals_out : vtmp;
+    const int shift = 8 * p;
+    hist_kernel<<<nb, kSortThreads, 0, stream>>>(ksrc, n, shift, nb, hist);
+    scan_kernel<<<1, 1024, 0, stream>>>(hist, static_cast<long>(256) * nb);
+    scatter_kernel<<<nb, kSortThreads, 0, stream>>>(ksrc, vsrc, n, shift, nb, hist, kdst, vdst);
+    ksrc = kdst;
+    vsrc = vdst;
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace amk

@@ -268,6 +268,26 @@ long amk_bh_tree_dump(amk_ctx* ctx, long n, const double* x, const double* y, co
                       const double* q, long leaf_capacity, long max_nodes, double* node_f64,
                       long* node_i64);
 
+/* ------------------------------------------------------------ allocation-free */
+/* No counterpart in the reference. The cutoff Coulomb solver (same results
+ * as amk_coulomb_standard / amk_solve_cutoff) for callers that cannot let a
+ * library allocate device memory -- a host code whose device memory is
+ * owned by its own pool allocator, or a per-step loop that cannot take the
+ * device-wide synchronisation of cudaMalloc/cudaFree. It allocates nothing:
+ * its scratch is one static device array (about 2.4 MB) that every GPU
+ * loading the library holds until exit. All pointers are device arrays on
+ * the current device; alive may be NULL (all alive); the work is queued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream).
+ * n <= AMK_NOALLOC_MAX_PARTICLES, else AMK_ERR_LIMIT. The first call on a
+ * device looks up the array's address; make it during set-up, before any
+ * stream capture. Calls share the array: calls that overlap on the GPU
+ * race. */
+#define AMK_NOALLOC_MAX_PARTICLES 65536
+int amk_coulomb_standard_noalloc(const double* x, const double* y, const double* z,
+                                 const double* q, const uint8_t* alive, long n,
+                                 double cutoff_radius, double* fx, double* fy, double* fz,
+                                 void* stream);
+
 /* ------------------------------------------------------------ profiling */
 /* Per-phase device time (CUDA events on the context stream) accumulated
  * since the last reset, in ms. Phases: see AMK_PHASE_*. */
