@@ -132,6 +132,7 @@ def lib():
                                     _dp, _dp, _dp, _dp]),
         "amk_bh_tree_dump": (C.c_long, [vp, C.c_long, _dp, _dp, _dp, _dp, C.c_long, C.c_long, _dp,
                                         C.POINTER(C.c_long)]),
+        "amk_fmm_stats": (C.c_int, [vp, C.POINTER(C.c_long), C.c_int]),
         "amk_set_profiling": (C.c_int, [vp, C.c_int]),
         "amk_phase_times": (C.c_int, [vp, _dp, C.POINTER(C.c_long), C.c_int]),
         "amk_reset_phase_times": (C.c_int, [vp]),
@@ -404,6 +405,13 @@ class Simulation:
                                          int(leaf_capacity), _d(fx), _d(fy), _d(fz), _d(phi)),
               "amk_solve_barnes_hut")
         return (fx, fy, fz, phi) if want_phi else (fx, fy, fz)
+
+    def fmm_stats(self):
+        out = (C.c_long * 8)()
+        check(lib().amk_fmm_stats(self._h, out, 8))
+        keys = ("cells", "leaves", "m2l_pairs", "p2p_leaf_pairs", "p2p_particle_pairs", "depth",
+                "sources", "order")
+        return dict(zip(keys, list(out)))
 
     def bh_tree(self, x, y, z, q, leaf_capacity=8):
         """Barnes-Hut octree nodes in the reference's order (see amk_bh_tree_dump)."""

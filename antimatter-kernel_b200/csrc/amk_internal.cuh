@@ -182,6 +182,8 @@ enum ScratchSlot {
   kSlotFmmWork3,
   kSlotFmmWork4,
   kSlotFmmWork5,
+  kSlotP2PWork,
+  kSlotP2PPart,
   kNumSlots
 };
 static_assert(kNumSlots <= 96, "scratch slots");

@@ -13,7 +13,8 @@
 // reference's); accepting lanes add the two monopoles, the others push the
 // children for themselves. Leaves are summed directly, skipping the target
 // itself and q = 0 sources. Pairs closer than 1e-30 m^2 are skipped
-// (barnes-hut.cc:33-41). All arithmetic is FP64.
+// (barnes-hut.cc:33-41). All arithmetic is FP64; inverse distances use
+// rsqrt where the reference divides by sqrt (an ulp-level difference).
 #include <algorithm>
 #include <vector>
 
@@ -94,9 +95,8 @@ __device__ __forceinline__ void add_point(double tx, double ty, double tz, doubl
   const double rx = tx - sx, ry = ty - sy, rz = tz - sz;
   const double d2 = dot_rn(rx, ry, rz);
   if (d2 < kMinSquaredDistance) return;
-  const double inv = 1.0 / sqrt(d2);
-  const double mag = kCoulombConstant * tq * sq / d2;
-  const double w = mag * inv;
+  const double inv = rsqrt(d2);
+  const double w = kCoulombConstant * tq * sq * (inv * inv * inv);
   f[0] += rx * w;
   f[1] += ry * w;
   f[2] += rz * w;
@@ -107,7 +107,7 @@ __device__ __forceinline__ void add_phi(double tx, double ty, double tz, double 
   const double rx = tx - sx, ry = ty - sy, rz = tz - sz;
   const double d2 = dot_rn(rx, ry, rz);
   if (d2 < kMinSquaredDistance) return;
-  *phi += sq / sqrt(d2);
+  *phi += sq * rsqrt(d2);
 }
 
 template <bool kPhi>

@@ -17,6 +17,7 @@ thread_local char g_error[1024] = "no error";
 struct EventPool {
   std::vector<cudaEvent_t> start, stop;
   size_t used = 0;
+  int open = 0;  // nesting depth: an inner begin/end of the same phase is not timed twice
 };
 std::map<const amk_ctx*, std::vector<EventPool>> g_events;
 }  // namespace
@@ -125,6 +126,7 @@ int phase_begin(amk_ctx* c, int phase) {
   auto& pools = g_events[c];
   if (pools.size() < AMK_NUM_PHASES) pools.resize(AMK_NUM_PHASES);
   EventPool& p = pools[phase];
+  if (p.open++ > 0) return AMK_OK;
   if (p.used == p.start.size()) {
     cudaEvent_t a, b;
     AMK_CUDA_TRY(cudaEventCreate(&a));
@@ -138,7 +140,11 @@ int phase_begin(amk_ctx* c, int phase) {
 
 int phase_end(amk_ctx* c, int phase) {
   if (!c->profiling) return AMK_OK;
-  EventPool& p = g_events[c][phase];
+  auto& pools = g_events[c];
+  if (pools.size() < AMK_NUM_PHASES) return AMK_OK;
+  EventPool& p = pools[phase];
+  if (p.open == 0) return AMK_OK;
+  if (--p.open > 0) return AMK_OK;
   AMK_CUDA_TRY(cudaEventRecord(p.stop[p.used], c->stream));
   p.used++;
   return AMK_OK;

@@ -11,16 +11,18 @@
 //   radii, P2M      leaves in parallel (a thread per leaf / a warp per leaf)
 //   M2M, L2L        level-synchronous, a warp per node, lanes over coefficients
 //   lists           the reference's dual-tree recursion run breadth-first over
-//                   (target, source) pairs; M2L and P2P pairs are grouped per
-//                   target and each group sorted by source index, so every
-//                   sum has a fixed order (run-to-run deterministic)
+//                   (target, source) pairs; M2L and P2P pairs are radix-sorted
+//                   by (target, source), so every sum has a fixed order
+//                   (run-to-run deterministic)
 //   M2L             a warp per target cell; per source the derivative tensor
 //                   is built degree by degree in shared memory (lanes over the
 //                   multi-indices of one degree) and contracted with the
 //                   source's multipole, lanes over local coefficients
-//   L2P + P2P       a warp per target leaf, a lane per target particle,
-//                   source leaves broadcast through warp shuffles
-// Arithmetic is FP64 throughout, as in the reference.
+//   L2P + P2P       work items of (target leaf, <= 8 source leaves); a warp
+//                   per item with lanes split into groups over the sources;
+//                   partials added in a fixed order
+// Arithmetic is FP64 throughout, as in the reference; inverse distances use
+// rsqrt (the reference divides by sqrt), a difference of an ulp.
 #include <algorithm>
 #include <array>
 #include <map>
@@ -157,6 +159,8 @@ struct FmmLists {
 struct Fmm {
   std::map<int, std::pair<DevBuf*, FmmDevTables>> tables;
   FmmLists lists;
+  // statistics of the last evaluation (amk_fmm_stats)
+  long stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   ~Fmm() {
     for (auto& kv : tables) delete kv.second.first;
   }
@@ -166,7 +170,6 @@ namespace {
 
 constexpr int kMaxOrder = 8;
 constexpr int kMaxNm = 165;  // n_m(8)
-constexpr int kMaxNd = 969;  // n_d(8): degree <= 16
 constexpr int kFmmWarps = 4;
 
 template <typename T>
@@ -360,52 +363,50 @@ __global__ void fmm_traverse_kernel(const Octree t, const double* __restrict__ r
   for (int k = 0; k < nk; ++k) next[base + k] = split_target ? make_int2(kids[k], si) : make_int2(ti, kids[k]);
 }
 
-// Group pairs by target: count, scan (host side helper), scatter, then sort
-// each group by source so that every sum runs in a fixed order.
-__global__ void pair_count_kernel(const int2* __restrict__ pairs, int n, int* __restrict__ count) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) atomicAdd(&count[pairs[i].x], 1);
-}
-
-__global__ void pair_scatter_kernel(const int2* __restrict__ pairs, int n, const int* __restrict__ off,
-                                    int* __restrict__ cursor, int* __restrict__ src) {
+// Group pairs by target: pack (target, source) into one key and radix-sort
+// it, so each target's sources are contiguous and in ascending source order
+// (a fixed summation order, independent of the emission order).
+__global__ void pair_pack_kernel(const int2* __restrict__ pairs, int n, int bits, uint64_t* __restrict__ keys,
+                                 uint32_t* __restrict__ vals) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int2 p = pairs[i];
-  src[off[p.x] + atomicAdd(&cursor[p.x], 1)] = p.y;
+  keys[i] = (static_cast<uint64_t>(p.x) << bits) | static_cast<uint64_t>(p.y);
+  vals[i] = static_cast<uint32_t>(i);
 }
 
-__global__ void segment_sort_kernel(const int* __restrict__ off, const int* __restrict__ count, int n_seg,
-                                    int* __restrict__ src) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n_seg) return;
-  const int b = off[s], e = b + count[s];
-  for (int i = b + 1; i < e; ++i) {  // insertion sort (groups are short)
-    const int v = src[i];
-    int j = i - 1;
-    while (j >= b && src[j] > v) {
-      src[j + 1] = src[j];
-      --j;
-    }
-    src[j + 1] = v;
-  }
+__global__ void pair_unpack_kernel(const uint64_t* __restrict__ keys, int n, int bits, int* __restrict__ src,
+                                   int* __restrict__ count) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint64_t k = keys[i];
+  src[i] = static_cast<int>(k & ((1ull << bits) - 1ull));
+  atomicAdd(&count[static_cast<int>(k >> bits)], 1);
 }
 
 // ------------------------------------------------------------ M2L
 // A warp per target cell (fast-multipole.cc:528-555). Derivatives
-// (fast-multipole.cc:207-232) are built degree by degree in shared memory.
+// (fast-multipole.cc:207-232) are built degree by degree in shared memory;
+// the M2L index map sits in shared memory as int16 with rows padded to
+// n_m + 1 entries (lanes read different rows without bank conflicts).
 __global__ void __launch_bounds__(32 * kFmmWarps)
 fmm_m2l_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, const int* __restrict__ count,
                const int* __restrict__ src, const double* __restrict__ M, double* __restrict__ L) {
-  __shared__ double sD[kFmmWarps][kMaxNd];
-  __shared__ double sM[kFmmWarps][kMaxNm];
+  extern __shared__ __align__(16) unsigned char m2l_smem[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int nm = T.n_m, nd = T.n_d, stride = nm + 1;
+  double* D = reinterpret_cast<double*>(m2l_smem) + static_cast<size_t>(w) * (nd + nm);
+  double* Ms = D + nd;
+  short* idx = reinterpret_cast<short*>(reinterpret_cast<double*>(m2l_smem) + static_cast<size_t>(kFmmWarps) * (nd + nm));
+  for (int e = threadIdx.x; e < nm * nm; e += blockDim.x) {
+    const int g = e / nm, a = e - g * nm;
+    idx[g * stride + a] = static_cast<short>(T.m2l_index[e]);
+  }
+  __syncthreads();
   const int ti = blockIdx.x * kFmmWarps + w;
   if (ti >= t.n_nodes) return;
   const int cnt = count[ti];
   if (cnt == 0) return;
-  double* D = sD[w];
-  double* Ms = sM[w];
   const double4 tc = t.center[ti];
   double acc[(kMaxNm + 31) / 32];
   for (int u = 0; u < (kMaxNm + 31) / 32; ++u) acc[u] = 0.0;
@@ -414,7 +415,7 @@ fmm_m2l_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, cons
     const int si = src[e];
     const double4 sc = t.center[si];
     const double xs[3] = {tc.x - sc.x, tc.y - sc.y, tc.z - sc.z};
-    for (int a = lane; a < T.n_m; a += 32) Ms[a] = T.sign[a] * M[static_cast<size_t>(si) * T.n_m + a];
+    for (int a = lane; a < nm; a += 32) Ms[a] = T.sign[a] * M[static_cast<size_t>(si) * nm + a];
     const double inv_r2 = 1.0 / (xs[0] * xs[0] + xs[1] * xs[1] + xs[2] * xs[2]);
     if (lane == 0) D[0] = sqrt(inv_r2);
     __syncwarp();
@@ -434,15 +435,20 @@ fmm_m2l_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, cons
       }
       __syncwarp();
     }
-    for (int u = 0, g = lane; g < T.n_m; ++u, g += 32) {
-      const int* idx = T.m2l_index + static_cast<size_t>(g) * T.n_m;
+    for (int u = 0, g = lane; g < nm; ++u, g += 32) {
+      const short* row = idx + g * stride;
       double s = 0.0;
-      for (int a = 0; a < T.n_m; ++a) s += Ms[a] * D[idx[a]];
+      for (int a = 0; a < nm; ++a) s += Ms[a] * D[row[a]];
       acc[u] += s * T.inv_fact[g];
     }
     __syncwarp();
   }
-  for (int u = 0, g = lane; g < T.n_m; ++u, g += 32) L[static_cast<size_t>(ti) * T.n_m + g] += acc[u];
+  for (int u = 0, g = lane; g < nm; ++u, g += 32) L[static_cast<size_t>(ti) * nm + g] += acc[u];
+}
+
+size_t m2l_smem_bytes(const FmmDevTables& T) {
+  return static_cast<size_t>(kFmmWarps) * (T.n_d + T.n_m) * sizeof(double) +
+         static_cast<size_t>(T.n_m) * (T.n_m + 1) * sizeof(short);
 }
 
 // ------------------------------------------------------------ L2L
@@ -472,82 +478,146 @@ fmm_l2l_kernel(const Octree t, FmmDevTables T, int depth, double* __restrict__ L
 }
 
 // ------------------------------------------------------------ L2P + P2P
-// A warp per target leaf, a lane per target particle (fast-multipole.cc:580-661).
-// Outputs in sorted order: ef = (Ex, Ey, Ez, phi) per unit target charge.
+// Work items = (target leaf, chunk of <= kP2PChunk source leaves of its P2P
+// list); every leaf has at least one item (its L2P). A warp takes one item;
+// its lanes are split into G = 32 / n_targets groups, group g summing every
+// G-th source particle for all the leaf's targets, so small leaves still
+// fill the warp. Group sums are added in group order and item partials in
+// chunk order (fast-multipole.cc:580-661), so results do not depend on
+// scheduling.
+constexpr int kP2PChunk = 8;
+
+__global__ void p2p_items_count_kernel(const Octree t, const int* __restrict__ count, int* __restrict__ items,
+                                       int* __restrict__ psize) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= t.n_nodes) return;
+  int it = 0;
+  if (t.meta[id].y) it = max(1, (count[id] + kP2PChunk - 1) / kP2PChunk);
+  const int2 r = t.range[id];
+  items[id] = it;
+  psize[id] = it * (r.y - r.x);
+}
+
+__global__ void p2p_items_fill_kernel(const Octree t, const int* __restrict__ items, const int* __restrict__ ibase,
+                                      int2* __restrict__ work, int* __restrict__ leaf_of) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= t.n_nodes || !t.meta[id].y) return;
+  const int b = ibase[id];
+  for (int c = 0; c < items[id]; ++c) work[b + c] = make_int2(id, c);
+  const int2 r = t.range[id];
+  for (int k = r.x; k < r.y; ++k) leaf_of[k] = id;
+}
+
 __global__ void __launch_bounds__(32 * kFmmWarps)
-fmm_l2p_p2p_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, const int* __restrict__ count,
-                   const int* __restrict__ src, const double* __restrict__ L, double min_sq, bool want_phi,
-                   double4* __restrict__ ef) {
-  const int lane = threadIdx.x & 31;
-  const int ti = blockIdx.x * kFmmWarps + (threadIdx.x >> 5);
-  if (ti >= t.n_nodes || !t.meta[ti].y) return;
+fmm_p2p_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, int n_work,
+               const int* __restrict__ off, const int* __restrict__ count, const int* __restrict__ src,
+               const int* __restrict__ pbase, const double* __restrict__ L, double min_sq, bool want_phi,
+               double4* __restrict__ part) {
+  __shared__ double4 red[kFmmWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int wi = blockIdx.x * kFmmWarps + w;
+  if (wi >= n_work) return;
+  const int2 item = work[wi];
+  const int ti = item.x, chunk = item.y;
   const double4 tc = t.center[ti];
   const int2 tr = t.range[ti];
-  const double* l = L + static_cast<size_t>(ti) * T.n_m;
+  const int nt_all = tr.y - tr.x;
+  const int sb = off[ti] + chunk * kP2PChunk;
+  const int se = min(off[ti] + count[ti], sb + kP2PChunk);
+  double4* out = part + pbase[ti] + static_cast<size_t>(chunk) * nt_all;
   for (int base = tr.x; base < tr.y; base += 32) {
-    const int i = base + lane;
-    const bool valid = i < tr.y;
+    const int nt = min(32, tr.y - base);
+    const int groups = 32 / nt;
+    const int g = lane / nt, tl = lane - g * nt;
+    const bool active = g < groups;
+    const int i = base + tl;
     double4 me = make_double4(0.0, 0.0, 0.0, 0.0);
-    if (valid) me = t.src[i];
+    if (active) me = t.src[i];
     double pot = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
-    if (valid) {
+    if (active && g == 0 && chunk == 0) {  // L2P, once per target
+      const double* l = L + static_cast<size_t>(ti) * T.n_m;
       double px[kMaxOrder + 1], py[kMaxOrder + 1], pz[kMaxOrder + 1];
       powers(T.p, me.x - tc.x, me.y - tc.y, me.z - tc.z, px, py, pz);
       if (want_phi)
-        for (int g = 0; g < T.n_m; ++g) {
-          const int4 m = T.multi[g];
-          pot += l[g] * (px[m.x] * py[m.y] * pz[m.z]);
+        for (int gg = 0; gg < T.n_m; ++gg) {
+          const int4 m = T.multi[gg];
+          pot += l[gg] * (px[m.x] * py[m.y] * pz[m.z]);
         }
       double gx = 0.0, gy = 0.0, gz = 0.0;
-      for (int g = 1; g < T.n_m; ++g) {
-        const int4 m = T.multi[g];
-        const int g0 = T.grad[3 * g], g1 = T.grad[3 * g + 1], g2 = T.grad[3 * g + 2];
+      for (int gg = 1; gg < T.n_m; ++gg) {
+        const int4 m = T.multi[gg];
+        const int g0 = T.grad[3 * gg], g1 = T.grad[3 * gg + 1], g2 = T.grad[3 * gg + 2];
         if (g0 >= 0) {
           const int4 q = T.multi[g0];
-          gx += m.x * l[g] * (px[q.x] * py[q.y] * pz[q.z]);
+          gx += m.x * l[gg] * (px[q.x] * py[q.y] * pz[q.z]);
         }
         if (g1 >= 0) {
           const int4 q = T.multi[g1];
-          gy += m.y * l[g] * (px[q.x] * py[q.y] * pz[q.z]);
+          gy += m.y * l[gg] * (px[q.x] * py[q.y] * pz[q.z]);
         }
         if (g2 >= 0) {
           const int4 q = T.multi[g2];
-          gz += m.z * l[g] * (px[q.x] * py[q.y] * pz[q.z]);
+          gz += m.z * l[gg] * (px[q.x] * py[q.y] * pz[q.z]);
         }
       }
       fx = -gx;
       fy = -gy;
       fz = -gz;
     }
-    const int sb = off[ti], se = sb + count[ti];
-    for (int e = sb; e < se; ++e) {
-      const int si = src[e];
-      const int2 sr = t.range[si];
-      for (int jb = sr.x; jb < sr.y; jb += 32) {
-        const int jn = min(32, sr.y - jb);
-        double4 sv = make_double4(0.0, 0.0, 0.0, 0.0);
-        if (lane < jn) sv = t.src[jb + lane];
-        for (int u = 0; u < jn; ++u) {
-          const double sx = __shfl_sync(0xffffffffu, sv.x, u);
-          const double sy = __shfl_sync(0xffffffffu, sv.y, u);
-          const double sz = __shfl_sync(0xffffffffu, sv.z, u);
-          const double sq = __shfl_sync(0xffffffffu, sv.w, u);
-          const int j = jb + u;
-          if (!valid || j == i || sq == 0.0) continue;
-          const double rx = me.x - sx, ry = me.y - sy, rz = me.z - sz;
+    if (active) {
+      for (int e = sb; e < se; ++e) {
+        const int2 sr = t.range[src[e]];
+        for (int j = sr.x + g; j < sr.y; j += groups) {
+          const double4 s = t.src[j];
+          if (j == i || s.w == 0.0) continue;
+          const double rx = me.x - s.x, ry = me.y - s.y, rz = me.z - s.z;
           const double r2 = rx * rx + ry * ry + rz * rz;
           if (r2 < min_sq) continue;
-          const double inv_r = 1.0 / sqrt(r2);
-          const double f = sq * inv_r / r2;
+          const double inv_r = rsqrt(r2);
+          const double f = s.w * (inv_r * inv_r * inv_r);
           fx += rx * f;
           fy += ry * f;
           fz += rz * f;
-          pot += sq * inv_r;
+          pot += s.w * inv_r;
         }
       }
     }
-    if (valid) ef[i] = make_double4(fx, fy, fz, pot);
+    red[w][lane] = make_double4(fx, fy, fz, pot);
+    __syncwarp();
+    if (active && g == 0) {
+      double4 a = red[w][tl];
+      for (int gg = 1; gg < groups; ++gg) {
+        const double4 b = red[w][gg * nt + tl];
+        a.x += b.x;
+        a.y += b.y;
+        a.z += b.z;
+        a.w += b.w;
+      }
+      out[i - tr.x] = a;
+    }
+    __syncwarp();
   }
+}
+
+// Per particle: item partials in chunk order.
+__global__ void fmm_p2p_reduce_kernel(const Octree t, const int* __restrict__ leaf_of, const int* __restrict__ items,
+                                      const int* __restrict__ pbase, const double4* __restrict__ part,
+                                      double4* __restrict__ ef) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= t.m) return;
+  const int leaf = leaf_of[k];
+  const int2 r = t.range[leaf];
+  const int nt = r.y - r.x;
+  const double4* p = part + pbase[leaf] + (k - r.x);
+  double4 a = p[0];
+  for (int c = 1; c < items[leaf]; ++c) {
+    const double4 b = p[static_cast<size_t>(c) * nt];
+    a.x += b.x;
+    a.y += b.y;
+    a.z += b.z;
+    a.w += b.w;
+  }
+  ef[k] = a;
 }
 
 __global__ void fmm_output_kernel(const Octree t, const double4* __restrict__ ef, double force_scale, View v,
@@ -562,6 +632,27 @@ __global__ void fmm_output_kernel(const Octree t, const double4* __restrict__ ef
   v.fy[i] = s * e.y;
   v.fz[i] = s * e.z;
   if (qphi) qphi[k] = q * e.w;
+}
+
+// sum over P2P leaf pairs of |T| * |S| (particle pairs before self/min_sq skips)
+__global__ void p2p_pair_count_kernel(const Octree t, const int2* __restrict__ pairs, int n,
+                                      unsigned long long* out) {
+  unsigned long long s = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int2 p = pairs[i];
+    const int2 a = t.range[p.x], b = t.range[p.y];
+    s += static_cast<unsigned long long>(a.y - a.x) * static_cast<unsigned long long>(b.y - b.x);
+  }
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
+}
+
+__global__ void leaf_count_kernel(const Octree t, unsigned long long* out) {
+  unsigned long long s = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < t.n_nodes; i += gridDim.x * blockDim.x)
+    s += t.meta[i].y ? 1 : 0;
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, s);
 }
 
 __global__ void zero_forces_kernel(View v) {
@@ -591,6 +682,7 @@ struct Grouped {
 
 int group_pairs(amk_ctx* c, const int2* pairs, long n_pairs, long n_nodes, int slot_off, int slot_cnt, int slot_src,
                 int slot_cursor, Grouped* g) {
+  (void)slot_cursor;
   int rc = AMK_OK;
   g->off = slot<int>(c, slot_off, n_nodes + 1, &rc);
   AMK_TRY(rc);
@@ -598,27 +690,28 @@ int group_pairs(amk_ctx* c, const int2* pairs, long n_pairs, long n_nodes, int s
   AMK_TRY(rc);
   g->src = slot<int>(c, slot_src, std::max<long>(n_pairs, 1), &rc);
   AMK_TRY(rc);
-  int* cursor = slot<int>(c, slot_cursor, n_nodes + 1, &rc);
-  AMK_TRY(rc);
   int* total = slot<int>(c, kSlotStatus, 8, &rc) + 6;
   AMK_TRY(rc);
   AMK_CUDA_TRY(cudaMemsetAsync(g->count, 0, (n_nodes + 1) * sizeof(int), c->stream));
-  AMK_CUDA_TRY(cudaMemsetAsync(cursor, 0, (n_nodes + 1) * sizeof(int), c->stream));
   if (n_pairs > 0) {
-    pair_count_kernel<<<static_cast<unsigned>((n_pairs + 255) / 256), 256, 0, c->stream>>>(pairs, static_cast<int>(n_pairs),
-                                                                                          g->count);
-    AMK_TRY(check_launch(c, "pair_count_kernel"));
+    int bits = 1;
+    while ((1L << bits) < n_nodes) ++bits;
+    uint64_t* keys = slot<uint64_t>(c, kSlotKeysA, n_pairs, &rc);
+    AMK_TRY(rc);
+    uint32_t* vals = slot<uint32_t>(c, kSlotValsA, n_pairs, &rc);
+    AMK_TRY(rc);
+    uint64_t* skeys = slot<uint64_t>(c, kSlotTreeKeys, n_pairs, &rc);
+    AMK_TRY(rc);
+    uint32_t* svals = slot<uint32_t>(c, kSlotSorted0, n_pairs, &rc);
+    AMK_TRY(rc);
+    const unsigned gp = static_cast<unsigned>((n_pairs + 255) / 256);
+    pair_pack_kernel<<<gp, 256, 0, c->stream>>>(pairs, static_cast<int>(n_pairs), bits, keys, vals);
+    AMK_TRY(check_launch(c, "pair_pack_kernel"));
+    AMK_TRY(radix_sort_pairs(c, keys, vals, skeys, svals, n_pairs, 2 * bits));
+    pair_unpack_kernel<<<gp, 256, 0, c->stream>>>(skeys, static_cast<int>(n_pairs), bits, g->src, g->count);
+    AMK_TRY(check_launch(c, "pair_unpack_kernel"));
   }
-  AMK_TRY(exclusive_scan_int(c, g->count, n_nodes, g->off, total));
-  if (n_pairs > 0) {
-    pair_scatter_kernel<<<static_cast<unsigned>((n_pairs + 255) / 256), 256, 0, c->stream>>>(
-        pairs, static_cast<int>(n_pairs), g->off, cursor, g->src);
-    AMK_TRY(check_launch(c, "pair_scatter_kernel"));
-    segment_sort_kernel<<<static_cast<unsigned>((n_nodes + 255) / 256), 256, 0, c->stream>>>(
-        g->off, g->count, static_cast<int>(n_nodes), g->src);
-    AMK_TRY(check_launch(c, "segment_sort_kernel"));
-  }
-  return AMK_OK;
+  return exclusive_scan_int(c, g->count, n_nodes, g->off, total);
 }
 
 }  // namespace
@@ -695,6 +788,29 @@ int fmm_forces(amk_ctx* c, const View& v, int order, double theta, long leaf_cap
     n_cur = out[2];
     lists.cur.swap(lists.next);
   }
+  {  // statistics: nodes, leaves, M2L pairs, P2P leaf pairs, P2P particle pairs, depth
+    unsigned long long* cnt = slot<unsigned long long>(c, kSlotFmmAux1, 4, &rc);
+    AMK_TRY(rc);
+    AMK_CUDA_TRY(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), c->stream));
+    if (n_p2p > 0) {
+      p2p_pair_count_kernel<<<148, 256, 0, c->stream>>>(t, lists.p2p.as<int2>(), static_cast<int>(n_p2p), cnt);
+      AMK_TRY(check_launch(c, "p2p_pair_count_kernel"));
+    }
+    leaf_count_kernel<<<148, 256, 0, c->stream>>>(t, cnt + 1);
+    AMK_TRY(check_launch(c, "leaf_count_kernel"));
+    unsigned long long h[2] = {0, 0};
+    AMK_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    long* st = c->fmm->stats;
+    st[0] = nn;
+    st[1] = static_cast<long>(h[1]);
+    st[2] = n_m2l;
+    st[3] = n_p2p;
+    st[4] = static_cast<long>(h[0]);
+    st[5] = t.max_depth;
+    st[6] = t.m;
+    st[7] = order;
+  }
   Grouped gm, gp;
   AMK_TRY(group_pairs(c, lists.m2l.as<int2>(), n_m2l, nn, kSlotFmmLists0, kSlotFmmLists1, kSlotFmmWork0,
                       kSlotFmmWork1, &gm));
@@ -705,7 +821,10 @@ int fmm_forces(amk_ctx* c, const View& v, int order, double theta, long leaf_cap
   // ---- M2L
   AMK_CUDA_TRY(cudaMemsetAsync(Lx, 0, static_cast<size_t>(nn) * T.n_m * sizeof(double), c->stream));
   AMK_TRY(phase_begin(c, AMK_PHASE_FMM_M2L));
-  fmm_m2l_kernel<<<gw, 32 * kFmmWarps, 0, c->stream>>>(t, T, gm.off, gm.count, gm.src, M, Lx);
+  const size_t m2l_smem = m2l_smem_bytes(T);
+  AMK_CUDA_TRY(cudaFuncSetAttribute(fmm_m2l_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(m2l_smem)));
+  fmm_m2l_kernel<<<gw, 32 * kFmmWarps, m2l_smem, c->stream>>>(t, T, gm.off, gm.count, gm.src, M, Lx);
   AMK_TRY(check_launch(c, "fmm_m2l_kernel"));
   AMK_TRY(phase_end(c, AMK_PHASE_FMM_M2L));
 
@@ -725,9 +844,39 @@ int fmm_forces(amk_ctx* c, const View& v, int order, double theta, long leaf_cap
   AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
   const double min_sq = kMinSquaredDistance / (hf.length * hf.length);
   AMK_TRY(phase_begin(c, AMK_PHASE_FMM_P2P));
-  fmm_l2p_p2p_kernel<<<gw, 32 * kFmmWarps, 0, c->stream>>>(t, T, gp.off, gp.count, gp.src, Lx, min_sq,
-                                                           energy_out != nullptr, ef);
-  AMK_TRY(check_launch(c, "fmm_l2p_p2p_kernel"));
+  {
+    int* items = slot<int>(c, kSlotFmmAux2, nn + 1, &rc);
+    AMK_TRY(rc);
+    int* psize = slot<int>(c, kSlotTreeCount, nn + 1, &rc);  // tree build scratch, free again
+    AMK_TRY(rc);
+    int* ibase = slot<int>(c, kSlotTreeBase, nn + 1, &rc);
+    AMK_TRY(rc);
+    int* pbase = slot<int>(c, kSlotTreeL, nn + 1, &rc);
+    AMK_TRY(rc);
+    int* totals = slot<int>(c, kSlotFmmAux1, 8, &rc);
+    AMK_TRY(rc);
+    p2p_items_count_kernel<<<gn, 256, 0, c->stream>>>(t, gp.count, items, psize);
+    AMK_TRY(check_launch(c, "p2p_items_count_kernel"));
+    AMK_TRY(exclusive_scan_int(c, items, nn, ibase, totals));
+    AMK_TRY(exclusive_scan_int(c, psize, nn, pbase, totals + 1));
+    int ht[2] = {0, 0};
+    AMK_CUDA_TRY(cudaMemcpyAsync(ht, totals, sizeof(ht), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    int2* work = slot<int2>(c, kSlotP2PWork, ht[0] + 1, &rc);
+    AMK_TRY(rc);
+    int* leaf_of = slot<int>(c, kSlotTreeLeafDepth, t.m + 1, &rc);
+    AMK_TRY(rc);
+    double4* part = slot<double4>(c, kSlotP2PPart, static_cast<size_t>(ht[1]) + 1, &rc);
+    AMK_TRY(rc);
+    p2p_items_fill_kernel<<<gn, 256, 0, c->stream>>>(t, items, ibase, work, leaf_of);
+    AMK_TRY(check_launch(c, "p2p_items_fill_kernel"));
+    fmm_p2p_kernel<<<static_cast<unsigned>((ht[0] + kFmmWarps - 1) / kFmmWarps), 32 * kFmmWarps, 0, c->stream>>>(
+        t, T, work, ht[0], gp.off, gp.count, gp.src, pbase, Lx, min_sq, energy_out != nullptr, part);
+    AMK_TRY(check_launch(c, "fmm_p2p_kernel"));
+    fmm_p2p_reduce_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, c->stream>>>(t, leaf_of, items, pbase,
+                                                                                          part, ef);
+    AMK_TRY(check_launch(c, "fmm_p2p_reduce_kernel"));
+  }
   AMK_TRY(phase_end(c, AMK_PHASE_FMM_P2P));
   double* qphi = nullptr;
   if (energy_out) {
@@ -750,6 +899,15 @@ int fmm_forces(amk_ctx* c, const View& v, int order, double theta, long leaf_cap
 }
 
 }  // namespace amk
+
+// Counts of the last FMM evaluation on this context: out[0] cells, [1] leaves,
+// [2] M2L pairs, [3] P2P leaf pairs, [4] P2P particle pairs, [5] depth,
+// [6] sources, [7] order.
+extern "C" int amk_fmm_stats(amk_ctx* c, long* out, int n) {
+  if (!c || !out) return amk::fail(AMK_ERR_INVALID, "null argument");
+  for (int k = 0; k < n && k < 8; ++k) out[k] = c->fmm ? c->fmm->stats[k] : 0;
+  return AMK_OK;
+}
 
 void fmm_destroy(amk_ctx* c) {
   delete c->fmm;

@@ -268,6 +268,12 @@ long amk_bh_tree_dump(amk_ctx* ctx, long n, const double* x, const double* y, co
                       const double* q, long leaf_capacity, long max_nodes, double* node_f64,
                       long* node_i64);
 
+/* Interaction counts of the context's last FMM evaluation: out[0] cells,
+ * [1] leaves, [2] M2L pairs, [3] P2P leaf pairs, [4] P2P particle pairs,
+ * [5] tree depth, [6] sources, [7] order (the quantities the reference's
+ * phases scale with, fast-multipole.cc:484-661). */
+int amk_fmm_stats(amk_ctx* ctx, long* out, int n);
+
 /* ------------------------------------------------------------ allocation-free */
 /* No counterpart in the reference. The cutoff Coulomb solver (same results
  * as amk_coulomb_standard / amk_solve_cutoff) for callers that cannot let a
