@@ -69,6 +69,7 @@ class EnergyOut(C.Structure):
 
 
 _dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
 _u8p = C.POINTER(C.c_uint8)
 _lib = None
 
@@ -133,6 +134,12 @@ def lib():
         "amk_bh_tree_dump": (C.c_long, [vp, C.c_long, _dp, _dp, _dp, _dp, C.c_long, C.c_long, _dp,
                                         C.POINTER(C.c_long)]),
         "amk_fmm_stats": (C.c_int, [vp, C.POINTER(C.c_long), C.c_int]),
+        "amk_mlp_num_params": (C.c_int, []),
+        "amk_mlp_set_params": (C.c_int, [vp, _fp, C.c_long]),
+        "amk_mlp_get_params": (C.c_int, [vp, _fp, C.c_long]),
+        "amk_mlp_forward": (C.c_int, [vp, _fp, C.c_long, _fp]),
+        "amk_mlp_gradients": (C.c_int, [vp, _fp, _fp, C.c_long, _fp, _fp, _fp]),
+        "amk_mlp_train": (C.c_int, [vp, _fp, _fp, C.c_long, C.c_int, C.c_long, C.c_float, _fp]),
         "amk_set_profiling": (C.c_int, [vp, C.c_int]),
         "amk_phase_times": (C.c_int, [vp, _dp, C.POINTER(C.c_long), C.c_int]),
         "amk_reset_phase_times": (C.c_int, [vp]),
@@ -412,6 +419,43 @@ class Simulation:
         keys = ("cells", "leaves", "m2l_pairs", "p2p_leaf_pairs", "p2p_particle_pairs", "depth",
                 "sources", "order")
         return dict(zip(keys, list(out)))
+
+    # -- learned correction (MLP)
+    def mlp_params(self):
+        n = lib().amk_mlp_num_params()
+        p = np.empty(n, np.float32)
+        check(lib().amk_mlp_get_params(self._h, p.ctypes.data_as(_fp), n), "amk_mlp_get_params")
+        return p
+
+    def set_mlp_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        check(lib().amk_mlp_set_params(self._h, p.ctypes.data_as(_fp), len(p)), "amk_mlp_set_params")
+
+    def mlp_forward(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.empty((len(x), 3), np.float32)
+        check(lib().amk_mlp_forward(self._h, x.ctypes.data_as(_fp), len(x), y.ctypes.data_as(_fp)),
+              "amk_mlp_forward")
+        return y
+
+    def mlp_gradients(self, x, t):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        g = np.empty(lib().amk_mlp_num_params(), np.float32)
+        yh = np.empty((len(x), 3), np.float32)
+        loss = C.c_float()
+        check(lib().amk_mlp_gradients(self._h, x.ctypes.data_as(_fp), t.ctypes.data_as(_fp), len(x),
+                                      g.ctypes.data_as(_fp), C.byref(loss), yh.ctypes.data_as(_fp)),
+              "amk_mlp_gradients")
+        return loss.value, g, yh
+
+    def mlp_train(self, x, t, steps, batch, lr):
+        x = np.ascontiguousarray(x, np.float32)
+        t = np.ascontiguousarray(t, np.float32)
+        loss = C.c_float()
+        check(lib().amk_mlp_train(self._h, x.ctypes.data_as(_fp), t.ctypes.data_as(_fp), len(x), int(steps),
+                                  int(batch), float(lr), C.byref(loss)), "amk_mlp_train")
+        return loss.value
 
     def bh_tree(self, x, y, z, q, leaf_capacity=8):
         """Barnes-Hut octree nodes in the reference's order (see amk_bh_tree_dump)."""

@@ -274,6 +274,26 @@ long amk_bh_tree_dump(amk_ctx* ctx, long n, const double* x, const double* y, co
  * phases scale with, fast-multipole.cc:484-661). */
 int amk_fmm_stats(amk_ctx* ctx, long* out, int n);
 
+/* ------------------------------------------------------------ learned correction */
+/* No counterpart in the reference. A 35 -> 128 -> 128 -> 128 -> 3 MLP (GELU,
+ * BF16 weights, FP32 accumulation) that corrects the p=2 FMM far field.
+ * Parameters are FP32 masters, flat: W1[128][35] b1[128] W2[128][128] b2
+ * W3[128][128] b3 W4[3][128] b4[3] (row = output unit). Inference runs on
+ * the tensor cores (tcgen05.mma, accumulators in tensor memory); training
+ * (forward, backward, Adam with beta = 0.9, 0.999) in FP32 on the CUDA cores
+ * with the same BF16-rounded weights. Loss: mean squared error. */
+int amk_mlp_num_params(void);
+int amk_mlp_set_params(amk_ctx* ctx, const float* params, long n);
+int amk_mlp_get_params(amk_ctx* ctx, float* params, long n);
+/* y[n][3] = MLP(x[n][35]) on the tensor cores (host buffers). */
+int amk_mlp_forward(amk_ctx* ctx, const float* x, long n, float* y);
+/* Loss and dLoss/dparams of one batch (FP32 path); grad, loss, yhat may be NULL. */
+int amk_mlp_gradients(amk_ctx* ctx, const float* x, const float* target, long n, float* grad,
+                      float* loss, float* yhat);
+/* `steps` Adam steps on consecutive windows of `batch` samples. */
+int amk_mlp_train(amk_ctx* ctx, const float* x, const float* target, long n, int steps, long batch,
+                  float lr, float* final_loss);
+
 /* ------------------------------------------------------------ allocation-free */
 /* No counterpart in the reference. The cutoff Coulomb solver (same results
  * as amk_coulomb_standard / amk_solve_cutoff) for callers that cannot let a
