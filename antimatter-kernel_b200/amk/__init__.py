@@ -59,6 +59,8 @@ class Params(C.Structure):
         ("annihilation_probability", C.c_double), ("n_species", C.c_int),
         ("species", C.c_int * 6), ("populations", C.c_long * 6),
         ("temperatures", C.c_double * 6), ("cloud_radii", C.c_double * 3),
+        ("learned_audit_interval", C.c_long), ("learned_error_budget", C.c_double),
+        ("learned_fallback_order", C.c_int), ("learned_audit_samples", C.c_long),
     ]
 
 
@@ -134,6 +136,10 @@ def lib():
         "amk_bh_tree_dump": (C.c_long, [vp, C.c_long, _dp, _dp, _dp, _dp, C.c_long, C.c_long, _dp,
                                         C.POINTER(C.c_long)]),
         "amk_fmm_stats": (C.c_int, [vp, C.POINTER(C.c_long), C.c_int]),
+        "amk_fmm_train_correction": (C.c_int, [vp, C.c_double, C.c_int, C.c_int, C.c_long, C.c_float, _fp,
+                                                C.POINTER(C.c_long)]),
+        "amk_fmm_audit": (C.c_int, [vp, C.c_int, C.c_double, C.c_int, C.c_long, _dp]),
+        "amk_fmm_learned_state": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]),
         "amk_mlp_num_params": (C.c_int, []),
         "amk_mlp_set_params": (C.c_int, [vp, _fp, C.c_long]),
         "amk_mlp_get_params": (C.c_int, [vp, _fp, C.c_long]),
@@ -419,6 +425,26 @@ class Simulation:
         keys = ("cells", "leaves", "m2l_pairs", "p2p_leaf_pairs", "p2p_particle_pairs", "depth",
                 "sources", "order")
         return dict(zip(keys, list(out)))
+
+    # -- learned FMM correction
+    def fmm_train_correction(self, theta=0.5, sample_leaves=4096, steps=2000, batch=4096, lr=1e-3):
+        loss = C.c_float()
+        samples = C.c_long()
+        check(lib().amk_fmm_train_correction(self._h, float(theta), int(sample_leaves), int(steps), int(batch),
+                                             float(lr), C.byref(loss), C.byref(samples)),
+              "amk_fmm_train_correction")
+        return loss.value, samples.value
+
+    def fmm_audit(self, order=2, theta=0.5, learned=False, samples=1024):
+        e = C.c_double()
+        check(lib().amk_fmm_audit(self._h, int(order), float(theta), 1 if learned else 0, int(samples),
+                                  C.byref(e)), "amk_fmm_audit")
+        return e.value
+
+    def fmm_learned_state(self):
+        t, f, e = C.c_int(), C.c_int(), C.c_double()
+        check(lib().amk_fmm_learned_state(self._h, C.byref(t), C.byref(f), C.byref(e)))
+        return {"trained": bool(t.value), "fallback": bool(f.value), "last_error": e.value}
 
     # -- learned correction (MLP)
     def mlp_params(self):

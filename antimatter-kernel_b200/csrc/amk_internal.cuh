@@ -236,6 +236,10 @@ struct amk_ctx {
 
   amk::Fmm* fmm = nullptr;
   amk::Mlp* mlp = nullptr;
+  // learned FMM correction state
+  bool learned_trained = false;
+  bool learned_fallback = false;
+  double learned_last_error = -1.0;
 };
 
 namespace amk {
@@ -274,6 +278,15 @@ int cutoff_forces(amk_ctx* c, const View& v, double cutoff, double* energy_out);
 int barnes_hut_forces(amk_ctx* c, const View& v, double theta, long leaf_capacity);
 int fmm_forces(amk_ctx* c, const View& v, int order, double theta, long leaf_capacity,
                bool learned, double* energy_out);
+
+// Learned correction (mlp.cu / fmm.cu).
+int mlp_forward_device(amk_ctx* c, const float* x, long n, float* y);
+int mlp_check_status(amk_ctx* c);
+int mlp_train_device(amk_ctx* c, const float* x, const float* target, long n, int steps, long batch, float lr,
+                     float* final_loss);
+int fmm_train_learned(amk_ctx* c, const View& v, double theta, int sample_leaves, int steps, long batch, float lr,
+                      float* loss_out, long* samples_out);
+int fmm_audit(amk_ctx* c, const View& v, int order, double theta, bool learned, long samples, double* rms);
 
 // Copies host sources into the context's auxiliary set (solver mirrors).
 int load_aux_view(amk_ctx* c, long n, const double* x, const double* y, const double* z, const double* q,

@@ -210,6 +210,10 @@ extern "C" int amk_params_default(amk_params* p) {
   p->populations[0] = 10;
   p->temperatures[0] = 4;
   p->cloud_radii[0] = p->cloud_radii[1] = p->cloud_radii[2] = 1e-4;
+  p->learned_audit_interval = 100;
+  p->learned_error_budget = 1e-5;
+  p->learned_fallback_order = 6;
+  p->learned_audit_samples = 1024;
   return AMK_OK;
 }
 
@@ -684,11 +688,42 @@ extern "C" int amk_coulomb_barnes_hut(amk_ctx* c, double theta) {
   return barnes_hut_forces(c, main_view(c), theta, 8);
 }
 
+// learned != 0 uses the p=2 far field plus the trained correction while it is
+// trained and its audits pass; otherwise plain FMM at learned_fallback_order.
 extern "C" int amk_coulomb_fmm(amk_ctx* c, int order, double theta, int learned) {
   if (!c) return fail(AMK_ERR_INVALID, "null context");
   if (c->n == 0) return AMK_OK;
-  AMK_TRY(ensure_staged(c));
-  return fmm_forces(c, main_view(c), order, theta, 32, learned != 0, nullptr);
+  if (learned) {
+    if (c->learned_trained && !c->learned_fallback) return fmm_forces(c, main_view(c), 2, theta, 32, true, nullptr);
+    order = c->p.learned_fallback_order;
+  }
+  return fmm_forces(c, main_view(c), order, theta, 32, false, nullptr);
+}
+
+extern "C" int amk_fmm_train_correction(amk_ctx* c, double theta, int sample_leaves, int steps, long batch, float lr,
+                                        float* final_loss, long* samples) {
+  if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (c->n == 0) return fail(AMK_ERR_STATE, "no particles");
+  AMK_TRY(fmm_train_learned(c, main_view(c), theta, sample_leaves, steps, batch, lr, final_loss, samples));
+  c->learned_trained = true;
+  c->learned_fallback = false;
+  return AMK_OK;
+}
+
+extern "C" int amk_fmm_audit(amk_ctx* c, int order, double theta, int learned, long samples, double* rms) {
+  if (!c || !rms) return fail(AMK_ERR_INVALID, "null argument");
+  *rms = 0.0;
+  if (c->n == 0) return AMK_OK;
+  if (learned && !c->learned_trained) return fail(AMK_ERR_STATE, "the learned correction is not trained");
+  return fmm_audit(c, main_view(c), order, theta, learned != 0, samples, rms);
+}
+
+extern "C" int amk_fmm_learned_state(amk_ctx* c, int* trained, int* fallback, double* last_error) {
+  if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (trained) *trained = c->learned_trained ? 1 : 0;
+  if (fallback) *fallback = c->learned_fallback ? 1 : 0;
+  if (last_error) *last_error = c->learned_last_error;
+  return AMK_OK;
 }
 
 extern "C" int amk_coulomb(amk_ctx* c) {
@@ -747,6 +782,17 @@ extern "C" int amk_step(amk_ctx* c, int nsteps) {
   if (nsteps < 0) return fail(AMK_ERR_INVALID, "nsteps < 0");
   AMK_CUDA_TRY(cudaSetDevice(c->device));
   for (int s = 0; s < nsteps; ++s) {
+    // periodic direct-sum audit of the learned correction; a failure switches
+    // the context to plain FMM at learned_fallback_order
+    const amk_params& p = c->p;
+    if (c->n > 0 && p.coulomb_forces_enabled && p.coulomb_method == AMK_METHOD_FAST_MULTIPOLE && p.fmm_learned &&
+        c->learned_trained && !c->learned_fallback && p.learned_audit_interval > 0 &&
+        c->step % p.learned_audit_interval == 0) {
+      double err = 0.0;
+      AMK_TRY(fmm_audit(c, main_view(c), 2, p.fast_multipole_theta, true, p.learned_audit_samples, &err));
+      c->learned_last_error = err;
+      if (!(err <= p.learned_error_budget)) c->learned_fallback = true;
+    }
     if (c->n > 0) AMK_TRY(amk_coulomb(c));
     AMK_TRY(amk_push(c));
     if (c->n > 0 && c->p.annihilation_enabled) AMK_TRY(amk_annihilate(c, nullptr));

@@ -716,10 +716,22 @@ int group_pairs(amk_ctx* c, const int2* pairs, long n_pairs, long n_nodes, int s
 
 }  // namespace
 
-int fmm_forces(amk_ctx* c, const View& v, int order, double theta, long leaf_capacity, bool learned,
-               double* energy_out) {
-  if (energy_out) *energy_out = 0.0;
-  if (learned) return fail(AMK_ERR_UNSUPPORTED, "learned FMM correction not built");
+// State of one FMM evaluation kept for the output, learned-correction and
+// audit steps (all device pointers into the context's scratch).
+struct FmmRun {
+  Octree t;
+  FmmDevTables T;
+  TreeFrame hf;
+  double* M = nullptr;
+  double* L = nullptr;
+  double* radius = nullptr;
+  double4* ef = nullptr;      // per sorted source: E (unit-cube units, per unit charge), phi
+  int* leaf_of = nullptr;     // sorted source -> leaf node
+  int* p2p_count = nullptr;   // per node: P2P source leaves
+};
+
+int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capacity, bool want_phi, FmmRun* run) {
+  run->t = Octree{};
   const long n = v.n;
   if (n == 0) return AMK_OK;
   order = std::min(std::max(order, 1), kMaxOrder);  // fast-multipole.cc:324-328
@@ -870,21 +882,45 @@ int fmm_forces(amk_ctx* c, const View& v, int order, double theta, long leaf_cap
     AMK_TRY(rc);
     p2p_items_fill_kernel<<<gn, 256, 0, c->stream>>>(t, items, ibase, work, leaf_of);
     AMK_TRY(check_launch(c, "p2p_items_fill_kernel"));
-    fmm_p2p_kernel<<<static_cast<unsigned>((ht[0] + kFmmWarps - 1) / kFmmWarps), 32 * kFmmWarps, 0, c->stream>>>(
-        t, T, work, ht[0], gp.off, gp.count, gp.src, pbase, Lx, min_sq, energy_out != nullptr, part);
+      fmm_p2p_kernel<<<static_cast<unsigned>((ht[0] + kFmmWarps - 1) / kFmmWarps), 32 * kFmmWarps, 0, c->stream>>>(
+        t, T, work, ht[0], gp.off, gp.count, gp.src, pbase, Lx, min_sq, want_phi, part);
     AMK_TRY(check_launch(c, "fmm_p2p_kernel"));
     fmm_p2p_reduce_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, c->stream>>>(t, leaf_of, items, pbase,
                                                                                           part, ef);
     AMK_TRY(check_launch(c, "fmm_p2p_reduce_kernel"));
+    run->leaf_of = leaf_of;
   }
   AMK_TRY(phase_end(c, AMK_PHASE_FMM_P2P));
+  run->t = t;
+  run->T = T;
+  run->hf = hf;
+  run->M = M;
+  run->L = Lx;
+  run->radius = radius;
+  run->ef = ef;
+  run->p2p_count = gp.count;
+  return AMK_OK;
+}
+
+int fmm_apply_learned(amk_ctx* c, const FmmRun& r);  // below
+
+int fmm_forces(amk_ctx* c, const View& v, int order, double theta, long leaf_capacity, bool learned,
+               double* energy_out) {
+  if (energy_out) *energy_out = 0.0;
+  if (v.n == 0) return AMK_OK;
+  FmmRun r;
+  AMK_TRY(fmm_run(c, v, learned ? 2 : order, theta, leaf_capacity, energy_out != nullptr, &r));
+  if (r.t.m == 0) return AMK_OK;
+  if (learned) AMK_TRY(fmm_apply_learned(c, r));
+  const Octree& t = r.t;
+  int rc = AMK_OK;
   double* qphi = nullptr;
   if (energy_out) {
     qphi = slot<double>(c, kSlotFmmWork5, t.m, &rc);
     AMK_TRY(rc);
   }
-  const double force_scale = kCoulombConstant / (hf.length * hf.length);
-  fmm_output_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, c->stream>>>(t, ef, force_scale, v, qphi);
+  const double force_scale = kCoulombConstant / (r.hf.length * r.hf.length);
+  fmm_output_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, c->stream>>>(t, r.ef, force_scale, v, qphi);
   AMK_TRY(check_launch(c, "fmm_output_kernel"));
   if (energy_out) {
     double* res = slot<double>(c, kSlotAuxState4, 8, &rc);
@@ -893,8 +929,262 @@ int fmm_forces(amk_ctx* c, const View& v, int order, double theta, long leaf_cap
     double h = 0.0;
     AMK_CUDA_TRY(cudaMemcpyAsync(&h, res, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    *energy_out = 0.5 * kCoulombConstant / hf.length * h;  // fast-multipole.cc:676-680
+    *energy_out = 0.5 * kCoulombConstant / r.hf.length * h;  // fast-multipole.cc:676-680
   }
+  return AMK_OK;
+}
+
+// ====================================================================== learned
+// Per-particle features of the learned far-field correction (35 values, all
+// dimensionless; x in unit-cube coordinates, leaf centre c, half edge h,
+// E = E_far + E_near the p=2 FMM field at the particle):
+//   0-2   u = (x - c) / h                    3-5   2 c (position in the cloud)
+//   6-8   E_far / |E|                        9-11  E_near / |E|
+//   12-14 degree-1 local coefficients / |E|  15-20 degree-2 local coefficients * h / |E|
+//   21    log2(h) / 10                       22-24 leaf charge centroid offset / h
+//   25-30 leaf second moments / (Q h^2)      31    leaf particle count / 32
+//   32    leaf radius / h                    33    P2P source leaves / 64
+//   34    1
+// The neglected far-field terms (higher derivatives of the far potential,
+// higher source moments) vary smoothly with position in the cloud, which is
+// what the network learns. It predicts 100 (E_exact - E_fmm) / |E|: the
+// relative far-field error, scaled to order one.
+constexpr int kFeat = 35;
+constexpr double kTargetScale = 100.0;
+
+__global__ void fmm_features_kernel(const Octree t, FmmDevTables T, const double* __restrict__ L,
+                                    const double* __restrict__ M, const double* __restrict__ radius,
+                                    const int* __restrict__ p2p_count, const int* __restrict__ leaf_of,
+                                    const double4* __restrict__ ef, const int* __restrict__ sel, int n_sel,
+                                    float* __restrict__ feat, double* __restrict__ scale) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_sel) return;
+  const int k = sel ? sel[s] : s;
+  const int leaf = leaf_of[k];
+  const double4 cc = t.center[leaf];
+  const double h = cc.w;
+  const double4 me = t.src[k];
+  const double dx = me.x - cc.x, dy = me.y - cc.y, dz = me.z - cc.z;
+  const double* l = L + static_cast<size_t>(leaf) * T.n_m;  // p = 2: 10 coefficients
+  // E_far = -grad sum_g L_g d^g for degree <= 2 (index order of FmmTables)
+  // indices: 0:(000) 1:(100) 2:(010) 3:(001) 4:(200) 5:(110) 6:(101) 7:(020) 8:(011) 9:(002)
+  const double efx = -(l[1] + 2.0 * l[4] * dx + l[5] * dy + l[6] * dz);
+  const double efy = -(l[2] + l[5] * dx + 2.0 * l[7] * dy + l[8] * dz);
+  const double efz = -(l[3] + l[6] * dx + l[8] * dy + 2.0 * l[9] * dz);
+  const double4 e = ef[k];
+  const double se = sqrt(e.x * e.x + e.y * e.y + e.z * e.z) + 1e-300;
+  float* f = feat + static_cast<size_t>(s) * kFeat;
+  f[0] = static_cast<float>(dx / h);
+  f[1] = static_cast<float>(dy / h);
+  f[2] = static_cast<float>(dz / h);
+  f[3] = static_cast<float>(2.0 * cc.x);
+  f[4] = static_cast<float>(2.0 * cc.y);
+  f[5] = static_cast<float>(2.0 * cc.z);
+  f[6] = static_cast<float>(efx / se);
+  f[7] = static_cast<float>(efy / se);
+  f[8] = static_cast<float>(efz / se);
+  f[9] = static_cast<float>((e.x - efx) / se);
+  f[10] = static_cast<float>((e.y - efy) / se);
+  f[11] = static_cast<float>((e.z - efz) / se);
+  for (int g = 1; g <= 3; ++g) f[11 + g] = static_cast<float>(l[g] / se);
+  for (int g = 4; g <= 9; ++g) f[11 + g] = static_cast<float>(l[g] * h / se);
+  f[21] = static_cast<float>(log2(h) / 10.0);
+  const double* mm = M + static_cast<size_t>(leaf) * T.n_m;
+  const double q0 = mm[0];
+  const bool has_q = q0 != 0.0;
+  for (int g = 1; g <= 3; ++g) f[21 + g] = has_q ? static_cast<float>(mm[g] / (q0 * h)) : 0.f;
+  for (int g = 4; g <= 9; ++g) f[21 + g] = has_q ? static_cast<float>(mm[g] / (q0 * h * h)) : 0.f;
+  const int2 rr = t.range[leaf];
+  f[31] = static_cast<float>(rr.y - rr.x) / 32.f;
+  f[32] = static_cast<float>(radius[leaf] / h);
+  f[33] = static_cast<float>(p2p_count[leaf]) / 64.f;
+  f[34] = 1.f;
+  scale[s] = se / kTargetScale;
+}
+
+__global__ void fmm_correct_kernel(const float* __restrict__ pred, const double* __restrict__ scale, int m,
+                                   double4* __restrict__ ef) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  double4 e = ef[k];
+  e.x += scale[k] * pred[3 * k + 0];
+  e.y += scale[k] * pred[3 * k + 1];
+  e.z += scale[k] * pred[3 * k + 2];
+  ef[k] = e;
+}
+
+int fmm_apply_learned(amk_ctx* c, const FmmRun& r) {
+  const int m = static_cast<int>(r.t.m);
+  int rc = AMK_OK;
+  float* feat = slot<float>(c, kSlotMlp5, static_cast<size_t>(m) * kFeat, &rc);
+  AMK_TRY(rc);
+  double* scale = slot<double>(c, kSlotAuxState0, m, &rc);
+  AMK_TRY(rc);
+  float* pred = slot<float>(c, kSlotMlp4, static_cast<size_t>(m) * 3, &rc);
+  AMK_TRY(rc);
+  fmm_features_kernel<<<(m + 255) / 256, 256, 0, c->stream>>>(r.t, r.T, r.L, r.M, r.radius, r.p2p_count, r.leaf_of,
+                                                               r.ef, nullptr, m, feat, scale);
+  AMK_TRY(check_launch(c, "fmm_features_kernel"));
+  AMK_TRY(mlp_forward_device(c, feat, m, pred));
+  fmm_correct_kernel<<<(m + 255) / 256, 256, 0, c->stream>>>(pred, scale, m, r.ef);
+  return check_launch(c, "fmm_correct_kernel");
+}
+
+// Exact FP64 field (unit-cube units, per unit charge) at selected sorted
+// sources from all sources: a thread per target, sources staged in tiles.
+__global__ void __launch_bounds__(256)
+exact_field_kernel(const Octree t, const int* __restrict__ sel, int n_sel, double min_sq, double4* __restrict__ out) {
+  __shared__ double4 tile[256];
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = s < n_sel ? sel[s] : -1;
+  double4 me = make_double4(0.0, 0.0, 0.0, 0.0);
+  if (k >= 0) me = t.src[k];
+  double ex = 0.0, ey = 0.0, ez = 0.0;
+  for (long base = 0; base < t.m; base += 256) {
+    __syncthreads();
+    const long j = base + threadIdx.x;
+    tile[threadIdx.x] = j < t.m ? t.src[j] : make_double4(0.0, 0.0, 0.0, 0.0);
+    __syncthreads();
+    const int cnt = static_cast<int>(min(256L, t.m - base));
+    if (k < 0) continue;
+    for (int u = 0; u < cnt; ++u) {
+      const double4 q = tile[u];
+      if (base + u == k || q.w == 0.0) continue;
+      const double rx = me.x - q.x, ry = me.y - q.y, rz = me.z - q.z;
+      const double r2 = rx * rx + ry * ry + rz * rz;
+      if (r2 < min_sq) continue;
+      const double inv = rsqrt(r2);
+      const double f = q.w * inv * inv * inv;
+      ex += rx * f;
+      ey += ry * f;
+      ez += rz * f;
+    }
+  }
+  if (k >= 0) out[s] = make_double4(ex, ey, ez, 0.0);
+}
+
+// Particles of every `stride`-th leaf (deterministic sample of leaves).
+__global__ void select_leaf_particles_kernel(const Octree t, const int* __restrict__ leaf_of, int stride,
+                                             int* __restrict__ flag) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= t.m) return;
+  const unsigned h = static_cast<unsigned>(leaf_of[k]) * 2654435761u;
+  flag[k] = (h % static_cast<unsigned>(stride)) == 0 ? 1 : 0;
+}
+
+__global__ void compact_kernel(const int* __restrict__ flag, const int* __restrict__ pos, int m, int* __restrict__ sel) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < m && flag[k]) sel[pos[k]] = k;
+}
+
+__global__ void residual_targets_kernel(const int* __restrict__ sel, int n_sel, const double4* __restrict__ exact,
+                                        const double4* __restrict__ ef, const double* __restrict__ scale,
+                                        float* __restrict__ target) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_sel) return;
+  const double4 a = exact[s], b = ef[sel[s]];
+  const double sc = scale[s];
+  target[3 * s + 0] = static_cast<float>((a.x - b.x) / sc);
+  target[3 * s + 1] = static_cast<float>((a.y - b.y) / sc);
+  target[3 * s + 2] = static_cast<float>((a.z - b.z) / sc);
+}
+
+__global__ void audit_error_kernel(const int* __restrict__ sel, int n_sel, const double4* __restrict__ exact,
+                                   const double4* __restrict__ ef, double* __restrict__ err) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n_sel) return;
+  const double4 a = exact[s], b = ef[sel[s]];
+  const double num = (a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y) + (a.z - b.z) * (a.z - b.z);
+  const double den = a.x * a.x + a.y * a.y + a.z * a.z;
+  err[s] = den > 0.0 ? num / den : 0.0;
+}
+
+__global__ void stride_select_kernel(int m, int n_sel, int* __restrict__ sel) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n_sel) sel[s] = static_cast<int>((static_cast<long>(s) * m) / n_sel);
+}
+
+// Trains the correction on the context's particles: p=2 FMM, particles of a
+// deterministic sample of about `sample_leaves` leaves, exact FP64 fields for
+// them, Adam on (features, 100 (E_exact - E_p2) / |E_p2|).
+int fmm_train_learned(amk_ctx* c, const View& v, double theta, int sample_leaves, int steps, long batch, float lr,
+                      float* loss_out, long* samples_out) {
+  FmmRun r;
+  AMK_TRY(fmm_run(c, v, 2, theta, 32, false, &r));
+  const int m = static_cast<int>(r.t.m);
+  if (m == 0) return fail(AMK_ERR_STATE, "no charged particles to train on");
+  const long leaves = c->fmm->stats[1];
+  const int stride = static_cast<int>(std::max<long>(1, leaves / std::max(1, sample_leaves)));
+  int rc = AMK_OK;
+  int* flag = slot<int>(c, kSlotFmmWork0, m + 1, &rc);
+  AMK_TRY(rc);
+  int* pos = slot<int>(c, kSlotFmmWork1, m + 1, &rc);
+  AMK_TRY(rc);
+  int* total = slot<int>(c, kSlotStatus, 8, &rc) + 7;
+  AMK_TRY(rc);
+  select_leaf_particles_kernel<<<(m + 255) / 256, 256, 0, c->stream>>>(r.t, r.leaf_of, stride, flag);
+  AMK_TRY(check_launch(c, "select_leaf_particles_kernel"));
+  AMK_TRY(exclusive_scan_int(c, flag, m, pos, total));
+  int n_sel = 0;
+  AMK_CUDA_TRY(cudaMemcpyAsync(&n_sel, total, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (n_sel == 0) return fail(AMK_ERR_STATE, "empty training sample");
+  int* sel = slot<int>(c, kSlotFmmWork2, n_sel, &rc);
+  AMK_TRY(rc);
+  compact_kernel<<<(m + 255) / 256, 256, 0, c->stream>>>(flag, pos, m, sel);
+  AMK_TRY(check_launch(c, "compact_kernel"));
+  float* feat = slot<float>(c, kSlotMlp5, static_cast<size_t>(n_sel) * kFeat, &rc);
+  AMK_TRY(rc);
+  double* scale = slot<double>(c, kSlotAuxState0, n_sel, &rc);
+  AMK_TRY(rc);
+  double4* exact = slot<double4>(c, kSlotAuxState1, n_sel, &rc);
+  AMK_TRY(rc);
+  float* target = slot<float>(c, kSlotMlp4, static_cast<size_t>(n_sel) * 3, &rc);
+  AMK_TRY(rc);
+  fmm_features_kernel<<<(n_sel + 255) / 256, 256, 0, c->stream>>>(r.t, r.T, r.L, r.M, r.radius, r.p2p_count,
+                                                                   r.leaf_of, r.ef, sel, n_sel, feat, scale);
+  AMK_TRY(check_launch(c, "fmm_features_kernel"));
+  const double min_sq = kMinSquaredDistance / (r.hf.length * r.hf.length);
+  exact_field_kernel<<<(n_sel + 255) / 256, 256, 0, c->stream>>>(r.t, sel, n_sel, min_sq, exact);
+  AMK_TRY(check_launch(c, "exact_field_kernel"));
+  residual_targets_kernel<<<(n_sel + 255) / 256, 256, 0, c->stream>>>(sel, n_sel, exact, r.ef, scale, target);
+  AMK_TRY(check_launch(c, "residual_targets_kernel"));
+  if (samples_out) *samples_out = n_sel;
+  return mlp_train_device(c, feat, target, n_sel, steps, batch, lr, loss_out);
+}
+
+// RMS of |E - E_exact| / |E_exact| over `samples` evenly spaced particles for
+// plain FMM of `order` or (learned) p=2 plus the correction.
+int fmm_audit(amk_ctx* c, const View& v, int order, double theta, bool learned, long samples, double* rms) {
+  FmmRun r;
+  AMK_TRY(fmm_run(c, v, learned ? 2 : order, theta, 32, false, &r));
+  const int m = static_cast<int>(r.t.m);
+  *rms = 0.0;
+  if (m == 0) return AMK_OK;
+  if (learned) AMK_TRY(fmm_apply_learned(c, r));
+  const int n_sel = static_cast<int>(std::min<long>(std::max<long>(1, samples), m));
+  int rc = AMK_OK;
+  int* sel = slot<int>(c, kSlotFmmWork2, n_sel, &rc);
+  AMK_TRY(rc);
+  double4* exact = slot<double4>(c, kSlotAuxState1, n_sel, &rc);
+  AMK_TRY(rc);
+  double* err = slot<double>(c, kSlotAuxState2, n_sel, &rc);
+  AMK_TRY(rc);
+  double* res = slot<double>(c, kSlotAuxState4, 8, &rc);
+  AMK_TRY(rc);
+  stride_select_kernel<<<(n_sel + 255) / 256, 256, 0, c->stream>>>(m, n_sel, sel);
+  AMK_TRY(check_launch(c, "stride_select_kernel"));
+  const double min_sq = kMinSquaredDistance / (r.hf.length * r.hf.length);
+  exact_field_kernel<<<(n_sel + 255) / 256, 256, 0, c->stream>>>(r.t, sel, n_sel, min_sq, exact);
+  AMK_TRY(check_launch(c, "exact_field_kernel"));
+  audit_error_kernel<<<(n_sel + 255) / 256, 256, 0, c->stream>>>(sel, n_sel, exact, r.ef, err);
+  AMK_TRY(check_launch(c, "audit_error_kernel"));
+  AMK_TRY(reduce_sum(c, err, n_sel, res));
+  double h = 0.0;
+  AMK_CUDA_TRY(cudaMemcpyAsync(&h, res, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  AMK_TRY(mlp_check_status(c));
+  *rms = std::sqrt(h / n_sel);
   return AMK_OK;
 }
 

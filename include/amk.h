@@ -96,6 +96,11 @@ typedef struct amk_params {
   long populations[AMK_MAX_SPECIES];
   double temperatures[AMK_MAX_SPECIES]; /* "particle_temperatures" [K]    */
   double cloud_radii[3];        /* "initial_cloud_radii" radius_x/y/z [m] */
+  /* learned p=2 FMM correction (no reference keys) */
+  long learned_audit_interval;  /* steps between direct-sum audits (0 = never) */
+  double learned_error_budget;  /* RMS relative force error allowed by the audit */
+  int learned_fallback_order;   /* plain FMM order used after a failed audit */
+  long learned_audit_samples;   /* particles checked per audit */
 } amk_params;
 
 /* Defaults of the reference's ParamGroups (physics_params.h:21-46,
@@ -293,6 +298,21 @@ int amk_mlp_gradients(amk_ctx* ctx, const float* x, const float* target, long n,
 /* `steps` Adam steps on consecutive windows of `batch` samples. */
 int amk_mlp_train(amk_ctx* ctx, const float* x, const float* target, long n, int steps, long batch,
                   float lr, float* final_loss);
+
+/* Trains the correction on the context's particles: p=2 FMM at theta, the
+ * particles of about `sample_leaves` leaves, exact FP64 fields for them, and
+ * `steps` Adam steps (batch, lr) on the residual (E_exact - E_p2)/|E_far|.
+ * Marks the correction usable and clears a previous fallback. */
+int amk_fmm_train_correction(amk_ctx* ctx, double theta, int sample_leaves, int steps, long batch,
+                             float lr, float* final_loss, long* samples);
+/* RMS relative force error against the exact FP64 sum over `samples` evenly
+ * spaced particles, for plain FMM of `order` (learned = 0) or the learned
+ * p=2 correction (learned = 1). */
+int amk_fmm_audit(amk_ctx* ctx, int order, double theta, int learned, long samples, double* rms);
+/* trained: the correction is usable; fallback: an audit failed and the
+ * context now runs plain FMM at learned_fallback_order; last_error: the
+ * last audit's RMS relative error. */
+int amk_fmm_learned_state(amk_ctx* ctx, int* trained, int* fallback, double* last_error);
 
 /* ------------------------------------------------------------ allocation-free */
 /* No counterpart in the reference. The cutoff Coulomb solver (same results

@@ -1,0 +1,60 @@
+"""Learned p=2 FMM correction: trained on the GPU by the library's own
+kernels on FP64 exact residuals, audited against the exact sum, and
+replaced by plain FMM when an audit exceeds the error budget (including
+after deliberately corrupted weights)."""
+import numpy as np
+import pytest
+
+import amk
+from conftest import E, gaussian_cloud
+
+pytestmark = pytest.mark.gpu
+
+
+def cloud_sim(n=65536, seed=50, **over):
+    x, y, z, _ = gaussian_cloud(n, seed, mixed=False)
+    kw = dict(populations={"positron": n}, coulomb_method="fast-multipole", fast_multipole_order=2.0,
+              fast_multipole_theta=0.5, fmm_learned=1, cooling_enabled=0)
+    kw.update(over)
+    s = amk.Simulation(amk.make_params(**kw))
+    s.set_particles(x, y, z, np.zeros(n), np.zeros(n), np.zeros(n), np.ones(n, np.uint8))
+    return s
+
+
+def test_training_and_measured_gain():
+    with cloud_sim() as s:
+        plain = s.fmm_audit(2, 0.5, False, 2048)
+        loss, samples = s.fmm_train_correction(0.5, sample_leaves=1024, steps=800, batch=2048, lr=1e-3)
+        assert samples > 1000 and np.isfinite(loss)
+        learned = s.fmm_audit(2, 0.5, True, 2048)
+        p6 = s.fmm_audit(6, 0.5, False, 2048)
+        print(f"RMS relative force error: p=2 {plain:.3e}, p=2 + MLP {learned:.3e}, p=6 {p6:.3e}")
+        assert np.isfinite(learned)
+        assert learned <= 1.1 * plain   # the correction must not make p=2 worse
+        assert s.fmm_learned_state()["trained"]
+
+
+def test_failed_audit_falls_back_to_plain_fmm():
+    with cloud_sim(learned_audit_interval=1, learned_error_budget=1e-5, learned_fallback_order=6) as s:
+        s.fmm_train_correction(0.5, sample_leaves=256, steps=50, batch=1024, lr=1e-3)
+        st = s.fmm_learned_state()
+        assert st["trained"] and not st["fallback"]
+        s.step(1)  # the audit before the step exceeds 1e-5 -> fallback
+        st = s.fmm_learned_state()
+        assert st["fallback"] and st["last_error"] > 1e-5
+        s.coulomb_fmm(2, 0.5, learned=True)
+        f_learned = s.get_forces()
+        s.coulomb_fmm(6, 0.5)
+        f_p6 = s.get_forces()
+        assert all(np.array_equal(a, b) for a, b in zip(f_learned, f_p6))
+
+
+def test_corrupted_weights_are_caught_by_the_audit():
+    with cloud_sim(n=20000, learned_audit_interval=1, learned_error_budget=0.05) as s:
+        s.fmm_train_correction(0.5, sample_leaves=256, steps=50, batch=1024, lr=1e-3)
+        p = s.mlp_params()
+        s.set_mlp_params(np.full_like(p, 50.0))  # garbage network
+        bad = s.fmm_audit(2, 0.5, True, 1024)
+        assert bad > 0.05
+        s.step(1)
+        assert s.fmm_learned_state()["fallback"]
