@@ -146,6 +146,11 @@ def lib():
         "amk_mlp_forward": (C.c_int, [vp, _fp, C.c_long, _fp]),
         "amk_mlp_gradients": (C.c_int, [vp, _fp, _fp, C.c_long, _fp, _fp, _fp]),
         "amk_mlp_train": (C.c_int, [vp, _fp, _fp, C.c_long, C.c_int, C.c_long, C.c_float, _fp]),
+        "amk_batch_set": (C.c_int, [vp, C.c_int, C.POINTER(Params), C.POINTER(C.c_long)]),
+        "amk_batch_step": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
+        "amk_batch_coulomb": (C.c_int, [vp]),
+        "amk_batch_status": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_long)]),
+        "amk_batch_info": (C.c_int, [vp, C.POINTER(C.c_long), C.POINTER(C.c_long), C.POINTER(C.c_int)]),
         "amk_set_profiling": (C.c_int, [vp, C.c_int]),
         "amk_phase_times": (C.c_int, [vp, _dp, C.POINTER(C.c_long), C.c_int]),
         "amk_reset_phase_times": (C.c_int, [vp]),
@@ -445,6 +450,36 @@ class Simulation:
         t, f, e = C.c_int(), C.c_int(), C.c_double()
         check(lib().amk_fmm_learned_state(self._h, C.byref(t), C.byref(f), C.byref(e)))
         return {"trained": bool(t.value), "fallback": bool(f.value), "last_error": e.value}
+
+    # -- batched instances
+    def batch_set(self, params, offsets):
+        """Splits the particle set into instances: params[i] steps particles
+        [offsets[i], offsets[i+1])."""
+        n = len(params)
+        arr = (Params * n)(*params)
+        off = np.ascontiguousarray(offsets, np.int64)
+        if len(off) != n + 1:
+            raise ValueError("offsets needs len(params) + 1 entries")
+        check(lib().amk_batch_set(self._h, n, arr, off.ctypes.data_as(C.POINTER(C.c_long))), "amk_batch_set")
+        self._batch_n = n
+
+    def batch_step(self, n: int = 1, graph_chunk: int = 0, serial: bool = False):
+        check(lib().amk_batch_step(self._h, int(n), int(graph_chunk), 1 if serial else 0), "amk_batch_step")
+
+    def batch_coulomb(self):
+        check(lib().amk_batch_coulomb(self._h), "amk_batch_coulomb")
+
+    def batch_status(self):
+        ov = C.c_int(0)
+        counts = np.zeros(getattr(self, "_batch_n", 0), np.int64)
+        check(lib().amk_batch_status(self._h, C.byref(ov), counts.ctypes.data_as(C.POINTER(C.c_long))),
+              "amk_batch_status")
+        return {"overflow": bool(ov.value), "alive": counts}
+
+    def batch_info(self):
+        n, u, g = C.c_long(), C.c_long(), C.c_int()
+        check(lib().amk_batch_info(self._h, C.byref(n), C.byref(u), C.byref(g)), "amk_batch_info")
+        return {"instances": n.value, "work_units": u.value, "graphable": bool(g.value)}
 
     # -- learned correction (MLP)
     def mlp_params(self):

@@ -393,7 +393,7 @@ int allpairs_forces(amk_ctx* c, const View& v) {
   const int n_tiles = (n + kThreads - 1) / kThreads;
 
   // ---- Morton order (reused for kResortEvery calls on the context's own set)
-  const bool main_set = v.x == c->x.as<double>();
+  const bool main_set = v.x == c->x.as<double>() && v.n == c->n;
   uint32_t* perm = nullptr;
   bool resort = true;
   if (main_set) {

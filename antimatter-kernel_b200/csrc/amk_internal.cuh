@@ -198,6 +198,7 @@ struct PhaseClock {
 
 struct Fmm;  // fmm.cu
 struct Mlp;  // mlp.cu
+struct Batch;  // batch.cu
 
 }  // namespace amk
 
@@ -236,6 +237,7 @@ struct amk_ctx {
 
   amk::Fmm* fmm = nullptr;
   amk::Mlp* mlp = nullptr;
+  amk::Batch* batch = nullptr;  // batched instances over segment offsets
   // learned FMM correction state
   bool learned_trained = false;
   bool learned_fallback = false;
@@ -343,5 +345,10 @@ int reduce_sum(amk_ctx* c, const double* in, long n, double* out_dev);
 // Per-step behaviours (push.cu, cellist.cu).
 int push_step(amk_ctx* c, uint64_t step_index);
 int annihilate_step(amk_ctx* c, uint64_t step_index, long* marked);
+// Annihilation on a view (indices, species and ids relative to the view).
+int annihilate_view(amk_ctx* c, const View& v, const uint8_t* species, const uint32_t* ids, double radius,
+                    double probability, uint32_t seed, uint64_t step_index, long* marked);
+// Batched instances (batch.cu).
+void batch_destroy(amk_ctx* c);
 
 }  // namespace amk

@@ -1,0 +1,674 @@
+// Batched multi-instance sweep: many independent trap instances of uneven
+// population stepped together. The reference runs one instance per process
+// (antimatter-kernel.cc:153-162 is its step loop); a sweep over temperature,
+// field and population is many such runs. Here the instances share one
+// particle set: instance i owns [offset[i], offset[i+1]) and has its own
+// trap, time step, cooling, annihilation and Coulomb parameters.
+//
+// One batched step is:
+//   * all-pairs instances: ONE persistent launch over (instance, 128-target
+//     block) units taken from a queue ordered by cost (largest instances
+//     first). Double-float pair differences, FP32 pair math, TwoSum-folded
+//     tile sums: each target's result depends only on its own instance, in
+//     a fixed order, so it is deterministic and independent of the batch;
+//   * cutoff, Barnes-Hut and FMM instances: the single-instance solver on
+//     the instance's view;
+//   * one push kernel (Boris + cooling, per-instance parameters, the same
+//     per-particle code as the single-instance push);
+//   * annihilation: one cell list whose keys start with the instance id (so
+//     contacts never cross instances), one contact kernel, and one matching
+//     kernel that reads the contact count on the device.
+// When no instance uses Barnes-Hut or the FMM a step has no host
+// synchronisation, and chunks of steps are captured in a CUDA graph and
+// replayed. Random streams use the instance's seed and the particle's index
+// within its instance, so an instance gives the same result in any batch.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "amk_internal.cuh"
+#include "contacts.cuh"
+#include "push.cuh"
+
+namespace amk {
+
+int push_range(amk_ctx* c, const PushParams& P, long begin, long end, bool stagger, uint64_t step_index);
+
+namespace {
+
+constexpr int kBT = 128;           // threads per all-pairs CTA = targets per unit = sources per tile
+constexpr int kGridBits = 10;      // annihilation cells per axis per instance: 2^10
+constexpr int kInstBits = 9;       // up to 512 instances
+constexpr int kMaxInstances = 1 << kInstBits;
+static_assert(kMaxInstances == AMK_BATCH_MAX_INSTANCES, "instance key bits");
+constexpr double kGridMax = (1 << kGridBits) - 1;
+
+struct InstanceDev {
+  PushParams push;
+  double contact_radius, probability;  // annihilation
+  double inv_l;                        // 1 / length scale (a power of two)
+  double origin[3], inv_cell;          // annihilation grid
+  long offset, count;
+  int annihilation;
+  uint32_t seed;
+};
+
+__device__ __forceinline__ void fold(float& hi, float& lo, float p) {
+  const float s = hi + p;
+  const float bp = s - hi;
+  lo += (hi - (s - bp)) + (p - bp);
+  hi = s;
+}
+
+__global__ void batch_local_ids_kernel(long n, const uint16_t* __restrict__ inst_of,
+                                       const InstanceDev* __restrict__ inst, uint32_t* __restrict__ ids) {
+  const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  ids[i] = static_cast<uint32_t>(i - inst[inst_of[i]].offset);
+}
+
+// Double-float staging with the instance's length scale: x / L = hq + lo.
+__global__ void batch_stage_kernel(long n, const double* __restrict__ x, const double* __restrict__ y,
+                                   const double* __restrict__ z, const double* __restrict__ q,
+                                   const uint8_t* __restrict__ alive, const uint16_t* __restrict__ inst_of,
+                                   const InstanceDev* __restrict__ inst, float4* __restrict__ hq,
+                                   float4* __restrict__ lo) {
+  const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  const double inv_l = inst[inst_of[i]].inv_l;
+  const double xs = x[i] * inv_l, ys = y[i] * inv_l, zs = z[i] * inv_l;
+  const bool ok = alive[i] && q[i] != 0.0 && isfinite(xs) && isfinite(ys) && isfinite(zs);
+  float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
+  if (ok) {
+    h = make_float4(__double2float_rn(xs), __double2float_rn(ys), __double2float_rn(zs),
+                    __double2float_rn(q[i] / kElementaryCharge));
+    l = make_float4(__double2float_rn(xs - static_cast<double>(h.x)), __double2float_rn(ys - static_cast<double>(h.y)),
+                    __double2float_rn(zs - static_cast<double>(h.z)), 0.f);
+  }
+  hq[i] = h;
+  lo[i] = l;
+}
+
+// Persistent all-pairs over (instance, target block) units; `queue` is the
+// work-queue head, zeroed before every launch. F_i = k e q_i / L^2 *
+// sum_j q_j (r_i - r_j) / |r_i - r_j|^3 in scaled units.
+__global__ void __launch_bounds__(kBT)
+batch_allpairs_kernel(const int2* __restrict__ units, int n_units, const InstanceDev* __restrict__ inst,
+                      const float4* __restrict__ hq, const float4* __restrict__ lo, const double* __restrict__ q,
+                      double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
+                      int* __restrict__ queue) {
+  __shared__ float4 sh[kBT], sl[kBT];
+  __shared__ int s_unit;
+  for (;;) {
+    if (threadIdx.x == 0) s_unit = atomicAdd(queue, 1);
+    __syncthreads();
+    const int u = s_unit;
+    if (u >= n_units) return;
+    const int2 un = units[u];
+    const long b = inst[un.x].offset, e = b + inst[un.x].count;
+    const double inv_l = inst[un.x].inv_l;
+    const long i = b + static_cast<long>(un.y) * kBT + threadIdx.x;
+    float4 th = make_float4(0.f, 0.f, 0.f, 0.f), tl = th;
+    if (i < e) {
+      th = hq[i];
+      tl = lo[i];
+    }
+    const float eps2 = static_cast<float>(fmax(kMinSquaredDistance * inv_l * inv_l, 1e-25));
+    float ahx = 0.f, ahy = 0.f, ahz = 0.f, alx = 0.f, aly = 0.f, alz = 0.f;
+    for (long t0 = b; t0 < e; t0 += kBT) {
+      const long j = t0 + threadIdx.x;
+      sh[threadIdx.x] = j < e ? hq[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+      sl[threadIdx.x] = j < e ? lo[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+      __syncthreads();
+      float px = 0.f, py = 0.f, pz = 0.f;
+      const int cnt = static_cast<int>(min(static_cast<long>(kBT), e - t0));
+#pragma unroll 8
+      for (int k = 0; k < cnt; ++k) {
+        const float4 s = sh[k], l = sl[k];
+        const float dx = (th.x - s.x) + (tl.x - l.x);
+        const float dy = (th.y - s.y) + (tl.y - l.y);
+        const float dz = (th.z - s.z) + (tl.z - l.z);
+        const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+        const float rinv = rsqrtf(d2);
+        // the self pair has d = 0 exactly and adds nothing
+        const float w = (s.w * rinv) * (rinv * rinv);
+        px = fmaf(w, dx, px);
+        py = fmaf(w, dy, py);
+        pz = fmaf(w, dz, pz);
+      }
+      fold(ahx, alx, px);
+      fold(ahy, aly, py);
+      fold(ahz, alz, pz);
+      __syncthreads();
+    }
+    if (i < e) {
+      const double coef = th.w != 0.f ? kCoulombConstant * kElementaryCharge * inv_l * inv_l * q[i] : 0.0;
+      fx[i] = coef * (static_cast<double>(ahx) + static_cast<double>(alx));
+      fy[i] = coef * (static_cast<double>(ahy) + static_cast<double>(aly));
+      fz[i] = coef * (static_cast<double>(ahz) + static_cast<double>(alz));
+    }
+  }
+}
+
+// LorentzForce + CyclotronCooling with each particle's instance parameters;
+// the step index is read on the device so that graph replays advance it.
+__global__ void __launch_bounds__(256)
+batch_push_kernel(long n, double* __restrict__ x, double* __restrict__ y, double* __restrict__ z,
+                  double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz, double* __restrict__ fx,
+                  double* __restrict__ fy, double* __restrict__ fz, const double* __restrict__ q,
+                  const double* __restrict__ m, const uint8_t* __restrict__ alive, const uint32_t* __restrict__ ids,
+                  const uint16_t* __restrict__ inst_of, const InstanceDev* __restrict__ inst,
+                  const unsigned long long* __restrict__ step_dev, int stagger) {
+  const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  const PushParams P = inst[inst_of[i]].push;
+  push_particle(i, x, y, z, vx, vy, vz, fx, fy, fz, q, m, alive, P, stagger, *step_dev, ids[i]);
+}
+
+// Step counter (advanced at the start of every batched step) and the
+// queue / contact-count reset.
+__global__ void batch_begin_step_kernel(unsigned long long* step_dev, int* queue, unsigned long long* contacts) {
+  *step_dev += 1ull;
+  *queue = 0;
+  contacts[0] = 0;
+}
+
+__device__ __forceinline__ void batch_cell(const InstanceDev& I, double x, double y, double z, uint32_t c[3]) {
+  const double p[3] = {x, y, z};
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    c[d] = static_cast<uint32_t>(fmin(fmax(floor((p[d] - I.origin[d]) * I.inv_cell), 0.0), kGridMax));
+}
+
+__device__ __forceinline__ bool has_partner(int s) {
+  return s == AMK_POSITRON || s == AMK_ELECTRON || s == AMK_PROTON || s == AMK_ANTIPROTON;
+}
+
+// Annihilation cell keys: instance id above a 30-bit Morton cell index
+// (10 bits per axis); particles that cannot annihilate sort last. Cells
+// are clamped to the instance's grid, which keeps neighbours within one
+// cell of each other, so a particle outside the grid is still found.
+__global__ void batch_cell_key_kernel(long n, const double* __restrict__ x, const double* __restrict__ y,
+                                      const double* __restrict__ z, const uint8_t* __restrict__ alive,
+                                      const uint8_t* __restrict__ species, const uint16_t* __restrict__ inst_of,
+                                      const InstanceDev* __restrict__ inst, uint64_t* __restrict__ keys,
+                                      uint32_t* __restrict__ vals) {
+  const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (i >= n) return;
+  vals[i] = static_cast<uint32_t>(i);
+  const InstanceDev& I = inst[inst_of[i]];
+  if (!alive[i] || !I.annihilation || !has_partner(species[i]) || !isfinite(x[i]) || !isfinite(y[i]) ||
+      !isfinite(z[i])) {
+    keys[i] = ~0ull;
+    return;
+  }
+  uint32_t c[3];
+  batch_cell(I, x[i], y[i], z[i], c);
+  keys[i] = (static_cast<uint64_t>(inst_of[i]) << (3 * kGridBits)) | morton3_21(c[0], c[1], c[2]);
+}
+
+__device__ __forceinline__ long lower_bound_key(const uint64_t* keys, long n, uint64_t k) {
+  long lo = 0, hi = n;
+  while (lo < hi) {
+    const long mid = (lo + hi) >> 1;
+    if (keys[mid] < k)
+      lo = mid + 1;
+    else
+      hi = mid;
+  }
+  return lo;
+}
+
+// Directed contacts owner -> partner within the contact radius whose Philox
+// draw is below the instance's probability (annihilation.cc:21-61 made
+// deterministic; the same rule as the single-instance contact kernel).
+__global__ void __launch_bounds__(128)
+batch_contact_kernel(long n, const double* __restrict__ x, const double* __restrict__ y, const double* __restrict__ z,
+                     const uint8_t* __restrict__ species, const uint32_t* __restrict__ ids,
+                     const uint16_t* __restrict__ inst_of, const InstanceDev* __restrict__ inst,
+                     const uint64_t* __restrict__ skeys, const uint32_t* __restrict__ sidx,
+                     const unsigned long long* __restrict__ step_dev, Contact* __restrict__ out,
+                     unsigned long long* count, long cap) {
+  const long s = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (s >= n || skeys[s] == ~0ull) return;
+  const long i = sidx[s];
+  const uint64_t prefix = skeys[s] & ~((1ull << (3 * kGridBits)) - 1ull);
+  const InstanceDev& I = inst[inst_of[i]];
+  const int si = species[i];
+  const double xi = x[i], yi = y[i], zi = z[i];
+  uint32_t c[3];
+  batch_cell(I, xi, yi, zi, c);
+  const double rc2 = I.contact_radius * I.contact_radius;
+  const double prob = I.probability;
+  const uint32_t seed = I.seed;
+  const uint64_t st = *step_dev;
+  for (int dz = -1; dz <= 1; ++dz) {
+    const int cz = static_cast<int>(c[2]) + dz;
+    if (cz < 0 || cz > static_cast<int>(kGridMax)) continue;
+    for (int dy = -1; dy <= 1; ++dy) {
+      const int cy = static_cast<int>(c[1]) + dy;
+      if (cy < 0 || cy > static_cast<int>(kGridMax)) continue;
+      for (int dx = -1; dx <= 1; ++dx) {
+        const int cx = static_cast<int>(c[0]) + dx;
+        if (cx < 0 || cx > static_cast<int>(kGridMax)) continue;
+        const uint64_t key = prefix | morton3_21(cx, cy, cz);
+        for (long k = lower_bound_key(skeys, n, key); k < n && skeys[k] == key; ++k) {
+          const long j = sidx[k];
+          if (j == i) continue;
+          const int sj = species[j];
+          const bool pair = (si == AMK_ANTIPROTON && sj == AMK_PROTON) || (si == AMK_PROTON && sj == AMK_ANTIPROTON) ||
+                            (si == AMK_POSITRON && sj == AMK_ELECTRON) || (si == AMK_ELECTRON && sj == AMK_POSITRON);
+          if (!pair) continue;
+          const double rx = xi - x[j], ry = yi - y[j], rz = zi - z[j];
+          const double d2 = __dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz));
+          if (!(d2 < rc2)) continue;
+          const Philox4 w = philox4x32(seed, kTagAnnihilation, ids[i], ids[j], static_cast<uint32_t>(st),
+                                       static_cast<uint32_t>(st >> 32));
+          if (!(u01(w.w[0]) < prob)) continue;
+          const unsigned long long slot_i = atomicAdd(count, 1ull);
+          if (static_cast<long>(slot_i) < cap) {
+            Contact e;
+            e.a = static_cast<uint32_t>(i);
+            e.b = static_cast<uint32_t>(j);
+            // instance id above the local ids: within an instance the greedy
+            // order is the single-instance order, and instances are disjoint
+            e.prio = (static_cast<uint64_t>(inst_of[i]) << 54) | (static_cast<uint64_t>(ids[i]) << 27) | ids[j];
+            out[slot_i] = e;
+          }
+        }
+      }
+    }
+  }
+}
+
+// Records a contact-buffer overflow in the sticky status word.
+__global__ void batch_overflow_kernel(const unsigned long long* contacts, long cap, unsigned long long* status) {
+  if (contacts[0] > static_cast<unsigned long long>(cap)) *status = 1ull;
+}
+
+__global__ void batch_alive_count_kernel(long n, const uint8_t* __restrict__ alive,
+                                         const uint16_t* __restrict__ inst_of, unsigned long long* counts) {
+  const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (i >= n || !alive[i]) return;
+  atomicAdd(&counts[inst_of[i]], 1ull);
+}
+
+}  // namespace
+
+struct Batch {
+  int n_inst = 0;
+  std::vector<amk_params> params;
+  std::vector<long> offsets;
+  std::vector<double> scale;
+  std::vector<PushParams> push;
+  std::vector<int> solver_instances;  // instances with a per-instance solver call
+  bool any_annihilation = false;
+  bool graphable = true;
+  DevBuf inst, inst_of, units, counters, contacts, best, flags, keys, vals, skeys, sidx;
+  long n_units = 0;
+  long contact_cap = 0;
+  int grid = 0;
+  uint64_t step = 0;  // host mirror of the device step counter
+  bool warm = false;  // one uncaptured step done (scratch reserved)
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  int graph_steps = 0;
+  long graph_launches = 0;
+  ~Batch() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+  // counters (64-bit words): [0] queue head (int), [1] step, [2] contact
+  // count, [3..4] match result, [5] overflow status
+  int* queue() const { return counters.as<int>(); }
+  unsigned long long* step_dev() const { return counters.as<unsigned long long>() + 1; }
+  unsigned long long* contact_count() const { return counters.as<unsigned long long>() + 2; }
+  unsigned long long* match_result() const { return counters.as<unsigned long long>() + 3; }
+  unsigned long long* overflow() const { return counters.as<unsigned long long>() + 5; }
+};
+
+void batch_destroy(amk_ctx* c) {
+  delete c->batch;
+  c->batch = nullptr;
+}
+
+namespace {
+
+View instance_view(amk_ctx* c, const Batch& B, int i) {
+  View v = main_view(c);
+  const long off = B.offsets[i];
+  v.n = B.offsets[i + 1] - off;
+  v.x += off;
+  v.y += off;
+  v.z += off;
+  v.q += off;
+  v.alive += off;
+  v.hq += off;
+  v.lo += off;
+  v.fx += off;
+  v.fy += off;
+  v.fz += off;
+  v.phi = nullptr;
+  v.length_scale = B.scale[i];
+  return v;
+}
+
+// The single-instance solver of instance i on its view.
+int instance_coulomb(amk_ctx* c, const Batch& B, int i) {
+  const amk_params& p = B.params[i];
+  View v = instance_view(c, B, i);
+  if (v.n == 0 || !p.coulomb_forces_enabled) return AMK_OK;
+  switch (p.coulomb_method) {
+    case AMK_METHOD_ALLPAIRS: return allpairs_forces(c, v);
+    case AMK_METHOD_STANDARD: return cutoff_forces(c, v, p.cutoff_radius, nullptr);
+    case AMK_METHOD_BARNES_HUT: return barnes_hut_forces(c, v, p.barnes_hut_theta, 8);
+    case AMK_METHOD_FAST_MULTIPOLE:
+      return fmm_forces(c, v, static_cast<int>(p.fast_multipole_order), p.fast_multipole_theta, 32, false, nullptr);
+    default: return fail(AMK_ERR_INVALID, "unknown coulomb method %d", p.coulomb_method);
+  }
+}
+
+int batch_annihilate(amk_ctx* c, Batch& B) {
+  const long n = c->n;
+  const unsigned gb = static_cast<unsigned>((n + 255) / 256);
+  AMK_TRY(phase_begin(c, AMK_PHASE_ANNIHILATION));
+  batch_cell_key_kernel<<<gb, 256, 0, c->stream>>>(n, c->x.as<double>(), c->y.as<double>(), c->z.as<double>(),
+                                                   c->alive.as<uint8_t>(), c->species.as<uint8_t>(),
+                                                   B.inst_of.as<uint16_t>(), B.inst.as<InstanceDev>(),
+                                                   B.keys.as<uint64_t>(), B.vals.as<uint32_t>());
+  AMK_TRY(check_launch(c, "batch_cell_key_kernel"));
+  AMK_TRY(radix_sort_pairs(c, B.keys.as<uint64_t>(), B.vals.as<uint32_t>(), B.skeys.as<uint64_t>(),
+                           B.sidx.as<uint32_t>(), n, kInstBits + 3 * kGridBits));
+  batch_contact_kernel<<<static_cast<unsigned>((n + 127) / 128), 128, 0, c->stream>>>(
+      n, c->x.as<double>(), c->y.as<double>(), c->z.as<double>(), c->species.as<uint8_t>(), c->ids.as<uint32_t>(),
+      B.inst_of.as<uint16_t>(), B.inst.as<InstanceDev>(), B.skeys.as<uint64_t>(), B.sidx.as<uint32_t>(),
+      B.step_dev(), B.contacts.as<Contact>(), B.contact_count(), B.contact_cap);
+  AMK_TRY(check_launch(c, "batch_contact_kernel"));
+  match_kernel<<<1, 1024, 0, c->stream>>>(B.contacts.as<Contact>(), B.contact_cap, B.contact_count(),
+                                          B.best.as<unsigned long long>(), B.flags.as<uint8_t>(),
+                                          B.flags.as<uint8_t>() + n, c->alive.as<uint8_t>(), B.match_result());
+  AMK_TRY(check_launch(c, "match_kernel"));
+  batch_overflow_kernel<<<1, 1, 0, c->stream>>>(B.contact_count(), B.contact_cap, B.overflow());
+  AMK_TRY(check_launch(c, "batch_overflow_kernel"));
+  return phase_end(c, AMK_PHASE_ANNIHILATION);
+}
+
+// Coulomb forces of every instance into the context's force arrays.
+int batch_coulomb(amk_ctx* c, Batch& B) {
+  const long n = c->n;
+  if (B.n_units > 0) {
+    AMK_TRY(phase_begin(c, AMK_PHASE_STAGE));
+    batch_stage_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, c->stream>>>(
+        n, c->x.as<double>(), c->y.as<double>(), c->z.as<double>(), c->q.as<double>(), c->alive.as<uint8_t>(),
+        B.inst_of.as<uint16_t>(), B.inst.as<InstanceDev>(), c->hq.as<float4>(), c->lo.as<float4>());
+    AMK_TRY(check_launch(c, "batch_stage_kernel"));
+    AMK_TRY(phase_end(c, AMK_PHASE_STAGE));
+    AMK_TRY(phase_begin(c, AMK_PHASE_ALLPAIRS));
+    batch_allpairs_kernel<<<B.grid, kBT, 0, c->stream>>>(B.units.as<int2>(), static_cast<int>(B.n_units),
+                                                         B.inst.as<InstanceDev>(), c->hq.as<float4>(),
+                                                         c->lo.as<float4>(), c->q.as<double>(), c->fx.as<double>(),
+                                                         c->fy.as<double>(), c->fz.as<double>(), B.queue());
+    AMK_TRY(check_launch(c, "batch_allpairs_kernel"));
+    AMK_TRY(phase_end(c, AMK_PHASE_ALLPAIRS));
+  }
+  for (int i : B.solver_instances) AMK_TRY(instance_coulomb(c, B, i));
+  return AMK_OK;
+}
+
+// One batched step; no host synchronisation unless a per-instance solver
+// needs one (Barnes-Hut, FMM).
+int batch_step_once(amk_ctx* c, Batch& B, bool stagger) {
+  const long n = c->n;
+  batch_begin_step_kernel<<<1, 1, 0, c->stream>>>(B.step_dev(), B.queue(), B.contact_count());
+  AMK_TRY(check_launch(c, "batch_begin_step_kernel"));
+  if (n == 0) return AMK_OK;
+  AMK_TRY(batch_coulomb(c, B));
+  AMK_TRY(phase_begin(c, AMK_PHASE_PUSH));
+  batch_push_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, c->stream>>>(
+      n, c->x.as<double>(), c->y.as<double>(), c->z.as<double>(), c->vx.as<double>(), c->vy.as<double>(),
+      c->vz.as<double>(), c->fx.as<double>(), c->fy.as<double>(), c->fz.as<double>(), c->q.as<double>(),
+      c->m.as<double>(), c->alive.as<uint8_t>(), c->ids.as<uint32_t>(), B.inst_of.as<uint16_t>(),
+      B.inst.as<InstanceDev>(), B.step_dev(), stagger ? 1 : 0);
+  AMK_TRY(check_launch(c, "batch_push_kernel"));
+  AMK_TRY(phase_end(c, AMK_PHASE_PUSH));
+  if (B.any_annihilation) AMK_TRY(batch_annihilate(c, B));
+  return AMK_OK;
+}
+
+// The same step with every instance run on its own, one after the other,
+// through the single-instance kernels (solver on the view, push on the
+// range, annihilation on the view): the comparison baseline for the batch.
+int serial_step_once(amk_ctx* c, Batch& B, bool stagger) {
+  batch_begin_step_kernel<<<1, 1, 0, c->stream>>>(B.step_dev(), B.queue(), B.contact_count());
+  AMK_TRY(check_launch(c, "batch_begin_step_kernel"));
+  const uint64_t st = B.step + 1;
+  for (int i = 0; i < B.n_inst; ++i) {
+    const long off = B.offsets[i], cnt = B.offsets[i + 1] - off;
+    if (cnt == 0) continue;
+    const amk_params& p = B.params[i];
+    AMK_TRY(instance_coulomb(c, B, i));
+    AMK_TRY(push_range(c, B.push[i], off, off + cnt, stagger, st));
+    if (p.annihilation_enabled && p.contact_radius > 0.0) {
+      View v = instance_view(c, B, i);
+      AMK_TRY(annihilate_view(c, v, c->species.as<uint8_t>() + off, c->ids.as<uint32_t>() + off, p.contact_radius,
+                              p.annihilation_probability, static_cast<uint32_t>(p.seed), st, nullptr));
+    }
+  }
+  return AMK_OK;
+}
+
+}  // namespace
+}  // namespace amk
+
+using namespace amk;
+
+extern "C" int amk_batch_set(amk_ctx* c, int n_inst, const amk_params* params, const long* offsets) {
+  if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (n_inst <= 0 || !params || !offsets) return fail(AMK_ERR_INVALID, "amk_batch_set: no instances");
+  if (n_inst > kMaxInstances) return fail(AMK_ERR_LIMIT, "%d instances exceed the maximum of %d", n_inst, kMaxInstances);
+  if (offsets[0] != 0 || offsets[n_inst] != c->n)
+    return fail(AMK_ERR_INVALID, "instance offsets must run from 0 to the particle count %ld", c->n);
+  for (int i = 0; i < n_inst; ++i) {
+    if (offsets[i + 1] < offsets[i]) return fail(AMK_ERR_INVALID, "instance offsets must not decrease");
+    if (offsets[i + 1] - offsets[i] >= (1L << 27))
+      return fail(AMK_ERR_LIMIT, "instance %d: more than 2^27 particles", i);
+    if (amk_params_validate(&params[i], 0) != AMK_OK) return AMK_ERR_INVALID;
+    if (!(params[i].dt > 0.0)) return fail(AMK_ERR_INVALID, "instance %d: dt must be positive", i);
+    if (params[i].coulomb_forces_enabled && params[i].coulomb_method == AMK_METHOD_FAST_MULTIPOLE &&
+        params[i].fmm_learned)
+      return fail(AMK_ERR_UNSUPPORTED, "instance %d: the learned correction is not available in batches", i);
+  }
+  AMK_CUDA_TRY(cudaSetDevice(c->device));
+  batch_destroy(c);
+  Batch* B = new Batch();
+  c->batch = B;
+  B->n_inst = n_inst;
+  B->params.assign(params, params + n_inst);
+  B->offsets.assign(offsets, offsets + n_inst + 1);
+  B->step = static_cast<uint64_t>(c->step);
+  const long n = c->n;
+  // host copies of the positions for the per-instance scales and grids
+  std::vector<double> hx(n), hy(n), hz(n);
+  if (n > 0) {
+    AMK_CUDA_TRY(cudaMemcpyAsync(hx.data(), c->x.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaMemcpyAsync(hy.data(), c->y.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaMemcpyAsync(hz.data(), c->z.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  }
+  std::vector<InstanceDev> inst(n_inst);
+  std::vector<uint16_t> inst_of(n);
+  std::vector<std::pair<long, int2>> units;  // (instance size, unit)
+  for (int i = 0; i < n_inst; ++i) {
+    const amk_params& p = params[i];
+    const long off = offsets[i], cnt = offsets[i + 1] - off;
+    double mx = 0.0;
+    for (long k = off; k < off + cnt; ++k) {
+      inst_of[k] = static_cast<uint16_t>(i);
+      const double a = std::max(std::fabs(hx[k]), std::max(std::fabs(hy[k]), std::fabs(hz[k])));
+      if (std::isfinite(a)) mx = std::max(mx, a);
+    }
+    InstanceDev& d = inst[i];
+    d.push = push_params_for(p);
+    B->push.push_back(d.push);
+    B->scale.push_back(length_scale_for(mx));
+    d.inv_l = 1.0 / B->scale.back();
+    d.annihilation = (p.annihilation_enabled && p.contact_radius > 0.0) ? 1 : 0;
+    B->any_annihilation = B->any_annihilation || d.annihilation;
+    d.contact_radius = p.contact_radius;
+    d.probability = p.annihilation_probability;
+    // grid over [-reach, reach)^3 with cells no smaller than the contact radius
+    const double reach = std::max(4.0 * mx, 1e-12);
+    const double cs = std::max(p.contact_radius * (1.0 + 1e-9), 2.0 * reach / (kGridMax - 1.0));
+    for (int k = 0; k < 3; ++k) d.origin[k] = -reach;
+    d.inv_cell = 1.0 / cs;
+    d.seed = static_cast<uint32_t>(p.seed);
+    d.offset = off;
+    d.count = cnt;
+    if (!p.coulomb_forces_enabled || cnt == 0) continue;
+    if (p.coulomb_method == AMK_METHOD_ALLPAIRS) {
+      for (long b = 0; b * kBT < cnt; ++b) units.push_back({cnt, make_int2(i, static_cast<int>(b))});
+    } else {
+      B->solver_instances.push_back(i);
+      if (p.coulomb_method == AMK_METHOD_BARNES_HUT || p.coulomb_method == AMK_METHOD_FAST_MULTIPOLE)
+        B->graphable = false;  // their tree builds read sizes back to the host
+    }
+  }
+  std::stable_sort(units.begin(), units.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+  std::vector<int2> hu(units.size());
+  for (size_t k = 0; k < units.size(); ++k) hu[k] = units[k].second;
+  B->n_units = static_cast<long>(hu.size());
+  B->contact_cap = std::max<long>(65536, n / 8);
+  int sms = 148, per_sm = 1;
+  AMK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+  AMK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_allpairs_kernel, kBT, 0));
+  B->grid = static_cast<int>(std::max<long>(1, std::min<long>(B->n_units, static_cast<long>(sms) * std::max(1, per_sm))));
+  const size_t nn = static_cast<size_t>(std::max<long>(n, 1));
+  AMK_TRY(B->inst.reserve(n_inst * sizeof(InstanceDev)));
+  AMK_TRY(B->inst_of.reserve(nn * sizeof(uint16_t)));
+  AMK_TRY(B->units.reserve(std::max<size_t>(1, hu.size()) * sizeof(int2)));
+  AMK_TRY(B->counters.reserve(64));
+  AMK_TRY(B->contacts.reserve(B->contact_cap * sizeof(Contact)));
+  AMK_TRY(B->best.reserve(nn * sizeof(unsigned long long)));
+  AMK_TRY(B->flags.reserve(nn + B->contact_cap));
+  AMK_TRY(B->keys.reserve(nn * sizeof(uint64_t)));
+  AMK_TRY(B->vals.reserve(nn * sizeof(uint32_t)));
+  AMK_TRY(B->skeys.reserve(nn * sizeof(uint64_t)));
+  AMK_TRY(B->sidx.reserve(nn * sizeof(uint32_t)));
+  AMK_CUDA_TRY(cudaMemcpyAsync(B->inst.ptr, inst.data(), n_inst * sizeof(InstanceDev), cudaMemcpyHostToDevice,
+                               c->stream));
+  if (n > 0)
+    AMK_CUDA_TRY(cudaMemcpyAsync(B->inst_of.ptr, inst_of.data(), n * sizeof(uint16_t), cudaMemcpyHostToDevice,
+                                 c->stream));
+  if (!hu.empty())
+    AMK_CUDA_TRY(cudaMemcpyAsync(B->units.ptr, hu.data(), hu.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream));
+  const unsigned long long init[8] = {0, B->step, 0, 0, 0, 0, 0, 0};
+  AMK_CUDA_TRY(cudaMemcpyAsync(B->counters.ptr, init, sizeof(init), cudaMemcpyHostToDevice, c->stream));
+  if (n > 0) {
+    // random streams and contact priorities use the index within the instance
+    batch_local_ids_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, c->stream>>>(
+        n, B->inst_of.as<uint16_t>(), B->inst.as<InstanceDev>(), c->ids.as<uint32_t>());
+    AMK_TRY(check_launch(c, "batch_local_ids_kernel"));
+  }
+  AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return AMK_OK;
+}
+
+extern "C" int amk_batch_step(amk_ctx* c, int nsteps, int graph_chunk, int serial) {
+  if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (!c->batch) return fail(AMK_ERR_STATE, "no batch: call amk_batch_set first");
+  if (nsteps < 0) return fail(AMK_ERR_INVALID, "nsteps < 0");
+  Batch& B = *c->batch;
+  AMK_CUDA_TRY(cudaSetDevice(c->device));
+  const bool use_graph = graph_chunk > 0 && !serial && B.graphable && !c->profiling;
+  int done = 0;
+  while (done < nsteps) {
+    const bool stagger = !c->staggered;
+    if (!use_graph || !B.warm || stagger || nsteps - done < graph_chunk) {
+      AMK_TRY(serial ? serial_step_once(c, B, stagger) : batch_step_once(c, B, stagger));
+      c->staggered = true;
+      B.warm = true;
+      B.step++;
+      c->step++;
+      ++done;
+      continue;
+    }
+    if (!B.exec || B.graph_steps != graph_chunk) {
+      if (B.exec) cudaGraphExecDestroy(B.exec);
+      if (B.graph) cudaGraphDestroy(B.graph);
+      B.exec = nullptr;
+      B.graph = nullptr;
+      const long launches0 = c->kernel_launches;
+      AMK_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+      int rc = AMK_OK;
+      for (int s = 0; s < graph_chunk && rc == AMK_OK; ++s) rc = batch_step_once(c, B, false);
+      cudaGraph_t g = nullptr;
+      const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+      B.graph_launches = c->kernel_launches - launches0;
+      c->kernel_launches = launches0;  // captured, not run
+      if (rc != AMK_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (e != cudaSuccess) return fail(AMK_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+      B.graph = g;
+      AMK_CUDA_TRY(cudaGraphInstantiate(&B.exec, B.graph, 0));
+      B.graph_steps = graph_chunk;
+    }
+    AMK_CUDA_TRY(cudaGraphLaunch(B.exec, c->stream));
+    c->kernel_launches += B.graph_launches;
+    B.step += static_cast<uint64_t>(graph_chunk);
+    c->step += graph_chunk;
+    done += graph_chunk;
+  }
+  c->stage_dirty = true;
+  return AMK_OK;
+}
+
+extern "C" int amk_batch_coulomb(amk_ctx* c) {
+  if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (!c->batch) return fail(AMK_ERR_STATE, "no batch: call amk_batch_set first");
+  AMK_CUDA_TRY(cudaSetDevice(c->device));
+  Batch& B = *c->batch;
+  if (c->n == 0) return AMK_OK;
+  // the all-pairs queue head is reset by the step prologue; reset it here
+  AMK_CUDA_TRY(cudaMemsetAsync(B.queue(), 0, sizeof(int), c->stream));
+  AMK_TRY(batch_coulomb(c, B));
+  return AMK_OK;
+}
+
+extern "C" int amk_batch_status(amk_ctx* c, int* overflow, long* alive_counts) {
+  if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (!c->batch) return fail(AMK_ERR_STATE, "no batch: call amk_batch_set first");
+  Batch& B = *c->batch;
+  AMK_CUDA_TRY(cudaSetDevice(c->device));
+  unsigned long long ov = 0;
+  AMK_CUDA_TRY(cudaMemcpyAsync(&ov, B.overflow(), sizeof(ov), cudaMemcpyDeviceToHost, c->stream));
+  std::vector<unsigned long long> h(B.n_inst, 0ull);
+  if (alive_counts) {
+    int rc = AMK_OK;
+    unsigned long long* cnt = slot<unsigned long long>(c, kSlotStatus, B.n_inst, &rc);
+    AMK_TRY(rc);
+    AMK_CUDA_TRY(cudaMemsetAsync(cnt, 0, B.n_inst * sizeof(unsigned long long), c->stream));
+    if (c->n > 0) {
+      batch_alive_count_kernel<<<static_cast<unsigned>((c->n + 255) / 256), 256, 0, c->stream>>>(
+          c->n, c->alive.as<uint8_t>(), B.inst_of.as<uint16_t>(), cnt);
+      AMK_TRY(check_launch(c, "batch_alive_count_kernel"));
+    }
+    AMK_CUDA_TRY(cudaMemcpyAsync(h.data(), cnt, B.n_inst * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                 c->stream));
+  }
+  AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (alive_counts)
+    for (int i = 0; i < B.n_inst; ++i) alive_counts[i] = static_cast<long>(h[i]);
+  if (overflow) *overflow = ov ? 1 : 0;
+  return AMK_OK;
+}
+
+extern "C" int amk_batch_info(const amk_ctx* c, long* n_instances, long* work_units, int* graphable) {
+  if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (!c->batch) return fail(AMK_ERR_STATE, "no batch: call amk_batch_set first");
+  if (n_instances) *n_instances = c->batch->n_inst;
+  if (work_units) *work_units = c->batch->n_units;
+  if (graphable) *graphable = c->batch->graphable ? 1 : 0;
+  return AMK_OK;
+}

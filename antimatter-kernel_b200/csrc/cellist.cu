@@ -203,12 +203,11 @@ __global__ void zero_forces_kernel(View v) {
   v.fz[i] = 0.0;
 }
 
-// ------------------------------------------------------------- annihilation
-struct Contact {
-  uint32_t a, b;   // owner, partner (indices)
-  uint64_t prio;   // (owner id << 32) | partner id
-};
-
+}  // namespace
+}  // namespace amk
+#include "contacts.cuh"
+namespace amk {
+namespace {
 __global__ void __launch_bounds__(128)
 contact_kernel(View v, const uint8_t* __restrict__ species, const uint32_t* __restrict__ ids,
                const unsigned long long* bb, double rc, double prob, uint32_t seed, uint64_t step,
@@ -259,67 +258,6 @@ contact_kernel(View v, const uint8_t* __restrict__ species, const uint32_t* __re
         }
       }
     }
-  }
-}
-
-// Greedy matching by locally-dominant selection, one CTA. Each round selects
-// every live contact whose priority is the minimum at both endpoints (these
-// are exactly the contacts the sequential greedy pass takes), then retires
-// contacts touching a matched particle. At least one contact (the global
-// minimum) is selected per round, so the loop ends within `m` rounds.
-__global__ void __launch_bounds__(1024)
-match_kernel(const Contact* __restrict__ e, long m, unsigned long long* best, uint8_t* matched, uint8_t* live_e,
-             uint8_t* alive, unsigned long long* result) {
-  __shared__ int s_remaining;
-  __shared__ unsigned long long s_marked;
-  for (long k = threadIdx.x; k < m; k += blockDim.x) {
-    live_e[k] = 1;
-    matched[e[k].a] = 0;
-    matched[e[k].b] = 0;
-  }
-  if (threadIdx.x == 0) s_marked = 0;
-  __syncthreads();
-  long rounds = 0;
-  for (;;) {
-    for (long k = threadIdx.x; k < m; k += blockDim.x)
-      if (live_e[k]) {
-        best[e[k].a] = ~0ull;
-        best[e[k].b] = ~0ull;
-      }
-    if (threadIdx.x == 0) s_remaining = 0;
-    __syncthreads();
-    for (long k = threadIdx.x; k < m; k += blockDim.x)
-      if (live_e[k]) {
-        atomicMin(&best[e[k].a], e[k].prio);
-        atomicMin(&best[e[k].b], e[k].prio);
-      }
-    __syncthreads();
-    for (long k = threadIdx.x; k < m; k += blockDim.x)
-      if (live_e[k] && best[e[k].a] == e[k].prio && best[e[k].b] == e[k].prio) {
-        matched[e[k].a] = 1;
-        matched[e[k].b] = 1;
-        alive[e[k].a] = 0;
-        alive[e[k].b] = 0;
-        atomicAdd(&s_marked, 2ull);
-      }
-    __syncthreads();
-    int rem = 0;
-    for (long k = threadIdx.x; k < m; k += blockDim.x)
-      if (live_e[k]) {
-        if (matched[e[k].a] || matched[e[k].b])
-          live_e[k] = 0;
-        else
-          rem = 1;
-      }
-    if (rem) atomicOr(&s_remaining, 1);
-    __syncthreads();
-    ++rounds;
-    if (s_remaining == 0 || rounds > m + 1) break;
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) {
-    result[0] = s_marked;
-    result[1] = s_remaining ? 1ull : 0ull;  // 1 = did not converge (cannot happen)
   }
 }
 
@@ -391,25 +329,22 @@ int cutoff_forces(amk_ctx* c, const View& v, double cutoff, double* energy_out) 
   return AMK_OK;
 }
 
-int annihilate_step(amk_ctx* c, uint64_t step_index, long* marked) {
+int annihilate_view(amk_ctx* c, const View& v, const uint8_t* species, const uint32_t* ids, double radius,
+                    double probability, uint32_t seed, uint64_t step_index, long* marked) {
   if (marked) *marked = 0;
-  const amk_params& p = c->p;
-  if (!(p.contact_radius > 0.0)) return AMK_OK;  // annihilation.cc:34-35
-  AMK_TRY(phase_begin(c, AMK_PHASE_ANNIHILATION));
-  View v = main_view(c);
+  if (!(radius > 0.0) || v.n == 0) return AMK_OK;  // annihilation.cc:34-35
   CellList cl;
-  AMK_TRY(build_cell_list(c, v, p.contact_radius, &cl));
+  AMK_TRY(build_cell_list(c, v, radius, &cl));
   int rc = AMK_OK;
   unsigned long long* counters = slot<unsigned long long>(c, kSlotAnnAux, 8, &rc);
   AMK_TRY(rc);
-  long cap = std::max<long>(1024, c->n / 16);
+  long cap = std::max<long>(1024, v.n / 16);
   for (int attempt = 0; attempt < 3; ++attempt) {
     Contact* edges = slot<Contact>(c, kSlotAnnEdges, static_cast<size_t>(cap), &rc);
     AMK_TRY(rc);
     AMK_CUDA_TRY(cudaMemsetAsync(counters, 0, 4 * sizeof(unsigned long long), c->stream));
-    contact_kernel<<<static_cast<unsigned>((c->n + 127) / 128), 128, 0, c->stream>>>(
-        v, c->species.as<uint8_t>(), c->ids.as<uint32_t>(), cl.bb, p.contact_radius, p.annihilation_probability,
-        static_cast<uint32_t>(p.seed), step_index, cl.skeys, cl.sidx, edges, counters, cap);
+    contact_kernel<<<static_cast<unsigned>((v.n + 127) / 128), 128, 0, c->stream>>>(
+        v, species, ids, cl.bb, radius, probability, seed, step_index, cl.skeys, cl.sidx, edges, counters, cap);
     AMK_TRY(check_launch(c, "contact_kernel"));
     unsigned long long m = 0;
     AMK_CUDA_TRY(cudaMemcpyAsync(&m, counters, sizeof(m), cudaMemcpyDeviceToHost, c->stream));
@@ -419,12 +354,12 @@ int annihilate_step(amk_ctx* c, uint64_t step_index, long* marked) {
       continue;
     }
     if (m == 0) break;
-    unsigned long long* best = slot<unsigned long long>(c, kSlotAnnBest, static_cast<size_t>(c->n), &rc);
+    unsigned long long* best = slot<unsigned long long>(c, kSlotAnnBest, static_cast<size_t>(v.n), &rc);
     AMK_TRY(rc);
-    uint8_t* flags = slot<uint8_t>(c, kSlotAuxState1, static_cast<size_t>(c->n) + static_cast<size_t>(m) + 16, &rc);
+    uint8_t* flags = slot<uint8_t>(c, kSlotAuxState1, static_cast<size_t>(v.n) + static_cast<size_t>(m) + 16, &rc);
     AMK_TRY(rc);
-    match_kernel<<<1, 1024, 0, c->stream>>>(edges, static_cast<long>(m), best, flags, flags + c->n,
-                                            c->alive.as<uint8_t>(), counters + 2);
+    match_kernel<<<1, 1024, 0, c->stream>>>(edges, static_cast<long>(m), nullptr, best, flags, flags + v.n, v.alive,
+                                            counters + 2);
     AMK_TRY(check_launch(c, "match_kernel"));
     unsigned long long res[2] = {0, 0};
     AMK_CUDA_TRY(cudaMemcpyAsync(res, counters + 2, sizeof(res), cudaMemcpyDeviceToHost, c->stream));
@@ -433,6 +368,16 @@ int annihilate_step(amk_ctx* c, uint64_t step_index, long* marked) {
     if (marked) *marked = static_cast<long>(res[0]);
     break;
   }
+  return AMK_OK;
+}
+
+int annihilate_step(amk_ctx* c, uint64_t step_index, long* marked) {
+  if (marked) *marked = 0;
+  const amk_params& p = c->p;
+  if (!(p.contact_radius > 0.0)) return AMK_OK;  // annihilation.cc:34-35
+  AMK_TRY(phase_begin(c, AMK_PHASE_ANNIHILATION));
+  AMK_TRY(annihilate_view(c, main_view(c), c->species.as<uint8_t>(), c->ids.as<uint32_t>(), p.contact_radius,
+                          p.annihilation_probability, static_cast<uint32_t>(p.seed), step_index, marked));
   AMK_TRY(phase_end(c, AMK_PHASE_ANNIHILATION));
   return AMK_OK;
 }

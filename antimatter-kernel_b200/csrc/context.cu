@@ -335,6 +335,7 @@ extern "C" int amk_destroy(amk_ctx* c) {
   cudaStreamSynchronize(c->stream);
   fmm_destroy(c);
   mlp_destroy(c);
+  batch_destroy(c);
   destroy_events(c);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -424,6 +425,7 @@ __global__ void max_abs_kernel(long n, const double* __restrict__ x, const doubl
 }
 
 static int finish_load(amk_ctx* c, long n) {
+  batch_destroy(c);  // instance offsets refer to the previous particle set
   c->n = n;
   c->ap_perm_n = -1;
   c->staggered = false;
@@ -760,6 +762,7 @@ extern "C" int amk_get_forces(amk_ctx* c, double* fx, double* fy, double* fz) {
 // of the same step uses that counter for its random stream.
 extern "C" int amk_push(amk_ctx* c) {
   if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (c->batch) return fail(AMK_ERR_STATE, "the context holds a batch: step it with amk_batch_step");
   if (c->n > 0) {
     AMK_TRY(push_step(c, static_cast<uint64_t>(c->step + 1)));
     c->stage_dirty = true;
@@ -770,6 +773,7 @@ extern "C" int amk_push(amk_ctx* c) {
 
 extern "C" int amk_annihilate(amk_ctx* c, long* marked) {
   if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (c->batch) return fail(AMK_ERR_STATE, "the context holds a batch: step it with amk_batch_step");
   if (marked) *marked = 0;
   if (c->n == 0 || !c->p.annihilation_enabled) return AMK_OK;
   AMK_TRY(annihilate_step(c, static_cast<uint64_t>(c->step > 0 ? c->step : 1), marked));
@@ -779,6 +783,7 @@ extern "C" int amk_annihilate(amk_ctx* c, long* marked) {
 
 extern "C" int amk_step(amk_ctx* c, int nsteps) {
   if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (c->batch) return fail(AMK_ERR_STATE, "the context holds a batch: step it with amk_batch_step");
   if (nsteps < 0) return fail(AMK_ERR_INVALID, "nsteps < 0");
   AMK_CUDA_TRY(cudaSetDevice(c->device));
   for (int s = 0; s < nsteps; ++s) {

@@ -1,127 +1,26 @@
-// Fused per-particle behaviours: LorentzForce::Run (Boris push in the ideal
-// Penning-trap field) followed by CyclotronCooling::Run (exact exponential
-// damping of v_perp plus Langevin noise). All arithmetic is FP64 in the
-// reference's operation order; the kernel is HBM-bound (x, v read and
-// written, F read and zeroed, q, m and alive read: 161 B per particle-step).
-#include "amk_internal.cuh"
-#include "philox.cuh"
+// Fused per-particle behaviours: LorentzForce::Run followed by
+// CyclotronCooling::Run (push.cuh holds the per-particle arithmetic). The
+// kernel is HBM-bound: x, v read and written, F read and zeroed, q, m, alive
+// and id read: 165 B per particle-step.
+#include "push.cuh"
 
 namespace amk {
 namespace {
 
-struct PushParams {
-  double radial;     // U / (2 d^2)      penning_trap.cc:22-33
-  double axial;      // U / d^2
-  double b0;         // B = (0, 0, b0)   penning_trap.cc:45-48
-  double dt;
-  int stagger;       // first call: v <- Boris(v, F, B, q, m, -dt/2)  lorentz.cc:56-60
-  int cooling;       // CyclotronCooling attached
-  double tau_scale;  // cooling_scale
-  double bath_temp;  // bath_temperature
-  uint32_t seed;
-  uint64_t step;
-};
-
-// BorisVelocity, lorentz.cc:18-35 (same operation order).
-__device__ __forceinline__ void boris(double v[3], const double f[3], const double b[3], double q, double m,
-                                      double dt) {
-  const double half_dt = 0.5 * dt;
-  double kick[3], vm[3], t[3], vp[3], s[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) kick[d] = f[d] * (half_dt / m);
-#pragma unroll
-  for (int d = 0; d < 3; ++d) vm[d] = v[d] + kick[d];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) t[d] = b[d] * (q * half_dt / m);
-  vp[0] = vm[0] + (vm[1] * t[2] - vm[2] * t[1]);
-  vp[1] = vm[1] + (vm[2] * t[0] - vm[0] * t[2]);
-  vp[2] = vm[2] + (vm[0] * t[1] - vm[1] * t[0]);
-  const double t2 = t[0] * t[0] + t[1] * t[1] + t[2] * t[2];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) s[d] = t[d] * (2.0 / (1.0 + t2));
-  const double px = vm[0] + (vp[1] * s[2] - vp[2] * s[1]);
-  const double py = vm[1] + (vp[2] * s[0] - vp[0] * s[2]);
-  const double pz = vm[2] + (vp[0] * s[1] - vp[1] * s[0]);
-  v[0] = px + kick[0];
-  v[1] = py + kick[1];
-  v[2] = pz + kick[2];
-}
-
 __global__ void __launch_bounds__(256)
-push_kernel(long n, double* __restrict__ x, double* __restrict__ y, double* __restrict__ z,
-            double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz,
-            double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
-            const double* __restrict__ q, const double* __restrict__ m, const uint8_t* __restrict__ alive,
-            const uint32_t* __restrict__ ids, PushParams P) {
-  const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
-  if (i >= n) return;
-  const bool live = alive[i] != 0;
-  const double qi = q[i], mi = m[i];
-  double px = x[i], py = y[i], pz = z[i];
-  if (live && mi > 0.0 && P.dt > 0.0) {
-    // ---- LorentzForce::Run, lorentz.cc:37-71
-    const double e[3] = {P.radial * px, P.radial * py, -P.axial * pz};
-    const double f[3] = {e[0] * qi + fx[i], e[1] * qi + fy[i], e[2] * qi + fz[i]};
-    const double b[3] = {0.0, 0.0, P.b0};
-    double v[3] = {vx[i], vy[i], vz[i]};
-    if (P.stagger) boris(v, f, b, qi, mi, -0.5 * P.dt);
-    boris(v, f, b, qi, mi, P.dt);
-    px = px + v[0] * P.dt;
-    py = py + v[1] * P.dt;
-    pz = pz + v[2] * P.dt;
-    fx[i] = 0.0;
-    fy[i] = 0.0;
-    fz[i] = 0.0;
-    // ---- CyclotronCooling::Run, cooling.cc:24-66
-    const double bmag = sqrt(P.b0 * P.b0);
-    if (P.cooling && qi != 0.0 && P.tau_scale > 0.0 && bmag > 0.0) {
-      const double aq = fabs(qi);
-      const double q2 = aq * aq;
-      const double denom = q2 * q2 * bmag * bmag;
-      const double tau_e = (0.75 / kCoulombConstant) * mi * mi * mi * kSpeedOfLight * kSpeedOfLight *
-                           kSpeedOfLight / denom;
-      const double tau = P.tau_scale * tau_e;
-      if (isfinite(tau)) {
-        const double bh[3] = {0.0, 0.0, P.b0 / bmag};
-        const double vpar = v[0] * bh[0] + v[1] * bh[1] + v[2] * bh[2];
-        const double vpv[3] = {bh[0] * vpar, bh[1] * vpar, bh[2] * vpar};
-        double vperp[3] = {v[0] - vpv[0], v[1] - vpv[1], v[2] - vpv[2]};
-        const double decay = exp(-P.dt / (2.0 * tau));
-#pragma unroll
-        for (int d = 0; d < 3; ++d) vperp[d] = vperp[d] * decay;
-        if (P.bath_temp > 0.0) {
-          const double sigma = sqrt(kBoltzmann * P.bath_temp / mi * (1.0 - decay * decay));
-          const Philox4 w = philox4x32(P.seed, kTagCooling, ids[i], static_cast<uint32_t>(P.step),
-                                       static_cast<uint32_t>(P.step >> 32), 0u);
-          const double u1 = u01(w.w[0]), u2 = u01(w.w[1]), u3 = u01(w.w[2]), u4 = u01(w.w[3]);
-          const double r1 = sqrt(-2.0 * log(u1));
-          const double r2 = sqrt(-2.0 * log(u3));
-          double noise[3] = {sigma * (r1 * cos(2.0 * kPi * u2)), sigma * (r1 * sin(2.0 * kPi * u2)),
-                             sigma * (r2 * cos(2.0 * kPi * u4))};
-          const double nb = noise[0] * bh[0] + noise[1] * bh[1] + noise[2] * bh[2];
-#pragma unroll
-          for (int d = 0; d < 3; ++d) noise[d] = noise[d] - bh[d] * nb;
-#pragma unroll
-          for (int d = 0; d < 3; ++d) vperp[d] = vperp[d] + noise[d];
-        }
-        v[0] = vpv[0] + vperp[0];
-        v[1] = vpv[1] + vperp[1];
-        v[2] = vpv[2] + vperp[2];
-      }
-    }
-    x[i] = px;
-    y[i] = py;
-    z[i] = pz;
-    vx[i] = v[0];
-    vy[i] = v[1];
-    vz[i] = v[2];
-  }
+push_kernel(long begin, long end, double* __restrict__ x, double* __restrict__ y, double* __restrict__ z,
+            double* __restrict__ vx, double* __restrict__ vy, double* __restrict__ vz, double* __restrict__ fx,
+            double* __restrict__ fy, double* __restrict__ fz, const double* __restrict__ q,
+            const double* __restrict__ m, const uint8_t* __restrict__ alive, const uint32_t* __restrict__ ids,
+            PushParams P, int stagger, uint64_t step) {
+  const long i = begin + blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (i >= end) return;
+  push_particle(i, x, y, z, vx, vy, vz, fx, fy, fz, q, m, alive, P, stagger, step, ids[i]);
 }
 
 }  // namespace
 
-int push_step(amk_ctx* c, uint64_t step_index) {
-  const amk_params& p = c->p;
+PushParams push_params_for(const amk_params& p) {
   const double d = sqrt((p.z0 * p.z0) / 2.0 + (p.rho0 * p.rho0) / 4.0);
   const double d2 = d * d;
   PushParams P;
@@ -129,19 +28,25 @@ int push_step(amk_ctx* c, uint64_t step_index) {
   P.axial = p.trap_voltage / d2;
   P.b0 = p.b0;
   P.dt = p.dt;
-  P.stagger = c->staggered ? 0 : 1;
   P.cooling = p.cooling_enabled ? 1 : 0;
   P.tau_scale = p.cooling_scale;
   P.bath_temp = p.bath_temperature;
   P.seed = static_cast<uint32_t>(p.seed);
-  P.step = step_index;
-  AMK_TRY(phase_begin(c, AMK_PHASE_PUSH));
-  const long n = c->n;
-  push_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, c->stream>>>(
-      n, c->x.as<double>(), c->y.as<double>(), c->z.as<double>(), c->vx.as<double>(), c->vy.as<double>(),
+  return P;
+}
+
+int push_range(amk_ctx* c, const PushParams& P, long begin, long end, bool stagger, uint64_t step_index) {
+  if (end <= begin) return AMK_OK;
+  push_kernel<<<static_cast<unsigned>((end - begin + 255) / 256), 256, 0, c->stream>>>(
+      begin, end, c->x.as<double>(), c->y.as<double>(), c->z.as<double>(), c->vx.as<double>(), c->vy.as<double>(),
       c->vz.as<double>(), c->fx.as<double>(), c->fy.as<double>(), c->fz.as<double>(), c->q.as<double>(),
-      c->m.as<double>(), c->alive.as<uint8_t>(), c->ids.as<uint32_t>(), P);
-  AMK_TRY(check_launch(c, "push_kernel"));
+      c->m.as<double>(), c->alive.as<uint8_t>(), c->ids.as<uint32_t>(), P, stagger ? 1 : 0, step_index);
+  return check_launch(c, "push_kernel");
+}
+
+int push_step(amk_ctx* c, uint64_t step_index) {
+  AMK_TRY(phase_begin(c, AMK_PHASE_PUSH));
+  AMK_TRY(push_range(c, push_params_for(c->p), 0, c->n, !c->staggered, step_index));
   AMK_TRY(phase_end(c, AMK_PHASE_PUSH));
   c->staggered = true;
   return AMK_OK;

@@ -314,6 +314,41 @@ int amk_fmm_audit(amk_ctx* ctx, int order, double theta, int learned, long sampl
  * last audit's RMS relative error. */
 int amk_fmm_learned_state(amk_ctx* ctx, int* trained, int* fallback, double* last_error);
 
+/* ------------------------------------------------------------ batched sweep */
+/* No counterpart in the reference, which runs one instance per process
+ * (antimatter-kernel.cc:153-162); a parameter sweep is many such runs. A
+ * batch splits the context's particle set into up to AMK_BATCH_MAX_INSTANCES
+ * independent instances: instance i owns particles [offsets[i],
+ * offsets[i+1]) (offsets[0] = 0, offsets[n_inst] = particle count) and
+ * steps with params[i] (trap, dt, cooling, annihilation, Coulomb method;
+ * seed per instance). Each instance gives the results it gives alone in a
+ * context of its own (random streams use the index within the instance).
+ * Setting a batch renumbers the particle ids within each instance; after it
+ * the single-instance amk_push / amk_annihilate / amk_step refuse the context
+ * (AMK_ERR_STATE) until amk_set_particles or amk_init_particles loads a new
+ * set. Per-instance learned FMM is not available (AMK_ERR_UNSUPPORTED). */
+#define AMK_BATCH_MAX_INSTANCES 512
+int amk_batch_set(amk_ctx* ctx, int n_inst, const amk_params* params, const long* offsets);
+/* nsteps steps of every instance. All-pairs instances share one persistent
+ * launch; cutoff, Barnes-Hut and FMM instances run their solver on their
+ * own slice. graph_chunk > 0 captures chunks of that many steps in a CUDA
+ * graph and replays them when no instance uses Barnes-Hut or the FMM (whose
+ * tree builds synchronise with the host). serial != 0 steps the instances
+ * one at a time with the single-instance kernels instead (the same results
+ * up to FP32 rounding of the all-pairs sums; the comparison baseline). */
+int amk_batch_step(amk_ctx* ctx, int nsteps, int graph_chunk, int serial);
+/* The Coulomb forces of every instance for the current positions (the first
+ * phase of a batched step), readable with amk_get_forces; the next step
+ * recomputes them. */
+int amk_batch_coulomb(amk_ctx* ctx);
+/* overflow: 1 if a step found more annihilation contacts than the batch's
+ * contact buffer (max(65536, n/8)) holds -- those beyond were dropped;
+ * alive_counts (n_inst entries, may be NULL): live particles per instance. */
+int amk_batch_status(amk_ctx* ctx, int* overflow, long* alive_counts);
+/* n_instances, all-pairs work units (instance, 128-target block) and
+ * whether the batch can run as CUDA graphs. */
+int amk_batch_info(const amk_ctx* ctx, long* n_instances, long* work_units, int* graphable);
+
 /* ------------------------------------------------------------ allocation-free */
 /* No counterpart in the reference. The cutoff Coulomb solver (same results
  * as amk_coulomb_standard / amk_solve_cutoff) for callers that cannot let a

@@ -1,0 +1,204 @@
+"""Batched multi-instance sweep: every instance of a batch must give what it
+gives alone in a context of its own (bit-exact where the kernels are the
+same, within the all-pairs tolerance where they differ), independently of
+the other instances in the batch, with or without CUDA graphs."""
+import numpy as np
+import pytest
+
+import amk
+import oracle_lib as O
+from conftest import E
+
+pytestmark = pytest.mark.gpu
+
+SPECIES = {"positron": 1, "electron": 3, "antiproton": 0, "proton": 4}
+
+
+def instance(n, seed, pair=("positron", "electron"), sigma=1e-4, vel=2e4, **over):
+    """Particles and params of one trap instance (seeded Gaussian cloud)."""
+    rng = np.random.default_rng(seed)
+    pos = rng.normal(0.0, sigma, (n, 3))
+    v = rng.normal(0.0, vel, (n, 3))
+    sp = np.where(np.arange(n) % 2 == 0, SPECIES[pair[0]], SPECIES[pair[1]]).astype(np.uint8)
+    kw = dict(seed=seed, b0=1.0 + 0.5 * (seed % 5), trap_voltage=10.0 + seed % 7, z0=0.01, rho0=0.01,
+              populations={pair[0]: n // 2, pair[1]: n - n // 2}, bath_temperature=4.0 + seed % 11,
+              cooling_scale=1e-9, coulomb_forces_enabled=1, coulomb_method="allpairs", cutoff_radius=1e-5,
+              annihilation_enabled=1, contact_radius=1.5e-5, annihilation_probability=0.5)
+    kw.update(over)
+    return pos, v, sp, amk.make_params(**kw)
+
+
+def load(sim, insts):
+    pos = np.concatenate([i[0] for i in insts])
+    vel = np.concatenate([i[1] for i in insts])
+    sp = np.concatenate([i[2] for i in insts])
+    sim.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
+    offsets = np.concatenate([[0], np.cumsum([len(i[0]) for i in insts])])
+    sim.batch_set([i[3] for i in insts], offsets)
+    return offsets
+
+
+def alone(inst, steps):
+    pos, vel, sp, p = inst
+    with amk.Simulation(p) as s:
+        s.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
+        s.step(steps)
+        return s.get_particles()
+
+
+def sliced(st, a, b):
+    return {k: v[a:b] for k, v in st.items()}
+
+
+def assert_same(a, b, keys=("x", "y", "z", "vx", "vy", "vz", "alive")):
+    for k in keys:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_push_cooling_annihilation_bit_exact_vs_single_instances():
+    # no Coulomb: push, cooling noise and annihilation use the same per-particle
+    # code and the same random streams as a context of its own
+    insts = [instance(600, 11, coulomb_forces_enabled=0), instance(17, 12, coulomb_forces_enabled=0),
+             instance(1500, 13, pair=("antiproton", "proton"), coulomb_forces_enabled=0),
+             instance(256, 14, coulomb_forces_enabled=0, annihilation_enabled=0),
+             instance(300, 15, coulomb_forces_enabled=0, cooling_enabled=0, contact_radius=4e-5,
+                      annihilation_probability=1.0)]
+    with amk.Simulation() as s:
+        off = load(s, insts)
+        s.batch_step(12)
+        st = s.get_particles()
+        status = s.batch_status()
+    assert not status["overflow"]
+    killed = 0
+    for i, inst in enumerate(insts):
+        ref = alone(inst, 12)
+        assert_same(sliced(st, off[i], off[i + 1]), ref)
+        assert status["alive"][i] == int(ref["alive"].sum())
+        killed += len(ref["alive"]) - int(ref["alive"].sum())
+    assert killed > 50  # the annihilation path did work
+
+
+def test_batched_allpairs_forces_match_fp64_oracle():
+    insts = [instance(3000, 21), instance(129, 22), instance(1, 23), instance(700, 24, sigma=3e-4)]
+    with amk.Simulation() as s:
+        off = load(s, insts)
+        s.batch_coulomb()
+        fx, fy, fz = s.get_forces()
+    for i, (pos, _, sp, _) in enumerate(insts):
+        q = np.where(np.isin(sp, (1, 4)), E, -E)
+        gx, gy, gz = O.allpairs(pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy(), q)
+        a, b = off[i], off[i + 1]
+        num = np.sqrt((fx[a:b] - gx) ** 2 + (fy[a:b] - gy) ** 2 + (fz[a:b] - gz) ** 2)
+        den = np.sqrt(gx ** 2 + gy ** 2 + gz ** 2)
+        if len(pos) == 1:
+            assert num.max() == 0.0
+            continue
+        assert np.sqrt(np.mean((num / den) ** 2)) < 1e-6, i
+        assert np.max(num / den) < 1e-5, i
+
+
+def test_instance_result_independent_of_batch_and_graphs():
+    insts = [instance(2000, 31), instance(500, 32), instance(90, 33, pair=("antiproton", "proton"))]
+    with amk.Simulation() as s:
+        off = load(s, insts)
+        s.batch_step(11)
+        full = s.get_particles()
+    with amk.Simulation() as s:
+        off2 = load(s, insts[1:2])
+        s.batch_step(11)
+        single = s.get_particles()
+    assert_same(sliced(full, off[1], off[2]), single)
+    # chunks of 4 steps captured in a CUDA graph: first step plain, two graph
+    # replays, two plain steps
+    with amk.Simulation() as s:
+        load(s, insts)
+        assert s.batch_info()["graphable"]
+        s.batch_step(11, graph_chunk=4)
+        graphed = s.get_particles()
+        assert s.step_count() == 11
+    assert_same(full, graphed)
+
+
+def test_allpairs_instances_track_single_instance_runs():
+    insts = [instance(1200, 41), instance(333, 42)]
+    with amk.Simulation() as s:
+        off = load(s, insts)
+        s.batch_step(3)
+        st = s.get_particles()
+    for i, inst in enumerate(insts):
+        ref = alone(inst, 3)
+        got = sliced(st, off[i], off[i + 1])
+        scale = np.max(np.abs(ref["x"]))
+        for k in ("x", "y", "z"):
+            assert np.max(np.abs(got[k] - ref[k])) <= 1e-9 * scale, k
+        assert np.array_equal(got["alive"], ref["alive"])
+
+
+def test_serial_baseline_matches_batched_step():
+    insts = [instance(900, 51), instance(64, 52), instance(2500, 53)]
+    with amk.Simulation() as s:
+        load(s, insts)
+        s.batch_step(3)
+        a = s.get_particles()
+    with amk.Simulation() as s:
+        load(s, insts)
+        s.batch_step(3, serial=True)
+        b = s.get_particles()
+    scale = np.max(np.abs(a["x"]))
+    for k in ("x", "y", "z"):
+        assert np.max(np.abs(a[k] - b[k])) <= 1e-9 * scale, k
+    assert np.array_equal(a["alive"], b["alive"])
+
+
+def test_per_instance_solvers_equal_single_instance_runs():
+    insts = [instance(800, 61, coulomb_method="standard", cutoff_radius=3e-5),
+             instance(1200, 62, coulomb_method="barnes-hut", barnes_hut_theta=0.5),
+             instance(3000, 63, coulomb_method="fast-multipole", fast_multipole_order=4,
+                      fast_multipole_theta=0.5),
+             instance(400, 64)]
+    with amk.Simulation() as s:
+        off = load(s, insts)
+        assert not s.batch_info()["graphable"]
+        s.batch_step(4, graph_chunk=2)
+        st = s.get_particles()
+    for i, inst in enumerate(insts[:3]):
+        assert_same(sliced(st, off[i], off[i + 1]), alone(inst, 4))
+
+
+def test_cutoff_batches_run_as_graphs():
+    insts = [instance(800, 71, coulomb_method="standard", cutoff_radius=3e-5), instance(300, 72)]
+    with amk.Simulation() as s:
+        off = load(s, insts)
+        assert s.batch_info()["graphable"]
+        s.batch_step(9, graph_chunk=4)
+        st = s.get_particles()
+    assert_same(sliced(st, off[0], off[1]), alone(insts[0], 9))
+
+
+def test_batch_argument_errors_and_state():
+    insts = [instance(100, 81), instance(50, 82)]
+    with amk.Simulation() as s:
+        pos = np.concatenate([i[0] for i in insts])
+        vel = np.concatenate([i[1] for i in insts])
+        sp = np.concatenate([i[2] for i in insts])
+        s.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
+        ps = [i[3] for i in insts]
+        with pytest.raises(amk.AmkError):
+            s.batch_step(1)  # no batch yet
+        with pytest.raises(amk.AmkError):
+            s.batch_set(ps, [0, 100, 149])  # does not end at the particle count
+        with pytest.raises(amk.AmkError):
+            s.batch_set(ps, [0, 120, 100])  # decreasing
+        with pytest.raises(amk.AmkError):
+            s.batch_set([ps[0]] * 513, np.zeros(514, np.int64))
+        learned = amk.make_params(coulomb_method="fast-multipole", fmm_learned=1)
+        with pytest.raises(amk.AmkError):
+            s.batch_set([ps[0], learned], [0, 100, 150])
+        s.batch_set(ps, [0, 100, 150])
+        with pytest.raises(amk.AmkError):
+            s.step(1)  # single-instance stepping refuses a batch
+        s.batch_step(2)
+        assert s.step_count() == 2
+        # loading a new particle set ends the batch
+        s.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
+        s.step(1)
