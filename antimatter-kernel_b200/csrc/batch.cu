@@ -281,9 +281,13 @@ batch_contact_kernel(long n, const double* __restrict__ x, const double* __restr
   }
 }
 
-// Records a contact-buffer overflow in the sticky status word.
+// Records a contact-buffer overflow in the sticky status word and in the
+// per-call word.
 __global__ void batch_overflow_kernel(const unsigned long long* contacts, long cap, unsigned long long* status) {
-  if (contacts[0] > static_cast<unsigned long long>(cap)) *status = 1ull;
+  if (contacts[0] > static_cast<unsigned long long>(cap)) {
+    status[0] = 1ull;
+    status[1] = 1ull;
+  }
 }
 
 __global__ void batch_alive_count_kernel(long n, const uint8_t* __restrict__ alive,
@@ -307,6 +311,7 @@ struct Batch {
   DevBuf inst, inst_of, units, counters, contacts, best, flags, keys, vals, skeys, sidx;
   long n_units = 0;
   long contact_cap = 0;
+  unsigned long long max_contacts = 0;  // largest contact count seen by a synchronised step
   int grid = 0;
   uint64_t step = 0;  // host mirror of the device step counter
   bool warm = false;  // one uncaptured step done (scratch reserved)
@@ -319,12 +324,31 @@ struct Batch {
     if (graph) cudaGraphDestroy(graph);
   }
   // counters (64-bit words): [0] queue head (int), [1] step, [2] contact
-  // count, [3..4] match result, [5] overflow status
+  // count, [3..4] match result, [5] sticky overflow status, [6] overflow
+  // inside the current call's graph replays
   int* queue() const { return counters.as<int>(); }
   unsigned long long* step_dev() const { return counters.as<unsigned long long>() + 1; }
   unsigned long long* contact_count() const { return counters.as<unsigned long long>() + 2; }
   unsigned long long* match_result() const { return counters.as<unsigned long long>() + 3; }
   unsigned long long* overflow() const { return counters.as<unsigned long long>() + 5; }
+  unsigned long long* call_overflow() const { return counters.as<unsigned long long>() + 6; }
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+    graph_steps = 0;
+  }
+  // Contact buffer of at least `cap` entries (drops a captured graph, which
+  // holds the old addresses).
+  int reserve_contacts(long cap, long n) {
+    if (cap <= contact_cap) return AMK_OK;
+    drop_graph();
+    AMK_TRY(contacts.reserve(static_cast<size_t>(cap) * sizeof(Contact)));
+    AMK_TRY(flags.reserve(static_cast<size_t>(std::max<long>(n, 1)) + static_cast<size_t>(cap)));
+    contact_cap = cap;
+    return AMK_OK;
+  }
 };
 
 void batch_destroy(amk_ctx* c) {
@@ -368,7 +392,10 @@ int instance_coulomb(amk_ctx* c, const Batch& B, int i) {
   }
 }
 
-int batch_annihilate(amk_ctx* c, Batch& B) {
+// `sync`: read the contact count back and enlarge the buffer and redo the
+// search when it overflowed (not possible inside a graph capture, where an
+// overflow is only recorded).
+int batch_annihilate(amk_ctx* c, Batch& B, bool sync) {
   const long n = c->n;
   const unsigned gb = static_cast<unsigned>((n + 255) / 256);
   AMK_TRY(phase_begin(c, AMK_PHASE_ANNIHILATION));
@@ -379,11 +406,21 @@ int batch_annihilate(amk_ctx* c, Batch& B) {
   AMK_TRY(check_launch(c, "batch_cell_key_kernel"));
   AMK_TRY(radix_sort_pairs(c, B.keys.as<uint64_t>(), B.vals.as<uint32_t>(), B.skeys.as<uint64_t>(),
                            B.sidx.as<uint32_t>(), n, kInstBits + 3 * kGridBits));
-  batch_contact_kernel<<<static_cast<unsigned>((n + 127) / 128), 128, 0, c->stream>>>(
-      n, c->x.as<double>(), c->y.as<double>(), c->z.as<double>(), c->species.as<uint8_t>(), c->ids.as<uint32_t>(),
-      B.inst_of.as<uint16_t>(), B.inst.as<InstanceDev>(), B.skeys.as<uint64_t>(), B.sidx.as<uint32_t>(),
-      B.step_dev(), B.contacts.as<Contact>(), B.contact_count(), B.contact_cap);
-  AMK_TRY(check_launch(c, "batch_contact_kernel"));
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    batch_contact_kernel<<<static_cast<unsigned>((n + 127) / 128), 128, 0, c->stream>>>(
+        n, c->x.as<double>(), c->y.as<double>(), c->z.as<double>(), c->species.as<uint8_t>(),
+        c->ids.as<uint32_t>(), B.inst_of.as<uint16_t>(), B.inst.as<InstanceDev>(), B.skeys.as<uint64_t>(),
+        B.sidx.as<uint32_t>(), B.step_dev(), B.contacts.as<Contact>(), B.contact_count(), B.contact_cap);
+    AMK_TRY(check_launch(c, "batch_contact_kernel"));
+    if (!sync) break;
+    unsigned long long m = 0;
+    AMK_CUDA_TRY(cudaMemcpyAsync(&m, B.contact_count(), sizeof(m), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    B.max_contacts = std::max(B.max_contacts, m);
+    if (m <= static_cast<unsigned long long>(B.contact_cap)) break;
+    AMK_TRY(B.reserve_contacts(static_cast<long>(m + m / 4 + 65536), n));
+    AMK_CUDA_TRY(cudaMemsetAsync(B.contact_count(), 0, sizeof(unsigned long long), c->stream));
+  }
   match_kernel<<<1, 1024, 0, c->stream>>>(B.contacts.as<Contact>(), B.contact_cap, B.contact_count(),
                                           B.best.as<unsigned long long>(), B.flags.as<uint8_t>(),
                                           B.flags.as<uint8_t>() + n, c->alive.as<uint8_t>(), B.match_result());
@@ -415,9 +452,10 @@ int batch_coulomb(amk_ctx* c, Batch& B) {
   return AMK_OK;
 }
 
-// One batched step; no host synchronisation unless a per-instance solver
-// needs one (Barnes-Hut, FMM).
-int batch_step_once(amk_ctx* c, Batch& B, bool stagger) {
+// One batched step; `sync` = false (graph capture) runs it without host
+// synchronisation, which needs every instance's solver to run without
+// (all-pairs, cutoff).
+int batch_step_once(amk_ctx* c, Batch& B, bool stagger, bool sync) {
   const long n = c->n;
   batch_begin_step_kernel<<<1, 1, 0, c->stream>>>(B.step_dev(), B.queue(), B.contact_count());
   AMK_TRY(check_launch(c, "batch_begin_step_kernel"));
@@ -431,7 +469,7 @@ int batch_step_once(amk_ctx* c, Batch& B, bool stagger) {
       B.inst.as<InstanceDev>(), B.step_dev(), stagger ? 1 : 0);
   AMK_TRY(check_launch(c, "batch_push_kernel"));
   AMK_TRY(phase_end(c, AMK_PHASE_PUSH));
-  if (B.any_annihilation) AMK_TRY(batch_annihilate(c, B));
+  if (B.any_annihilation) AMK_TRY(batch_annihilate(c, B, sync));
   return AMK_OK;
 }
 
@@ -537,7 +575,7 @@ extern "C" int amk_batch_set(amk_ctx* c, int n_inst, const amk_params* params, c
   std::vector<int2> hu(units.size());
   for (size_t k = 0; k < units.size(); ++k) hu[k] = units[k].second;
   B->n_units = static_cast<long>(hu.size());
-  B->contact_cap = std::max<long>(65536, n / 8);
+  B->contact_cap = 0;
   int sms = 148, per_sm = 1;
   AMK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
   AMK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_allpairs_kernel, kBT, 0));
@@ -547,9 +585,8 @@ extern "C" int amk_batch_set(amk_ctx* c, int n_inst, const amk_params* params, c
   AMK_TRY(B->inst_of.reserve(nn * sizeof(uint16_t)));
   AMK_TRY(B->units.reserve(std::max<size_t>(1, hu.size()) * sizeof(int2)));
   AMK_TRY(B->counters.reserve(64));
-  AMK_TRY(B->contacts.reserve(B->contact_cap * sizeof(Contact)));
+  AMK_TRY(B->reserve_contacts(std::max<long>(65536, n / 8), n));
   AMK_TRY(B->best.reserve(nn * sizeof(unsigned long long)));
-  AMK_TRY(B->flags.reserve(nn + B->contact_cap));
   AMK_TRY(B->keys.reserve(nn * sizeof(uint64_t)));
   AMK_TRY(B->vals.reserve(nn * sizeof(uint32_t)));
   AMK_TRY(B->skeys.reserve(nn * sizeof(uint64_t)));
@@ -581,10 +618,11 @@ extern "C" int amk_batch_step(amk_ctx* c, int nsteps, int graph_chunk, int seria
   AMK_CUDA_TRY(cudaSetDevice(c->device));
   const bool use_graph = graph_chunk > 0 && !serial && B.graphable && !c->profiling;
   int done = 0;
+  bool graphed = false;
   while (done < nsteps) {
     const bool stagger = !c->staggered;
     if (!use_graph || !B.warm || stagger || nsteps - done < graph_chunk) {
-      AMK_TRY(serial ? serial_step_once(c, B, stagger) : batch_step_once(c, B, stagger));
+      AMK_TRY(serial ? serial_step_once(c, B, stagger) : batch_step_once(c, B, stagger, true));
       c->staggered = true;
       B.warm = true;
       B.step++;
@@ -593,14 +631,14 @@ extern "C" int amk_batch_step(amk_ctx* c, int nsteps, int graph_chunk, int seria
       continue;
     }
     if (!B.exec || B.graph_steps != graph_chunk) {
-      if (B.exec) cudaGraphExecDestroy(B.exec);
-      if (B.graph) cudaGraphDestroy(B.graph);
-      B.exec = nullptr;
-      B.graph = nullptr;
+      B.drop_graph();
+      // head room over the largest contact count seen so far: inside the
+      // graph an overflow can only be recorded
+      AMK_TRY(B.reserve_contacts(static_cast<long>(2 * B.max_contacts), c->n));
       const long launches0 = c->kernel_launches;
       AMK_CUDA_TRY(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
       int rc = AMK_OK;
-      for (int s = 0; s < graph_chunk && rc == AMK_OK; ++s) rc = batch_step_once(c, B, false);
+      for (int s = 0; s < graph_chunk && rc == AMK_OK; ++s) rc = batch_step_once(c, B, false, false);
       cudaGraph_t g = nullptr;
       const cudaError_t e = cudaStreamEndCapture(c->stream, &g);
       B.graph_launches = c->kernel_launches - launches0;
@@ -614,6 +652,8 @@ extern "C" int amk_batch_step(amk_ctx* c, int nsteps, int graph_chunk, int seria
       AMK_CUDA_TRY(cudaGraphInstantiate(&B.exec, B.graph, 0));
       B.graph_steps = graph_chunk;
     }
+    if (!graphed) AMK_CUDA_TRY(cudaMemsetAsync(B.call_overflow(), 0, sizeof(unsigned long long), c->stream));
+    graphed = true;
     AMK_CUDA_TRY(cudaGraphLaunch(B.exec, c->stream));
     c->kernel_launches += B.graph_launches;
     B.step += static_cast<uint64_t>(graph_chunk);
@@ -621,6 +661,18 @@ extern "C" int amk_batch_step(amk_ctx* c, int nsteps, int graph_chunk, int seria
     done += graph_chunk;
   }
   c->stage_dirty = true;
+  if (graphed) {
+    unsigned long long ov = 0;
+    AMK_CUDA_TRY(cudaMemcpyAsync(&ov, B.call_overflow(), sizeof(ov), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (ov) {
+      AMK_TRY(B.reserve_contacts(2 * B.contact_cap, c->n));  // the next capture gets a larger buffer
+      return fail(AMK_ERR_LIMIT,
+                  "annihilation contacts overflowed the contact buffer inside a CUDA graph chunk: the "
+                  "steps of this call dropped contacts (the buffer is now larger; step without graphs "
+                  "to avoid it)");
+    }
+  }
   return AMK_OK;
 }
 

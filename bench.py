@@ -68,7 +68,60 @@ def workload_direct65k():
     return p, config
 
 
-WORKLOADS = {"direct65k": workload_direct65k}
+KB = 1.380649e-23
+MASS = {0: 1.67262192369e-27, 1: 9.1093837015e-31, 3: 9.1093837015e-31, 4: 1.67262192369e-27}
+
+
+def make_sweep(n_inst=512, seed=2024, method_split=8192, order=4):
+    """The batched sweep: n_inst independent trap instances, populations
+    log-uniform in [1e2, 1e5] (even, 1:1 species pairs e-/e+ or e+/pbar per
+    instance), temperatures log-uniform 4..1e4 K, b0 U(1, 5) T, trap_voltage
+    U(5, 50) V, cloud radii U(5e-5, 5e-4) m per axis (uniform ellipsoid),
+    Maxwellian velocities, cooling (bath 4 K, scale 1) and annihilation
+    (contact 5e-6 m, p = 0.5) on. Coulomb: all-pairs below `method_split`
+    particles, FMM of `order` (theta 0.5) from there (method_split=None: all
+    instances all-pairs). Returns [(pos, vel, species, params)]."""
+    import amk
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n_inst):
+        n = max(2, int(round(10 ** rng.uniform(2.0, 5.0))) // 2 * 2)
+        pair = (3, 1) if rng.random() < 0.5 else (1, 0)  # (electron, positron) / (positron, antiproton)
+        temp = 10 ** rng.uniform(np.log10(4.0), 4.0)
+        b0 = rng.uniform(1.0, 5.0)
+        volt = rng.uniform(5.0, 50.0)
+        radii = rng.uniform(5e-5, 5e-4, 3)
+        d = rng.normal(size=(n, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        pos = d * rng.random((n, 1)) ** (1.0 / 3.0) * radii
+        sp = np.repeat(np.array(pair, np.uint8), n // 2)
+        m = np.array([MASS[int(k)] for k in pair]).repeat(n // 2)
+        vel = rng.normal(size=(n, 3)) * np.sqrt(KB * temp / m)[:, None]
+        names = {0: "antiproton", 1: "positron", 3: "electron"}
+        method = "allpairs" if method_split is None or n < method_split else "fast-multipole"
+        p = amk.make_params(seed=1000 + i, b0=b0, trap_voltage=volt, z0=0.01, rho0=0.01,
+                            populations={names[pair[0]]: n // 2, names[pair[1]]: n // 2},
+                            temperatures={names[pair[0]]: temp, names[pair[1]]: temp},
+                            cloud_radii=tuple(radii), bath_temperature=4.0, cooling_scale=1.0,
+                            cooling_enabled=1, coulomb_forces_enabled=1, coulomb_method=method,
+                            energy_method="allpairs", cutoff_radius=1e-5, fast_multipole_order=order,
+                            fast_multipole_theta=0.5, annihilation_enabled=1, contact_radius=5e-6,
+                            annihilation_probability=0.5)
+        out.append((pos, vel, sp, p))
+    return out
+
+
+def load_sweep(sim, insts):
+    pos = np.concatenate([i[0] for i in insts])
+    vel = np.concatenate([i[1] for i in insts])
+    sp = np.concatenate([i[2] for i in insts])
+    sim.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
+    offsets = np.concatenate([[0], np.cumsum([len(i[0]) for i in insts])])
+    sim.batch_set([i[3] for i in insts], offsets)
+    return pos, vel, sp, offsets
+
+
+WORKLOADS = {"direct65k": workload_direct65k, "sweep512": None}
 
 
 # ------------------------------------------------------------------ clocks
@@ -208,6 +261,234 @@ def run_reference(args):
                              "sample": f"per step: tree over all {len(x)} sources, theta=0 walks for "
                                        f"{sample} sampled targets extrapolated to {len(x)}, FP64 "
                                        f"push of all {len(x)}"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ batched sweep
+def cpu_sweep_step_time(insts, n_sample=64):
+    """Reference CPU step of every instance on a bounded sample: the
+    reference's Barnes-Hut tree at theta = 0 (exact all-pairs) built over
+    each instance's sources and walked for up to n_sample targets,
+    extrapolated to the instance, plus the FP64 push of every particle."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_lib as O
+    total = 0.0
+    kind = "reference" if O.ref_available() else "port"
+    for pos, vel, sp, p in insts:
+        n = len(pos)
+        m, q = O.species_props(sp)
+        x, y, z = pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy()
+        k = min(n, n_sample)
+        targets = np.arange(k) * (n // k)
+        t_build = 0.0
+        if kind == "reference":
+            t0 = time.perf_counter()
+            O.ref_bh_forces_subset(x, y, z, q, 0.0, targets[:1], 8)  # tree build + one walk
+            t_build = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            O.ref_bh_forces_subset(x, y, z, q, 0.0, targets, 8)
+            t_walk = max(time.perf_counter() - t0 - t_build, 1e-9)
+        else:
+            t0 = time.perf_counter()
+            O.allpairs_subset(x, y, z, q, targets)
+            t_walk = time.perf_counter() - t0
+        state = dict(x=x, y=y, z=z, vx=vel[:, 0].copy(), vy=vel[:, 1].copy(), vz=vel[:, 2].copy(),
+                     q=q, m=m, alive=np.ones(n, np.uint8))
+        t0 = time.perf_counter()
+        O.boris_push(state, np.zeros(n), np.zeros(n), np.zeros(n), p.b0, p.trap_voltage, p.z0, p.rho0,
+                     p.dt, True)
+        t_push = time.perf_counter() - t0
+        total += t_build + t_walk * n / k + t_push
+    return total, kind
+
+
+def run_sweep(args):
+    """Batched 512-instance sweep: batched step (one persistent all-pairs
+    launch, CUDA-graph chunks) against the same instances stepped one at a
+    time with the single-instance kernels."""
+    import torch
+    import amk
+    world, rank, local = dist_setup()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    # every rank runs its own sweep of 512 instances (seeded by rank): the
+    # instances are independent, so the sweep shards with no collective
+    insts = make_sweep(seed=2024 + rank, method_split=None)
+    n_total = int(sum(len(i[0]) for i in insts))
+    sim = amk.Simulation(device=local)
+    load_sweep(sim, insts)
+    chunk = min(100, args.steps)
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def timed(fn):
+        # events on the stream of the context in use (contexts are replaced below)
+        st = torch.cuda.ExternalStream(sim.stream(), device=device)
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(st)
+        fn()
+        ev1.record(st)
+        torch.cuda.synchronize()
+        barrier()
+        return ev0.elapsed_time(ev1)
+
+    # warm-up: plain steps (the first is the staggered one), then one chunk to
+    # capture and instantiate the graph outside the timed region
+    sim.batch_step(args.warmup)
+    sim.batch_step(chunk, graph_chunk=chunk)
+    sim.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = sim.kernel_launches()
+    ms = timed(lambda: sim.batch_step(args.steps, graph_chunk=chunk))
+    launches = sim.kernel_launches() - launches0
+    clocks = sampler.stop()
+    ms = max_over_ranks(ms, world, device)
+    value = world * n_total * args.steps / (ms * 1e-3)
+
+    # per-phase device time (profiling runs plain steps, no graph)
+    prof_steps = 2
+    sim.set_profiling(True)
+    sim.reset_phase_times()
+    sim.batch_step(prof_steps)
+    sim.synchronize()
+    phases = sim.phase_times()
+    sim.set_profiling(False)
+    ap_ms, ap_launches = phases["allpairs"]
+    ap_avg = ap_ms / max(ap_launches, 1)
+    pairs = float(sum(len(i[0]) * (len(i[0]) - 1) for i in insts))
+    peak = sim.measure_fp32_peak()
+    achieved = 20.0 * pairs / (ap_avg * 1e-3) / 1e12
+    roofline = {"bound": "fp32", "kernel": "batch_allpairs_kernel", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "peak_source": "measured in this run: FFMA probe kernel over all SMs (2 flop/FFMA)",
+                "flops_per_launch": 20.0 * pairs,
+                "flop_convention": "20 flop per pair interaction x sum_i N_i(N_i-1)",
+                "avg_launch_ms": ap_avg,
+                "phase_ms_per_step": {k: v[0] / prof_steps for k, v in phases.items() if v[1]}}
+
+    # baseline: the same instances one at a time with the single-instance kernels
+    serial_steps = max(1, min(args.steps, args.serial_steps))
+    serial_ms = max_over_ranks(timed(lambda: sim.batch_step(serial_steps, serial=True)), world, device)
+    serial_value = world * n_total * serial_steps / (serial_ms * 1e-3)
+    sim.close()
+    # the sweep's own method split (FMM p=4 from 8,192 particles), both ways
+    split = make_sweep(seed=2024 + rank, method_split=8192, order=4)
+    sim = amk.Simulation(device=local)
+    load_sweep(sim, split)
+    sim.batch_step(args.warmup)
+    split_ms = max_over_ranks(timed(lambda: sim.batch_step(serial_steps)), world, device)
+    split_serial_ms = max_over_ranks(timed(lambda: sim.batch_step(serial_steps, serial=True)), world, device)
+
+    # end to end through the C ABI with host buffers (one step per call)
+    L = amk.lib()
+    sim.close()
+    sim = amk.Simulation(device=local)
+    load_sweep(sim, insts)
+    sim.batch_step(args.warmup)
+    host = {k: torch.empty(n_total, dtype=torch.float64, pin_memory=True) for k in
+            ("x", "y", "z", "vx", "vy", "vz")}
+    alive = torch.empty(n_total, dtype=torch.uint8, pin_memory=True)
+    order = ("x", "y", "z", "vx", "vy", "vz")
+    ptr = {k: v.data_ptr() for k, v in host.items()}
+    amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k]) for k in order],
+                                  C.cast(C.c_void_p(alive.data_ptr()), C.POINTER(C.c_uint8))))
+    e2e_steps = max(1, min(args.steps, 10))
+
+    def e2e_loop():
+        for _ in range(e2e_steps):
+            sim.update_state(*[ptr[k2] for k2 in order])
+            sim.batch_step(1)
+            amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k2]) for k2 in order],
+                                          C.cast(C.c_void_p(alive.data_ptr()), C.POINTER(C.c_uint8))))
+    e2e_ms = max_over_ranks(timed(e2e_loop), world, device)
+    e2e = {"value": world * n_total * e2e_steps / (e2e_ms * 1e-3), "unit": UNIT,
+           "h2d_bytes_per_step": 6 * 8 * n_total, "d2h_bytes_per_step": 6 * 8 * n_total + n_total,
+           "steps": e2e_steps,
+           "api": "amk_update_state + amk_batch_step + amk_get_particles (pinned host buffers)"}
+    status = sim.batch_status()
+    sim.close()
+
+    cpu = None
+    if rank == 0 and world == 1:
+        t_cpu, kind = cpu_sweep_step_time(insts)
+        cpu = {"value": n_total / t_cpu, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
+               "sample": "per instance: reference Barnes-Hut theta=0 tree over all its sources walked "
+                         "for 64 evenly spaced targets (extrapolated), + FP64 push of all particles; "
+                         "all 512 instances, OpenMP on all host cores"}
+    if rank == 0:
+        sizes = np.array([len(i[0]) for i in insts])
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+                "data": "synthetic (seeded sweep generator)",
+                "config": {"workload": "batched sweep: 512 trap instances, N_i log-uniform 1e2..1e5 "
+                                       f"(total {n_total:,}), e-/e+ or e+/pbar 1:1, T 4..1e4 K, b0 1..5 T, "
+                                       "U 5..50 V, radii 5e-5..5e-4 m, cooling (4 K) and annihilation "
+                                       "(5e-6 m, p=0.5) on",
+                           "solver": "all-pairs for every instance (one persistent launch, "
+                                     "cost-ordered work queue), FP64 state",
+                           "graph_chunk": chunk, "instances": len(insts), "n_particles": n_total,
+                           "instance_sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)),
+                                              "max": int(sizes.max())},
+                           "l2": "not flushed: state of 7.4 M particles (> 700 MB) exceeds L2",
+                           "parallelism": f"dp{world}: one 512-instance sweep per GPU, no collective"},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clocks,
+                "one_at_a_time": {"value": serial_value, "steps": serial_steps,
+                                  "ms_per_step": serial_ms / serial_steps,
+                                  "speedup_batched": value / serial_value,
+                                  "api": "amk_batch_step(serial=1): each instance through the "
+                                         "single-instance kernels, one after another"},
+                "method_split_8192_fmm_p4": {
+                    "batched_value": world * n_total * serial_steps / (split_ms * 1e-3),
+                    "one_at_a_time_value": world * n_total * serial_steps / (split_serial_ms * 1e-3),
+                    "note": "all-pairs below 8,192 particles, FMM p=4 theta=0.5 above (RMS error "
+                            "about 7e-5, above the 1e-5 bar); per-instance FMM calls synchronise "
+                            "with the host, so no graphs"},
+                "contact_overflow": bool(status["overflow"])}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def run_reference_sweep(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    insts = make_sweep(seed=2024, method_split=None)
+    n_total = int(sum(len(i[0]) for i in insts))
+    times = []
+    kind = "reference"
+    for k in range(args.warmup + args.steps):
+        t, kind = cpu_sweep_step_time(insts, n_sample=16)
+        if k >= args.warmup:
+            times.append(t)
+    t_step = float(np.mean(times))
+    value = n_total / t_step
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded sweep generator)",
+            "config": {"workload": f"batched sweep: 512 trap instances, {n_total:,} particles"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
+                             "sample": "per instance and step: theta=0 tree over all sources, 16 "
+                                       "targets walked (extrapolated), FP64 push of all"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -377,10 +658,16 @@ def main():
                     help="targets walked by the CPU baseline leg")
     ap.add_argument("--ref-sample", type=int, default=256,
                     help="targets walked per step by the reference arm")
+    ap.add_argument("--serial-steps", type=int, default=3,
+                    help="steps of the one-at-a-time comparison (sweep workload)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least three untimed warm-up steps
     if args.impl == "reference":
+        if args.workload == "sweep512":
+            return run_reference_sweep(args)
         return run_reference(args)
+    if args.workload == "sweep512":
+        return run_sweep(args)
     return run_amk(args)
 
 

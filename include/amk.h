@@ -341,9 +341,12 @@ int amk_batch_step(amk_ctx* ctx, int nsteps, int graph_chunk, int serial);
  * phase of a batched step), readable with amk_get_forces; the next step
  * recomputes them. */
 int amk_batch_coulomb(amk_ctx* ctx);
-/* overflow: 1 if a step found more annihilation contacts than the batch's
- * contact buffer (max(65536, n/8)) holds -- those beyond were dropped;
- * alive_counts (n_inst entries, may be NULL): live particles per instance. */
+/* overflow: 1 if a step inside a CUDA graph chunk found more annihilation
+ * contacts than the contact buffer held (those beyond were dropped; that
+ * amk_batch_step call returned AMK_ERR_LIMIT). Steps outside graphs read the
+ * contact count back and enlarge the buffer instead; a graph is captured with
+ * twice the largest count seen so far. alive_counts (n_inst entries, may be
+ * NULL): live particles per instance. */
 int amk_batch_status(amk_ctx* ctx, int* overflow, long* alive_counts);
 /* n_instances, all-pairs work units (instance, 128-target block) and
  * whether the batch can run as CUDA graphs. */
