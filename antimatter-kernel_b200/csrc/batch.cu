@@ -47,8 +47,10 @@ struct InstanceDev {
   PushParams push;
   double contact_radius, probability;  // annihilation
   double inv_l;                        // 1 / length scale (a power of two)
-  double origin[3], inv_cell;          // annihilation grid
+  double origin[3], inv_cell;          // annihilation grid (cells >= the contact radius)
+  double inv_sort_cell;                // all-pairs ordering grid: 1022 cells over the same cube
   long offset, count;
+  long tile0;                          // first all-pairs tile of the instance
   int annihilation;
   uint32_t seed;
 };
@@ -67,81 +69,203 @@ __global__ void batch_local_ids_kernel(long n, const uint16_t* __restrict__ inst
   ids[i] = static_cast<uint32_t>(i - inst[inst_of[i]].offset);
 }
 
-// Double-float staging with the instance's length scale: x / L = hq + lo.
-__global__ void batch_stage_kernel(long n, const double* __restrict__ x, const double* __restrict__ y,
-                                   const double* __restrict__ z, const double* __restrict__ q,
-                                   const uint8_t* __restrict__ alive, const uint16_t* __restrict__ inst_of,
-                                   const InstanceDev* __restrict__ inst, float4* __restrict__ hq,
-                                   float4* __restrict__ lo) {
+// ---------------------------------------------------------------- all-pairs
+// Per step, every particle gets the key (instance << 30 | 30-bit Morton cell
+// in its instance's grid); usable particles (alive, charged, finite) sort
+// before the others of their instance. The stable sort keeps each instance
+// inside its own [offset, offset + count) range, so sorted position k holds
+// a particle of the same instance as original index k. Tiles of 128 sorted
+// positions within an instance get a box; tile pairs whose boxes are
+// separated by more than their half-extents use FP32 offsets from the source
+// tile's centre (12 FP32 ops per pair), the others exact double-float
+// differences (18 ops per pair, the self pair gives exactly 0).
+__global__ void batch_sort_key_kernel(long n, const double* __restrict__ x, const double* __restrict__ y,
+                                      const double* __restrict__ z, const double* __restrict__ q,
+                                      const uint8_t* __restrict__ alive, const uint16_t* __restrict__ inst_of,
+                                      const InstanceDev* __restrict__ inst, uint64_t* __restrict__ keys,
+                                      uint32_t* __restrict__ vals) {
   const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
   if (i >= n) return;
-  const double inv_l = inst[inst_of[i]].inv_l;
-  const double xs = x[i] * inv_l, ys = y[i] * inv_l, zs = z[i] * inv_l;
-  const bool ok = alive[i] && q[i] != 0.0 && isfinite(xs) && isfinite(ys) && isfinite(zs);
-  float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
-  if (ok) {
-    h = make_float4(__double2float_rn(xs), __double2float_rn(ys), __double2float_rn(zs),
-                    __double2float_rn(q[i] / kElementaryCharge));
-    l = make_float4(__double2float_rn(xs - static_cast<double>(h.x)), __double2float_rn(ys - static_cast<double>(h.y)),
-                    __double2float_rn(zs - static_cast<double>(h.z)), 0.f);
+  vals[i] = static_cast<uint32_t>(i);
+  const uint16_t k = inst_of[i];
+  const InstanceDev& I = inst[k];
+  const uint64_t prefix = static_cast<uint64_t>(k) << 30;
+  if (!alive[i] || q[i] == 0.0 || !isfinite(x[i]) || !isfinite(y[i]) || !isfinite(z[i])) {
+    keys[i] = prefix | ((1ull << 30) - 1ull);
+    return;
   }
-  hq[i] = h;
-  lo[i] = l;
+  const double p[3] = {x[i], y[i], z[i]};
+  uint32_t c[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d)
+    c[d] = static_cast<uint32_t>(fmin(fmax(floor((p[d] - I.origin[d]) * I.inv_sort_cell), 0.0), 1022.0));
+  keys[i] = prefix | morton3_21(c[0], c[1], c[2]);
 }
 
-// Persistent all-pairs over (instance, target block) units; `queue` is the
-// work-queue head, zeroed before every launch. F_i = k e q_i / L^2 *
-// sum_j q_j (r_i - r_j) / |r_i - r_j|^3 in scaled units.
+struct TileBox {
+  float4 c;   // centre (scaled, hi part); w = 1 when the tile has usable particles
+  float4 cl;  // centre, lo part
+  float4 h;   // half-extents (rounded up); w = |h|
+};
+
+// One CTA per all-pairs unit = tile of up to 128 sorted positions: the
+// double-float staging, the offsets from the tile centre and the tile box.
+__global__ void __launch_bounds__(kBT)
+batch_tile_stage_kernel(const int2* __restrict__ units, const InstanceDev* __restrict__ inst,
+                        const uint32_t* __restrict__ perm, const double* __restrict__ x,
+                        const double* __restrict__ y, const double* __restrict__ z, const double* __restrict__ q,
+                        const uint8_t* __restrict__ alive, float4* __restrict__ hq, float4* __restrict__ lo,
+                        float4* __restrict__ rel, TileBox* __restrict__ boxes) {
+  __shared__ double red[6][kBT / 32];
+  __shared__ double box[6];
+  const int2 un = units[blockIdx.x];
+  const InstanceDev& I = inst[un.x];
+  const long e = I.offset + I.count;
+  const long k = I.offset + static_cast<long>(un.y) * kBT + threadIdx.x;
+  double xs = 0.0, ys = 0.0, zs = 0.0, qe = 0.0;
+  bool ok = false;
+  if (k < e) {
+    const long i = perm[k];
+    xs = x[i] * I.inv_l;
+    ys = y[i] * I.inv_l;
+    zs = z[i] * I.inv_l;
+    ok = alive[i] && q[i] != 0.0 && isfinite(xs) && isfinite(ys) && isfinite(zs);
+    qe = q[i] / kElementaryCharge;
+  }
+  double m[6] = {ok ? xs : INFINITY, ok ? ys : INFINITY, ok ? zs : INFINITY,
+                 ok ? -xs : INFINITY, ok ? -ys : INFINITY, ok ? -zs : INFINITY};
+#pragma unroll
+  for (int d = 0; d < 6; ++d)
+    for (int o = 16; o > 0; o >>= 1) m[d] = fmin(m[d], __shfl_xor_sync(0xffffffffu, m[d], o));
+  if ((threadIdx.x & 31) == 0)
+    for (int d = 0; d < 6; ++d) red[d][threadIdx.x >> 5] = m[d];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    double r = INFINITY;
+    for (int w = 0; w < kBT / 32; ++w) r = fmin(r, red[threadIdx.x][w]);
+    box[threadIdx.x] = r;
+  }
+  __syncthreads();
+  const bool any = isfinite(box[0]);
+  const double cx = any ? 0.5 * (box[0] - box[3]) : 0.0;
+  const double cy = any ? 0.5 * (box[1] - box[4]) : 0.0;
+  const double cz = any ? 0.5 * (box[2] - box[5]) : 0.0;
+  float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h, u = h;
+  if (ok) {
+    h = make_float4(__double2float_rn(xs), __double2float_rn(ys), __double2float_rn(zs), __double2float_rn(qe));
+    l = make_float4(__double2float_rn(xs - static_cast<double>(h.x)), __double2float_rn(ys - static_cast<double>(h.y)),
+                    __double2float_rn(zs - static_cast<double>(h.z)), 0.f);
+    u = make_float4(__double2float_rn(xs - cx), __double2float_rn(ys - cy), __double2float_rn(zs - cz), h.w);
+  }
+  if (k < e) {
+    hq[k] = h;
+    lo[k] = l;
+    rel[k] = u;
+  }
+  if (threadIdx.x == 0) {
+    TileBox b;
+    b.c = make_float4(__double2float_rn(cx), __double2float_rn(cy), __double2float_rn(cz), any ? 1.f : 0.f);
+    b.cl = make_float4(__double2float_rn(cx - static_cast<double>(b.c.x)),
+                       __double2float_rn(cy - static_cast<double>(b.c.y)),
+                       __double2float_rn(cz - static_cast<double>(b.c.z)), 0.f);
+    const double hx = any ? 0.5 * (-box[3] - box[0]) : 0.0;
+    const double hy = any ? 0.5 * (-box[4] - box[1]) : 0.0;
+    const double hz = any ? 0.5 * (-box[5] - box[2]) : 0.0;
+    b.h = make_float4(__double2float_ru(hx), __double2float_ru(hy), __double2float_ru(hz),
+                      __double2float_ru(sqrt(hx * hx + hy * hy + hz * hz)));
+    boxes[I.tile0 + un.y] = b;
+  }
+}
+
+// Persistent all-pairs over (instance, target tile) units taken from a queue
+// (`queue` zeroed before every launch): F_i = k e q_i / L^2 * sum_j q_j
+// (r_i - r_j) / |r_i - r_j|^3 in scaled units, written to the particle's
+// original index.
 __global__ void __launch_bounds__(kBT)
 batch_allpairs_kernel(const int2* __restrict__ units, int n_units, const InstanceDev* __restrict__ inst,
-                      const float4* __restrict__ hq, const float4* __restrict__ lo, const double* __restrict__ q,
-                      double* __restrict__ fx, double* __restrict__ fy, double* __restrict__ fz,
-                      int* __restrict__ queue) {
-  __shared__ float4 sh[kBT], sl[kBT];
+                      const float4* __restrict__ hq, const float4* __restrict__ lo, const float4* __restrict__ rel,
+                      const TileBox* __restrict__ boxes, const uint32_t* __restrict__ perm,
+                      const double* __restrict__ q, double* __restrict__ fx, double* __restrict__ fy,
+                      double* __restrict__ fz, int* __restrict__ queue) {
+  __shared__ float4 sa[kBT], sb[kBT];
   __shared__ int s_unit;
+  const int tid = threadIdx.x;
   for (;;) {
-    if (threadIdx.x == 0) s_unit = atomicAdd(queue, 1);
+    if (tid == 0) s_unit = atomicAdd(queue, 1);
     __syncthreads();
     const int u = s_unit;
     if (u >= n_units) return;
     const int2 un = units[u];
     const long b = inst[un.x].offset, e = b + inst[un.x].count;
+    const long tile0 = inst[un.x].tile0;
+    const int n_tiles = static_cast<int>((e - b + kBT - 1) / kBT);
     const double inv_l = inst[un.x].inv_l;
-    const long i = b + static_cast<long>(un.y) * kBT + threadIdx.x;
+    const long k = b + static_cast<long>(un.y) * kBT + tid;
     float4 th = make_float4(0.f, 0.f, 0.f, 0.f), tl = th;
-    if (i < e) {
-      th = hq[i];
-      tl = lo[i];
+    if (k < e) {
+      th = hq[k];
+      tl = lo[k];
     }
+    const TileBox tb = boxes[tile0 + un.y];
     const float eps2 = static_cast<float>(fmax(kMinSquaredDistance * inv_l * inv_l, 1e-25));
     float ahx = 0.f, ahy = 0.f, ahz = 0.f, alx = 0.f, aly = 0.f, alz = 0.f;
-    for (long t0 = b; t0 < e; t0 += kBT) {
-      const long j = t0 + threadIdx.x;
-      sh[threadIdx.x] = j < e ? hq[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-      sl[threadIdx.x] = j < e ? lo[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int t = 0; t < n_tiles; ++t) {
+      const TileBox sbx = boxes[tile0 + t];
+      if (sbx.c.w == 0.f || tb.c.w == 0.f) continue;  // no usable sources or targets (uniform)
+      const float gx = fmaxf(fabsf(tb.c.x - sbx.c.x) - (tb.h.x + sbx.h.x), 0.f);
+      const float gy = fmaxf(fabsf(tb.c.y - sbx.c.y) - (tb.h.y + sbx.h.y), 0.f);
+      const float gz = fmaxf(fabsf(tb.c.z - sbx.c.z) - (tb.h.z + sbx.h.z), 0.f);
+      const float lim = 1.01f * (tb.h.w + sbx.h.w);
+      const bool near = gx * gx + gy * gy + gz * gz <= lim * lim;
+      const long j = b + static_cast<long>(t) * kBT + tid;
+      __syncthreads();  // the previous tile's readers are done with the buffers
+      if (near) {
+        sa[tid] = j < e ? hq[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        sb[tid] = j < e ? lo[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+      } else {
+        sa[tid] = j < e ? rel[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
       __syncthreads();
+      const int cnt = static_cast<int>(min(static_cast<long>(kBT), e - (b + static_cast<long>(t) * kBT)));
       float px = 0.f, py = 0.f, pz = 0.f;
-      const int cnt = static_cast<int>(min(static_cast<long>(kBT), e - t0));
+      if (near) {
 #pragma unroll 8
-      for (int k = 0; k < cnt; ++k) {
-        const float4 s = sh[k], l = sl[k];
-        const float dx = (th.x - s.x) + (tl.x - l.x);
-        const float dy = (th.y - s.y) + (tl.y - l.y);
-        const float dz = (th.z - s.z) + (tl.z - l.z);
-        const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-        const float rinv = rsqrtf(d2);
-        // the self pair has d = 0 exactly and adds nothing
-        const float w = (s.w * rinv) * (rinv * rinv);
-        px = fmaf(w, dx, px);
-        py = fmaf(w, dy, py);
-        pz = fmaf(w, dz, pz);
+        for (int s = 0; s < cnt; ++s) {
+          const float4 sh = sa[s], sl = sb[s];
+          const float dx = (th.x - sh.x) + (tl.x - sl.x);
+          const float dy = (th.y - sh.y) + (tl.y - sl.y);
+          const float dz = (th.z - sh.z) + (tl.z - sl.z);
+          const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+          const float rinv = rsqrtf(d2);
+          const float w = (sh.w * rinv) * (rinv * rinv);
+          px = fmaf(w, dx, px);
+          py = fmaf(w, dy, py);
+          pz = fmaf(w, dz, pz);
+        }
+      } else {
+        const float ax = (th.x - sbx.c.x) + (tl.x - sbx.cl.x);
+        const float ay = (th.y - sbx.c.y) + (tl.y - sbx.cl.y);
+        const float az = (th.z - sbx.c.z) + (tl.z - sbx.cl.z);
+#pragma unroll 8
+        for (int s = 0; s < cnt; ++s) {
+          const float4 sr = sa[s];
+          const float dx = ax - sr.x;
+          const float dy = ay - sr.y;
+          const float dz = az - sr.z;
+          const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+          const float rinv = rsqrtf(d2);
+          const float w = (sr.w * rinv) * (rinv * rinv);
+          px = fmaf(w, dx, px);
+          py = fmaf(w, dy, py);
+          pz = fmaf(w, dz, pz);
+        }
       }
       fold(ahx, alx, px);
       fold(ahy, aly, py);
       fold(ahz, alz, pz);
-      __syncthreads();
     }
-    if (i < e) {
+    if (k < e) {
+      const long i = perm[k];
       const double coef = th.w != 0.f ? kCoulombConstant * kElementaryCharge * inv_l * inv_l * q[i] : 0.0;
       fx[i] = coef * (static_cast<double>(ahx) + static_cast<double>(alx));
       fy[i] = coef * (static_cast<double>(ahy) + static_cast<double>(aly));
@@ -309,6 +433,7 @@ struct Batch {
   bool any_annihilation = false;
   bool graphable = true;
   DevBuf inst, inst_of, units, counters, contacts, best, flags, keys, vals, skeys, sidx;
+  DevBuf perm, rel, boxes;  // all-pairs order, tile offsets, tile boxes
   long n_units = 0;
   long contact_cap = 0;
   unsigned long long max_contacts = 0;  // largest contact count seen by a synchronised step
@@ -435,16 +560,23 @@ int batch_coulomb(amk_ctx* c, Batch& B) {
   const long n = c->n;
   if (B.n_units > 0) {
     AMK_TRY(phase_begin(c, AMK_PHASE_STAGE));
-    batch_stage_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, c->stream>>>(
+    batch_sort_key_kernel<<<static_cast<unsigned>((n + 255) / 256), 256, 0, c->stream>>>(
         n, c->x.as<double>(), c->y.as<double>(), c->z.as<double>(), c->q.as<double>(), c->alive.as<uint8_t>(),
-        B.inst_of.as<uint16_t>(), B.inst.as<InstanceDev>(), c->hq.as<float4>(), c->lo.as<float4>());
-    AMK_TRY(check_launch(c, "batch_stage_kernel"));
+        B.inst_of.as<uint16_t>(), B.inst.as<InstanceDev>(), B.keys.as<uint64_t>(), B.vals.as<uint32_t>());
+    AMK_TRY(check_launch(c, "batch_sort_key_kernel"));
+    AMK_TRY(radix_sort_pairs(c, B.keys.as<uint64_t>(), B.vals.as<uint32_t>(), B.skeys.as<uint64_t>(),
+                             B.perm.as<uint32_t>(), n, kInstBits + 30));
+    batch_tile_stage_kernel<<<static_cast<unsigned>(B.n_units), kBT, 0, c->stream>>>(
+        B.units.as<int2>(), B.inst.as<InstanceDev>(), B.perm.as<uint32_t>(), c->x.as<double>(), c->y.as<double>(),
+        c->z.as<double>(), c->q.as<double>(), c->alive.as<uint8_t>(), c->hq.as<float4>(), c->lo.as<float4>(),
+        B.rel.as<float4>(), B.boxes.as<TileBox>());
+    AMK_TRY(check_launch(c, "batch_tile_stage_kernel"));
     AMK_TRY(phase_end(c, AMK_PHASE_STAGE));
     AMK_TRY(phase_begin(c, AMK_PHASE_ALLPAIRS));
-    batch_allpairs_kernel<<<B.grid, kBT, 0, c->stream>>>(B.units.as<int2>(), static_cast<int>(B.n_units),
-                                                         B.inst.as<InstanceDev>(), c->hq.as<float4>(),
-                                                         c->lo.as<float4>(), c->q.as<double>(), c->fx.as<double>(),
-                                                         c->fy.as<double>(), c->fz.as<double>(), B.queue());
+    batch_allpairs_kernel<<<B.grid, kBT, 0, c->stream>>>(
+        B.units.as<int2>(), static_cast<int>(B.n_units), B.inst.as<InstanceDev>(), c->hq.as<float4>(),
+        c->lo.as<float4>(), B.rel.as<float4>(), B.boxes.as<TileBox>(), B.perm.as<uint32_t>(), c->q.as<double>(),
+        c->fx.as<double>(), c->fy.as<double>(), c->fz.as<double>(), B.queue());
     AMK_TRY(check_launch(c, "batch_allpairs_kernel"));
     AMK_TRY(phase_end(c, AMK_PHASE_ALLPAIRS));
   }
@@ -536,6 +668,7 @@ extern "C" int amk_batch_set(amk_ctx* c, int n_inst, const amk_params* params, c
   std::vector<InstanceDev> inst(n_inst);
   std::vector<uint16_t> inst_of(n);
   std::vector<std::pair<long, int2>> units;  // (instance size, unit)
+  long n_tiles = 0;
   for (int i = 0; i < n_inst; ++i) {
     const amk_params& p = params[i];
     const long off = offsets[i], cnt = offsets[i + 1] - off;
@@ -559,6 +692,9 @@ extern "C" int amk_batch_set(amk_ctx* c, int n_inst, const amk_params* params, c
     const double cs = std::max(p.contact_radius * (1.0 + 1e-9), 2.0 * reach / (kGridMax - 1.0));
     for (int k = 0; k < 3; ++k) d.origin[k] = -reach;
     d.inv_cell = 1.0 / cs;
+    d.inv_sort_cell = 1022.0 / (2.0 * reach);
+    d.tile0 = n_tiles;
+    if (p.coulomb_forces_enabled && p.coulomb_method == AMK_METHOD_ALLPAIRS) n_tiles += (cnt + kBT - 1) / kBT;
     d.seed = static_cast<uint32_t>(p.seed);
     d.offset = off;
     d.count = cnt;
@@ -591,6 +727,9 @@ extern "C" int amk_batch_set(amk_ctx* c, int n_inst, const amk_params* params, c
   AMK_TRY(B->vals.reserve(nn * sizeof(uint32_t)));
   AMK_TRY(B->skeys.reserve(nn * sizeof(uint64_t)));
   AMK_TRY(B->sidx.reserve(nn * sizeof(uint32_t)));
+  AMK_TRY(B->perm.reserve(nn * sizeof(uint32_t)));
+  AMK_TRY(B->rel.reserve(nn * sizeof(float4)));
+  AMK_TRY(B->boxes.reserve(static_cast<size_t>(std::max<long>(n_tiles, 1)) * sizeof(TileBox)));
   AMK_CUDA_TRY(cudaMemcpyAsync(B->inst.ptr, inst.data(), n_inst * sizeof(InstanceDev), cudaMemcpyHostToDevice,
                                c->stream));
   if (n > 0)

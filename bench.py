@@ -321,7 +321,7 @@ def run_sweep(args):
     torch.cuda.set_device(device)
     # every rank runs its own sweep of 512 instances (seeded by rank): the
     # instances are independent, so the sweep shards with no collective
-    insts = make_sweep(seed=2024 + rank, method_split=None)
+    insts = make_sweep(n_inst=args.instances, seed=2024 + rank, method_split=None)
     n_total = int(sum(len(i[0]) for i in insts))
     sim = amk.Simulation(device=local)
     load_sweep(sim, insts)
@@ -382,15 +382,17 @@ def run_sweep(args):
 
     # baseline: the same instances one at a time with the single-instance kernels
     serial_steps = max(1, min(args.steps, args.serial_steps))
+    sim.batch_step(1, serial=True)  # untimed: grows the single-instance scratch to its largest size
     serial_ms = max_over_ranks(timed(lambda: sim.batch_step(serial_steps, serial=True)), world, device)
     serial_value = world * n_total * serial_steps / (serial_ms * 1e-3)
     sim.close()
     # the sweep's own method split (FMM p=4 from 8,192 particles), both ways
-    split = make_sweep(seed=2024 + rank, method_split=8192, order=4)
+    split = make_sweep(n_inst=args.instances, seed=2024 + rank, method_split=8192, order=4)
     sim = amk.Simulation(device=local)
     load_sweep(sim, split)
     sim.batch_step(args.warmup)
     split_ms = max_over_ranks(timed(lambda: sim.batch_step(serial_steps)), world, device)
+    sim.batch_step(1, serial=True)
     split_serial_ms = max_over_ranks(timed(lambda: sim.batch_step(serial_steps, serial=True)), world, device)
 
     # end to end through the C ABI with host buffers (one step per call)
@@ -428,14 +430,14 @@ def run_sweep(args):
         cpu = {"value": n_total / t_cpu, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
                "sample": "per instance: reference Barnes-Hut theta=0 tree over all its sources walked "
                          "for 64 evenly spaced targets (extrapolated), + FP64 push of all particles; "
-                         "all 512 instances, OpenMP on all host cores"}
+                         "all instances, OpenMP on all host cores"}
     if rank == 0:
         sizes = np.array([len(i[0]) for i in insts])
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
                 "data": "synthetic (seeded sweep generator)",
-                "config": {"workload": "batched sweep: 512 trap instances, N_i log-uniform 1e2..1e5 "
+                "config": {"workload": f"batched sweep: {len(insts)} trap instances, N_i log-uniform 1e2..1e5 "
                                        f"(total {n_total:,}), e-/e+ or e+/pbar 1:1, T 4..1e4 K, b0 1..5 T, "
                                        "U 5..50 V, radii 5e-5..5e-4 m, cooling (4 K) and annihilation "
                                        "(5e-6 m, p=0.5) on",
@@ -445,7 +447,7 @@ def run_sweep(args):
                            "instance_sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)),
                                               "max": int(sizes.max())},
                            "l2": "not flushed: state of 7.4 M particles (> 700 MB) exceeds L2",
-                           "parallelism": f"dp{world}: one 512-instance sweep per GPU, no collective"},
+                           "parallelism": f"dp{world}: one {len(insts)}-instance sweep per GPU, no collective"},
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
                 "clocks": clocks,
                 "one_at_a_time": {"value": serial_value, "steps": serial_steps,
@@ -471,7 +473,7 @@ def run_reference_sweep(args):
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    insts = make_sweep(seed=2024, method_split=None)
+    insts = make_sweep(n_inst=args.instances, seed=2024, method_split=None)
     n_total = int(sum(len(i[0]) for i in insts))
     times = []
     kind = "reference"
@@ -485,7 +487,7 @@ def run_reference_sweep(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded sweep generator)",
-            "config": {"workload": f"batched sweep: 512 trap instances, {n_total:,} particles"},
+            "config": {"workload": f"batched sweep: {len(insts)} trap instances, {n_total:,} particles"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
                              "sample": "per instance and step: theta=0 tree over all sources, 16 "
                                        "targets walked (extrapolated), FP64 push of all"},
@@ -660,6 +662,8 @@ def main():
                     help="targets walked per step by the reference arm")
     ap.add_argument("--serial-steps", type=int, default=3,
                     help="steps of the one-at-a-time comparison (sweep workload)")
+    ap.add_argument("--instances", type=int, default=512,
+                    help="trap instances of the sweep workload (the first k of the 512-instance sweep)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least three untimed warm-up steps
     if args.impl == "reference":
