@@ -4,24 +4,30 @@
 // (barnes-hut.h:22-24, barnes-hut.cc:183-221): F_i = sum_{j != i} k q_i q_j
 // r_ij / r^3, skipping q_j = 0 and r^2 < 1e-30. Design:
 //   * particles are ordered along a 30-bit Morton curve (radix sort; the
-//     order is reused for 16 calls on a context's own particle set -- tile
-//     boxes are rebuilt on every call, so a stale order costs speed only);
-//     tiles of 256 consecutive particles get an axis-aligned box;
-//   * positions are scaled by a power of two L. For tile pairs whose boxes
-//     are closer than their combined half-extents ("near"), positions are a
-//     float pair (hi, lo) and r_ij = (xi_hi - xj_hi) + (xi_lo - xj_lo) is
-//     exact to FP32 rounding of |r_ij| (Sterbenz) -- 18 FP32 ops per pair;
-//   * for separated tile pairs ("far", |r_ij| >= the boxes' gap >= their
-//     half-extents) each source carries its offset from its tile centre in
-//     FP32 and each target forms a_i = x_i - c_tile once per tile, so
-//     r_ij = a_i - u_j costs one FADD per component and stays within ~2 eps
-//     of |r_ij| -- 12 FP32 ops per pair;
+//     order is reused for 16 calls on a context's own particle set -- boxes
+//     are rebuilt on every call, so a stale order costs speed only); every
+//     32 consecutive sorted particles form a sub-tile with an axis-aligned
+//     box, and each warp owns 64 consecutive targets (two sub-tiles);
+//   * positions are scaled by a power of two L. The near/far decision is
+//     made per (warp, 32-source sub-tile), uniform across the warp. Near
+//     pairs (the warp's box and the sub-tile's box closer than a quarter of
+//     their summed half-extent norms) use a float pair (hi, lo):
+//     r_ij = (xi_hi - xj_hi) + (xi_lo - xj_lo), exact to FP32 rounding of
+//     |r_ij| (Sterbenz) -- 18 FP32 ops per pair; the self pair and exact
+//     duplicates give r = 0 exactly;
+//   * far pairs: each source carries its FP32 offset u_j from its sub-tile
+//     centre and each target forms a_i = x_i - c_sub once per sub-tile, so
+//     r_ij = a_i - u_j costs one FADD per component -- 12 FP32 ops per pair.
+//     Its relative error is at most eps (1 + 1.5 / 0.25) = 7 eps of |r_ij|
+//     for the closest far pairs (gap >= 0.25 (|h_w| + |h_s|)) and ~eps for
+//     the bulk; about 5 % of the sub-tile pairs of a 65,536-particle cloud
+//     are near;
 //   * r^2 gets eps2 = max(1e-30 m^2 / L^2, 1e-25) added so that the self pair
 //     (r = 0) contributes exactly 0 without a branch and rinv^3 cannot
 //     overflow (the reference skips pairs closer than 1e-15 m; such pairs,
 //     and pairs closer than 3e-13 L, are softened here instead);
-//   * each 256-source tile is summed in FP32 and folded into a (hi, lo) float
-//     pair with TwoSum (compensated accumulation);
+//   * each 256-source chunk (8 sub-tiles) is summed in FP32 and folded into a
+//     (hi, lo) float pair with TwoSum (compensated accumulation);
 //   * a persistent grid of (SM count x resident CTAs) walks contiguous
 //     ranges of (target block, source chunk) units, keeping a target block's
 //     sums in registers across its chunks; the finalize kernel adds the
@@ -35,8 +41,11 @@
 namespace amk {
 namespace {
 
-constexpr int kThreads = 256;  // threads per CTA = particles per tile
-constexpr int kR = 2;          // targets per thread (a target block = 2 tiles)
+constexpr int kThreads = 256;  // threads per CTA = sources per chunk
+constexpr int kR = 2;          // targets per thread (a warp owns 64 consecutive targets)
+constexpr int kSub = 32;       // particles per sub-tile (box granularity)
+constexpr int kSubPerChunk = kThreads / kSub;
+constexpr float kNearFactor = 0.25f;
 constexpr int kResortEvery = 16;
 
 __device__ __forceinline__ void two_sum_fold(float& hi, float& lo, float p) {
@@ -107,15 +116,13 @@ struct TileBox {
   float4 h;   // half-extent per axis (rounded up); w = |h|
 };
 
-// One CTA per tile of 256 sorted particles: double-float positions, offsets
-// from the tile centre, and the tile box of its usable particles.
+// One warp per sub-tile of 32 sorted particles: double-float positions,
+// offsets from the sub-tile centre, and the box of its usable particles.
 __global__ void __launch_bounds__(kThreads)
 ap_stage_kernel(View v, const uint32_t* __restrict__ perm, double inv_l, float4* __restrict__ hq,
                 float4* __restrict__ lo, float4* __restrict__ rel, TileBox* __restrict__ boxes) {
-  __shared__ double red[6][kThreads / 32];
-  __shared__ double box[6];
-  const int t = blockIdx.x;
-  const long k = static_cast<long>(t) * kThreads + threadIdx.x;
+  const long k = static_cast<long>(blockIdx.x) * kThreads + threadIdx.x;
+  const long sub = k / kSub;
   double xs = 0.0, ys = 0.0, zs = 0.0, qe = 0.0;
   bool ok = false;
   if (k < v.n) {
@@ -130,21 +137,13 @@ ap_stage_kernel(View v, const uint32_t* __restrict__ perm, double inv_l, float4*
   }
   double m[6] = {ok ? xs : INFINITY, ok ? ys : INFINITY, ok ? zs : INFINITY,
                  ok ? -xs : INFINITY, ok ? -ys : INFINITY, ok ? -zs : INFINITY};
+#pragma unroll
   for (int d = 0; d < 6; ++d)
     for (int o = 16; o > 0; o >>= 1) m[d] = fmin(m[d], __shfl_xor_sync(0xffffffffu, m[d], o));
-  if ((threadIdx.x & 31) == 0)
-    for (int d = 0; d < 6; ++d) red[d][threadIdx.x >> 5] = m[d];
-  __syncthreads();
-  if (threadIdx.x < 6) {
-    double r = INFINITY;
-    for (int w = 0; w < kThreads / 32; ++w) r = fmin(r, red[threadIdx.x][w]);
-    box[threadIdx.x] = r;
-  }
-  __syncthreads();
-  const bool any = isfinite(box[0]);
-  const double cx = any ? 0.5 * (box[0] - box[3]) : 0.0;
-  const double cy = any ? 0.5 * (box[1] - box[4]) : 0.0;
-  const double cz = any ? 0.5 * (box[2] - box[5]) : 0.0;
+  const bool any = isfinite(m[0]);
+  const double cx = any ? 0.5 * (m[0] - m[3]) : 0.0;
+  const double cy = any ? 0.5 * (m[1] - m[4]) : 0.0;
+  const double cz = any ? 0.5 * (m[2] - m[5]) : 0.0;
   float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h, u = h;
   if (ok) {
     h.x = __double2float_rn(xs);
@@ -164,18 +163,18 @@ ap_stage_kernel(View v, const uint32_t* __restrict__ perm, double inv_l, float4*
     lo[k] = l;
     rel[k] = u;
   }
-  if (threadIdx.x == 0) {
+  if ((threadIdx.x & 31) == 0) {
     TileBox b;
     b.c = make_float4(__double2float_rn(cx), __double2float_rn(cy), __double2float_rn(cz), any ? 1.f : 0.f);
     b.cl = make_float4(__double2float_rn(cx - static_cast<double>(b.c.x)),
                        __double2float_rn(cy - static_cast<double>(b.c.y)),
                        __double2float_rn(cz - static_cast<double>(b.c.z)), 0.f);
-    const double hx = any ? 0.5 * (-box[3] - box[0]) : 0.0;
-    const double hy = any ? 0.5 * (-box[4] - box[1]) : 0.0;
-    const double hz = any ? 0.5 * (-box[5] - box[2]) : 0.0;
+    const double hx = any ? 0.5 * (-m[3] - m[0]) : 0.0;
+    const double hy = any ? 0.5 * (-m[4] - m[1]) : 0.0;
+    const double hz = any ? 0.5 * (-m[5] - m[2]) : 0.0;
     b.h = make_float4(__double2float_ru(hx), __double2float_ru(hy), __double2float_ru(hz),
                       __double2float_ru(sqrt(hx * hx + hy * hy + hz * hz)));
-    boxes[t] = b;
+    boxes[sub] = b;
   }
 }
 
@@ -186,6 +185,8 @@ __device__ __forceinline__ long unit_start(long c, long units, long grid) { retu
 // units [start(c), start(c+1)), start(c) = floor(c * units / grid). A target
 // block's sums stay in registers over its consecutive units; a run is
 // flushed to partial slot (first chunk of the run) when the block changes.
+// Target block tb = sorted targets [512 tb, 512 tb + 512); warp w owns
+// [512 tb + 64 w, + 64): lane l holds targets +l (r = 0) and +32+l (r = 1).
 template <bool kPhi>
 __global__ void __launch_bounds__(kThreads, 3)
 allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, const float4* __restrict__ rel,
@@ -193,7 +194,11 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, co
                 int tiles_per_chunk, float eps2, float4* __restrict__ part) {
   __shared__ float4 sa[kThreads];
   __shared__ float4 sb[kThreads];
+  __shared__ float4 sc[kThreads];
+  __shared__ TileBox sbox[kSubPerChunk];
   const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int n_sub = (n + kSub - 1) / kSub;
   const long units = static_cast<long>(n_tb) * n_split;
   const long u_begin = unit_start(blockIdx.x, units, gridDim.x);
   const long u_end = unit_start(blockIdx.x + 1, units, gridDim.x);
@@ -201,13 +206,15 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, co
 
   float tx[kR], ty[kR], tz[kR], ux[kR], uy[kR], uz[kR];
   float ahx[kR], ahy[kR], ahz[kR], ahp[kR], alx[kR], aly[kR], alz[kR], alp[kR];
-  float4 bc = make_float4(0.f, 0.f, 0.f, 0.f), bh = bc;  // target block box
+  float4 wc = make_float4(0.f, 0.f, 0.f, 0.f), wh = wc;  // this warp's target box
+  bool warp_live = false;
   int run_tb = -1, run_split = 0;
 
+  auto target = [&](int tb, int r) { return tb * (kThreads * kR) + warp * (kSub * kR) + r * kSub + lane; };
   auto flush = [&]() {
 #pragma unroll
     for (int r = 0; r < kR; ++r) {
-      const int i = run_tb * (kThreads * kR) + r * kThreads + tid;
+      const int i = target(run_tb, r);
       if (i < n) {
         part[(static_cast<size_t>(run_split) * 2 + 0) * n + i] = make_float4(ahx[r], ahy[r], ahz[r], ahp[r]);
         part[(static_cast<size_t>(run_split) * 2 + 1) * n + i] = make_float4(alx[r], aly[r], alz[r], alp[r]);
@@ -224,7 +231,7 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, co
       run_split = split;
 #pragma unroll
       for (int r = 0; r < kR; ++r) {
-        const int i = tb * (kThreads * kR) + r * kThreads + tid;
+        const int i = target(tb, r);
         float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
         if (i < n) {
           h = hq[i];
@@ -235,91 +242,95 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, co
         ahx[r] = ahy[r] = ahz[r] = ahp[r] = 0.f;
         alx[r] = aly[r] = alz[r] = alp[r] = 0.f;
       }
-      // union box of the block's (up to two) tiles
-      TileBox b0 = boxes[kR * tb];
-      TileBox b1 = (kR * tb + 1 < n_tiles) ? boxes[kR * tb + 1] : b0;
+      // union box of the warp's two target sub-tiles (warp-uniform loads)
+      const int s0 = (tb * (kThreads * kR) + warp * (kSub * kR)) / kSub;
+      TileBox b0 = s0 < n_sub ? boxes[s0] : TileBox{};
+      TileBox b1 = s0 + 1 < n_sub ? boxes[s0 + 1] : TileBox{};
       if (b1.c.w == 0.f) b1 = b0;
       if (b0.c.w == 0.f) b0 = b1;
+      warp_live = b0.c.w != 0.f;
       const float lx = fminf(b0.c.x - b0.h.x, b1.c.x - b1.h.x), hx = fmaxf(b0.c.x + b0.h.x, b1.c.x + b1.h.x);
       const float ly = fminf(b0.c.y - b0.h.y, b1.c.y - b1.h.y), hy = fmaxf(b0.c.y + b0.h.y, b1.c.y + b1.h.y);
       const float lz = fminf(b0.c.z - b0.h.z, b1.c.z - b1.h.z), hz = fmaxf(b0.c.z + b0.h.z, b1.c.z + b1.h.z);
-      bc = make_float4(0.5f * (lx + hx), 0.5f * (ly + hy), 0.5f * (lz + hz), 0.f);
-      bh = make_float4(0.5001f * (hx - lx), 0.5001f * (hy - ly), 0.5001f * (hz - lz), 0.f);
-      bh.w = 1.0001f * sqrtf(bh.x * bh.x + bh.y * bh.y + bh.z * bh.z);
+      wc = make_float4(0.5f * (lx + hx), 0.5f * (ly + hy), 0.5f * (lz + hz), 0.f);
+      wh = make_float4(0.5001f * (hx - lx), 0.5001f * (hy - ly), 0.5001f * (hz - lz), 0.f);
+      wh.w = 1.0001f * sqrtf(wh.x * wh.x + wh.y * wh.y + wh.z * wh.z);
     }
     const int t_begin = split * tiles_per_chunk;
     const int t_end = min(n_tiles, t_begin + tiles_per_chunk);
 
     for (int t = t_begin; t < t_end; ++t) {
-      const TileBox sbox = boxes[t];
-      if (sbox.c.w == 0.f) continue;  // no usable sources in this tile (uniform)
-      // near: the boxes' gap is below their summed half-extents
-      const float gx = fmaxf(fabsf(bc.x - sbox.c.x) - (bh.x + sbox.h.x), 0.f);
-      const float gy = fmaxf(fabsf(bc.y - sbox.c.y) - (bh.y + sbox.h.y), 0.f);
-      const float gz = fmaxf(fabsf(bc.z - sbox.c.z) - (bh.z + sbox.h.z), 0.f);
-      const float lim = 1.01f * (bh.w + sbox.h.w);
-      const bool near = gx * gx + gy * gy + gz * gz < lim * lim;
       const int j = t * kThreads + tid;
-      __syncthreads();  // the previous tile's readers are done with the buffers
-      if (near) {
-        float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
-        if (j < n) {
-          h = hq[j];
-          l = lo[j];
-        }
-        sa[tid] = h;
-        sb[tid] = l;
+      __syncthreads();  // the previous chunk's readers are done with the buffers
+      if (j < n) {
+        sa[tid] = hq[j];
+        sb[tid] = lo[j];
+        sc[tid] = rel[j];
       } else {
-        sa[tid] = (j < n) ? rel[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        sa[tid] = sb[tid] = sc[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      if (tid < kSubPerChunk) {
+        const int sidx = t * kSubPerChunk + tid;
+        sbox[tid] = sidx < n_sub ? boxes[sidx] : TileBox{};
       }
       __syncthreads();
+      if (!warp_live) continue;  // no usable target in this warp (uniform)
       float px[kR], py[kR], pz[kR], pp[kR];
 #pragma unroll
       for (int r = 0; r < kR; ++r) px[r] = py[r] = pz[r] = pp[r] = 0.f;
-      if (near) {
+      for (int q = 0; q < kSubPerChunk; ++q) {
+        const TileBox sbx = sbox[q];
+        if (sbx.c.w == 0.f) continue;  // no usable sources (uniform)
+        const float gx = fmaxf(fabsf(wc.x - sbx.c.x) - (wh.x + sbx.h.x), 0.f);
+        const float gy = fmaxf(fabsf(wc.y - sbx.c.y) - (wh.y + sbx.h.y), 0.f);
+        const float gz = fmaxf(fabsf(wc.z - sbx.c.z) - (wh.z + sbx.h.z), 0.f);
+        const float lim = kNearFactor * (wh.w + sbx.h.w);
+        const int base = q * kSub;
+        if (gx * gx + gy * gy + gz * gz <= lim * lim) {
 #pragma unroll 8
-        for (int k = 0; k < kThreads; ++k) {
-          const float4 s = sa[k];
-          const float4 l = sb[k];
+          for (int k = 0; k < kSub; ++k) {
+            const float4 s = sa[base + k];
+            const float4 l = sb[base + k];
 #pragma unroll
-          for (int r = 0; r < kR; ++r) {
-            const float dx = (tx[r] - s.x) + (ux[r] - l.x);
-            const float dy = (ty[r] - s.y) + (uy[r] - l.y);
-            const float dz = (tz[r] - s.z) + (uz[r] - l.z);
-            const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-            const float rinv = rsqrtf(d2);
-            const float qr = s.w * rinv;
-            const float w = qr * (rinv * rinv);
-            px[r] = fmaf(w, dx, px[r]);
-            py[r] = fmaf(w, dy, py[r]);
-            pz[r] = fmaf(w, dz, pz[r]);
-            if (kPhi) pp[r] += (d2 >= self_cut) ? qr : 0.0f;
+            for (int r = 0; r < kR; ++r) {
+              const float dx = (tx[r] - s.x) + (ux[r] - l.x);
+              const float dy = (ty[r] - s.y) + (uy[r] - l.y);
+              const float dz = (tz[r] - s.z) + (uz[r] - l.z);
+              const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+              const float rinv = rsqrtf(d2);
+              const float qr = s.w * rinv;
+              const float w = qr * (rinv * rinv);
+              px[r] = fmaf(w, dx, px[r]);
+              py[r] = fmaf(w, dy, py[r]);
+              pz[r] = fmaf(w, dz, pz[r]);
+              if (kPhi) pp[r] += (d2 >= self_cut) ? qr : 0.0f;
+            }
           }
-        }
-      } else {
-        float ax[kR], ay[kR], az[kR];
-#pragma unroll
-        for (int r = 0; r < kR; ++r) {
-          ax[r] = (tx[r] - sbox.c.x) + (ux[r] - sbox.cl.x);
-          ay[r] = (ty[r] - sbox.c.y) + (uy[r] - sbox.cl.y);
-          az[r] = (tz[r] - sbox.c.z) + (uz[r] - sbox.cl.z);
-        }
-#pragma unroll 8
-        for (int k = 0; k < kThreads; ++k) {
-          const float4 s = sa[k];
+        } else {
+          float ax[kR], ay[kR], az[kR];
 #pragma unroll
           for (int r = 0; r < kR; ++r) {
-            const float dx = ax[r] - s.x;
-            const float dy = ay[r] - s.y;
-            const float dz = az[r] - s.z;
-            const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-            const float rinv = rsqrtf(d2);
-            const float qr = s.w * rinv;
-            const float w = qr * (rinv * rinv);
-            px[r] = fmaf(w, dx, px[r]);
-            py[r] = fmaf(w, dy, py[r]);
-            pz[r] = fmaf(w, dz, pz[r]);
-            if (kPhi) pp[r] += qr;
+            ax[r] = (tx[r] - sbx.c.x) + (ux[r] - sbx.cl.x);
+            ay[r] = (ty[r] - sbx.c.y) + (uy[r] - sbx.cl.y);
+            az[r] = (tz[r] - sbx.c.z) + (uz[r] - sbx.cl.z);
+          }
+#pragma unroll 8
+          for (int k = 0; k < kSub; ++k) {
+            const float4 s = sc[base + k];
+#pragma unroll
+            for (int r = 0; r < kR; ++r) {
+              const float dx = ax[r] - s.x;
+              const float dy = ay[r] - s.y;
+              const float dz = az[r] - s.z;
+              const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+              const float rinv = rsqrtf(d2);
+              const float qr = s.w * rinv;
+              const float w = qr * (rinv * rinv);
+              px[r] = fmaf(w, dx, px[r]);
+              py[r] = fmaf(w, dy, py[r]);
+              pz[r] = fmaf(w, dz, pz[r]);
+              if (kPhi) pp[r] += qr;
+            }
           }
         }
       }
@@ -434,7 +445,9 @@ int allpairs_forces(amk_ctx* c, const View& v) {
   AMK_TRY(rc);
   float4* rel = slot<float4>(c, kSlotTreeAux0, n, &rc);
   AMK_TRY(rc);
-  TileBox* boxes = slot<TileBox>(c, kSlotTreeAux1, n_tiles + 1, &rc);
+  // one box per sub-tile of every staged chunk (the stage kernel's warps past
+  // n write empty boxes)
+  TileBox* boxes = slot<TileBox>(c, kSlotTreeAux1, static_cast<size_t>(n_tiles) * kSubPerChunk, &rc);
   AMK_TRY(rc);
   const double l = v.length_scale;
   ap_stage_kernel<<<n_tiles, kThreads, 0, c->stream>>>(v, perm, 1.0 / l, hq, lo, rel, boxes);
