@@ -188,7 +188,7 @@ __device__ __forceinline__ long unit_start(long c, long units, long grid) { retu
 // Target block tb = sorted targets [512 tb, 512 tb + 512); warp w owns
 // [512 tb + 64 w, + 64): lane l holds targets +l (r = 0) and +32+l (r = 1).
 template <bool kPhi>
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kThreads, 4)
 allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, const float4* __restrict__ rel,
                 const TileBox* __restrict__ boxes, int n, int n_tiles, int n_tb, int n_split,
                 int tiles_per_chunk, float eps2, float4* __restrict__ part) {
@@ -206,7 +206,7 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, co
 
   float tx[kR], ty[kR], tz[kR], ux[kR], uy[kR], uz[kR];
   float ahx[kR], ahy[kR], ahz[kR], ahp[kR], alx[kR], aly[kR], alz[kR], alp[kR];
-  float4 wc = make_float4(0.f, 0.f, 0.f, 0.f), wh = wc;  // this warp's target box
+  __shared__ float4 swc[kThreads / 32], swh[kThreads / 32];  // each warp's target box
   bool warp_live = false;
   int run_tb = -1, run_split = 0;
 
@@ -252,9 +252,14 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, co
       const float lx = fminf(b0.c.x - b0.h.x, b1.c.x - b1.h.x), hx = fmaxf(b0.c.x + b0.h.x, b1.c.x + b1.h.x);
       const float ly = fminf(b0.c.y - b0.h.y, b1.c.y - b1.h.y), hy = fmaxf(b0.c.y + b0.h.y, b1.c.y + b1.h.y);
       const float lz = fminf(b0.c.z - b0.h.z, b1.c.z - b1.h.z), hz = fmaxf(b0.c.z + b0.h.z, b1.c.z + b1.h.z);
-      wc = make_float4(0.5f * (lx + hx), 0.5f * (ly + hy), 0.5f * (lz + hz), 0.f);
-      wh = make_float4(0.5001f * (hx - lx), 0.5001f * (hy - ly), 0.5001f * (hz - lz), 0.f);
+      float4 wh = make_float4(0.5001f * (hx - lx), 0.5001f * (hy - ly), 0.5001f * (hz - lz), 0.f);
       wh.w = 1.0001f * sqrtf(wh.x * wh.x + wh.y * wh.y + wh.z * wh.z);
+      __syncwarp();
+      if (lane == 0) {
+        swc[warp] = make_float4(0.5f * (lx + hx), 0.5f * (ly + hy), 0.5f * (lz + hz), 0.f);
+        swh[warp] = wh;
+      }
+      __syncwarp();
     }
     const int t_begin = split * tiles_per_chunk;
     const int t_end = min(n_tiles, t_begin + tiles_per_chunk);
@@ -278,6 +283,7 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, co
       float px[kR], py[kR], pz[kR], pp[kR];
 #pragma unroll
       for (int r = 0; r < kR; ++r) px[r] = py[r] = pz[r] = pp[r] = 0.f;
+      const float4 wc = swc[warp], wh = swh[warp];
       for (int q = 0; q < kSubPerChunk; ++q) {
         const TileBox sbx = sbox[q];
         if (sbx.c.w == 0.f) continue;  // no usable sources (uniform)
