@@ -64,6 +64,11 @@ class Params(C.Structure):
     ]
 
 
+class TuneCandidate(C.Structure):
+    _fields_ = [("method", C.c_int), ("order", C.c_int), ("theta", C.c_double), ("leaf", C.c_int),
+                ("ms", C.c_double), ("rms", C.c_double), ("meets", C.c_int)]
+
+
 class EnergyOut(C.Structure):
     _fields_ = [("kinetic", C.c_double), ("trap_potential", C.c_double),
                 ("coulomb_potential", C.c_double), ("total", C.c_double),
@@ -146,6 +151,11 @@ def lib():
         "amk_mlp_forward": (C.c_int, [vp, _fp, C.c_long, _fp]),
         "amk_mlp_gradients": (C.c_int, [vp, _fp, _fp, C.c_long, _fp, _fp, _fp]),
         "amk_mlp_train": (C.c_int, [vp, _fp, _fp, C.c_long, C.c_int, C.c_long, C.c_float, _fp]),
+        "amk_force_error": (C.c_int, [vp, C.c_long, _dp, _dp]),
+        "amk_set_leaf_sizes": (C.c_int, [vp, C.c_int, C.c_int]),
+        "amk_get_leaf_sizes": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "amk_autotune": (C.c_int, [vp, C.c_double, C.c_long, C.c_int, C.POINTER(TuneCandidate), C.c_int,
+                                   C.POINTER(C.c_int), C.POINTER(C.c_int)]),
         "amk_batch_set": (C.c_int, [vp, C.c_int, C.POINTER(Params), C.POINTER(C.c_long)]),
         "amk_batch_step": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
         "amk_batch_coulomb": (C.c_int, [vp]),
@@ -450,6 +460,32 @@ class Simulation:
         t, f, e = C.c_int(), C.c_int(), C.c_double()
         check(lib().amk_fmm_learned_state(self._h, C.byref(t), C.byref(f), C.byref(e)))
         return {"trained": bool(t.value), "fallback": bool(f.value), "last_error": e.value}
+
+    # -- audit and tuning
+    def force_error(self, samples=1024):
+        """(rms, max) relative error of the current forces vs the FP64 exact sum."""
+        r, m = C.c_double(), C.c_double()
+        check(lib().amk_force_error(self._h, int(samples), C.byref(r), C.byref(m)), "amk_force_error")
+        return r.value, m.value
+
+    def set_leaf_sizes(self, fmm_leaf=32, bh_leaf=8):
+        check(lib().amk_set_leaf_sizes(self._h, int(fmm_leaf), int(bh_leaf)), "amk_set_leaf_sizes")
+
+    def leaf_sizes(self):
+        a, b = C.c_int(), C.c_int()
+        check(lib().amk_get_leaf_sizes(self._h, C.byref(a), C.byref(b)), "amk_get_leaf_sizes")
+        return a.value, b.value
+
+    def autotune(self, error_budget=1e-5, samples=1024, flags=0):
+        """Runs the autotuner; returns (candidates, chosen index)."""
+        out = (TuneCandidate * 64)()
+        n, ch = C.c_int(0), C.c_int(-1)
+        rc = lib().amk_autotune(self._h, float(error_budget), int(samples), int(flags), out, 64, C.byref(n),
+                                C.byref(ch))
+        cands = [{"method": out[k].method, "order": out[k].order, "theta": out[k].theta, "leaf": out[k].leaf,
+                  "ms": out[k].ms, "rms": out[k].rms, "meets": bool(out[k].meets)} for k in range(n.value)]
+        check(rc, "amk_autotune")
+        return cands, ch.value
 
     # -- batched instances
     def batch_set(self, params, offsets):

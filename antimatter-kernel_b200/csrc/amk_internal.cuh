@@ -238,6 +238,10 @@ struct amk_ctx {
   amk::Fmm* fmm = nullptr;
   amk::Mlp* mlp = nullptr;
   amk::Batch* batch = nullptr;  // batched instances over segment offsets
+  // leaf capacities of the context's own solver calls (the reference's 32 and
+  // 8 unless amk_autotune or amk_set_leaf_sizes changed them)
+  int fmm_leaf = 32;
+  int bh_leaf = 8;
   // learned FMM correction state
   bool learned_trained = false;
   bool learned_fallback = false;

@@ -662,15 +662,6 @@ extern "C" long amk_num_alive(amk_ctx* c) {
 }
 
 // ============================================================== forces
-static int ensure_staged(amk_ctx* c) {
-  if (!c->stage_dirty) return AMK_OK;
-  AMK_TRY(phase_begin(c, AMK_PHASE_STAGE));
-  AMK_TRY(stage_view(c, main_view(c)));
-  AMK_TRY(phase_end(c, AMK_PHASE_STAGE));
-  c->stage_dirty = false;
-  return AMK_OK;
-}
-
 extern "C" int amk_coulomb_allpairs(amk_ctx* c) {
   if (!c) return fail(AMK_ERR_INVALID, "null context");
   if (c->n == 0) return AMK_OK;
@@ -686,8 +677,7 @@ extern "C" int amk_coulomb_standard(amk_ctx* c, double cutoff) {
 extern "C" int amk_coulomb_barnes_hut(amk_ctx* c, double theta) {
   if (!c) return fail(AMK_ERR_INVALID, "null context");
   if (c->n == 0) return AMK_OK;
-  AMK_TRY(ensure_staged(c));
-  return barnes_hut_forces(c, main_view(c), theta, 8);
+  return barnes_hut_forces(c, main_view(c), theta, c->bh_leaf);
 }
 
 // learned != 0 uses the p=2 far field plus the trained correction while it is
@@ -696,10 +686,11 @@ extern "C" int amk_coulomb_fmm(amk_ctx* c, int order, double theta, int learned)
   if (!c) return fail(AMK_ERR_INVALID, "null context");
   if (c->n == 0) return AMK_OK;
   if (learned) {
-    if (c->learned_trained && !c->learned_fallback) return fmm_forces(c, main_view(c), 2, theta, 32, true, nullptr);
+    if (c->learned_trained && !c->learned_fallback)
+      return fmm_forces(c, main_view(c), 2, theta, c->fmm_leaf, true, nullptr);
     order = c->p.learned_fallback_order;
   }
-  return fmm_forces(c, main_view(c), order, theta, 32, false, nullptr);
+  return fmm_forces(c, main_view(c), order, theta, c->fmm_leaf, false, nullptr);
 }
 
 extern "C" int amk_fmm_train_correction(amk_ctx* c, double theta, int sample_leaves, int steps, long batch, float lr,
@@ -725,6 +716,22 @@ extern "C" int amk_fmm_learned_state(amk_ctx* c, int* trained, int* fallback, do
   if (trained) *trained = c->learned_trained ? 1 : 0;
   if (fallback) *fallback = c->learned_fallback ? 1 : 0;
   if (last_error) *last_error = c->learned_last_error;
+  return AMK_OK;
+}
+
+extern "C" int amk_set_leaf_sizes(amk_ctx* c, int fmm_leaf, int bh_leaf) {
+  if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (fmm_leaf < 1 || fmm_leaf > 256 || bh_leaf < 1 || bh_leaf > 256)
+    return fail(AMK_ERR_INVALID, "leaf capacities must be in [1, 256]");
+  c->fmm_leaf = fmm_leaf;
+  c->bh_leaf = bh_leaf;
+  return AMK_OK;
+}
+
+extern "C" int amk_get_leaf_sizes(const amk_ctx* c, int* fmm_leaf, int* bh_leaf) {
+  if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (fmm_leaf) *fmm_leaf = c->fmm_leaf;
+  if (bh_leaf) *bh_leaf = c->bh_leaf;
   return AMK_OK;
 }
 

@@ -314,6 +314,42 @@ int amk_fmm_audit(amk_ctx* ctx, int order, double theta, int learned, long sampl
  * last audit's RMS relative error. */
 int amk_fmm_learned_state(amk_ctx* ctx, int* trained, int* fallback, double* last_error);
 
+/* ------------------------------------------------------------ audit and tuning */
+/* No counterpart in the reference. RMS and maximum relative error of the
+ * context's current forces (as left by the last amk_coulomb* call) against
+ * an FP64 exact Coulomb sum (the reference's theta = 0 force) for `samples`
+ * evenly spaced alive, charged particles. max_rel may be NULL. */
+int amk_force_error(amk_ctx* ctx, long samples, double* rms, double* max_rel);
+
+/* Leaf capacities used by amk_coulomb_fmm / amk_coulomb_barnes_hut and
+ * amk_step (defaults 32 and 8, the reference's fast-multipole.h:50 and
+ * barnes-hut.h:30). Other values build other trees than the reference's. */
+int amk_set_leaf_sizes(amk_ctx* ctx, int fmm_leaf, int bh_leaf);
+int amk_get_leaf_sizes(const amk_ctx* ctx, int* fmm_leaf, int* bh_leaf);
+
+typedef struct amk_tune_candidate {
+  int method;    /* AMK_METHOD_*                                 */
+  int order;     /* FMM order (0 otherwise)                      */
+  double theta;  /* FMM / Barnes-Hut opening angle               */
+  int leaf;      /* leaf capacity (0 for all-pairs)              */
+  double ms;     /* median device time of one force evaluation; -1 = skipped */
+  double rms;    /* RMS relative force error vs FP64 exact; -1 = skipped     */
+  int meets;     /* rms <= the error budget                      */
+} amk_tune_candidate;
+#define AMK_TUNE_NO_ALLPAIRS 1
+#define AMK_TUNE_NO_FMM 2
+#define AMK_TUNE_NO_BARNES_HUT 4
+/* Autotuner: on the context's own particles, times (CUDA events, median of
+ * 3 after a warm call) and audits (amk_force_error with `samples`) the
+ * all-pairs solver, the FMM for orders 4/6/8 x theta 0.5/0.35 x leaf
+ * 16/32/64 (higher orders skipped once a lower one meets the budget) and
+ * Barnes-Hut for theta 0.5/0.3/0.2, then sets the context's Coulomb method,
+ * order, theta and leaf size to the fastest candidate whose RMS error is
+ * <= error_budget. out (max_out entries, may be NULL) receives every
+ * candidate; chosen = its index (-1 and AMK_ERR_LIMIT when none meets). */
+int amk_autotune(amk_ctx* ctx, double error_budget, long samples, int flags, amk_tune_candidate* out,
+                 int max_out, int* n_out, int* chosen);
+
 /* ------------------------------------------------------------ batched sweep */
 /* No counterpart in the reference, which runs one instance per process
  * (antimatter-kernel.cc:153-162); a parameter sweep is many such runs. A
