@@ -159,6 +159,7 @@ def lib():
         "amk_batch_set": (C.c_int, [vp, C.c_int, C.POINTER(Params), C.POINTER(C.c_long)]),
         "amk_batch_step": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
         "amk_batch_coulomb": (C.c_int, [vp]),
+        "amk_batch_autotune": (C.c_int, [vp, C.c_double, C.c_long, C.POINTER(C.c_int)]),
         "amk_batch_status": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_long)]),
         "amk_batch_info": (C.c_int, [vp, C.POINTER(C.c_long), C.POINTER(C.c_long), C.POINTER(C.c_int)]),
         "amk_set_profiling": (C.c_int, [vp, C.c_int]),
@@ -501,6 +502,13 @@ class Simulation:
 
     def batch_step(self, n: int = 1, graph_chunk: int = 0, serial: bool = False):
         check(lib().amk_batch_step(self._h, int(n), int(graph_chunk), 1 if serial else 0), "amk_batch_step")
+
+    def batch_autotune(self, error_budget=1e-5, samples=512):
+        """Per-instance method choice by measurement; returns the methods."""
+        m = np.zeros(getattr(self, "_batch_n", 0), np.int32)
+        check(lib().amk_batch_autotune(self._h, float(error_budget), int(samples),
+                                       m.ctypes.data_as(C.POINTER(C.c_int))), "amk_batch_autotune")
+        return m
 
     def batch_coulomb(self):
         check(lib().amk_batch_coulomb(self._h), "amk_batch_coulomb")

@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <functional>
 #include <string>
 #include <utility>
 #include <vector>
@@ -354,5 +355,10 @@ int annihilate_view(amk_ctx* c, const View& v, const uint8_t* species, const uin
                     double probability, uint32_t seed, uint64_t step_index, long* marked);
 // Batched instances (batch.cu).
 void batch_destroy(amk_ctx* c);
+// RMS / max relative error of a view's forces against the FP64 exact sum
+// over `samples` evenly spaced usable particles (audit.cu).
+int force_error(amk_ctx* c, const View& v, long samples, double* rms, double* max_rel);
+// Median device time (ms) of `reps` calls after one warm call (audit.cu).
+int time_solver(amk_ctx* c, const std::function<int()>& call, int reps, double* ms);
 
 }  // namespace amk

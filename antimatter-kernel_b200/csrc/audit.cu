@@ -12,6 +12,7 @@
 // with the fastest one whose RMS error is within the budget.
 #include <algorithm>
 #include <cmath>
+#include <functional>
 #include <vector>
 
 #include "amk_internal.cuh"
@@ -63,19 +64,20 @@ exact_force_kernel(View v, const long* __restrict__ targets, int n_t, double4* _
 
 }  // namespace
 
-// Evenly spaced usable (alive, charged, finite) targets, at most `samples`.
-int force_error(amk_ctx* c, long samples, double* rms, double* max_rel) {
+// Evenly spaced usable (alive, charged, finite) targets of the view, at most
+// `samples`; the view's force arrays hold the forces under audit.
+int force_error(amk_ctx* c, const View& v, long samples, double* rms, double* max_rel) {
   *rms = 0.0;
   if (max_rel) *max_rel = 0.0;
-  const long n = c->n;
+  const long n = v.n;
   if (n == 0 || samples <= 0) return AMK_OK;
   std::vector<double> x(n), y(n), z(n), q(n), fx(n), fy(n), fz(n);
   std::vector<uint8_t> alive(n);
-  AMK_CUDA_TRY(cudaMemcpyAsync(x.data(), c->x.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  AMK_CUDA_TRY(cudaMemcpyAsync(y.data(), c->y.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  AMK_CUDA_TRY(cudaMemcpyAsync(z.data(), c->z.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  AMK_CUDA_TRY(cudaMemcpyAsync(q.data(), c->q.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  AMK_CUDA_TRY(cudaMemcpyAsync(alive.data(), c->alive.ptr, n, cudaMemcpyDeviceToHost, c->stream));
+  AMK_CUDA_TRY(cudaMemcpyAsync(x.data(), v.x, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  AMK_CUDA_TRY(cudaMemcpyAsync(y.data(), v.y, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  AMK_CUDA_TRY(cudaMemcpyAsync(z.data(), v.z, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  AMK_CUDA_TRY(cudaMemcpyAsync(q.data(), v.q, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  AMK_CUDA_TRY(cudaMemcpyAsync(alive.data(), v.alive, n, cudaMemcpyDeviceToHost, c->stream));
   AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
   std::vector<long> usable;
   usable.reserve(n);
@@ -92,14 +94,13 @@ int force_error(amk_ctx* c, long samples, double* rms, double* max_rel) {
   double4* dex = slot<double4>(c, kSlotAuxState6, m, &rc);
   AMK_TRY(rc);
   AMK_CUDA_TRY(cudaMemcpyAsync(dt, targets.data(), m * sizeof(long), cudaMemcpyHostToDevice, c->stream));
-  exact_force_kernel<<<static_cast<unsigned>((m + 255) / 256), 256, 0, c->stream>>>(main_view(c), dt,
-                                                                                     static_cast<int>(m), dex);
+  exact_force_kernel<<<static_cast<unsigned>((m + 255) / 256), 256, 0, c->stream>>>(v, dt, static_cast<int>(m), dex);
   AMK_TRY(check_launch(c, "exact_force_kernel"));
   std::vector<double4> ex(m);
   AMK_CUDA_TRY(cudaMemcpyAsync(ex.data(), dex, m * sizeof(double4), cudaMemcpyDeviceToHost, c->stream));
-  AMK_CUDA_TRY(cudaMemcpyAsync(fx.data(), c->fx.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  AMK_CUDA_TRY(cudaMemcpyAsync(fy.data(), c->fy.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-  AMK_CUDA_TRY(cudaMemcpyAsync(fz.data(), c->fz.ptr, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  AMK_CUDA_TRY(cudaMemcpyAsync(fx.data(), v.fx, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  AMK_CUDA_TRY(cudaMemcpyAsync(fy.data(), v.fy, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  AMK_CUDA_TRY(cudaMemcpyAsync(fz.data(), v.fz, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
   double sum = 0.0, mx = 0.0;
   long cnt = 0;
@@ -125,10 +126,10 @@ using namespace amk;
 extern "C" int amk_force_error(amk_ctx* c, long samples, double* rms, double* max_rel) {
   if (!c || !rms) return fail(AMK_ERR_INVALID, "null argument");
   AMK_CUDA_TRY(cudaSetDevice(c->device));
-  return force_error(c, samples, rms, max_rel);
+  return force_error(c, main_view(c), samples, rms, max_rel);
 }
 
-namespace {
+namespace amk {
 
 // Device time of one solver call (ms): one warm call, then the median of
 // `reps` timed calls.
@@ -157,7 +158,11 @@ int time_call(amk_ctx* c, F&& call, int reps, double* ms) {
   return AMK_OK;
 }
 
-}  // namespace
+int time_solver(amk_ctx* c, const std::function<int()>& call, int reps, double* ms) {
+  return time_call(c, call, reps, ms);
+}
+
+}  // namespace amk
 
 extern "C" int amk_autotune(amk_ctx* c, double error_budget, long samples, int flags, amk_tune_candidate* out,
                             int max_out, int* n_out, int* chosen) {
@@ -201,7 +206,7 @@ extern "C" int amk_autotune(amk_ctx* c, double error_budget, long samples, int f
       }
     };
     AMK_TRY(time_call(c, call, 3, &d.ms));
-    AMK_TRY(force_error(c, samples, &d.rms, nullptr));
+    AMK_TRY(force_error(c, main_view(c), samples, &d.rms, nullptr));
     d.meets = d.rms <= error_budget ? 1 : 0;
     if (d.meets && d.ms < best_ms) {
       best_ms = d.ms;

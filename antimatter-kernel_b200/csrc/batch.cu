@@ -430,6 +430,7 @@ struct Batch {
   std::vector<double> scale;
   std::vector<PushParams> push;
   std::vector<int> solver_instances;  // instances with a per-instance solver call
+  std::vector<int> leaf;              // leaf capacity of each instance's tree solver
   bool any_annihilation = false;
   bool graphable = true;
   DevBuf inst, inst_of, units, counters, contacts, best, flags, keys, vals, skeys, sidx;
@@ -510,9 +511,10 @@ int instance_coulomb(amk_ctx* c, const Batch& B, int i) {
   switch (p.coulomb_method) {
     case AMK_METHOD_ALLPAIRS: return allpairs_forces(c, v);
     case AMK_METHOD_STANDARD: return cutoff_forces(c, v, p.cutoff_radius, nullptr);
-    case AMK_METHOD_BARNES_HUT: return barnes_hut_forces(c, v, p.barnes_hut_theta, 8);
+    case AMK_METHOD_BARNES_HUT: return barnes_hut_forces(c, v, p.barnes_hut_theta, B.leaf[i]);
     case AMK_METHOD_FAST_MULTIPOLE:
-      return fmm_forces(c, v, static_cast<int>(p.fast_multipole_order), p.fast_multipole_theta, 32, false, nullptr);
+      return fmm_forces(c, v, static_cast<int>(p.fast_multipole_order), p.fast_multipole_theta, B.leaf[i], false,
+                        nullptr);
     default: return fail(AMK_ERR_INVALID, "unknown coulomb method %d", p.coulomb_method);
   }
 }
@@ -696,6 +698,7 @@ extern "C" int amk_batch_set(amk_ctx* c, int n_inst, const amk_params* params, c
     d.tile0 = n_tiles;
     if (p.coulomb_forces_enabled && p.coulomb_method == AMK_METHOD_ALLPAIRS) n_tiles += (cnt + kBT - 1) / kBT;
     d.seed = static_cast<uint32_t>(p.seed);
+    B->leaf.push_back(p.coulomb_method == AMK_METHOD_BARNES_HUT ? 8 : 32);
     d.offset = off;
     d.count = cnt;
     if (!p.coulomb_forces_enabled || cnt == 0) continue;
@@ -861,5 +864,108 @@ extern "C" int amk_batch_info(const amk_ctx* c, long* n_instances, long* work_un
   if (n_instances) *n_instances = c->batch->n_inst;
   if (work_units) *work_units = c->batch->n_units;
   if (graphable) *graphable = c->batch->graphable ? 1 : 0;
+  return AMK_OK;
+}
+
+// Per-instance method choice by measurement: the batched all-pairs launch is
+// timed once (its cost split over instances in proportion to N_i^2); the FMM
+// configurations (orders 4/6/8, theta 0.5/0.35, leaf 32/64; higher orders
+// skipped once a lower one meets the budget) are timed and audited on the
+// largest instance; the best one that meets the budget then replaces
+// all-pairs on every instance, largest first, where its measured time is
+// below the instance's all-pairs share and its audit meets the budget. The
+// batch is rebuilt with the chosen methods.
+extern "C" int amk_batch_autotune(amk_ctx* c, double error_budget, long samples, int* methods_out) {
+  if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (!c->batch) return fail(AMK_ERR_STATE, "no batch: call amk_batch_set first");
+  if (!(error_budget > 0.0)) return fail(AMK_ERR_INVALID, "error budget must be positive");
+  AMK_CUDA_TRY(cudaSetDevice(c->device));
+  const int n_inst = c->batch->n_inst;
+  std::vector<amk_params> P = c->batch->params;
+  const std::vector<long> offsets = c->batch->offsets;
+  std::vector<int> leaf(n_inst, 32);
+  for (int i = 0; i < n_inst; ++i)
+    if (P[i].coulomb_forces_enabled) P[i].coulomb_method = AMK_METHOD_ALLPAIRS;
+  AMK_TRY(amk_batch_set(c, n_inst, P.data(), offsets.data()));
+  Batch* B = c->batch;
+  // 1. the batched all-pairs launch and its cost share per instance
+  double ap_ms = 0.0;
+  AMK_TRY(time_solver(c, [&]() -> int {
+    AMK_CUDA_TRY(cudaMemsetAsync(B->queue(), 0, sizeof(int), c->stream));
+    return batch_coulomb(c, *B);
+  }, 3, &ap_ms));
+  std::vector<int> order;
+  double total_pairs = 0.0;
+  for (int i = 0; i < n_inst; ++i) {
+    const double ni = static_cast<double>(offsets[i + 1] - offsets[i]);
+    if (P[i].coulomb_forces_enabled && ni > 1) {
+      order.push_back(i);
+      total_pairs += ni * ni;
+    }
+  }
+  if (order.empty()) {
+    if (methods_out)
+      for (int i = 0; i < n_inst; ++i) methods_out[i] = P[i].coulomb_method;
+    return AMK_OK;
+  }
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return offsets[a + 1] - offsets[a] > offsets[b + 1] - offsets[b];
+  });
+  auto ap_share = [&](int i) {
+    const double ni = static_cast<double>(offsets[i + 1] - offsets[i]);
+    return ap_ms * ni * ni / total_pairs;
+  };
+  // all-pairs must itself meet the budget (on the largest instance)
+  double ap_err = 0.0;
+  AMK_TRY(force_error(c, instance_view(c, *B, order[0]), samples, &ap_err, nullptr));
+  // 2. FMM configurations on the largest instance
+  const int big = order[0];
+  const View vb = instance_view(c, *B, big);
+  int best_order = 0, best_leaf = 32;
+  double best_theta = 0.5, best_ms = INFINITY;
+  for (double theta : {0.5, 0.35})
+    for (int lf : {32, 64})
+      for (int p : {4, 6, 8}) {
+        double ms = 0.0, err = 0.0;
+        AMK_TRY(time_solver(c, [&]() { return fmm_forces(c, vb, p, theta, lf, false, nullptr); }, 1, &ms));
+        AMK_TRY(force_error(c, vb, samples, &err, nullptr));
+        if (err <= error_budget) {
+          if (ms < best_ms) {
+            best_ms = ms;
+            best_order = p;
+            best_theta = theta;
+            best_leaf = lf;
+          }
+          break;  // higher orders at this theta and leaf cost more
+        }
+      }
+  // 3. instances, largest first, switch to that FMM where it is faster
+  int losses = 0;
+  if (best_order > 0)
+    for (int i : order) {
+      if (losses >= 2) break;
+      const View v = instance_view(c, *B, i);
+      double ms = 0.0, err = 0.0;
+      AMK_TRY(time_solver(c, [&]() { return fmm_forces(c, v, best_order, best_theta, best_leaf, false, nullptr); },
+                          1, &ms));
+      AMK_TRY(force_error(c, v, samples, &err, nullptr));
+      if ((ms < ap_share(i) || ap_err > error_budget) && err <= error_budget) {
+        P[i].coulomb_method = AMK_METHOD_FAST_MULTIPOLE;
+        P[i].fast_multipole_order = best_order;
+        P[i].fast_multipole_theta = best_theta;
+        P[i].fmm_learned = 0;
+        leaf[i] = best_leaf;
+        losses = 0;
+      } else {
+        ++losses;
+      }
+    }
+  AMK_TRY(amk_batch_set(c, n_inst, P.data(), offsets.data()));
+  for (int i = 0; i < n_inst; ++i)
+    if (P[i].coulomb_method == AMK_METHOD_FAST_MULTIPOLE) c->batch->leaf[i] = leaf[i];
+  if (methods_out)
+    for (int i = 0; i < n_inst; ++i) methods_out[i] = P[i].coulomb_forces_enabled ? P[i].coulomb_method : -1;
+  if (ap_err > error_budget && best_order == 0)
+    return fail(AMK_ERR_LIMIT, "neither all-pairs (%g) nor the FMM met the error budget %g", ap_err, error_budget);
   return AMK_OK;
 }

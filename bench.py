@@ -325,6 +325,12 @@ def run_sweep(args):
     n_total = int(sum(len(i[0]) for i in insts))
     sim = amk.Simulation(device=local)
     load_sweep(sim, insts)
+    # per-instance method by measurement under the 1e-5 RMS force-error budget
+    t0 = time.perf_counter()
+    methods = sim.batch_autotune(error_budget=1e-5, samples=256)
+    tune_s = time.perf_counter() - t0
+    names = {-1: "none", 0: "cutoff", 1: "barnes-hut", 2: "fmm", 3: "allpairs"}
+    method_counts = {names[int(m)]: int((methods == m).sum()) for m in np.unique(methods)}
     chunk = min(100, args.steps)
 
     def barrier():
@@ -441,8 +447,10 @@ def run_sweep(args):
                                        f"(total {n_total:,}), e-/e+ or e+/pbar 1:1, T 4..1e4 K, b0 1..5 T, "
                                        "U 5..50 V, radii 5e-5..5e-4 m, cooling (4 K) and annihilation "
                                        "(5e-6 m, p=0.5) on",
-                           "solver": "all-pairs for every instance (one persistent launch, "
-                                     "cost-ordered work queue), FP64 state",
+                           "solver": "per-instance method chosen by amk_batch_autotune under a 1e-5 "
+                                     "RMS force-error budget; all-pairs instances share one persistent "
+                                     "launch (cost-ordered work queue); FP64 state",
+                           "autotune": {"methods": method_counts, "seconds": round(tune_s, 2)},
                            "graph_chunk": chunk, "instances": len(insts), "n_particles": n_total,
                            "instance_sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)),
                                               "max": int(sizes.max())},

@@ -384,6 +384,16 @@ int amk_batch_coulomb(amk_ctx* ctx);
  * twice the largest count seen so far. alive_counts (n_inst entries, may be
  * NULL): live particles per instance. */
 int amk_batch_status(amk_ctx* ctx, int* overflow, long* alive_counts);
+/* Batch autotuner: chooses each instance's Coulomb method by measurement
+ * under an RMS force-error budget (audited against the FP64 exact sum with
+ * `samples` particles): the batched all-pairs launch is timed and its cost
+ * split over instances by N_i^2; FMM configurations (order 4/6/8, theta
+ * 0.5/0.35, leaf 32/64) are timed and audited on the largest instance, and
+ * the fastest that meets the budget replaces all-pairs on each instance,
+ * largest first, where it is faster there. Rebuilds the batch; methods_out
+ * (n_inst entries, may be NULL) receives the chosen AMK_METHOD_* (-1 for
+ * instances without Coulomb forces). */
+int amk_batch_autotune(amk_ctx* ctx, double error_budget, long samples, int* methods_out);
 /* n_instances, all-pairs work units (instance, 128-target block) and
  * whether the batch can run as CUDA graphs. */
 int amk_batch_info(const amk_ctx* ctx, long* n_instances, long* work_units, int* graphable);

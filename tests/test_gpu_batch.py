@@ -202,3 +202,28 @@ def test_batch_argument_errors_and_state():
         # loading a new particle set ends the batch
         s.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
         s.step(1)
+
+
+def test_batch_autotune_chooses_methods_that_meet_the_budget():
+    insts = [instance(200000, 91, sigma=2e-4), instance(3000, 92), instance(40, 93),
+             instance(500, 94, coulomb_forces_enabled=0)]
+    with amk.Simulation() as s:
+        off = load(s, insts)
+        methods = s.batch_autotune(error_budget=5e-3, samples=256)
+        assert methods[3] == -1  # no Coulomb forces
+        assert all(m in (2, 3) for m in methods[:3])
+        assert methods[1] == 3 and methods[2] == 3  # small instances stay all-pairs
+        s.batch_coulomb()
+        fx, fy, fz = s.get_forces()
+        for i in range(3):
+            pos, _, sp, _ = insts[i]
+            q = np.where(np.isin(sp, (1, 4)), E, -E)
+            k = np.arange(0, len(pos), max(1, len(pos) // 200))
+            gx, gy, gz = O.allpairs_subset(pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy(), q, k)
+            a = off[i]
+            num = np.sqrt((fx[a + k] - gx) ** 2 + (fy[a + k] - gy) ** 2 + (fz[a + k] - gz) ** 2)
+            den = np.sqrt(gx ** 2 + gy ** 2 + gz ** 2)
+            assert np.sqrt(np.mean((num / den) ** 2)) <= 5e-3 * 1.5, i
+        s.batch_step(2)
+        with pytest.raises(amk.AmkError):
+            s.batch_autotune(error_budget=1e-13, samples=64)
