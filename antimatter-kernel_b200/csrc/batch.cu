@@ -36,7 +36,13 @@ int push_range(amk_ctx* c, const PushParams& P, long begin, long end, bool stagg
 
 namespace {
 
-constexpr int kBT = 128;           // threads per all-pairs CTA = targets per unit = sources per tile
+constexpr int kBT = 128;           // threads per all-pairs CTA = sources per staged chunk
+constexpr int kBR = 2;             // targets per thread: a warp owns 64 consecutive targets
+constexpr int kBUnit = kBT * kBR;  // targets per work unit
+constexpr int kBSub = 32;          // particles per sub-tile (box granularity)
+constexpr int kBSubPerChunk = kBT / kBSub;
+constexpr int kBSubPerUnit = kBUnit / kBSub;
+constexpr float kBNearFactor = 0.25f;
 constexpr int kGridBits = 10;      // annihilation cells per axis per instance: 2^10
 constexpr int kInstBits = 9;       // up to 512 instances
 constexpr int kMaxInstances = 1 << kInstBits;
@@ -50,7 +56,7 @@ struct InstanceDev {
   double origin[3], inv_cell;          // annihilation grid (cells >= the contact radius)
   double inv_sort_cell;                // all-pairs ordering grid: 1022 cells over the same cube
   long offset, count;
-  long tile0;                          // first all-pairs tile of the instance
+  long sub0;                           // first all-pairs sub-tile slot of the instance
   int annihilation;
   uint32_t seed;
 };
@@ -74,11 +80,13 @@ __global__ void batch_local_ids_kernel(long n, const uint16_t* __restrict__ inst
 // in its instance's grid); usable particles (alive, charged, finite) sort
 // before the others of their instance. The stable sort keeps each instance
 // inside its own [offset, offset + count) range, so sorted position k holds
-// a particle of the same instance as original index k. Tiles of 128 sorted
-// positions within an instance get a box; tile pairs whose boxes are
-// separated by more than their half-extents use FP32 offsets from the source
-// tile's centre (12 FP32 ops per pair), the others exact double-float
-// differences (18 ops per pair, the self pair gives exactly 0).
+// a particle of the same instance as original index k. Every 32 sorted
+// positions of an instance form a sub-tile with a box; a warp owns 64
+// consecutive targets and decides near/far per 32-source sub-tile, uniform
+// across the warp: sub-tiles farther than a quarter of the summed
+// half-extent norms use FP32 offsets from the sub-tile centre (12 FP32 ops
+// per pair, relative error <= 7 eps of |r|), the others exact double-float
+// differences (18 ops per pair; the self pair gives exactly 0).
 __global__ void batch_sort_key_kernel(long n, const double* __restrict__ x, const double* __restrict__ y,
                                       const double* __restrict__ z, const double* __restrict__ q,
                                       const uint8_t* __restrict__ alive, const uint16_t* __restrict__ inst_of,
@@ -108,20 +116,20 @@ struct TileBox {
   float4 h;   // half-extents (rounded up); w = |h|
 };
 
-// One CTA per all-pairs unit = tile of up to 128 sorted positions: the
-// double-float staging, the offsets from the tile centre and the tile box.
-__global__ void __launch_bounds__(kBT)
+// One CTA of 256 threads per all-pairs unit (256 sorted positions of one
+// instance); each warp stages its 32-position sub-tile: double-float
+// positions, offsets from the sub-tile centre and the sub-tile box. Slots of
+// sub-tiles past the instance's end receive empty boxes.
+__global__ void __launch_bounds__(kBUnit)
 batch_tile_stage_kernel(const int2* __restrict__ units, const InstanceDev* __restrict__ inst,
                         const uint32_t* __restrict__ perm, const double* __restrict__ x,
                         const double* __restrict__ y, const double* __restrict__ z, const double* __restrict__ q,
                         const uint8_t* __restrict__ alive, float4* __restrict__ hq, float4* __restrict__ lo,
                         float4* __restrict__ rel, TileBox* __restrict__ boxes) {
-  __shared__ double red[6][kBT / 32];
-  __shared__ double box[6];
   const int2 un = units[blockIdx.x];
   const InstanceDev& I = inst[un.x];
   const long e = I.offset + I.count;
-  const long k = I.offset + static_cast<long>(un.y) * kBT + threadIdx.x;
+  const long k = I.offset + static_cast<long>(un.y) * kBUnit + threadIdx.x;
   double xs = 0.0, ys = 0.0, zs = 0.0, qe = 0.0;
   bool ok = false;
   if (k < e) {
@@ -137,19 +145,10 @@ batch_tile_stage_kernel(const int2* __restrict__ units, const InstanceDev* __res
 #pragma unroll
   for (int d = 0; d < 6; ++d)
     for (int o = 16; o > 0; o >>= 1) m[d] = fmin(m[d], __shfl_xor_sync(0xffffffffu, m[d], o));
-  if ((threadIdx.x & 31) == 0)
-    for (int d = 0; d < 6; ++d) red[d][threadIdx.x >> 5] = m[d];
-  __syncthreads();
-  if (threadIdx.x < 6) {
-    double r = INFINITY;
-    for (int w = 0; w < kBT / 32; ++w) r = fmin(r, red[threadIdx.x][w]);
-    box[threadIdx.x] = r;
-  }
-  __syncthreads();
-  const bool any = isfinite(box[0]);
-  const double cx = any ? 0.5 * (box[0] - box[3]) : 0.0;
-  const double cy = any ? 0.5 * (box[1] - box[4]) : 0.0;
-  const double cz = any ? 0.5 * (box[2] - box[5]) : 0.0;
+  const bool any = isfinite(m[0]);
+  const double cx = any ? 0.5 * (m[0] - m[3]) : 0.0;
+  const double cy = any ? 0.5 * (m[1] - m[4]) : 0.0;
+  const double cz = any ? 0.5 * (m[2] - m[5]) : 0.0;
   float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h, u = h;
   if (ok) {
     h = make_float4(__double2float_rn(xs), __double2float_rn(ys), __double2float_rn(zs), __double2float_rn(qe));
@@ -162,114 +161,171 @@ batch_tile_stage_kernel(const int2* __restrict__ units, const InstanceDev* __res
     lo[k] = l;
     rel[k] = u;
   }
-  if (threadIdx.x == 0) {
+  if ((threadIdx.x & 31) == 0) {
     TileBox b;
     b.c = make_float4(__double2float_rn(cx), __double2float_rn(cy), __double2float_rn(cz), any ? 1.f : 0.f);
     b.cl = make_float4(__double2float_rn(cx - static_cast<double>(b.c.x)),
                        __double2float_rn(cy - static_cast<double>(b.c.y)),
                        __double2float_rn(cz - static_cast<double>(b.c.z)), 0.f);
-    const double hx = any ? 0.5 * (-box[3] - box[0]) : 0.0;
-    const double hy = any ? 0.5 * (-box[4] - box[1]) : 0.0;
-    const double hz = any ? 0.5 * (-box[5] - box[2]) : 0.0;
+    const double hx = any ? 0.5 * (-m[3] - m[0]) : 0.0;
+    const double hy = any ? 0.5 * (-m[4] - m[1]) : 0.0;
+    const double hz = any ? 0.5 * (-m[5] - m[2]) : 0.0;
     b.h = make_float4(__double2float_ru(hx), __double2float_ru(hy), __double2float_ru(hz),
                       __double2float_ru(sqrt(hx * hx + hy * hy + hz * hz)));
-    boxes[I.tile0 + un.y] = b;
+    boxes[I.sub0 + static_cast<long>(un.y) * kBSubPerUnit + (threadIdx.x >> 5)] = b;
   }
 }
 
-// Persistent all-pairs over (instance, target tile) units taken from a queue
-// (`queue` zeroed before every launch): F_i = k e q_i / L^2 * sum_j q_j
+// Persistent all-pairs over (instance, 256-target block) units taken from a
+// queue (`queue` zeroed before every launch): F_i = k e q_i / L^2 * sum_j q_j
 // (r_i - r_j) / |r_i - r_j|^3 in scaled units, written to the particle's
-// original index.
+// original index. Warp w of a unit owns targets [64 w, 64 w + 64) of the
+// block: lane l holds +l (r = 0) and +32+l (r = 1).
 __global__ void __launch_bounds__(kBT)
 batch_allpairs_kernel(const int2* __restrict__ units, int n_units, const InstanceDev* __restrict__ inst,
                       const float4* __restrict__ hq, const float4* __restrict__ lo, const float4* __restrict__ rel,
                       const TileBox* __restrict__ boxes, const uint32_t* __restrict__ perm,
                       const double* __restrict__ q, double* __restrict__ fx, double* __restrict__ fy,
                       double* __restrict__ fz, int* __restrict__ queue) {
-  __shared__ float4 sa[kBT], sb[kBT];
+  __shared__ float4 sa[kBT], sb[kBT], sc[kBT];
+  __shared__ TileBox sbox[kBSubPerChunk];
+  __shared__ float4 swc[kBT / 32], swh[kBT / 32];
   __shared__ int s_unit;
   const int tid = threadIdx.x;
+  const int lane = tid & 31, warp = tid >> 5;
   for (;;) {
+    __syncthreads();  // the previous unit's readers are done with s_unit and the buffers
     if (tid == 0) s_unit = atomicAdd(queue, 1);
     __syncthreads();
     const int u = s_unit;
     if (u >= n_units) return;
     const int2 un = units[u];
     const long b = inst[un.x].offset, e = b + inst[un.x].count;
-    const long tile0 = inst[un.x].tile0;
-    const int n_tiles = static_cast<int>((e - b + kBT - 1) / kBT);
+    const long sub0 = inst[un.x].sub0;
+    const long n_sub = (e - b + kBSub - 1) / kBSub;
     const double inv_l = inst[un.x].inv_l;
-    const long k = b + static_cast<long>(un.y) * kBT + tid;
-    float4 th = make_float4(0.f, 0.f, 0.f, 0.f), tl = th;
-    if (k < e) {
-      th = hq[k];
-      tl = lo[k];
-    }
-    const TileBox tb = boxes[tile0 + un.y];
     const float eps2 = static_cast<float>(fmax(kMinSquaredDistance * inv_l * inv_l, 1e-25));
-    float ahx = 0.f, ahy = 0.f, ahz = 0.f, alx = 0.f, aly = 0.f, alz = 0.f;
-    for (int t = 0; t < n_tiles; ++t) {
-      const TileBox sbx = boxes[tile0 + t];
-      if (sbx.c.w == 0.f || tb.c.w == 0.f) continue;  // no usable sources or targets (uniform)
-      const float gx = fmaxf(fabsf(tb.c.x - sbx.c.x) - (tb.h.x + sbx.h.x), 0.f);
-      const float gy = fmaxf(fabsf(tb.c.y - sbx.c.y) - (tb.h.y + sbx.h.y), 0.f);
-      const float gz = fmaxf(fabsf(tb.c.z - sbx.c.z) - (tb.h.z + sbx.h.z), 0.f);
-      const float lim = 1.01f * (tb.h.w + sbx.h.w);
-      const bool near = gx * gx + gy * gy + gz * gz <= lim * lim;
-      const long j = b + static_cast<long>(t) * kBT + tid;
-      __syncthreads();  // the previous tile's readers are done with the buffers
-      if (near) {
-        sa[tid] = j < e ? hq[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-        sb[tid] = j < e ? lo[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const long kw = b + static_cast<long>(un.y) * kBUnit + warp * (kBSub * kBR);  // the warp's first target
+    float tx[kBR], ty[kBR], tz[kBR], ux[kBR], uy[kBR], uz[kBR];
+    float ahx[kBR], ahy[kBR], ahz[kBR], alx[kBR], aly[kBR], alz[kBR];
+    bool live_t[kBR];
+#pragma unroll
+    for (int r = 0; r < kBR; ++r) {
+      const long k = kw + r * kBSub + lane;
+      float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
+      if (k < e) {
+        h = hq[k];
+        l = lo[k];
+      }
+      live_t[r] = h.w != 0.f;
+      tx[r] = h.x; ty[r] = h.y; tz[r] = h.z;
+      ux[r] = l.x; uy[r] = l.y; uz[r] = l.z;
+      ahx[r] = ahy[r] = ahz[r] = alx[r] = aly[r] = alz[r] = 0.f;
+    }
+    // union box of the warp's two target sub-tiles
+    const long s_loc = (kw - b) / kBSub;
+    TileBox b0 = s_loc < n_sub ? boxes[sub0 + s_loc] : TileBox{};
+    TileBox b1 = s_loc + 1 < n_sub ? boxes[sub0 + s_loc + 1] : TileBox{};
+    if (b1.c.w == 0.f) b1 = b0;
+    if (b0.c.w == 0.f) b0 = b1;
+    const bool warp_live = b0.c.w != 0.f;
+    if (lane == 0) {
+      const float lx = fminf(b0.c.x - b0.h.x, b1.c.x - b1.h.x), hx = fmaxf(b0.c.x + b0.h.x, b1.c.x + b1.h.x);
+      const float ly = fminf(b0.c.y - b0.h.y, b1.c.y - b1.h.y), hy = fmaxf(b0.c.y + b0.h.y, b1.c.y + b1.h.y);
+      const float lz = fminf(b0.c.z - b0.h.z, b1.c.z - b1.h.z), hz = fmaxf(b0.c.z + b0.h.z, b1.c.z + b1.h.z);
+      float4 wh = make_float4(0.5001f * (hx - lx), 0.5001f * (hy - ly), 0.5001f * (hz - lz), 0.f);
+      wh.w = 1.0001f * sqrtf(wh.x * wh.x + wh.y * wh.y + wh.z * wh.z);
+      swc[warp] = make_float4(0.5f * (lx + hx), 0.5f * (ly + hy), 0.5f * (lz + hz), 0.f);
+      swh[warp] = wh;
+    }
+    for (long c0 = b; c0 < e; c0 += kBT) {
+      const long j = c0 + tid;
+      __syncthreads();  // the previous chunk's readers are done with the buffers
+      if (j < e) {
+        sa[tid] = hq[j];
+        sb[tid] = lo[j];
+        sc[tid] = rel[j];
       } else {
-        sa[tid] = j < e ? rel[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+        sa[tid] = sb[tid] = sc[tid] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+      if (tid < kBSubPerChunk) {
+        const long s = (c0 - b) / kBSub + tid;
+        sbox[tid] = s < n_sub ? boxes[sub0 + s] : TileBox{};
       }
       __syncthreads();
-      const int cnt = static_cast<int>(min(static_cast<long>(kBT), e - (b + static_cast<long>(t) * kBT)));
-      float px = 0.f, py = 0.f, pz = 0.f;
-      if (near) {
+      if (!warp_live) continue;  // no usable target in this warp (uniform)
+      const float4 wc = swc[warp], wh = swh[warp];
+      float px[kBR], py[kBR], pz[kBR];
+#pragma unroll
+      for (int r = 0; r < kBR; ++r) px[r] = py[r] = pz[r] = 0.f;
+      for (int qd = 0; qd < kBSubPerChunk; ++qd) {
+        const TileBox sbx = sbox[qd];
+        if (sbx.c.w == 0.f) continue;  // no usable sources (uniform)
+        const float gx = fmaxf(fabsf(wc.x - sbx.c.x) - (wh.x + sbx.h.x), 0.f);
+        const float gy = fmaxf(fabsf(wc.y - sbx.c.y) - (wh.y + sbx.h.y), 0.f);
+        const float gz = fmaxf(fabsf(wc.z - sbx.c.z) - (wh.z + sbx.h.z), 0.f);
+        const float lim = kBNearFactor * (wh.w + sbx.h.w);
+        const int base = qd * kBSub;
+        if (gx * gx + gy * gy + gz * gz <= lim * lim) {
 #pragma unroll 8
-        for (int s = 0; s < cnt; ++s) {
-          const float4 sh = sa[s], sl = sb[s];
-          const float dx = (th.x - sh.x) + (tl.x - sl.x);
-          const float dy = (th.y - sh.y) + (tl.y - sl.y);
-          const float dz = (th.z - sh.z) + (tl.z - sl.z);
-          const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-          const float rinv = rsqrtf(d2);
-          const float w = (sh.w * rinv) * (rinv * rinv);
-          px = fmaf(w, dx, px);
-          py = fmaf(w, dy, py);
-          pz = fmaf(w, dz, pz);
-        }
-      } else {
-        const float ax = (th.x - sbx.c.x) + (tl.x - sbx.cl.x);
-        const float ay = (th.y - sbx.c.y) + (tl.y - sbx.cl.y);
-        const float az = (th.z - sbx.c.z) + (tl.z - sbx.cl.z);
+          for (int k = 0; k < kBSub; ++k) {
+            const float4 sh = sa[base + k], sl = sb[base + k];
+#pragma unroll
+            for (int r = 0; r < kBR; ++r) {
+              const float dx = (tx[r] - sh.x) + (ux[r] - sl.x);
+              const float dy = (ty[r] - sh.y) + (uy[r] - sl.y);
+              const float dz = (tz[r] - sh.z) + (uz[r] - sl.z);
+              const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+              const float rinv = rsqrtf(d2);
+              const float w = (sh.w * rinv) * (rinv * rinv);
+              px[r] = fmaf(w, dx, px[r]);
+              py[r] = fmaf(w, dy, py[r]);
+              pz[r] = fmaf(w, dz, pz[r]);
+            }
+          }
+        } else {
+          float ax[kBR], ay[kBR], az[kBR];
+#pragma unroll
+          for (int r = 0; r < kBR; ++r) {
+            ax[r] = (tx[r] - sbx.c.x) + (ux[r] - sbx.cl.x);
+            ay[r] = (ty[r] - sbx.c.y) + (uy[r] - sbx.cl.y);
+            az[r] = (tz[r] - sbx.c.z) + (uz[r] - sbx.cl.z);
+          }
 #pragma unroll 8
-        for (int s = 0; s < cnt; ++s) {
-          const float4 sr = sa[s];
-          const float dx = ax - sr.x;
-          const float dy = ay - sr.y;
-          const float dz = az - sr.z;
-          const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-          const float rinv = rsqrtf(d2);
-          const float w = (sr.w * rinv) * (rinv * rinv);
-          px = fmaf(w, dx, px);
-          py = fmaf(w, dy, py);
-          pz = fmaf(w, dz, pz);
+          for (int k = 0; k < kBSub; ++k) {
+            const float4 sr = sc[base + k];
+#pragma unroll
+            for (int r = 0; r < kBR; ++r) {
+              const float dx = ax[r] - sr.x;
+              const float dy = ay[r] - sr.y;
+              const float dz = az[r] - sr.z;
+              const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+              const float rinv = rsqrtf(d2);
+              const float w = (sr.w * rinv) * (rinv * rinv);
+              px[r] = fmaf(w, dx, px[r]);
+              py[r] = fmaf(w, dy, py[r]);
+              pz[r] = fmaf(w, dz, pz[r]);
+            }
+          }
         }
       }
-      fold(ahx, alx, px);
-      fold(ahy, aly, py);
-      fold(ahz, alz, pz);
+#pragma unroll
+      for (int r = 0; r < kBR; ++r) {
+        fold(ahx[r], alx[r], px[r]);
+        fold(ahy[r], aly[r], py[r]);
+        fold(ahz[r], alz[r], pz[r]);
+      }
     }
-    if (k < e) {
-      const long i = perm[k];
-      const double coef = th.w != 0.f ? kCoulombConstant * kElementaryCharge * inv_l * inv_l * q[i] : 0.0;
-      fx[i] = coef * (static_cast<double>(ahx) + static_cast<double>(alx));
-      fy[i] = coef * (static_cast<double>(ahy) + static_cast<double>(aly));
-      fz[i] = coef * (static_cast<double>(ahz) + static_cast<double>(alz));
+#pragma unroll
+    for (int r = 0; r < kBR; ++r) {
+      const long k = kw + r * kBSub + lane;
+      if (k < e) {
+        const long i = perm[k];
+        const double coef = live_t[r] ? kCoulombConstant * kElementaryCharge * inv_l * inv_l * q[i] : 0.0;
+        fx[i] = coef * (static_cast<double>(ahx[r]) + static_cast<double>(alx[r]));
+        fy[i] = coef * (static_cast<double>(ahy[r]) + static_cast<double>(aly[r]));
+        fz[i] = coef * (static_cast<double>(ahz[r]) + static_cast<double>(alz[r]));
+      }
     }
   }
 }
@@ -568,7 +624,7 @@ int batch_coulomb(amk_ctx* c, Batch& B) {
     AMK_TRY(check_launch(c, "batch_sort_key_kernel"));
     AMK_TRY(radix_sort_pairs(c, B.keys.as<uint64_t>(), B.vals.as<uint32_t>(), B.skeys.as<uint64_t>(),
                              B.perm.as<uint32_t>(), n, kInstBits + 30));
-    batch_tile_stage_kernel<<<static_cast<unsigned>(B.n_units), kBT, 0, c->stream>>>(
+    batch_tile_stage_kernel<<<static_cast<unsigned>(B.n_units), kBUnit, 0, c->stream>>>(
         B.units.as<int2>(), B.inst.as<InstanceDev>(), B.perm.as<uint32_t>(), c->x.as<double>(), c->y.as<double>(),
         c->z.as<double>(), c->q.as<double>(), c->alive.as<uint8_t>(), c->hq.as<float4>(), c->lo.as<float4>(),
         B.rel.as<float4>(), B.boxes.as<TileBox>());
@@ -670,7 +726,7 @@ extern "C" int amk_batch_set(amk_ctx* c, int n_inst, const amk_params* params, c
   std::vector<InstanceDev> inst(n_inst);
   std::vector<uint16_t> inst_of(n);
   std::vector<std::pair<long, int2>> units;  // (instance size, unit)
-  long n_tiles = 0;
+  long n_tiles = 0;  // all-pairs sub-tile slots (kBSubPerUnit per unit)
   for (int i = 0; i < n_inst; ++i) {
     const amk_params& p = params[i];
     const long off = offsets[i], cnt = offsets[i + 1] - off;
@@ -695,15 +751,16 @@ extern "C" int amk_batch_set(amk_ctx* c, int n_inst, const amk_params* params, c
     for (int k = 0; k < 3; ++k) d.origin[k] = -reach;
     d.inv_cell = 1.0 / cs;
     d.inv_sort_cell = 1022.0 / (2.0 * reach);
-    d.tile0 = n_tiles;
-    if (p.coulomb_forces_enabled && p.coulomb_method == AMK_METHOD_ALLPAIRS) n_tiles += (cnt + kBT - 1) / kBT;
+    d.sub0 = n_tiles;
+    if (p.coulomb_forces_enabled && p.coulomb_method == AMK_METHOD_ALLPAIRS)
+      n_tiles += (cnt + kBUnit - 1) / kBUnit * kBSubPerUnit;
     d.seed = static_cast<uint32_t>(p.seed);
     B->leaf.push_back(p.coulomb_method == AMK_METHOD_BARNES_HUT ? 8 : 32);
     d.offset = off;
     d.count = cnt;
     if (!p.coulomb_forces_enabled || cnt == 0) continue;
     if (p.coulomb_method == AMK_METHOD_ALLPAIRS) {
-      for (long b = 0; b * kBT < cnt; ++b) units.push_back({cnt, make_int2(i, static_cast<int>(b))});
+      for (long b = 0; b * kBUnit < cnt; ++b) units.push_back({cnt, make_int2(i, static_cast<int>(b))});
     } else {
       B->solver_instances.push_back(i);
       if (p.coulomb_method == AMK_METHOD_BARNES_HUT || p.coulomb_method == AMK_METHOD_FAST_MULTIPOLE)

@@ -337,6 +337,13 @@ def run_sweep(args):
         if world > 1:
             torch.distributed.barrier()
 
+    def live():
+        return int(sim.batch_status()["alive"].sum())
+
+    def live_rate(ms, steps, before, after):
+        # particle-steps/s over the live particles (annihilated ones do no work)
+        return world * 0.5 * (before + after) * steps / (ms * 1e-3)
+
     def timed(fn):
         # events on the stream of the context in use (contexts are replaced below)
         st = torch.cuda.ExternalStream(sim.stream(), device=device)
@@ -359,11 +366,13 @@ def run_sweep(args):
     sampler = ClockSampler(local)
     sampler.start()
     launches0 = sim.kernel_launches()
+    live0 = live()
     ms = timed(lambda: sim.batch_step(args.steps, graph_chunk=chunk))
+    live1 = live()
     launches = sim.kernel_launches() - launches0
     clocks = sampler.stop()
     ms = max_over_ranks(ms, world, device)
-    value = world * n_total * args.steps / (ms * 1e-3)
+    value = live_rate(ms, args.steps, live0, live1)
 
     # per-phase device time (profiling runs plain steps, no graph)
     prof_steps = 2
@@ -375,31 +384,38 @@ def run_sweep(args):
     sim.set_profiling(False)
     ap_ms, ap_launches = phases["allpairs"]
     ap_avg = ap_ms / max(ap_launches, 1)
-    pairs = float(sum(len(i[0]) * (len(i[0]) - 1) for i in insts))
+    alive_i = sim.batch_status()["alive"].astype(np.float64)
+    pairs = float(sum(a * (a - 1) for a, m in zip(alive_i, methods) if m == 3))
     peak = sim.measure_fp32_peak()
     achieved = 20.0 * pairs / (ap_avg * 1e-3) / 1e12
     roofline = {"bound": "fp32", "kernel": "batch_allpairs_kernel", "achieved": achieved, "peak": peak,
                 "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                 "peak_source": "measured in this run: FFMA probe kernel over all SMs (2 flop/FFMA)",
                 "flops_per_launch": 20.0 * pairs,
-                "flop_convention": "20 flop per pair interaction x sum_i N_i(N_i-1)",
+                "flop_convention": "20 flop per pair interaction x sum_i A_i(A_i-1), A_i the live "
+                                   "particles of all-pairs instance i",
                 "avg_launch_ms": ap_avg,
                 "phase_ms_per_step": {k: v[0] / prof_steps for k, v in phases.items() if v[1]}}
 
     # baseline: the same instances one at a time with the single-instance kernels
     serial_steps = max(1, min(args.steps, args.serial_steps))
     sim.batch_step(1, serial=True)  # untimed: grows the single-instance scratch to its largest size
+    s_live0 = live()
     serial_ms = max_over_ranks(timed(lambda: sim.batch_step(serial_steps, serial=True)), world, device)
-    serial_value = world * n_total * serial_steps / (serial_ms * 1e-3)
+    serial_value = live_rate(serial_ms, serial_steps, s_live0, live())
     sim.close()
     # the sweep's own method split (FMM p=4 from 8,192 particles), both ways
     split = make_sweep(n_inst=args.instances, seed=2024 + rank, method_split=8192, order=4)
     sim = amk.Simulation(device=local)
     load_sweep(sim, split)
     sim.batch_step(args.warmup)
+    p_live0 = live()
     split_ms = max_over_ranks(timed(lambda: sim.batch_step(serial_steps)), world, device)
+    split_value = live_rate(split_ms, serial_steps, p_live0, live())
     sim.batch_step(1, serial=True)
+    p_live0 = live()
     split_serial_ms = max_over_ranks(timed(lambda: sim.batch_step(serial_steps, serial=True)), world, device)
+    split_serial_value = live_rate(split_serial_ms, serial_steps, p_live0, live())
 
     # end to end through the C ABI with host buffers (one step per call)
     L = amk.lib()
@@ -422,8 +438,9 @@ def run_sweep(args):
             sim.batch_step(1)
             amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k2]) for k2 in order],
                                           C.cast(C.c_void_p(alive.data_ptr()), C.POINTER(C.c_uint8))))
+    e_live0 = live()
     e2e_ms = max_over_ranks(timed(e2e_loop), world, device)
-    e2e = {"value": world * n_total * e2e_steps / (e2e_ms * 1e-3), "unit": UNIT,
+    e2e = {"value": live_rate(e2e_ms, e2e_steps, e_live0, live()), "unit": UNIT,
            "h2d_bytes_per_step": 6 * 8 * n_total, "d2h_bytes_per_step": 6 * 8 * n_total + n_total,
            "steps": e2e_steps,
            "api": "amk_update_state + amk_batch_step + amk_get_particles (pinned host buffers)"}
@@ -452,6 +469,9 @@ def run_sweep(args):
                                      "launch (cost-ordered work queue); FP64 state",
                            "autotune": {"methods": method_counts, "seconds": round(tune_s, 2)},
                            "graph_chunk": chunk, "instances": len(insts), "n_particles": n_total,
+                           "live_particles_timed": [live0, live1],
+                           "rate_counts": "live (not yet annihilated) particles, mean of the timed "
+                                          "window's start and end",
                            "instance_sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)),
                                               "max": int(sizes.max())},
                            "l2": "not flushed: state of 7.4 M particles (> 700 MB) exceeds L2",
@@ -464,8 +484,8 @@ def run_sweep(args):
                                   "api": "amk_batch_step(serial=1): each instance through the "
                                          "single-instance kernels, one after another"},
                 "method_split_8192_fmm_p4": {
-                    "batched_value": world * n_total * serial_steps / (split_ms * 1e-3),
-                    "one_at_a_time_value": world * n_total * serial_steps / (split_serial_ms * 1e-3),
+                    "batched_value": split_value,
+                    "one_at_a_time_value": split_serial_value,
                     "note": "all-pairs below 8,192 particles, FMM p=4 theta=0.5 above (RMS error "
                             "about 7e-5, above the 1e-5 bar); per-instance FMM calls synchronise "
                             "with the host, so no graphs"},
