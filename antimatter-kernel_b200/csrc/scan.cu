@@ -84,6 +84,7 @@ scan_down_kernel(const int* in, long n, const int* sums, int* out) {
 }  // namespace
 
 // out[i] = sum_{j < i} in[i]; *total_dev = sum of all (device pointer).
+// out may equal in (each thread reads its items before writing them).
 int exclusive_scan_int(amk_ctx* c, const int* in, long n, int* out, int* total_dev) {
   if (n <= 0) {
     AMK_CUDA_TRY(cudaMemsetAsync(total_dev, 0, sizeof(int), c->stream));

@@ -116,6 +116,8 @@ int radix_sort_pairs(amk_ctx* c, const uint64_t* keys_in, const uint32_t* vals_i
   AMK_TRY(rc);
   uint32_t* hist = slot<uint32_t>(c, kSlotSortHist, static_cast<size_t>(256) * nb, &rc);
   AMK_TRY(rc);
+  int* total = slot<int>(c, kSlotSortFlags, 8, &rc);
+  AMK_TRY(rc);
   const uint64_t* ksrc = keys_in;
   const uint32_t* vsrc = vals_in;
   for (int p = 0; p < passes; ++p) {
@@ -125,8 +127,14 @@ int radix_sort_pairs(amk_ctx* c, const uint64_t* keys_in, const uint32_t* vals_i
     const int shift = 8 * p;
     hist_kernel<<<nb, kSortThreads, 0, c->stream>>>(ksrc, n, shift, nb, hist);
     AMK_TRY(check_launch(c, "hist_kernel"));
-    scan_kernel<<<1, 1024, 0, c->stream>>>(hist, static_cast<long>(256) * nb);
-    AMK_TRY(check_launch(c, "scan_kernel"));
+    if (static_cast<long>(256) * nb > 65536) {
+      // many tiles: the multi-CTA scan (in place; counts stay below 2^31)
+      AMK_TRY(exclusive_scan_int(c, reinterpret_cast<const int*>(hist), static_cast<long>(256) * nb,
+                                 reinterpret_cast<int*>(hist), total));
+    } else {
+      scan_kernel<<<1, 1024, 0, c->stream>>>(hist, static_cast<long>(256) * nb);
+      AMK_TRY(check_launch(c, "scan_kernel"));
+    }
     scatter_kernel<<<nb, kSortThreads, 0, c->stream>>>(ksrc, vsrc, n, shift, nb, hist, kdst, vdst);
     AMK_TRY(check_launch(c, "scatter_kernel"));
     ksrc = kdst;

@@ -121,7 +121,25 @@ def load_sweep(sim, insts):
     return pos, vel, sp, offsets
 
 
-WORKLOADS = {"direct65k": workload_direct65k, "sweep512": None}
+WORKLOADS = {"direct65k": workload_direct65k, "sweep512": None, "tree1m": None}
+
+
+def tree_cloud(n=1 << 20, seed=42):
+    """N positrons, Gaussian cloud sigma 1e-4, 1e-4, 3e-4 m, 5 K Maxwellian."""
+    rng = np.random.default_rng(seed)
+    pos = rng.normal(0.0, 1.0, (n, 3)) * np.array([1e-4, 1e-4, 3e-4])
+    vel = rng.normal(0.0, 1.0, (n, 3)) * np.sqrt(KB * 5.0 / MASS[1])
+    return pos, vel, np.ones(n, np.uint8)
+
+
+TREE_METHODS = [
+    ("allpairs", dict(coulomb_method="allpairs")),
+    ("barnes-hut theta=0.7", dict(coulomb_method="barnes-hut", barnes_hut_theta=0.7)),
+    ("fmm p=4 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=4, fast_multipole_theta=0.5)),
+    ("fmm p=6 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=6, fast_multipole_theta=0.5)),
+    ("learned p=2 + MLP theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=2,
+                                        fast_multipole_theta=0.5, fmm_learned=1, learned_audit_interval=0)),
+]
 
 
 # ------------------------------------------------------------------ clocks
@@ -497,6 +515,35 @@ def run_sweep(args):
     return 0
 
 
+def run_reference_tree(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    pos, _, _ = tree_cloud()
+    n = len(pos)
+    x, y, z = pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy()
+    q = np.full(n, E)
+    m = np.full(n, MASS[1])
+    times = []
+    kind = "reference"
+    for k in range(args.warmup + args.steps):
+        t, kind, _, _ = cpu_reference_step_time(x, y, z, q, m, args.ref_sample, seed=k)
+        if k >= args.warmup:
+            times.append(t)
+    t_step = float(np.mean(times))
+    value = n / t_step
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian cloud)",
+            "config": {"workload": f"tree solvers at N={n:,} positrons (exact force)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
+                             "sample": f"per step: theta=0 tree over all {n} sources, {args.ref_sample} targets "
+                                       f"walked (extrapolated), FP64 push of all"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference_sweep(args):
     world, rank, _ = dist_setup()
     if rank != 0:
@@ -521,6 +568,144 @@ def run_reference_sweep(args):
                                        "targets walked (extrapolated), FP64 push of all"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ tree solvers at 1M
+def run_tree(args):
+    """N = 1,048,576 positrons: every Coulomb method timed per step (force +
+    push) and audited against the FP64 exact sum; `value` is the fastest
+    method whose RMS relative force error is within 1e-5."""
+    import torch
+    import amk
+    world, rank, local = dist_setup()
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    pos, vel, sp = tree_cloud()
+    n = len(pos)
+    steps = max(1, min(args.steps, 5))
+    results = {}
+    best = None
+    for name, over in TREE_METHODS:
+        kw = dict(seed=42, b0=1.0, trap_voltage=10.0, z0=0.01, rho0=0.01, num_steps=500,
+                  populations={"positron": n}, temperatures={"positron": 5.0}, cloud_radii=(1e-4, 1e-4, 3e-4),
+                  bath_temperature=0.0, cooling_scale=0.0, cooling_enabled=0, coulomb_forces_enabled=1,
+                  energy_method="allpairs", annihilation_enabled=0)
+        kw.update(over)
+        sim = amk.Simulation(amk.make_params(**kw), device=local)
+        sim.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
+        entry = {}
+        if over.get("fmm_learned"):
+            t0 = time.perf_counter()
+            loss, samples = sim.fmm_train_correction(0.5, sample_leaves=4096, steps=2000, batch=4096, lr=1e-3)
+            entry["training"] = {"seconds": round(time.perf_counter() - t0, 2), "samples": samples,
+                                 "final_loss": loss}
+        sim.coulomb()
+        rms, mx = sim.force_error(1024)
+        entry.update({"rms_rel": rms, "max_rel": mx, "meets_1e-5": bool(rms <= 1e-5)})
+        stream = torch.cuda.ExternalStream(sim.stream(), device=device)
+        sim.step(max(1, args.warmup))
+        sim.synchronize()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        sim.step(steps)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1) / steps
+        entry.update(ms_per_step=ms, value=n / (ms * 1e-3), steps=steps)
+        sim.set_profiling(True)
+        sim.reset_phase_times()
+        sim.step(1)
+        sim.synchronize()
+        entry["phase_ms"] = {k: round(v[0], 3) for k, v in sim.phase_times().items() if v[1]}
+        sim.set_profiling(False)
+        results[name] = entry
+        if entry["meets_1e-5"] and (best is None or entry["value"] > results[best]["value"]):
+            best = name
+        sim.close()
+    # the winner again: roofline of its dominant kernel, e2e through the C ABI
+    name = best if best is not None else "allpairs"
+    over = dict(TREE_METHODS)[name]
+    kw = dict(seed=42, b0=1.0, trap_voltage=10.0, populations={"positron": n}, cooling_enabled=0,
+              energy_method="allpairs", annihilation_enabled=0)
+    kw.update(over)
+    sim = amk.Simulation(amk.make_params(**kw), device=local)
+    sim.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
+    sim.step(1)
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = sim.kernel_launches()
+    stream = torch.cuda.ExternalStream(sim.stream(), device=device)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    sim.step(steps)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    launches = sim.kernel_launches() - launches0
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1) / steps
+    value = n / (ms * 1e-3)
+    roofline = None
+    if over["coulomb_method"] == "allpairs":
+        sim.set_profiling(True)
+        sim.reset_phase_times()
+        sim.step(1)
+        sim.synchronize()
+        ap_ms, ap_n = sim.phase_times()["allpairs"]
+        sim.set_profiling(False)
+        peak = sim.measure_fp32_peak()
+        achieved = 20.0 * n * (n - 1) / (ap_ms / ap_n * 1e-3) / 1e12
+        roofline = {"bound": "fp32", "kernel": "allpairs_kernel", "achieved": achieved, "peak": peak,
+                    "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                    "peak_source": "measured in this run: FFMA probe kernel over all SMs (2 flop/FFMA)",
+                    "flop_convention": "20 flop per pair interaction x N(N-1) pairs",
+                    "avg_launch_ms": ap_ms / ap_n}
+    host = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in ("x", "y", "z", "vx", "vy", "vz")}
+    alive = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    order = ("x", "y", "z", "vx", "vy", "vz")
+    ptr = {k: v.data_ptr() for k, v in host.items()}
+    L = amk.lib()
+    amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k]) for k in order],
+                                  C.cast(C.c_void_p(alive.data_ptr()), C.POINTER(C.c_uint8))))
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(steps):
+        sim.update_state(*[ptr[k] for k in order])
+        sim.step(1)
+        amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k]) for k in order],
+                                      C.cast(C.c_void_p(alive.data_ptr()), C.POINTER(C.c_uint8))))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = ev0.elapsed_time(ev1)
+    e2e = {"value": n * steps / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 48 * n,
+           "d2h_bytes_per_step": 49 * n, "steps": steps,
+           "api": "amk_update_state + amk_step + amk_get_particles (pinned host buffers)"}
+    st = sim.get_particles()
+    sim.close()
+    cpu = None
+    if rank == 0 and world == 1:
+        q = np.full(n, E)
+        m = np.full(n, MASS[1])
+        t_step, kind, _, _ = cpu_reference_step_time(st["x"], st["y"], st["z"], q, m, args.cpu_sample)
+        cpu = {"value": n / t_step, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
+               "sample": f"reference Barnes-Hut theta=0 (exact all-pairs) tree over all {n} sources walked for "
+                         f"{args.cpu_sample} sampled targets, extrapolated to {n}, + FP64 push of all {n}"}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "fp32" if over["coulomb_method"] == "allpairs" else "f64",
+            "data": "synthetic (seeded Gaussian cloud)",
+            "config": {"workload": "tree solvers at N=1,048,576 positrons, Gaussian sigma 1e-4 x 1e-4 x 3e-4 m, "
+                                   "5 K Maxwellian, b0=1 T, U=10 V; value = fastest method within 1e-5 RMS "
+                                   "relative force error vs the FP64 exact sum (1,024 audited particles)",
+                       "chosen": name, "methods": results,
+                       "l2": "not flushed: state of 1 M particles (> 100 MB) exceeds L2",
+                       "parallelism": "replicas x1 (single instance)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     return 0
 
 
@@ -697,9 +882,13 @@ def main():
     if args.impl == "reference":
         if args.workload == "sweep512":
             return run_reference_sweep(args)
+        if args.workload == "tree1m":
+            return run_reference_tree(args)
         return run_reference(args)
     if args.workload == "sweep512":
         return run_sweep(args)
+    if args.workload == "tree1m":
+        return run_tree(args)
     return run_amk(args)
 
 

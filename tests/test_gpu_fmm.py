@@ -102,3 +102,16 @@ def test_fmm_energy_method_in_context():
         e = s.energy(time_centre=False)
         eref = float(g["e_p4_theta0.5"])
         assert abs(e["coulomb_potential"] - eref) <= 1e-10 * abs(eref)
+
+
+def test_fmm_above_a_million_particles_matches_reference(sim):
+    # more than 2^20 sources: the radix sorts of the tree keys and of the
+    # interaction pairs take their multi-CTA histogram-scan path
+    if not O.ref_available():
+        pytest.skip("reference library not built")
+    x, y, z, _ = gaussian_cloud(1_100_000, 77)
+    q = np.full(len(x), E)
+    f = sim.solve_fmm(x, y, z, q, 2, 0.5)
+    (rx, ry, rz), _ = O.ref_fmm(x, y, z, q, 2, 0.5, 32)
+    rel, _ = rel_errors(f, (rx, ry, rz))
+    assert np.max(rel) < FMM_TOL
