@@ -275,6 +275,26 @@ def ref_bh_tree(x, y, z, q, leaf_capacity=8):
     return f[:nn], g[:nn], order
 
 
+def ref_driver(method, x, y, z, q, alive, theta, order=0):
+    """The reference's own drop-in drivers on ChargedAntiparticle agents:
+    method "barnes-hut" (ComputeBarnesHutCoulombForces, barnes-hut.cc:271-299)
+    or "fast-multipole" (ComputeFastMultipoleCoulombForces,
+    fast-multipole.cc:682-709). Annihilated agents keep a zero force slot."""
+    x, y, z, q = map(_f64, (x, y, z, q))
+    n = len(x)
+    al = np.ascontiguousarray(alive, np.uint8)
+    fx, fy, fz = np.zeros(n), np.zeros(n), np.zeros(n)
+    if method == "barnes-hut":
+        ref().amkref_compute_barnes_hut_coulomb_forces(C.c_long(n), _ptr(x), _ptr(y), _ptr(z), _ptr(q),
+                                                       _ptr(al, _u8p), C.c_double(theta), _ptr(fx), _ptr(fy),
+                                                       _ptr(fz))
+    else:
+        ref().amkref_compute_fast_multipole_coulomb_forces(C.c_long(n), _ptr(x), _ptr(y), _ptr(z), _ptr(q),
+                                                           _ptr(al, _u8p), C.c_int(order), C.c_double(theta),
+                                                           _ptr(fx), _ptr(fy), _ptr(fz))
+    return fx, fy, fz
+
+
 def ref_fmm(x, y, z, q, order, theta, leaf_capacity=32, forces=True, energy=False):
     x, y, z, q = map(_f64, (x, y, z, q))
     n = len(x)
