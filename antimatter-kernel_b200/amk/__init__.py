@@ -159,6 +159,7 @@ def lib():
         "amk_batch_set": (C.c_int, [vp, C.c_int, C.POINTER(Params), C.POINTER(C.c_long)]),
         "amk_batch_step": (C.c_int, [vp, C.c_int, C.c_int, C.c_int]),
         "amk_batch_coulomb": (C.c_int, [vp]),
+        "amk_batch_energy": (C.c_int, [vp, C.c_int, C.POINTER(EnergyOut)]),
         "amk_batch_autotune": (C.c_int, [vp, C.c_double, C.c_long, C.POINTER(C.c_int)]),
         "amk_batch_status": (C.c_int, [vp, C.POINTER(C.c_int), C.POINTER(C.c_long)]),
         "amk_batch_info": (C.c_int, [vp, C.POINTER(C.c_long), C.POINTER(C.c_long), C.POINTER(C.c_int)]),
@@ -509,6 +510,15 @@ class Simulation:
         check(lib().amk_batch_autotune(self._h, float(error_budget), int(samples),
                                        m.ctypes.data_as(C.POINTER(C.c_int))), "amk_batch_autotune")
         return m
+
+    def batch_energy(self, time_centre: bool = True):
+        """Per-instance energies: a list of dicts like energy()."""
+        n = getattr(self, "_batch_n", 0)
+        arr = (EnergyOut * max(n, 1))()
+        check(lib().amk_batch_energy(self._h, 1 if time_centre else 0, arr), "amk_batch_energy")
+        return [{"kinetic": e.kinetic, "trap_potential": e.trap_potential,
+                 "coulomb_potential": e.coulomb_potential, "total": e.total, "num_active": e.num_active}
+                for e in arr[:n]]
 
     def batch_coulomb(self):
         check(lib().amk_batch_coulomb(self._h), "amk_batch_coulomb")

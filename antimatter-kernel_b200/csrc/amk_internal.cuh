@@ -355,6 +355,8 @@ int annihilate_view(amk_ctx* c, const View& v, const uint8_t* species, const uin
                     double probability, uint32_t seed, uint64_t step_index, long* marked);
 // Batched instances (batch.cu).
 void batch_destroy(amk_ctx* c);
+// Coulomb potential energy (J) of a view under an energy method (energy.cu).
+int coulomb_energy_view(amk_ctx* c, View v, const amk_params& p, int method, double* out_host);
 // RMS / max relative error of a view's forces against the FP64 exact sum
 // over `samples` evenly spaced usable particles (audit.cu).
 int force_error(amk_ctx* c, const View& v, long samples, double* rms, double* max_rel);

@@ -470,6 +470,37 @@ __global__ void batch_overflow_kernel(const unsigned long long* contacts, long c
   }
 }
 
+// Kinetic energy, trap potential energy and live count of each instance:
+// one CTA per instance, fixed reduction order (energy_analysis.cc:84-125
+// per instance; trap potential q U (2 z^2 - rho^2) / (4 d^2),
+// penning_trap.cc:35-43).
+__global__ void __launch_bounds__(256)
+batch_energy_kernel(const InstanceDev* __restrict__ inst, const double* __restrict__ x, const double* __restrict__ y,
+                    const double* __restrict__ z, const double* __restrict__ vx, const double* __restrict__ vy,
+                    const double* __restrict__ vz, const double* __restrict__ q, const double* __restrict__ m,
+                    const uint8_t* __restrict__ alive, double* __restrict__ out) {
+  __shared__ double s[3][256];
+  const InstanceDev& I = inst[blockIdx.x];
+  const double trap_coef = 0.5 * I.push.radial;  // U / (4 d^2)
+  double ke = 0.0, pe = 0.0, cnt = 0.0;
+  for (long i = I.offset + threadIdx.x; i < I.offset + I.count; i += 256) {
+    if (!alive[i]) continue;
+    ke += 0.5 * m[i] * (vx[i] * vx[i] + vy[i] * vy[i] + vz[i] * vz[i]);
+    pe += q[i] * (trap_coef * (2.0 * z[i] * z[i] - (x[i] * x[i] + y[i] * y[i])));
+    cnt += 1.0;
+  }
+  s[0][threadIdx.x] = ke;
+  s[1][threadIdx.x] = pe;
+  s[2][threadIdx.x] = cnt;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (threadIdx.x < w)
+      for (int k = 0; k < 3; ++k) s[k][threadIdx.x] += s[k][threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) out[3 * blockIdx.x + threadIdx.x] = s[threadIdx.x][0];
+}
+
 __global__ void batch_alive_count_kernel(long n, const uint8_t* __restrict__ alive,
                                          const uint16_t* __restrict__ inst_of, unsigned long long* counts) {
   const long i = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
@@ -500,6 +531,9 @@ struct Batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   int graph_steps = 0;
+  // energy time-centring history per instance (EnergyHistory, energy_analysis.h:23-28)
+  std::vector<double> prev_trap, prev_coulomb;
+  bool energy_has_previous = false;
   long graph_launches = 0;
   ~Batch() {
     if (exec) cudaGraphExecDestroy(exec);
@@ -1025,4 +1059,54 @@ extern "C" int amk_batch_autotune(amk_ctx* c, double error_budget, long samples,
   if (ap_err > error_budget && best_order == 0)
     return fail(AMK_ERR_LIMIT, "neither all-pairs (%g) nor the FMM met the error budget %g", ap_err, error_budget);
   return AMK_OK;
+}
+
+// Energies of every instance (amk_energy per instance): kinetic and trap
+// terms from one CTA per instance, the Coulomb term from the instance's
+// energy method on its own slice, and per-instance time-centring.
+extern "C" int amk_batch_energy(amk_ctx* c, int time_centre, amk_energy_out* out) {
+  if (!c || !out) return fail(AMK_ERR_INVALID, "null argument");
+  if (!c->batch) return fail(AMK_ERR_STATE, "no batch: call amk_batch_set first");
+  AMK_CUDA_TRY(cudaSetDevice(c->device));
+  Batch& B = *c->batch;
+  const int ni = B.n_inst;
+  int rc = AMK_OK;
+  double* part = slot<double>(c, kSlotAuxState3, 3 * static_cast<size_t>(ni) + 8, &rc);
+  AMK_TRY(rc);
+  AMK_TRY(phase_begin(c, AMK_PHASE_ENERGY));
+  batch_energy_kernel<<<ni, 256, 0, c->stream>>>(B.inst.as<InstanceDev>(), c->x.as<double>(), c->y.as<double>(),
+                                                 c->z.as<double>(), c->vx.as<double>(), c->vy.as<double>(),
+                                                 c->vz.as<double>(), c->q.as<double>(), c->m.as<double>(),
+                                                 c->alive.as<uint8_t>(), part);
+  AMK_TRY(check_launch(c, "batch_energy_kernel"));
+  std::vector<double> h(3 * static_cast<size_t>(ni));
+  AMK_CUDA_TRY(cudaMemcpyAsync(h.data(), part, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (B.prev_trap.size() != static_cast<size_t>(ni)) {
+    B.prev_trap.assign(ni, 0.0);
+    B.prev_coulomb.assign(ni, 0.0);
+  }
+  for (int i = 0; i < ni; ++i) {
+    const amk_params& p = B.params[i];
+    double coul = 0.0;
+    if (p.coulomb_forces_enabled && B.offsets[i + 1] > B.offsets[i])
+      AMK_TRY(coulomb_energy_view(c, instance_view(c, B, i), p, p.energy_method, &coul));
+    amk_energy_out& o = out[i];
+    o.kinetic = h[3 * i];
+    o.trap_potential = h[3 * i + 1];
+    o.coulomb_potential = coul;
+    o.num_active = static_cast<long>(h[3 * i + 2]);
+    if (time_centre) {  // energy_analysis.cc:126-142
+      const double raw_trap = o.trap_potential, raw_coul = o.coulomb_potential;
+      if (B.energy_has_previous) {
+        o.trap_potential = 0.5 * (B.prev_trap[i] + raw_trap);
+        o.coulomb_potential = 0.5 * (B.prev_coulomb[i] + raw_coul);
+      }
+      B.prev_trap[i] = raw_trap;
+      B.prev_coulomb[i] = raw_coul;
+    }
+    o.total = o.kinetic + o.trap_potential + o.coulomb_potential;
+  }
+  if (time_centre) B.energy_has_previous = true;
+  return phase_end(c, AMK_PHASE_ENERGY);
 }

@@ -92,37 +92,37 @@ int reduce_sum(amk_ctx* c, const double* in, long n, double* out_dev) {
   return check_launch(c, "sum_kernel");
 }
 
-// Coulomb potential energy of the main particle set per method (J).
-static int coulomb_energy(amk_ctx* c, int method, double* out_host) {
+// Coulomb potential energy (J) of a view under the energy method and the
+// parameters p (cutoff radius, opening angles, FMM order). The view's force
+// outputs are redirected to scratch: the force slots are not touched.
+int coulomb_energy_view(amk_ctx* c, View v, const amk_params& p, int method, double* out_host) {
   *out_host = 0.0;
-  View v = main_view(c);
+  if (v.n == 0) return AMK_OK;
   int rc = AMK_OK;
   // per-particle potential buffer
-  double* phi = slot<double>(c, kSlotAuxState6, static_cast<size_t>(c->n) + 8, &rc);
+  double* phi = slot<double>(c, kSlotAuxState6, static_cast<size_t>(v.n) + 8, &rc);
   AMK_TRY(rc);
-  // forces of the energy evaluation go to scratch, not the force slot
-  double* tf = slot<double>(c, kSlotAuxState5, 3 * static_cast<size_t>(c->n) + 8, &rc);
+  double* tf = slot<double>(c, kSlotAuxState5, 3 * static_cast<size_t>(v.n) + 8, &rc);
   AMK_TRY(rc);
   v.fx = tf;
-  v.fy = tf + c->n;
-  v.fz = tf + 2 * c->n;
+  v.fy = tf + v.n;
+  v.fz = tf + 2 * v.n;
   v.phi = phi;
   switch (method) {
     case AMK_METHOD_STANDARD: {
       double e = 0.0;
-      AMK_TRY(cutoff_forces(c, v, c->p.cutoff_radius, &e));
+      AMK_TRY(cutoff_forces(c, v, p.cutoff_radius, &e));
       *out_host = e;
       return AMK_OK;
     }
     case AMK_METHOD_FAST_MULTIPOLE: {
       double e = 0.0;
-      AMK_TRY(fmm_forces(c, v, static_cast<int>(c->p.fast_multipole_order), c->p.fast_multipole_theta, 32,
-                         false, &e));
+      AMK_TRY(fmm_forces(c, v, static_cast<int>(p.fast_multipole_order), p.fast_multipole_theta, 32, false, &e));
       *out_host = e;
       return AMK_OK;
     }
     case AMK_METHOD_BARNES_HUT:
-      AMK_TRY(barnes_hut_forces(c, v, c->p.barnes_hut_theta, 8));
+      AMK_TRY(barnes_hut_forces(c, v, p.barnes_hut_theta, 8));
       break;
     case AMK_METHOD_ALLPAIRS:
       AMK_TRY(allpairs_forces(c, v));
@@ -134,7 +134,7 @@ static int coulomb_energy(amk_ctx* c, int method, double* out_host) {
   AMK_TRY(rc);
   double* res = slot<double>(c, kSlotAuxState4, 8, &rc);
   AMK_TRY(rc);
-  q_phi_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(c->n, v.q, phi, v.alive, part);
+  q_phi_kernel<<<kRedBlocks, kRedThreads, 0, c->stream>>>(v.n, v.q, phi, v.alive, part);
   AMK_TRY(check_launch(c, "q_phi_kernel"));
   sum_kernel<<<1, kRedThreads, 0, c->stream>>>(kRedBlocks, part, res);
   AMK_TRY(check_launch(c, "sum_kernel"));
@@ -179,7 +179,7 @@ extern "C" int amk_energy(amk_ctx* c, int time_centre, amk_energy_out* out) {
       AMK_TRY(stage_view(c, main_view(c)));
       c->stage_dirty = false;
     }
-    AMK_TRY(coulomb_energy(c, c->p.energy_method, &coul));
+    AMK_TRY(coulomb_energy_view(c, main_view(c), c->p, c->p.energy_method, &coul));
   }
   AMK_TRY(phase_end(c, AMK_PHASE_ENERGY));
   out->kinetic = ke;

@@ -394,7 +394,11 @@ int amk_batch_status(amk_ctx* ctx, int* overflow, long* alive_counts);
  * (n_inst entries, may be NULL) receives the chosen AMK_METHOD_* (-1 for
  * instances without Coulomb forces). */
 int amk_batch_autotune(amk_ctx* ctx, double error_budget, long samples, int* methods_out);
-/* n_instances, all-pairs work units (instance, 128-target block) and
+/* amk_energy for every instance of the batch: out[i] (n_inst entries) with
+ * instance i's kinetic, trap and Coulomb energies under its own parameters
+ * and energy method, and its own time-centring history. */
+int amk_batch_energy(amk_ctx* ctx, int time_centre, amk_energy_out* out);
+/* n_instances, all-pairs work units (instance, 256-target block) and
  * whether the batch can run as CUDA graphs. */
 int amk_batch_info(const amk_ctx* ctx, long* n_instances, long* work_units, int* graphable);
 
