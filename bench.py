@@ -407,7 +407,11 @@ def run_sweep(args):
     peak = sim.measure_fp32_peak()
     achieved = 20.0 * pairs / (ap_avg * 1e-3) / 1e12
     roofline = {"bound": "fp32", "kernel": "batch_allpairs_kernel", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": 116.2e6 * n_total / 1380664,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of batch_allpairs_kernel "
+                                  "on the 64-instance case (116.2 MB for 1,380,664 particles, "
+                                  "profiles/batch_allpairs_kernel_sweep.md), scaled by particle count (the "
+                                  "staged particle data read once plus the force writes)",
                 "peak_source": "measured in this run: FFMA probe kernel over all SMs (2 flop/FFMA)",
                 "flops_per_launch": 20.0 * pairs,
                 "flop_convention": "20 flop per pair interaction x sum_i A_i(A_i-1), A_i the live "
@@ -659,7 +663,10 @@ def run_tree(args):
         peak = sim.measure_fp32_peak()
         achieved = 20.0 * n * (n - 1) / (ap_ms / ap_n * 1e-3) / 1e12
         roofline = {"bound": "fp32", "kernel": "allpairs_kernel", "achieved": achieved, "peak": peak,
-                    "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                    "unit": "TFLOP/s", "frac": achieved / peak, "traffic": 3.276e6 * n / 65536,
+                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of allpairs_kernel at "
+                                      "N = 65,536 (3.276 MB, profiles/allpairs_kernel_direct65k.md), scaled by N "
+                                      "(sources are read from DRAM once per launch and re-read from L2)",
                     "peak_source": "measured in this run: FFMA probe kernel over all SMs (2 flop/FFMA)",
                     "flop_convention": "20 flop per pair interaction x N(N-1) pairs",
                     "avg_launch_ms": ap_ms / ap_n}
@@ -780,7 +787,9 @@ def run_amk(args):
     achieved = flops_per_launch / (ap_avg_ms * 1e-3) / 1e12
     peak = sim.measure_fp32_peak()
     roofline = {"bound": "fp32", "kernel": "allpairs_kernel", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": 3.276e6,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one allpairs_kernel "
+                                  "launch of this workload (profiles/allpairs_kernel_direct65k.md)",
                 "peak_source": "measured in this run: FFMA probe kernel over all SMs "
                                "(2 flop/FFMA); no FP32 figure in the driver's peak file",
                 "flops_per_launch": flops_per_launch,
