@@ -385,23 +385,109 @@ __global__ void pair_unpack_kernel(const uint64_t* __restrict__ keys, int n, int
 }
 
 // ------------------------------------------------------------ M2L
-// A warp per target cell (fast-multipole.cc:528-555). Derivatives
-// (fast-multipole.cc:207-232) are built degree by degree in shared memory;
-// the M2L index map sits in shared memory as int16 with rows padded to
-// n_m + 1 entries (lanes read different rows without bank conflicts).
+// A warp per target cell (fast-multipole.cc:528-555).
+//
+// Derivative tensors from a table: cube centres lie on a lattice, so for a
+// pair c_t - c_s = u v with u = the smaller half edge and v an integer
+// vector (up to the rounding of the centres, ~1e-15 relative), and
+// D_k(u v) = u^{-|k|-1} D_k(v) (D is homogeneous of degree -1-|k|). The
+// distinct offsets v with |v_i| <= kM2LReach are found once per evaluation
+// and their D(v) built once (fast-multipole.cc:207-232 recurrence, FP64);
+// each pair then loads D(v) and scales it by powers of 1/u. Pairs off the
+// lattice or farther out use the recurrence directly. The contraction runs
+// through the M2L index map in shared memory (int16, rows padded to n_m + 1
+// entries so that lanes read different rows without bank conflicts).
+constexpr int kM2LReach = 31;
+constexpr int kM2LSide = 2 * kM2LReach + 1;
+constexpr int kM2LCodes = kM2LSide * kM2LSide * kM2LSide;
+
+// Lattice offset code of a pair (-1 = off the lattice or out of reach) and u.
+__device__ __forceinline__ int m2l_code(const double4& tc, const double4& sc, double* u_out) {
+  const double u = fmin(tc.w, sc.w);
+  *u_out = u;
+  const double vx = (tc.x - sc.x) / u, vy = (tc.y - sc.y) / u, vz = (tc.z - sc.z) / u;
+  const double rx = rint(vx), ry = rint(vy), rz = rint(vz);
+  if (fabs(vx - rx) > 1e-6 || fabs(vy - ry) > 1e-6 || fabs(vz - rz) > 1e-6) return -1;
+  if (fabs(rx) > kM2LReach || fabs(ry) > kM2LReach || fabs(rz) > kM2LReach) return -1;
+  return ((static_cast<int>(rx) + kM2LReach) * kM2LSide + (static_cast<int>(ry) + kM2LReach)) * kM2LSide +
+         (static_cast<int>(rz) + kM2LReach);
+}
+
+__global__ void m2l_mark_kernel(const Octree t, const int2* __restrict__ pairs, long n, int* __restrict__ used) {
+  const long e = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (e >= n) return;
+  double u;
+  const int code = m2l_code(t.center[pairs[e].x], t.center[pairs[e].y], &u);
+  if (code >= 0) used[code] = 1;
+}
+
+__global__ void m2l_list_kernel(const int* __restrict__ used, const int* __restrict__ index, int* __restrict__ codes) {
+  const int code = blockIdx.x * blockDim.x + threadIdx.x;
+  if (code < kM2LCodes && used[code]) codes[index[code]] = code;
+}
+
+__global__ void m2l_class_map_kernel(const int* __restrict__ used, int* __restrict__ class_of) {
+  const int code = blockIdx.x * blockDim.x + threadIdx.x;
+  if (code < kM2LCodes && !used[code]) class_of[code] = -1;
+}
+
+// D recurrence for displacement xs into D[0, n_d), one warp.
+__device__ __forceinline__ void m2l_derivatives(const FmmDevTables& T, int lane, const double xs[3], double* D) {
+  const double inv_r2 = 1.0 / (xs[0] * xs[0] + xs[1] * xs[1] + xs[2] * xs[2]);
+  if (lane == 0) D[0] = sqrt(inv_r2);
+  __syncwarp();
+  for (int deg = 1; deg <= 2 * T.p; ++deg) {
+    for (int k = T.deg_start[deg] + lane; k < T.deg_start[deg + 1]; k += 32) {
+      const int i = T.rec_axis[k];
+      const int di = T.rec_delta[3 * k + i];
+      double sum = (2 * di - 1) * xs[i] * D[T.rec_m1[3 * k + i]];
+      if (T.rec_m2[3 * k + i] >= 0) sum += (di - 1) * (di - 1) * D[T.rec_m2[3 * k + i]];
+      for (int j = 0; j < 3; ++j) {
+        const int dj = T.rec_delta[3 * k + j];
+        if (j == i || dj == 0) continue;
+        sum += 2.0 * dj * xs[j] * D[T.rec_m1[3 * k + j]];
+        if (T.rec_m2[3 * k + j] >= 0) sum += dj * (dj - 1) * D[T.rec_m2[3 * k + j]];
+      }
+      D[k] = -sum * inv_r2;
+    }
+    __syncwarp();
+  }
+}
+
+// D(v) of every used offset: a warp per offset, into table[class * n_d + k].
+__global__ void __launch_bounds__(32 * kFmmWarps)
+m2l_table_kernel(FmmDevTables T, const int* __restrict__ codes, int n_classes, double* __restrict__ table) {
+  extern __shared__ __align__(16) unsigned char tab_smem[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double* D = reinterpret_cast<double*>(tab_smem) + static_cast<size_t>(w) * T.n_d;
+  const int cls = blockIdx.x * kFmmWarps + w;
+  if (cls >= n_classes) return;
+  const int code = codes[cls];
+  const double xs[3] = {static_cast<double>(code / (kM2LSide * kM2LSide) - kM2LReach),
+                        static_cast<double>((code / kM2LSide) % kM2LSide - kM2LReach),
+                        static_cast<double>(code % kM2LSide - kM2LReach)};
+  m2l_derivatives(T, lane, xs, D);
+  for (int k = lane; k < T.n_d; k += 32) table[static_cast<size_t>(cls) * T.n_d + k] = D[k];
+}
+
 __global__ void __launch_bounds__(32 * kFmmWarps)
 fmm_m2l_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, const int* __restrict__ count,
-               const int* __restrict__ src, const double* __restrict__ M, double* __restrict__ L) {
+               const int* __restrict__ src, const double* __restrict__ M, double* __restrict__ L,
+               const int* __restrict__ class_of, const double* __restrict__ table) {
   extern __shared__ __align__(16) unsigned char m2l_smem[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int nm = T.n_m, nd = T.n_d, stride = nm + 1;
-  double* D = reinterpret_cast<double*>(m2l_smem) + static_cast<size_t>(w) * (nd + nm);
+  const int nm = T.n_m, nd = T.n_d, stride = nm + 1, p2 = 2 * T.p;
+  double* D = reinterpret_cast<double*>(m2l_smem) + static_cast<size_t>(w) * (nd + nm + p2 + 2);
   double* Ms = D + nd;
-  short* idx = reinterpret_cast<short*>(reinterpret_cast<double*>(m2l_smem) + static_cast<size_t>(kFmmWarps) * (nd + nm));
+  double* upw = Ms + nm;  // u^-d, d = 0 .. 2p + 1
+  short* idx = reinterpret_cast<short*>(reinterpret_cast<double*>(m2l_smem) +
+                                        static_cast<size_t>(kFmmWarps) * (nd + nm + p2 + 2));
+  unsigned char* degk = reinterpret_cast<unsigned char*>(idx + nm * stride);
   for (int e = threadIdx.x; e < nm * nm; e += blockDim.x) {
     const int g = e / nm, a = e - g * nm;
     idx[g * stride + a] = static_cast<short>(T.m2l_index[e]);
   }
+  for (int k = threadIdx.x; k < nd; k += blockDim.x) degk[k] = static_cast<unsigned char>(T.multi[k].w);
   __syncthreads();
   const int ti = blockIdx.x * kFmmWarps + w;
   if (ti >= t.n_nodes) return;
@@ -414,32 +500,32 @@ fmm_m2l_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, cons
   for (int e = b; e < b + cnt; ++e) {
     const int si = src[e];
     const double4 sc = t.center[si];
-    const double xs[3] = {tc.x - sc.x, tc.y - sc.y, tc.z - sc.z};
     for (int a = lane; a < nm; a += 32) Ms[a] = T.sign[a] * M[static_cast<size_t>(si) * nm + a];
-    const double inv_r2 = 1.0 / (xs[0] * xs[0] + xs[1] * xs[1] + xs[2] * xs[2]);
-    if (lane == 0) D[0] = sqrt(inv_r2);
-    __syncwarp();
-    for (int deg = 1; deg <= 2 * T.p; ++deg) {
-      for (int k = T.deg_start[deg] + lane; k < T.deg_start[deg + 1]; k += 32) {
-        const int i = T.rec_axis[k];
-        const int di = T.rec_delta[3 * k + i];
-        double sum = (2 * di - 1) * xs[i] * D[T.rec_m1[3 * k + i]];
-        if (T.rec_m2[3 * k + i] >= 0) sum += (di - 1) * (di - 1) * D[T.rec_m2[3 * k + i]];
-        for (int j = 0; j < 3; ++j) {
-          const int dj = T.rec_delta[3 * k + j];
-          if (j == i || dj == 0) continue;
-          sum += 2.0 * dj * xs[j] * D[T.rec_m1[3 * k + j]];
-          if (T.rec_m2[3 * k + j] >= 0) sum += dj * (dj - 1) * D[T.rec_m2[3 * k + j]];
+    double u;
+    const int code = m2l_code(tc, sc, &u);
+    const int cls = code >= 0 ? class_of[code] : -1;
+    if (cls >= 0) {
+      if (lane == 0) {
+        const double iu = 1.0 / u;
+        double pw = 1.0;
+        for (int d = 0; d <= p2 + 1; ++d) {
+          upw[d] = pw;
+          pw *= iu;
         }
-        D[k] = -sum * inv_r2;
       }
       __syncwarp();
+      const double* tab = table + static_cast<size_t>(cls) * nd;
+      for (int k = lane; k < nd; k += 32) D[k] = tab[k] * upw[degk[k] + 1];
+      __syncwarp();
+    } else {
+      const double xs[3] = {tc.x - sc.x, tc.y - sc.y, tc.z - sc.z};
+      m2l_derivatives(T, lane, xs, D);
     }
-    for (int u = 0, g = lane; g < nm; ++u, g += 32) {
+    for (int uu = 0, g = lane; g < nm; ++uu, g += 32) {
       const short* row = idx + g * stride;
       double s = 0.0;
       for (int a = 0; a < nm; ++a) s += Ms[a] * D[row[a]];
-      acc[u] += s * T.inv_fact[g];
+      acc[uu] += s * T.inv_fact[g];
     }
     __syncwarp();
   }
@@ -447,8 +533,8 @@ fmm_m2l_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, cons
 }
 
 size_t m2l_smem_bytes(const FmmDevTables& T) {
-  return static_cast<size_t>(kFmmWarps) * (T.n_d + T.n_m) * sizeof(double) +
-         static_cast<size_t>(T.n_m) * (T.n_m + 1) * sizeof(short);
+  return static_cast<size_t>(kFmmWarps) * (T.n_d + T.n_m + 2 * T.p + 2) * sizeof(double) +
+         static_cast<size_t>(T.n_m) * (T.n_m + 1) * sizeof(short) + static_cast<size_t>(T.n_d) + 16;
 }
 
 // ------------------------------------------------------------ L2L
@@ -833,10 +919,46 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
   // ---- M2L
   AMK_CUDA_TRY(cudaMemsetAsync(Lx, 0, static_cast<size_t>(nn) * T.n_m * sizeof(double), c->stream));
   AMK_TRY(phase_begin(c, AMK_PHASE_FMM_M2L));
+  int* class_of = nullptr;
+  double* table = nullptr;
+  if (n_m2l > 0) {  // derivative tensors of the lattice offsets in use
+    int* used = slot<int>(c, kSlotFmmWork1, kM2LCodes + 1, &rc);
+    AMK_TRY(rc);
+    class_of = slot<int>(c, kSlotFmmAux2, kM2LCodes + 1, &rc);
+    AMK_TRY(rc);
+    int* n_cls_dev = slot<int>(c, kSlotSortFlags, 8, &rc);
+    AMK_TRY(rc);
+    AMK_CUDA_TRY(cudaMemsetAsync(used, 0, (kM2LCodes + 1) * sizeof(int), c->stream));
+    m2l_mark_kernel<<<static_cast<unsigned>((n_m2l + 255) / 256), 256, 0, c->stream>>>(t, lists.m2l.as<int2>(),
+                                                                                      n_m2l, used);
+    AMK_TRY(check_launch(c, "m2l_mark_kernel"));
+    AMK_TRY(exclusive_scan_int(c, used, kM2LCodes, class_of, n_cls_dev));
+    int n_cls = 0;
+    AMK_CUDA_TRY(cudaMemcpyAsync(&n_cls, n_cls_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    int* codes = slot<int>(c, kSlotFmmWork3, static_cast<size_t>(n_cls) + 1, &rc);
+    AMK_TRY(rc);
+    table = slot<double>(c, kSlotFmmWork5, static_cast<size_t>(n_cls) * T.n_d + 1, &rc);
+    AMK_TRY(rc);
+    m2l_list_kernel<<<(kM2LCodes + 255) / 256, 256, 0, c->stream>>>(used, class_of, codes);
+    AMK_TRY(check_launch(c, "m2l_list_kernel"));
+    // class_of[code] = class index for used codes, -1 otherwise
+    m2l_class_map_kernel<<<(kM2LCodes + 255) / 256, 256, 0, c->stream>>>(used, class_of);
+    AMK_TRY(check_launch(c, "m2l_class_map_kernel"));
+    if (n_cls > 0) {
+      const size_t tsm = static_cast<size_t>(kFmmWarps) * T.n_d * sizeof(double);
+      AMK_CUDA_TRY(cudaFuncSetAttribute(m2l_table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(tsm)));
+      m2l_table_kernel<<<(n_cls + kFmmWarps - 1) / kFmmWarps, 32 * kFmmWarps, tsm, c->stream>>>(T, codes, n_cls,
+                                                                                              table);
+      AMK_TRY(check_launch(c, "m2l_table_kernel"));
+    }
+  }
   const size_t m2l_smem = m2l_smem_bytes(T);
   AMK_CUDA_TRY(cudaFuncSetAttribute(fmm_m2l_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(m2l_smem)));
-  fmm_m2l_kernel<<<gw, 32 * kFmmWarps, m2l_smem, c->stream>>>(t, T, gm.off, gm.count, gm.src, M, Lx);
+  fmm_m2l_kernel<<<gw, 32 * kFmmWarps, m2l_smem, c->stream>>>(t, T, gm.off, gm.count, gm.src, M, Lx, class_of,
+                                                              table);
   AMK_TRY(check_launch(c, "fmm_m2l_kernel"));
   AMK_TRY(phase_end(c, AMK_PHASE_FMM_M2L));
 
