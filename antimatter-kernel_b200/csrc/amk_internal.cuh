@@ -185,6 +185,23 @@ enum ScratchSlot {
   kSlotFmmWork5,
   kSlotP2PWork,
   kSlotP2PPart,
+  kSlotM2lCodes,
+  kSlotM2lTarget,
+  kSlotM2lHist,
+  kSlotM2lStart,
+  kSlotM2lUsed,
+  kSlotM2lClassIndex,
+  kSlotM2lTiles,
+  kSlotM2lTileStart,
+  kSlotM2lCounters,
+  kSlotM2lPerm,
+  kSlotM2lFallback,
+  kSlotM2lClassCode,
+  kSlotM2lClassEnd,
+  kSlotM2lTileClass,
+  kSlotM2lTilePos,
+  kSlotM2lTable,
+  kSlotM2lHash,
   kNumSlots
 };
 static_assert(kNumSlots <= 96, "scratch slots");

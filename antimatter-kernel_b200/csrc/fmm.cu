@@ -44,6 +44,7 @@ struct FmmHostTables {
   std::vector<int> rec_axis;                 // per k
   std::vector<int> rec_delta, rec_m1, rec_m2;  // 3 per k
   std::vector<int> m2l_index;                // [g * n_m + a]
+  std::vector<short> m2l_index_t;            // [a * n_m + g]
   std::vector<int> m2m_off, m2m_b, m2m_c;    // CSR by a
   std::vector<int> l2l_off, l2l_b, l2l_c;    // CSR by a
   std::vector<int> grad;                     // 3 per g, -1 none
@@ -100,6 +101,10 @@ struct FmmHostTables {
       for (int a = 0; a < n_m; ++a)
         m2l_index[static_cast<size_t>(g) * n_m + a] =
             index(multi[a].x + multi[g].x, multi[a].y + multi[g].y, multi[a].z + multi[g].z);
+    m2l_index_t.assign(static_cast<size_t>(n_m) * n_m, 0);
+    for (int a = 0; a < n_m; ++a)
+      for (int g = 0; g < n_m; ++g)
+        m2l_index_t[static_cast<size_t>(a) * n_m + g] = static_cast<short>(m2l_index[static_cast<size_t>(g) * n_m + a]);
     m2m_off.push_back(0);
     l2l_off.push_back(0);
     for (int a = 0; a < n_m; ++a) {
@@ -143,6 +148,7 @@ struct FmmDevTables {
   const int* rec_m1;
   const int* rec_m2;
   const int* m2l_index;
+  const short* m2l_index_t;
   const int* m2m_off;
   const int* m2m_b;
   const int* m2m_c;
@@ -159,10 +165,20 @@ struct FmmLists {
 struct Fmm {
   std::map<int, std::pair<DevBuf*, FmmDevTables>> tables;
   FmmLists lists;
+  DevBuf m2l_out[2];  // per-pair M2L products of two chunks in flight
+  // the per-target M2L sums of one chunk run on `side` while the products
+  // of the next chunk run on the context stream
+  cudaStream_t side = nullptr;
+  cudaEvent_t products_done[2] = {nullptr, nullptr}, sums_done[2] = {nullptr, nullptr};
   // statistics of the last evaluation (amk_fmm_stats)
   long stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
   ~Fmm() {
     for (auto& kv : tables) delete kv.second.first;
+    for (int i = 0; i < 2; ++i) {
+      if (products_done[i]) cudaEventDestroy(products_done[i]);
+      if (sums_done[i]) cudaEventDestroy(sums_done[i]);
+    }
+    if (side) cudaStreamDestroy(side);
   }
 };
 
@@ -193,7 +209,7 @@ int get_tables(amk_ctx* c, int order, FmmDevTables* out) {
   const size_t o_multi = append(blob, h.multi), o_fact = append(blob, h.fact), o_if = append(blob, h.inv_fact),
                o_sign = append(blob, h.sign), o_ds = append(blob, h.deg_start), o_ax = append(blob, h.rec_axis),
                o_de = append(blob, h.rec_delta), o_m1 = append(blob, h.rec_m1), o_m2 = append(blob, h.rec_m2),
-               o_idx = append(blob, h.m2l_index), o_mo = append(blob, h.m2m_off), o_mb = append(blob, h.m2m_b),
+               o_idx = append(blob, h.m2l_index), o_idt = append(blob, h.m2l_index_t), o_mo = append(blob, h.m2m_off), o_mb = append(blob, h.m2m_b),
                o_mc = append(blob, h.m2m_c), o_lo = append(blob, h.l2l_off), o_lb = append(blob, h.l2l_b),
                o_lc = append(blob, h.l2l_c), o_g = append(blob, h.grad);
   DevBuf* buf = new DevBuf();
@@ -218,6 +234,7 @@ int get_tables(amk_ctx* c, int order, FmmDevTables* out) {
   t.rec_m1 = reinterpret_cast<const int*>(b + o_m1);
   t.rec_m2 = reinterpret_cast<const int*>(b + o_m2);
   t.m2l_index = reinterpret_cast<const int*>(b + o_idx);
+  t.m2l_index_t = reinterpret_cast<const short*>(b + o_idt);
   t.m2m_off = reinterpret_cast<const int*>(b + o_mo);
   t.m2m_b = reinterpret_cast<const int*>(b + o_mb);
   t.m2m_c = reinterpret_cast<const int*>(b + o_mc);
@@ -384,54 +401,177 @@ __global__ void pair_unpack_kernel(const uint64_t* __restrict__ keys, int n, int
   atomicAdd(&count[static_cast<int>(k >> bits)], 1);
 }
 
-// ------------------------------------------------------------ M2L
-// A warp per target cell (fast-multipole.cc:528-555).
-//
-// Derivative tensors from a table: cube centres lie on a lattice, so for a
-// pair c_t - c_s = u v with u = the smaller half edge and v an integer
-// vector (up to the rounding of the centres, ~1e-15 relative), and
-// D_k(u v) = u^{-|k|-1} D_k(v) (D is homogeneous of degree -1-|k|). The
-// distinct offsets v with |v_i| <= kM2LReach are found once per evaluation
-// and their D(v) built once (fast-multipole.cc:207-232 recurrence, FP64);
-// each pair then loads D(v) and scales it by powers of 1/u. Pairs off the
-// lattice or farther out use the recurrence directly. The contraction runs
-// through the M2L index map in shared memory (int16, rows padded to n_m + 1
-// entries so that lanes read different rows without bank conflicts).
-constexpr int kM2LReach = 31;
-constexpr int kM2LSide = 2 * kM2LReach + 1;
-constexpr int kM2LCodes = kM2LSide * kM2LSide * kM2LSide;
+struct Grouped {
+  int* off = nullptr;
+  int* count = nullptr;
+  int* src = nullptr;
+};
 
-// Lattice offset code of a pair (-1 = off the lattice or out of reach) and u.
-__device__ __forceinline__ int m2l_code(const double4& tc, const double4& sc, double* u_out) {
+// ------------------------------------------------------------ M2L
+// L_g(t) = 1/g! sum_a (-1)^|a| M_a(s) D_{g+a}(c_t - c_s) for every M2L pair
+// (fast-multipole.cc:528-555), evaluated as dense products per displacement
+// class.
+//
+// Cube centres lie on a lattice: for a pair with depths d_t, d_s and half
+// edges h_t, h_s, c_t - c_s = u v with u = min(h_t, h_s) and v an integer
+// vector (up to the rounding of the centres, ~1e-15 relative). D is
+// homogeneous, D_k(u v) = u^{-|k|-1} D_k(v), so with per-cell rescaled
+// expansions
+//     Mh_a(s) = (-1)^|a| M_a(s) h_s^{-|a|},   L_g(t) = h_t^{-|g|-1} Lh_g(t)
+// a pair contributes Lh(t) += A_{v,dd} Mh(s) with the n_m x n_m matrix
+//     A_{v,dd}[g][a] = 1/g! (h_t/u)^{|g|+1} (h_s/u)^{|a|} D_{g+a}(v),
+// which depends only on the class (v, dd = d_t - d_s): h_t/u and h_s/u are
+// powers of two. Pairs are sorted by class and each class is one FP64
+// product A (n_m x n_m) x [Mh of its sources] (n_m x k), in tiles of 64
+// pairs, up to 8 tiles of one class per block. The products are written per pair and summed per target in the
+// pairs' (target, source) order, so the result is run-to-run deterministic.
+// A class is found through an open-addressing hash of (d_t - d_s, v) with
+// bounded probing; pairs off the lattice, beyond the class reach or left
+// without a hash slot take a per-pair path with the derivative recurrence.
+// The pairs are processed in chunks that bound the per-pair scratch.
+constexpr int kM2lTileP = 64;      // pairs per product tile
+constexpr int kM2lUnitTiles = 8;   // tiles of one class per block
+constexpr int kM2lUnitPairs = kM2lUnitTiles * kM2lTileP;
+constexpr int kM2lMinClass = 8;    // smaller classes take the per-pair path
+constexpr size_t kM2lChunkBytes = size_t(4) << 30;  // per-pair products of one chunk
+constexpr int kM2lHashBits = 21;
+constexpr long kM2lHashSlots = 1L << kM2lHashBits;
+constexpr int kM2lHashProbes = 64;
+constexpr int kM2lVBias = 1 << 18;             // v components biased into 19 bits
+constexpr int kM2lMaxReach = kM2lVBias - 1;    // |v_i| covered by the classes
+constexpr unsigned long long kM2lEmpty = ~0ull;
+
+__host__ __device__ __forceinline__ unsigned long long m2l_key(int dd, int vx, int vy, int vz) {
+  return (static_cast<unsigned long long>(dd + 32) << 57) |
+         (static_cast<unsigned long long>(vx + kM2lVBias) << 38) |
+         (static_cast<unsigned long long>(vy + kM2lVBias) << 19) | static_cast<unsigned long long>(vz + kM2lVBias);
+}
+__device__ __forceinline__ int m2l_key_dd(unsigned long long k) { return static_cast<int>(k >> 57) - 32; }
+__device__ __forceinline__ int m2l_key_v(unsigned long long k, int axis) {
+  return static_cast<int>((k >> (38 - 19 * axis)) & ((1u << 19) - 1)) - kM2lVBias;
+}
+
+// Class key of a pair, kM2lEmpty = off the lattice or out of reach.
+__device__ __forceinline__ unsigned long long m2l_class_key(const Octree& t, int ti, int si, int reach) {
+  const double4 tc = t.center[ti], sc = t.center[si];
+  const int dd = static_cast<int>(t.meta[ti].x) - static_cast<int>(t.meta[si].x);
   const double u = fmin(tc.w, sc.w);
-  *u_out = u;
   const double vx = (tc.x - sc.x) / u, vy = (tc.y - sc.y) / u, vz = (tc.z - sc.z) / u;
   const double rx = rint(vx), ry = rint(vy), rz = rint(vz);
-  if (fabs(vx - rx) > 1e-6 || fabs(vy - ry) > 1e-6 || fabs(vz - rz) > 1e-6) return -1;
-  if (fabs(rx) > kM2LReach || fabs(ry) > kM2LReach || fabs(rz) > kM2LReach) return -1;
-  return ((static_cast<int>(rx) + kM2LReach) * kM2LSide + (static_cast<int>(ry) + kM2LReach)) * kM2LSide +
-         (static_cast<int>(rz) + kM2LReach);
+  if (fabs(vx - rx) > 1e-6 || fabs(vy - ry) > 1e-6 || fabs(vz - rz) > 1e-6) return kM2lEmpty;
+  if (fabs(rx) > reach || fabs(ry) > reach || fabs(rz) > reach) return kM2lEmpty;
+  return m2l_key(dd, static_cast<int>(rx), static_cast<int>(ry), static_cast<int>(rz));
 }
 
-__global__ void m2l_mark_kernel(const Octree t, const int2* __restrict__ pairs, long n, int* __restrict__ used) {
+// Slot of a key in the class hash (inserted if absent), -1 if no slot
+// within the probe limit.
+__device__ __forceinline__ int m2l_hash_slot(unsigned long long* keys, unsigned long long key) {
+  unsigned long long h = key;  // splitmix64 finaliser
+  h = (h ^ (h >> 30)) * 0xbf58476d1ce4e5b9ull;
+  h = (h ^ (h >> 27)) * 0x94d049bb133111ebull;
+  h ^= h >> 31;
+  long slot = static_cast<long>(h & (kM2lHashSlots - 1));
+  for (int probe = 0; probe < kM2lHashProbes; ++probe) {
+    const unsigned long long k = keys[slot];
+    if (k == key) return static_cast<int>(slot);
+    if (k == kM2lEmpty) {
+      const unsigned long long old = atomicCAS(keys + slot, kM2lEmpty, key);
+      if (old == kM2lEmpty || old == key) return static_cast<int>(slot);
+    }
+    slot = (slot + 1) & (kM2lHashSlots - 1);
+  }
+  return -1;
+}
+
+// Mh[s][a] = (-1)^|a| M[s][a] h_s^{-|a|}
+__global__ void m2l_rescale_kernel(const Octree t, FmmDevTables T, const double* __restrict__ M,
+                                   double* __restrict__ Mh) {
   const long e = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
-  if (e >= n) return;
-  double u;
-  const int code = m2l_code(t.center[pairs[e].x], t.center[pairs[e].y], &u);
-  if (code >= 0) used[code] = 1;
+  if (e >= t.n_nodes * T.n_m) return;
+  const int s = static_cast<int>(e / T.n_m), a = static_cast<int>(e - static_cast<long>(s) * T.n_m);
+  const double ih = 1.0 / t.center[s].w;
+  double f = T.sign[a];
+  for (int d = 0; d < T.multi[a].w; ++d) f *= ih;
+  Mh[e] = M[e] * f;
 }
 
-__global__ void m2l_list_kernel(const int* __restrict__ used, const int* __restrict__ index, int* __restrict__ codes) {
-  const int code = blockIdx.x * blockDim.x + threadIdx.x;
-  if (code < kM2LCodes && used[code]) codes[index[code]] = code;
+// Class slot (-1: per-pair path) and target of every pair (a warp per target).
+__global__ void m2l_classify_kernel(const Octree t, const int* __restrict__ off, const int* __restrict__ count,
+                                    const int* __restrict__ src, int reach, unsigned long long* __restrict__ keys,
+                                    int* __restrict__ codes, int* __restrict__ tgt) {
+  const int lane = threadIdx.x & 31;
+  const long w0 = (blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x) >> 5;
+  const long nw = (static_cast<long>(gridDim.x) * blockDim.x) >> 5;
+  for (long ti = w0; ti < t.n_nodes; ti += nw) {
+    const int b = off[ti], n = count[ti];
+    for (int e = b + lane; e < b + n; e += 32) {
+      const unsigned long long key = m2l_class_key(t, static_cast<int>(ti), src[e], reach);
+      codes[e] = key == kM2lEmpty ? -1 : m2l_hash_slot(keys, key);
+      tgt[e] = static_cast<int>(ti);
+    }
+  }
 }
 
-__global__ void m2l_class_map_kernel(const int* __restrict__ used, int* __restrict__ class_of) {
-  const int code = blockIdx.x * blockDim.x + threadIdx.x;
-  if (code < kM2LCodes && !used[code]) class_of[code] = -1;
+// Pairs per class code in [e0, e1); off-lattice pairs listed for the per-pair path.
+__global__ void m2l_histogram_kernel(const int* __restrict__ codes, long e0, long e1, int* __restrict__ hist,
+                                     int* __restrict__ fallback, int* __restrict__ n_fallback) {
+  const long e = e0 + blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (e >= e1) return;
+  const int code = codes[e];
+  if (code >= 0)
+    atomicAdd(hist + code, 1);
+  else
+    fallback[atomicAdd(n_fallback, 1)] = static_cast<int>(e);
 }
 
-// D recurrence for displacement xs into D[0, n_d), one warp.
+// Classes of fewer than kM2lMinClass pairs go the per-pair path (a product
+// tile with a handful of pairs costs more than their recurrences).
+__global__ void m2l_code_flags_kernel(const int* __restrict__ hist, long n_codes, int* __restrict__ used,
+                                      int* __restrict__ units) {
+  const long code = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (code >= n_codes) return;
+  const int n = hist[code];
+  used[code] = n >= kM2lMinClass;
+  units[code] = n >= kM2lMinClass ? (n + kM2lUnitPairs - 1) / kM2lUnitPairs : 0;
+}
+
+// Class list and product units (<= 8 tiles of one class) from the scanned
+// per-code counts.
+__global__ void m2l_class_fill_kernel(const int* __restrict__ hist, const int* __restrict__ start,
+                                      const int* __restrict__ cls_index, const int* __restrict__ unit_start,
+                                      long n_codes, int* __restrict__ cls_code, int* __restrict__ cls_end,
+                                      int* __restrict__ unit_cls, int* __restrict__ unit_pos) {
+  const long code = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (code >= n_codes) return;
+  const int n = hist[code];
+  if (n < kM2lMinClass) return;
+  const int cls = cls_index[code];
+  cls_code[cls] = static_cast<int>(code);
+  cls_end[cls] = start[code] + n;
+  const int nu = (n + kM2lUnitPairs - 1) / kM2lUnitPairs;
+  for (int k = 0; k < nu; ++k) {
+    unit_cls[unit_start[code] + k] = cls;
+    unit_pos[unit_start[code] + k] = start[code] + k * kM2lUnitPairs;
+  }
+}
+
+// Pair positions grouped by class (order inside a class is irrelevant: every
+// pair's product is computed on its own); pairs of small classes join the
+// per-pair list. Consumes hist.
+__global__ void m2l_scatter_kernel(const int* __restrict__ codes, long e0, long e1, const int* __restrict__ start,
+                                   const int* __restrict__ used, int* __restrict__ hist, int* __restrict__ perm,
+                                   int* __restrict__ fallback, int* __restrict__ n_fallback) {
+  const long e = e0 + blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (e >= e1) return;
+  const int code = codes[e];
+  if (code < 0) return;
+  if (used[code])
+    perm[start[code] + atomicSub(hist + code, 1) - 1] = static_cast<int>(e);
+  else
+    fallback[atomicAdd(n_fallback, 1)] = static_cast<int>(e);
+}
+
+// D recurrence (fast-multipole.cc:207-232) for displacement xs into D[0, n_d), one warp.
 __device__ __forceinline__ void m2l_derivatives(const FmmDevTables& T, int lane, const double xs[3], double* D) {
   const double inv_r2 = 1.0 / (xs[0] * xs[0] + xs[1] * xs[1] + xs[2] * xs[2]);
   if (lane == 0) D[0] = sqrt(inv_r2);
@@ -454,87 +594,453 @@ __device__ __forceinline__ void m2l_derivatives(const FmmDevTables& T, int lane,
   }
 }
 
-// D(v) of every used offset: a warp per offset, into table[class * n_d + k].
+// D(v) of every class: a warp per class, into table[class * n_d + k].
 __global__ void __launch_bounds__(32 * kFmmWarps)
-m2l_table_kernel(FmmDevTables T, const int* __restrict__ codes, int n_classes, double* __restrict__ table) {
+m2l_table_kernel(FmmDevTables T, const int* __restrict__ cls_code, int n_classes,
+                 const unsigned long long* __restrict__ keys, double* __restrict__ table) {
   extern __shared__ __align__(16) unsigned char tab_smem[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double* D = reinterpret_cast<double*>(tab_smem) + static_cast<size_t>(w) * T.n_d;
   const int cls = blockIdx.x * kFmmWarps + w;
   if (cls >= n_classes) return;
-  const int code = codes[cls];
-  const double xs[3] = {static_cast<double>(code / (kM2LSide * kM2LSide) - kM2LReach),
-                        static_cast<double>((code / kM2LSide) % kM2LSide - kM2LReach),
-                        static_cast<double>(code % kM2LSide - kM2LReach)};
+  const unsigned long long key = keys[cls_code[cls]];
+  const double xs[3] = {static_cast<double>(m2l_key_v(key, 0)), static_cast<double>(m2l_key_v(key, 1)),
+                        static_cast<double>(m2l_key_v(key, 2))};
   m2l_derivatives(T, lane, xs, D);
   for (int k = lane; k < T.n_d; k += 32) table[static_cast<size_t>(cls) * T.n_d + k] = D[k];
 }
 
-__global__ void __launch_bounds__(32 * kFmmWarps)
-fmm_m2l_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, const int* __restrict__ count,
-               const int* __restrict__ src, const double* __restrict__ M, double* __restrict__ L,
-               const int* __restrict__ class_of, const double* __restrict__ table) {
-  extern __shared__ __align__(16) unsigned char m2l_smem[];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  const int nm = T.n_m, nd = T.n_d, stride = nm + 1, p2 = 2 * T.p;
-  double* D = reinterpret_cast<double*>(m2l_smem) + static_cast<size_t>(w) * (nd + nm + p2 + 2);
-  double* Ms = D + nd;
-  double* upw = Ms + nm;  // u^-d, d = 0 .. 2p + 1
-  short* idx = reinterpret_cast<short*>(reinterpret_cast<double*>(m2l_smem) +
-                                        static_cast<size_t>(kFmmWarps) * (nd + nm + p2 + 2));
-  unsigned char* degk = reinterpret_cast<unsigned char*>(idx + nm * stride);
-  for (int e = threadIdx.x; e < nm * nm; e += blockDim.x) {
-    const int g = e / nm, a = e - g * nm;
-    idx[g * stride + a] = static_cast<short>(T.m2l_index[e]);
-  }
-  for (int k = threadIdx.x; k < nd; k += blockDim.x) degk[k] = static_cast<unsigned char>(T.multi[k].w);
-  __syncthreads();
-  const int ti = blockIdx.x * kFmmWarps + w;
-  if (ti >= t.n_nodes) return;
-  const int cnt = count[ti];
-  if (cnt == 0) return;
-  const double4 tc = t.center[ti];
-  double acc[(kMaxNm + 31) / 32];
-  for (int u = 0; u < (kMaxNm + 31) / 32; ++u) acc[u] = 0.0;
-  const int b = off[ti];
-  for (int e = b; e < b + cnt; ++e) {
-    const int si = src[e];
-    const double4 sc = t.center[si];
-    for (int a = lane; a < nm; a += 32) Ms[a] = T.sign[a] * M[static_cast<size_t>(si) * nm + a];
-    double u;
-    const int code = m2l_code(tc, sc, &u);
-    const int cls = code >= 0 ? class_of[code] : -1;
-    if (cls >= 0) {
-      if (lane == 0) {
-        const double iu = 1.0 / u;
-        double pw = 1.0;
-        for (int d = 0; d <= p2 + 1; ++d) {
-          upw[d] = pw;
-          pw *= iu;
-        }
-      }
-      __syncwarp();
-      const double* tab = table + static_cast<size_t>(cls) * nd;
-      for (int k = lane; k < nd; k += 32) D[k] = tab[k] * upw[degk[k] + 1];
-      __syncwarp();
-    } else {
-      const double xs[3] = {tc.x - sc.x, tc.y - sc.y, tc.z - sc.z};
-      m2l_derivatives(T, lane, xs, D);
-    }
-    for (int uu = 0, g = lane; g < nm; ++uu, g += 32) {
-      const short* row = idx + g * stride;
-      double s = 0.0;
-      for (int a = 0; a < nm; ++a) s += Ms[a] * D[row[a]];
-      acc[uu] += s * T.inv_fact[g];
-    }
-    __syncwarp();
-  }
-  for (int u = 0, g = lane; g < nm; ++u, g += 32) L[static_cast<size_t>(ti) * nm + g] += acc[u];
+// Tile shape per order: kTy row groups x kRg rows cover the n_m local
+// coefficients (kTy * kRg >= n_m, kTy a multiple of 4 so a warp is 4 row
+// groups x 8 pair groups), each thread owns 8 pairs; the k dimension runs in
+// chunks of kKc, a divisor of n_m. Up to order 6 the whole class matrix stays
+// in shared memory; above, it is regenerated chunk by chunk.
+template <int P>
+struct M2lShape;
+#define AMK_M2L_SHAPE(P, TY, RG, KC)                                                   \
+  template <>                                                                          \
+  struct M2lShape<P> {                                                                 \
+    static constexpr int kNm = (P + 1) * (P + 2) * (P + 3) / 6;                        \
+    static constexpr int kNd = (2 * P + 1) * (2 * P + 2) * (2 * P + 3) / 6;            \
+    static constexpr int kTy = TY, kRg = RG, kKc = KC, kNg = TY * RG;                   \
+    static constexpr int kThreads = 8 * TY;                                            \
+    static constexpr bool kFullA = P <= 6;                                             \
+    static_assert(kNg >= kNm && kNm % kKc == 0 && TY % 4 == 0, "M2L tile shape");      \
+  };
+AMK_M2L_SHAPE(1, 4, 1, 4)
+AMK_M2L_SHAPE(2, 4, 3, 10)
+AMK_M2L_SHAPE(3, 4, 5, 10)
+AMK_M2L_SHAPE(4, 12, 3, 7)
+AMK_M2L_SHAPE(5, 8, 7, 14)
+AMK_M2L_SHAPE(6, 12, 7, 12)
+AMK_M2L_SHAPE(7, 20, 6, 15)
+AMK_M2L_SHAPE(8, 24, 7, 15)
+#undef AMK_M2L_SHAPE
+constexpr int kM2lRp = 8;               // pairs per thread
+constexpr int kM2lBs = kM2lTileP + 2;   // B row stride (doubles): 16-byte rows, 2-way store conflicts
+constexpr int kM2lStages = 3;           // B pipeline depth (k chunks)
+
+template <int P>
+__host__ __device__ constexpr size_t m2l_a_doubles() {
+  using S = M2lShape<P>;
+  return S::kFullA ? static_cast<size_t>(S::kNm) * S::kNg : static_cast<size_t>(2) * S::kKc * S::kNg;
 }
 
-size_t m2l_smem_bytes(const FmmDevTables& T) {
-  return static_cast<size_t>(kFmmWarps) * (T.n_d + T.n_m + 2 * T.p + 2) * sizeof(double) +
-         static_cast<size_t>(T.n_m) * (T.n_m + 1) * sizeof(short) + static_cast<size_t>(T.n_d) + 16;
+template <int P>
+size_t m2l_product_smem() {
+  using S = M2lShape<P>;
+  return sizeof(double) * (m2l_a_doubles<P>() + static_cast<size_t>(kM2lStages) * S::kKc * kM2lBs + S::kNd +
+                           S::kNg + S::kNm) +
+         2 * kM2lUnitPairs * sizeof(int);
+}
+
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  const int n = valid ? 8 : 0;  // 0: zero fill, nothing read
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// One unit: up to 8 tiles of 64 pairs of one class. Thread (tx, ty) owns
+// rows g = ty + kTy i and pairs p = 16 (j / 2) + 2 tx + j % 2 of the current
+// tile (each 16-byte shared load of a B row is then conflict-free). A = the
+// class matrix with the source scaling folded in, from the class's D(v)
+// through the transposed index map; B = the sources' rescaled multipoles,
+// streamed k chunk by k chunk through a 3-stage cp.async pipeline that runs
+// on across the unit's tiles.
+template <int P>
+__global__ void __launch_bounds__(M2lShape<P>::kThreads)
+m2l_class_product_kernel(FmmDevTables T, const int* __restrict__ unit_cls, const int* __restrict__ unit_pos,
+                         const int* __restrict__ cls_code, const int* __restrict__ cls_end,
+                         const int* __restrict__ perm, const int* __restrict__ src, const double* __restrict__ Mh,
+                         const double* __restrict__ table, const unsigned long long* __restrict__ keys, long e0,
+                         double* __restrict__ out) {
+  using S = M2lShape<P>;
+  constexpr int kNm = S::kNm, kKc = S::kKc, kNg = S::kNg, kTh = S::kThreads, kChunks = kNm / kKc;
+  extern __shared__ __align__(16) unsigned char prod_smem[];
+  double* As = reinterpret_cast<double*>(prod_smem);
+  double* Bs = As + m2l_a_doubles<P>();           // [kM2lStages][kKc][kM2lBs]
+  double* Ds = Bs + kM2lStages * kKc * kM2lBs;    // [kNd]
+  double* rowf = Ds + S::kNd;                     // [kNg]
+  double* colf = rowf + kNg;                      // [kNm]
+  int* pe = reinterpret_cast<int*>(colf + kNm);   // [kM2lUnitPairs]
+  int* ps = pe + kM2lUnitPairs;                   // [kM2lUnitPairs]
+  const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
+  const int cls = unit_cls[blockIdx.x], pos0 = unit_pos[blockIdx.x];
+  const int np = min(kM2lUnitPairs, cls_end[cls] - pos0);
+  const int n_tiles = (np + kM2lTileP - 1) / kM2lTileP, n_steps = n_tiles * kChunks;
+  const int dd = m2l_key_dd(keys[cls_code[cls]]);
+  const int et = dd < 0 ? -dd : 0, es = dd > 0 ? dd : 0;  // log2(h_t / u), log2(h_s / u)
+  for (int k = tid; k < S::kNd; k += kTh) Ds[k] = table[static_cast<size_t>(cls) * S::kNd + k];
+  for (int g = tid; g < kNg; g += kTh) rowf[g] = g < kNm ? ldexp(T.inv_fact[g], (T.multi[g].w + 1) * et) : 0.0;
+  for (int a = tid; a < kNm; a += kTh) colf[a] = ldexp(1.0, T.multi[a].w * es);
+  for (int p = tid; p < n_tiles * kM2lTileP; p += kTh) {
+    const int e = p < np ? perm[pos0 + p] : -1;
+    pe[p] = e;
+    ps[p] = e >= 0 ? src[e] : -1;
+  }
+  __syncthreads();
+  // rows [a0, a0 + n) of A (rows = source coefficients) into dst[(a - a0) * kNg + g]
+  auto fill_a = [&](double* dst, int a0, int n) {
+    for (int x = tid; x < n * kNg; x += kTh) {
+      const int r = x / kNg, g = x - r * kNg, a = a0 + r;
+      dst[x] = g < kNm ? Ds[T.m2l_index_t[a * kNm + g]] * colf[a] : 0.0;
+    }
+  };
+  auto issue = [&](int step) {
+    if (step < n_steps) {
+      const int tile = step / kChunks, chunk = step - tile * kChunks;
+      double* B = Bs + (step % kM2lStages) * kKc * kM2lBs;
+      for (int x = tid; x < kKc * kM2lTileP; x += kTh) {
+        const int p = x / kKc, kk = x - p * kKc;
+        const int sp = ps[tile * kM2lTileP + p];
+        cp_async8(B + kk * kM2lBs + p, sp >= 0 ? Mh + static_cast<size_t>(sp) * kNm + chunk * kKc + kk : Mh, sp >= 0);
+      }
+    }
+    cp_async_commit();
+  };
+  for (int st = 0; st < kM2lStages - 1; ++st) issue(st);
+  if (S::kFullA) fill_a(As, 0, kNm);
+  double acc[S::kRg][kM2lRp];
+#pragma unroll
+  for (int i = 0; i < S::kRg; ++i)
+#pragma unroll
+    for (int j = 0; j < kM2lRp; ++j) acc[i][j] = 0.0;
+#pragma unroll 1
+  for (int step = 0; step < n_steps; ++step) {
+    const int tile = step / kChunks, chunk = step - tile * kChunks;
+    const double* A;
+    if (S::kFullA) {
+      A = As + chunk * kKc * kNg;
+    } else {
+      double* Ab = As + (step & 1) * kKc * kNg;
+      fill_a(Ab, chunk * kKc, kKc);
+      A = Ab;
+    }
+    cp_async_wait<kM2lStages - 2>();
+    __syncthreads();
+    issue(step + kM2lStages - 1);
+    const double* B = Bs + (step % kM2lStages) * kKc * kM2lBs;
+#pragma unroll
+    for (int kk = 0; kk < kKc; ++kk) {
+      double b[kM2lRp], av[S::kRg];
+#pragma unroll
+      for (int q = 0; q < kM2lRp / 2; ++q) {
+        const double2 v = *reinterpret_cast<const double2*>(B + kk * kM2lBs + 16 * q + 2 * tx);
+        b[2 * q] = v.x;
+        b[2 * q + 1] = v.y;
+      }
+#pragma unroll
+      for (int i = 0; i < S::kRg; ++i) av[i] = A[kk * kNg + ty + S::kTy * i];
+#pragma unroll
+      for (int i = 0; i < S::kRg; ++i)
+#pragma unroll
+        for (int j = 0; j < kM2lRp; ++j) acc[i][j] = fma(av[i], b[j], acc[i][j]);
+    }
+    if (chunk == kChunks - 1) {
+#pragma unroll
+      for (int j = 0; j < kM2lRp; ++j) {
+        const int e = pe[tile * kM2lTileP + 16 * (j >> 1) + 2 * tx + (j & 1)];
+#pragma unroll
+        for (int i = 0; i < S::kRg; ++i) {
+          const int g = ty + S::kTy * i;
+          if (e >= 0 && g < kNm) out[static_cast<size_t>(e - e0) * kNm + g] = acc[i][j] * rowf[g];
+          acc[i][j] = 0.0;
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+}
+
+// Pairs outside the classes: a warp per pair, the derivative tensor by the
+// recurrence, the product written in the rescaled form Lh = h_t^{|g|+1} L.
+__global__ void __launch_bounds__(32 * kFmmWarps)
+m2l_pair_kernel(const Octree t, FmmDevTables T, const int* __restrict__ list, int n, const int* __restrict__ tgt,
+                const int* __restrict__ src, const double* __restrict__ M, long e0, double* __restrict__ out) {
+  extern __shared__ __align__(16) unsigned char pair_smem[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  double* D = reinterpret_cast<double*>(pair_smem) + static_cast<size_t>(w) * (T.n_d + T.n_m);
+  double* Ms = D + T.n_d;
+  const int k = blockIdx.x * kFmmWarps + w;
+  if (k >= n) return;
+  const int e = list[k], ti = tgt[e], si = src[e];
+  const double4 tc = t.center[ti], sc = t.center[si];
+  for (int a = lane; a < T.n_m; a += 32) Ms[a] = T.sign[a] * M[static_cast<size_t>(si) * T.n_m + a];
+  const double xs[3] = {tc.x - sc.x, tc.y - sc.y, tc.z - sc.z};
+  m2l_derivatives(T, lane, xs, D);
+  for (int g = lane; g < T.n_m; g += 32) {
+    double s = 0.0;
+    for (int a = 0; a < T.n_m; ++a) s += Ms[a] * D[T.m2l_index[g * T.n_m + a]];
+    double f = T.inv_fact[g];
+    for (int d = 0; d <= T.multi[g].w; ++d) f *= tc.w;
+    out[static_cast<size_t>(e - e0) * T.n_m + g] = s * f;
+  }
+}
+
+// L(t) += h_t^{-|g|-1} sum over the target's pairs in [e0, e1) in pair order;
+// a warp per target, lanes over coefficients (R rows of 32), four pairs'
+// rows in flight.
+template <int R>
+__global__ void __launch_bounds__(256)
+m2l_reduce_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, const int* __restrict__ count,
+                  int t_first, int n_targets, long e0, long e1, const double* __restrict__ out,
+                  double* __restrict__ L) {
+  constexpr int kU = 4;
+  const int lane = threadIdx.x & 31;
+  const int k = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (k >= n_targets) return;
+  const int ti = t_first + k, nm = T.n_m;
+  const long b = max(static_cast<long>(off[ti]), e0), end = min(static_cast<long>(off[ti]) + count[ti], e1);
+  if (b >= end) return;
+  double s[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) s[r] = 0.0;
+  const double* o = out + static_cast<size_t>(b - e0) * nm;
+  long e = b;
+  for (; e + kU <= end; e += kU, o += kU * nm) {
+    double v[kU][R];
+#pragma unroll
+    for (int u = 0; u < kU; ++u)
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const int g = lane + 32 * r;
+        v[u][r] = g < nm ? o[u * nm + g] : 0.0;
+      }
+#pragma unroll
+    for (int u = 0; u < kU; ++u)
+#pragma unroll
+      for (int r = 0; r < R; ++r) s[r] += v[u][r];
+  }
+  for (; e < end; ++e, o += nm)
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int g = lane + 32 * r;
+      if (g < nm) s[r] += o[g];
+    }
+  const double ih = 1.0 / t.center[ti].w;
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int g = lane + 32 * r;
+    if (g >= nm) continue;
+    double f = s[r];
+    for (int d = 0; d <= T.multi[g].w; ++d) f *= ih;
+    L[static_cast<size_t>(ti) * nm + g] += f;
+  }
+}
+
+int m2l_reduce(amk_ctx* c, cudaStream_t stream, const Octree& t, const FmmDevTables& T, const int* off,
+               const int* count, int t_first, int n_targets, long e0, long e1, const double* out, double* L) {
+  const unsigned grid = static_cast<unsigned>((n_targets + 7) / 8);
+  switch ((T.n_m + 31) / 32) {
+    case 1:
+      m2l_reduce_kernel<1><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
+      break;
+    case 2:
+      m2l_reduce_kernel<2><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
+      break;
+    case 3:
+      m2l_reduce_kernel<3><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
+      break;
+    case 4:
+      m2l_reduce_kernel<4><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
+      break;
+    default:
+      static_assert((kMaxNm + 31) / 32 == 6, "rows per lane");
+      m2l_reduce_kernel<6><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
+      break;
+  }
+  return check_launch(c, "m2l_reduce_kernel");
+}
+
+template <int P>
+int launch_class_product(amk_ctx* c, const FmmDevTables& T, int n_units, const int* unit_cls, const int* unit_pos,
+                         const int* cls_code, const int* cls_end, const int* perm, const int* src, const double* Mh,
+                         const double* table, const unsigned long long* keys, long e0, double* out) {
+  const size_t smem = m2l_product_smem<P>();
+  AMK_CUDA_TRY(cudaFuncSetAttribute(m2l_class_product_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
+  m2l_class_product_kernel<P><<<n_units, M2lShape<P>::kThreads, smem, c->stream>>>(
+      T, unit_cls, unit_pos, cls_code, cls_end, perm, src, Mh, table, keys, e0, out);
+  return check_launch(c, "m2l_class_product_kernel");
+}
+
+int class_product(amk_ctx* c, int order, const FmmDevTables& T, int n_units, const int* unit_cls,
+                  const int* unit_pos, const int* cls_code, const int* cls_end, const int* perm, const int* src,
+                  const double* Mh, const double* table, const unsigned long long* keys, long e0, double* out) {
+#define AMK_M2L_CASE(P)                                                                                         \
+  case P:                                                                                                     \
+    return launch_class_product<P>(c, T, n_units, unit_cls, unit_pos, cls_code, cls_end, perm, src, Mh, table, \
+                                   keys, e0, out);
+  switch (order) {
+    AMK_M2L_CASE(1)
+    AMK_M2L_CASE(2)
+    AMK_M2L_CASE(3)
+    AMK_M2L_CASE(4)
+    AMK_M2L_CASE(5)
+    AMK_M2L_CASE(6)
+    AMK_M2L_CASE(7)
+    AMK_M2L_CASE(8)
+    default:
+      return fail(AMK_ERR_INVALID, "FMM order %d outside [1, %d]", order, kMaxOrder);
+  }
+#undef AMK_M2L_CASE
+}
+
+// Class reach; AMK_FMM_M2L_REACH narrows it, which sends the pairs beyond it
+// through the per-pair path (tests of that path).
+int m2l_reach() {
+  const char* s = getenv("AMK_FMM_M2L_REACH");
+  if (!s || !*s) return kM2lMaxReach;
+  const int r = atoi(s);
+  return r < 0 ? 0 : (r > kM2lMaxReach ? kM2lMaxReach : r);
+}
+
+// All M2L pairs (grouped by target in gm) into L.
+int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, const Grouped& gm, long n_m2l,
+                 const double* M, double* L) {
+  int rc = AMK_OK;
+  const long nn = t.n_nodes;
+  const int reach = m2l_reach();
+  const long n_codes = kM2lHashSlots;
+  unsigned long long* keys = slot<unsigned long long>(c, kSlotM2lHash, kM2lHashSlots, &rc);
+  AMK_TRY(rc);
+  double* Mh = slot<double>(c, kSlotFmmWork5, static_cast<size_t>(nn) * T.n_m, &rc);
+  AMK_TRY(rc);
+  int* codes = slot<int>(c, kSlotM2lCodes, n_m2l, &rc);
+  AMK_TRY(rc);
+  int* tgt = slot<int>(c, kSlotM2lTarget, n_m2l, &rc);
+  AMK_TRY(rc);
+  int* hist = slot<int>(c, kSlotM2lHist, n_codes + 1, &rc);
+  AMK_TRY(rc);
+  int* start = slot<int>(c, kSlotM2lStart, n_codes + 1, &rc);
+  AMK_TRY(rc);
+  int* used = slot<int>(c, kSlotM2lUsed, n_codes + 1, &rc);
+  AMK_TRY(rc);
+  int* cls_index = slot<int>(c, kSlotM2lClassIndex, n_codes + 1, &rc);
+  AMK_TRY(rc);
+  int* nunit = slot<int>(c, kSlotM2lTiles, n_codes + 1, &rc);
+  AMK_TRY(rc);
+  int* unit_start = slot<int>(c, kSlotM2lTileStart, n_codes + 1, &rc);
+  AMK_TRY(rc);
+  int* counters = slot<int>(c, kSlotM2lCounters, 8, &rc);  // pairs, classes, units, fallback pairs
+  AMK_TRY(rc);
+  const long total = nn * T.n_m;
+  m2l_rescale_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, c->stream>>>(t, T, M, Mh);
+  AMK_TRY(check_launch(c, "m2l_rescale_kernel"));
+  AMK_CUDA_TRY(cudaMemsetAsync(keys, 0xff, kM2lHashSlots * sizeof(unsigned long long), c->stream));
+  m2l_classify_kernel<<<4 * 148, 256, 0, c->stream>>>(t, gm.off, gm.count, gm.src, reach, keys, codes, tgt);
+  AMK_TRY(check_launch(c, "m2l_classify_kernel"));
+  long cap = std::max<long>(1L << 20, static_cast<long>(kM2lChunkBytes / (sizeof(double) * T.n_m)));
+  if (const char* env = getenv("AMK_FMM_M2L_CHUNK_PAIRS")) {  // smaller chunks (tests of the chunk seams)
+    const long v = atol(env);
+    if (v > 0) cap = std::min(cap, v);
+  }
+  Fmm* f = c->fmm;
+  if (!f->side) {
+    AMK_CUDA_TRY(cudaStreamCreateWithFlags(&f->side, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i) {
+      AMK_CUDA_TRY(cudaEventCreateWithFlags(&f->products_done[i], cudaEventDisableTiming));
+      AMK_CUDA_TRY(cudaEventCreateWithFlags(&f->sums_done[i], cudaEventDisableTiming));
+    }
+  }
+  const long max_cls = std::min<long>(cap, n_codes) + 1, max_units = cap / kM2lUnitPairs + max_cls + 1;
+  int* perm = slot<int>(c, kSlotM2lPerm, std::min(cap, n_m2l), &rc);
+  AMK_TRY(rc);
+  int* fallback = slot<int>(c, kSlotM2lFallback, std::min(cap, n_m2l), &rc);
+  AMK_TRY(rc);
+  int* cls_code = slot<int>(c, kSlotM2lClassCode, max_cls, &rc);
+  AMK_TRY(rc);
+  int* cls_end = slot<int>(c, kSlotM2lClassEnd, max_cls, &rc);
+  AMK_TRY(rc);
+  int* unit_cls = slot<int>(c, kSlotM2lTileClass, max_units, &rc);
+  AMK_TRY(rc);
+  int* unit_pos = slot<int>(c, kSlotM2lTilePos, max_units, &rc);
+  AMK_TRY(rc);
+  const int n_buf = n_m2l > cap ? 2 : 1;
+  for (int i = 0; i < n_buf; ++i)
+    AMK_TRY(f->m2l_out[i].reserve(static_cast<size_t>(std::min(cap, n_m2l)) * T.n_m * sizeof(double)));
+  int chunk = 0;
+  for (long e0 = 0; e0 < n_m2l; e0 += cap, ++chunk) {
+    const long e1 = std::min(n_m2l, e0 + cap), ne = e1 - e0;
+    const int buf = chunk & 1;
+    double* out = f->m2l_out[buf].as<double>();
+    AMK_CUDA_TRY(cudaMemsetAsync(hist, 0, n_codes * sizeof(int), c->stream));
+    AMK_CUDA_TRY(cudaMemsetAsync(counters, 0, 8 * sizeof(int), c->stream));
+    const unsigned ge = static_cast<unsigned>((ne + 255) / 256), gc = static_cast<unsigned>((n_codes + 255) / 256);
+    m2l_histogram_kernel<<<ge, 256, 0, c->stream>>>(codes, e0, e1, hist, fallback, counters + 3);
+    AMK_TRY(check_launch(c, "m2l_histogram_kernel"));
+    AMK_TRY(exclusive_scan_int(c, hist, n_codes, start, counters));
+    m2l_code_flags_kernel<<<gc, 256, 0, c->stream>>>(hist, n_codes, used, nunit);
+    AMK_TRY(check_launch(c, "m2l_code_flags_kernel"));
+    AMK_TRY(exclusive_scan_int(c, used, n_codes, cls_index, counters + 1));
+    AMK_TRY(exclusive_scan_int(c, nunit, n_codes, unit_start, counters + 2));
+    m2l_class_fill_kernel<<<gc, 256, 0, c->stream>>>(hist, start, cls_index, unit_start, n_codes, cls_code, cls_end,
+                                                     unit_cls, unit_pos);
+    AMK_TRY(check_launch(c, "m2l_class_fill_kernel"));
+    m2l_scatter_kernel<<<ge, 256, 0, c->stream>>>(codes, e0, e1, start, used, hist, perm, fallback, counters + 3);
+    AMK_TRY(check_launch(c, "m2l_scatter_kernel"));
+    int h[4] = {0, 0, 0, 0}, tr[2] = {0, 0};
+    AMK_CUDA_TRY(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaMemcpyAsync(tr, tgt + e0, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaMemcpyAsync(tr + 1, tgt + e1 - 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const int n_cls = h[1], n_units = h[2], n_fb = h[3];
+    // the sums of the chunk before the previous one still read this buffer
+    if (chunk >= 2) AMK_CUDA_TRY(cudaStreamWaitEvent(c->stream, f->sums_done[buf], 0));
+    if (n_cls > 0) {
+      double* table = slot<double>(c, kSlotM2lTable, static_cast<size_t>(n_cls) * T.n_d, &rc);
+      AMK_TRY(rc);
+      const size_t tsm = static_cast<size_t>(kFmmWarps) * T.n_d * sizeof(double);
+      AMK_CUDA_TRY(cudaFuncSetAttribute(m2l_table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(tsm)));
+      m2l_table_kernel<<<(n_cls + kFmmWarps - 1) / kFmmWarps, 32 * kFmmWarps, tsm, c->stream>>>(T, cls_code, n_cls,
+                                                                                              keys, table);
+      AMK_TRY(check_launch(c, "m2l_table_kernel"));
+      AMK_TRY(class_product(c, order, T, n_units, unit_cls, unit_pos, cls_code, cls_end, perm, gm.src, Mh, table,
+                            keys, e0, out));
+    }
+    if (n_fb > 0) {
+      const size_t psm = static_cast<size_t>(kFmmWarps) * (T.n_d + T.n_m) * sizeof(double);
+      AMK_CUDA_TRY(cudaFuncSetAttribute(m2l_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(psm)));
+      m2l_pair_kernel<<<(n_fb + kFmmWarps - 1) / kFmmWarps, 32 * kFmmWarps, psm, c->stream>>>(t, T, fallback, n_fb,
+                                                                                            tgt, gm.src, M, e0, out);
+      AMK_TRY(check_launch(c, "m2l_pair_kernel"));
+    }
+    // per-target sums on the side stream, in chunk order
+    AMK_CUDA_TRY(cudaEventRecord(f->products_done[buf], c->stream));
+    AMK_CUDA_TRY(cudaStreamWaitEvent(f->side, f->products_done[buf], 0));
+    AMK_TRY(m2l_reduce(c, f->side, t, T, gm.off, gm.count, tr[0], tr[1] - tr[0] + 1, e0, e1, out, L));
+    AMK_CUDA_TRY(cudaEventRecord(f->sums_done[buf], f->side));
+  }
+  // the context stream resumes after the last sums
+  AMK_CUDA_TRY(cudaStreamWaitEvent(c->stream, f->sums_done[(chunk - 1) & 1], 0));
+  return AMK_OK;
 }
 
 // ------------------------------------------------------------ L2L
@@ -760,11 +1266,6 @@ int grow_keep(amk_ctx* c, DevBuf& b, size_t used_bytes, size_t want_bytes) {
   return AMK_OK;
 }
 
-struct Grouped {
-  int* off = nullptr;
-  int* count = nullptr;
-  int* src = nullptr;
-};
 
 int group_pairs(amk_ctx* c, const int2* pairs, long n_pairs, long n_nodes, int slot_off, int slot_cnt, int slot_src,
                 int slot_cursor, Grouped* g) {
@@ -919,47 +1420,7 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
   // ---- M2L
   AMK_CUDA_TRY(cudaMemsetAsync(Lx, 0, static_cast<size_t>(nn) * T.n_m * sizeof(double), c->stream));
   AMK_TRY(phase_begin(c, AMK_PHASE_FMM_M2L));
-  int* class_of = nullptr;
-  double* table = nullptr;
-  if (n_m2l > 0) {  // derivative tensors of the lattice offsets in use
-    int* used = slot<int>(c, kSlotFmmWork1, kM2LCodes + 1, &rc);
-    AMK_TRY(rc);
-    class_of = slot<int>(c, kSlotFmmAux2, kM2LCodes + 1, &rc);
-    AMK_TRY(rc);
-    int* n_cls_dev = slot<int>(c, kSlotSortFlags, 8, &rc);
-    AMK_TRY(rc);
-    AMK_CUDA_TRY(cudaMemsetAsync(used, 0, (kM2LCodes + 1) * sizeof(int), c->stream));
-    m2l_mark_kernel<<<static_cast<unsigned>((n_m2l + 255) / 256), 256, 0, c->stream>>>(t, lists.m2l.as<int2>(),
-                                                                                      n_m2l, used);
-    AMK_TRY(check_launch(c, "m2l_mark_kernel"));
-    AMK_TRY(exclusive_scan_int(c, used, kM2LCodes, class_of, n_cls_dev));
-    int n_cls = 0;
-    AMK_CUDA_TRY(cudaMemcpyAsync(&n_cls, n_cls_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    int* codes = slot<int>(c, kSlotFmmWork3, static_cast<size_t>(n_cls) + 1, &rc);
-    AMK_TRY(rc);
-    table = slot<double>(c, kSlotFmmWork5, static_cast<size_t>(n_cls) * T.n_d + 1, &rc);
-    AMK_TRY(rc);
-    m2l_list_kernel<<<(kM2LCodes + 255) / 256, 256, 0, c->stream>>>(used, class_of, codes);
-    AMK_TRY(check_launch(c, "m2l_list_kernel"));
-    // class_of[code] = class index for used codes, -1 otherwise
-    m2l_class_map_kernel<<<(kM2LCodes + 255) / 256, 256, 0, c->stream>>>(used, class_of);
-    AMK_TRY(check_launch(c, "m2l_class_map_kernel"));
-    if (n_cls > 0) {
-      const size_t tsm = static_cast<size_t>(kFmmWarps) * T.n_d * sizeof(double);
-      AMK_CUDA_TRY(cudaFuncSetAttribute(m2l_table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(tsm)));
-      m2l_table_kernel<<<(n_cls + kFmmWarps - 1) / kFmmWarps, 32 * kFmmWarps, tsm, c->stream>>>(T, codes, n_cls,
-                                                                                              table);
-      AMK_TRY(check_launch(c, "m2l_table_kernel"));
-    }
-  }
-  const size_t m2l_smem = m2l_smem_bytes(T);
-  AMK_CUDA_TRY(cudaFuncSetAttribute(fmm_m2l_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    static_cast<int>(m2l_smem)));
-  fmm_m2l_kernel<<<gw, 32 * kFmmWarps, m2l_smem, c->stream>>>(t, T, gm.off, gm.count, gm.src, M, Lx, class_of,
-                                                              table);
-  AMK_TRY(check_launch(c, "fmm_m2l_kernel"));
+  if (n_m2l > 0) AMK_TRY(m2l_products(c, order, t, T, gm, n_m2l, M, Lx));
   AMK_TRY(phase_end(c, AMK_PHASE_FMM_M2L));
 
   // ---- L2L

@@ -115,3 +115,30 @@ def test_fmm_above_a_million_particles_matches_reference(sim):
     (rx, ry, rz), _ = O.ref_fmm(x, y, z, q, 2, 0.5, 32)
     rel, _ = rel_errors(f, (rx, ry, rz))
     assert np.max(rel) < FMM_TOL
+
+
+@pytest.mark.parametrize("reach,chunk", [(1, None), (3, None), (None, 1000), (2, 777)])
+def test_fmm_per_pair_path_and_chunk_seams(sim, monkeypatch, reach, chunk):
+    # M2L pairs run as per-class products; a narrowed class reach sends the
+    # pairs beyond it through the per-pair recurrence path, and a small chunk
+    # size splits targets' pair lists across chunks
+    g = np.load(os.path.join(GOLD, "fmm_n2000.npz"))
+    if reach is not None:
+        monkeypatch.setenv("AMK_FMM_M2L_REACH", str(reach))
+    if chunk is not None:
+        monkeypatch.setenv("AMK_FMM_M2L_CHUNK_PAIRS", str(chunk))
+    for order in (2, 6):
+        f = sim.solve_fmm(g["x"], g["y"], g["z"], g["q"], order, 0.5)
+        rel, _ = rel_errors(f, g[f"f_p{order}_theta0.5"].T)
+        assert np.max(rel) < FMM_TOL, (order, np.max(rel))
+
+
+@pytest.mark.parametrize("order", [7, 8])
+def test_fmm_high_orders_match_reference(sim, order):
+    if not O.ref_available():
+        pytest.skip("reference library not built")
+    x, y, z, q = gaussian_cloud(3000, 43)
+    f = sim.solve_fmm(x, y, z, q, order, 0.5)
+    (rx, ry, rz), _ = O.ref_fmm(x, y, z, q, order, 0.5, 32)
+    rel, _ = rel_errors(f, (rx, ry, rz))
+    assert np.max(rel) < FMM_TOL, np.max(rel)
