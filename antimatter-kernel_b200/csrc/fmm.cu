@@ -432,7 +432,7 @@ struct Grouped {
 constexpr int kM2lTileP = 64;      // pairs per product tile
 constexpr int kM2lUnitTiles = 8;   // tiles of one class per block
 constexpr int kM2lUnitPairs = kM2lUnitTiles * kM2lTileP;
-constexpr int kM2lMinClass = 8;    // smaller classes take the per-pair path
+constexpr int kM2lMinClass = 4;    // classes below this size take the per-pair path
 constexpr size_t kM2lChunkBytes = size_t(4) << 30;  // per-pair products of one chunk
 constexpr int kM2lHashBits = 21;
 constexpr long kM2lHashSlots = 1L << kM2lHashBits;
@@ -524,8 +524,7 @@ __global__ void m2l_histogram_kernel(const int* __restrict__ codes, long e0, lon
     fallback[atomicAdd(n_fallback, 1)] = static_cast<int>(e);
 }
 
-// Classes of fewer than kM2lMinClass pairs go the per-pair path (a product
-// tile with a handful of pairs costs more than their recurrences).
+// Classes of fewer than kM2lMinClass pairs go the per-pair path.
 __global__ void m2l_code_flags_kernel(const int* __restrict__ hist, long n_codes, int* __restrict__ used,
                                       int* __restrict__ units) {
   const long code = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
@@ -610,49 +609,8 @@ m2l_table_kernel(FmmDevTables T, const int* __restrict__ cls_code, int n_classes
   for (int k = lane; k < T.n_d; k += 32) table[static_cast<size_t>(cls) * T.n_d + k] = D[k];
 }
 
-// Tile shape per order: kTy row groups x kRg rows cover the n_m local
-// coefficients (kTy * kRg >= n_m, kTy a multiple of 4 so a warp is 4 row
-// groups x 8 pair groups), each thread owns 8 pairs; the k dimension runs in
-// chunks of kKc, a divisor of n_m. Up to order 6 the whole class matrix stays
-// in shared memory; above, it is regenerated chunk by chunk.
-template <int P>
-struct M2lShape;
-#define AMK_M2L_SHAPE(P, TY, RG, KC)                                                   \
-  template <>                                                                          \
-  struct M2lShape<P> {                                                                 \
-    static constexpr int kNm = (P + 1) * (P + 2) * (P + 3) / 6;                        \
-    static constexpr int kNd = (2 * P + 1) * (2 * P + 2) * (2 * P + 3) / 6;            \
-    static constexpr int kTy = TY, kRg = RG, kKc = KC, kNg = TY * RG;                   \
-    static constexpr int kThreads = 8 * TY;                                            \
-    static constexpr bool kFullA = P <= 6;                                             \
-    static_assert(kNg >= kNm && kNm % kKc == 0 && TY % 4 == 0, "M2L tile shape");      \
-  };
-AMK_M2L_SHAPE(1, 4, 1, 4)
-AMK_M2L_SHAPE(2, 4, 3, 10)
-AMK_M2L_SHAPE(3, 4, 5, 10)
-AMK_M2L_SHAPE(4, 12, 3, 7)
-AMK_M2L_SHAPE(5, 8, 7, 14)
-AMK_M2L_SHAPE(6, 12, 7, 12)
-AMK_M2L_SHAPE(7, 20, 6, 15)
-AMK_M2L_SHAPE(8, 24, 7, 15)
-#undef AMK_M2L_SHAPE
-constexpr int kM2lRp = 8;               // pairs per thread
 constexpr int kM2lBs = kM2lTileP + 2;   // B row stride (doubles): 16-byte rows, 2-way store conflicts
 constexpr int kM2lStages = 3;           // B pipeline depth (k chunks)
-
-template <int P>
-__host__ __device__ constexpr size_t m2l_a_doubles() {
-  using S = M2lShape<P>;
-  return S::kFullA ? static_cast<size_t>(S::kNm) * S::kNg : static_cast<size_t>(2) * S::kKc * S::kNg;
-}
-
-template <int P>
-size_t m2l_product_smem() {
-  using S = M2lShape<P>;
-  return sizeof(double) * (m2l_a_doubles<P>() + static_cast<size_t>(kM2lStages) * S::kKc * kM2lBs + S::kNd +
-                           S::kNg + S::kNm) +
-         2 * kM2lUnitPairs * sizeof(int);
-}
 
 __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
   const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
@@ -665,140 +623,197 @@ __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// One unit: up to 8 tiles of 64 pairs of one class. Thread (tx, ty) owns
-// rows g = ty + kTy i and pairs p = 16 (j / 2) + 2 tx + j % 2 of the current
-// tile (each 16-byte shared load of a B row is then conflict-free). A = the
-// class matrix with the source scaling folded in, from the class's D(v)
-// through the transposed index map; B = the sources' rescaled multipoles,
-// streamed k chunk by k chunk through a 3-stage cp.async pipeline that runs
-// on across the unit's tiles.
+// Tensor-core form of the class product: mma.m8n8k4 with FP64 operands
+// (256 FMAs per warp instruction, the same FP64 rate as FMA instructions but
+// an eighth of the issue slots). A block covers 8 * kGb >= n_m rows and 64
+// pairs; warp (wr, wc) owns kWr x kWc 8 x 8 output tiles. A fragments are
+// gathered from the class's D(v) through the transposed index map (both in
+// shared memory) and scaled by the source factor; B fragments come from the
+// cp.async pipeline ([k][pair] rows, k padded to a multiple of 4 with zeros,
+// so padded A entries only need to be finite).
 template <int P>
-__global__ void __launch_bounds__(M2lShape<P>::kThreads)
-m2l_class_product_kernel(FmmDevTables T, const int* __restrict__ unit_cls, const int* __restrict__ unit_pos,
-                         const int* __restrict__ cls_code, const int* __restrict__ cls_end,
-                         const int* __restrict__ perm, const int* __restrict__ src, const double* __restrict__ Mh,
-                         const double* __restrict__ table, const unsigned long long* __restrict__ keys, long e0,
-                         double* __restrict__ out) {
-  using S = M2lShape<P>;
-  constexpr int kNm = S::kNm, kKc = S::kKc, kNg = S::kNg, kTh = S::kThreads, kChunks = kNm / kKc;
-  extern __shared__ __align__(16) unsigned char prod_smem[];
-  double* As = reinterpret_cast<double*>(prod_smem);
-  double* Bs = As + m2l_a_doubles<P>();           // [kM2lStages][kKc][kM2lBs]
-  double* Ds = Bs + kM2lStages * kKc * kM2lBs;    // [kNd]
-  double* rowf = Ds + S::kNd;                     // [kNg]
-  double* colf = rowf + kNg;                      // [kNm]
-  int* pe = reinterpret_cast<int*>(colf + kNm);   // [kM2lUnitPairs]
-  int* ps = pe + kM2lUnitPairs;                   // [kM2lUnitPairs]
-  const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
-  const int cls = unit_cls[blockIdx.x], pos0 = unit_pos[blockIdx.x];
-  const int np = min(kM2lUnitPairs, cls_end[cls] - pos0);
-  const int n_tiles = (np + kM2lTileP - 1) / kM2lTileP, n_steps = n_tiles * kChunks;
-  const int dd = m2l_key_dd(keys[cls_code[cls]]);
-  const int et = dd < 0 ? -dd : 0, es = dd > 0 ? dd : 0;  // log2(h_t / u), log2(h_s / u)
-  for (int k = tid; k < S::kNd; k += kTh) Ds[k] = table[static_cast<size_t>(cls) * S::kNd + k];
-  for (int g = tid; g < kNg; g += kTh) rowf[g] = g < kNm ? ldexp(T.inv_fact[g], (T.multi[g].w + 1) * et) : 0.0;
-  for (int a = tid; a < kNm; a += kTh) colf[a] = ldexp(1.0, T.multi[a].w * es);
-  for (int p = tid; p < n_tiles * kM2lTileP; p += kTh) {
-    const int e = p < np ? perm[pos0 + p] : -1;
-    pe[p] = e;
-    ps[p] = e >= 0 ? src[e] : -1;
-  }
-  __syncthreads();
-  // rows [a0, a0 + n) of A (rows = source coefficients) into dst[(a - a0) * kNg + g]
-  auto fill_a = [&](double* dst, int a0, int n) {
-    for (int x = tid; x < n * kNg; x += kTh) {
-      const int r = x / kNg, g = x - r * kNg, a = a0 + r;
-      dst[x] = g < kNm ? Ds[T.m2l_index_t[a * kNm + g]] * colf[a] : 0.0;
-    }
+struct M2lMma;
+#define AMK_M2L_MMA(P, WR, WC, KC)                                                               \
+  template <>                                                                                    \
+  struct M2lMma<P> {                                                                             \
+    static constexpr int kNm = (P + 1) * (P + 2) * (P + 3) / 6;                                  \
+    static constexpr int kNd = (2 * P + 1) * (2 * P + 2) * (2 * P + 3) / 6;                      \
+    static constexpr int kGb = (kNm + 7) / 8, kNg = 8 * kGb, kNk = 4 * ((kNm + 3) / 4);           \
+    static constexpr int kWr = WR, kWc = WC, kKc = KC;                                           \
+    static constexpr int kWarpsR = kGb / WR, kWarps = kWarpsR * (8 / WC), kThreads = 32 * kWarps; \
+    static_assert(kGb % WR == 0 && 8 % WC == 0 && kNk % KC == 0 && KC % 4 == 0, "M2L mma shape"); \
   };
-  auto issue = [&](int step) {
-    if (step < n_steps) {
-      const int tile = step / kChunks, chunk = step - tile * kChunks;
-      double* B = Bs + (step % kM2lStages) * kKc * kM2lBs;
-      for (int x = tid; x < kKc * kM2lTileP; x += kTh) {
-        const int p = x / kKc, kk = x - p * kKc;
-        const int sp = ps[tile * kM2lTileP + p];
-        cp_async8(B + kk * kM2lBs + p, sp >= 0 ? Mh + static_cast<size_t>(sp) * kNm + chunk * kKc + kk : Mh, sp >= 0);
-      }
-    }
-    cp_async_commit();
-  };
-  for (int st = 0; st < kM2lStages - 1; ++st) issue(st);
-  if (S::kFullA) fill_a(As, 0, kNm);
-  double acc[S::kRg][kM2lRp];
-#pragma unroll
-  for (int i = 0; i < S::kRg; ++i)
-#pragma unroll
-    for (int j = 0; j < kM2lRp; ++j) acc[i][j] = 0.0;
-#pragma unroll 1
-  for (int step = 0; step < n_steps; ++step) {
-    const int tile = step / kChunks, chunk = step - tile * kChunks;
-    const double* A;
-    if (S::kFullA) {
-      A = As + chunk * kKc * kNg;
-    } else {
-      double* Ab = As + (step & 1) * kKc * kNg;
-      fill_a(Ab, chunk * kKc, kKc);
-      A = Ab;
-    }
-    cp_async_wait<kM2lStages - 2>();
-    __syncthreads();
-    issue(step + kM2lStages - 1);
-    const double* B = Bs + (step % kM2lStages) * kKc * kM2lBs;
-#pragma unroll
-    for (int kk = 0; kk < kKc; ++kk) {
-      double b[kM2lRp], av[S::kRg];
-#pragma unroll
-      for (int q = 0; q < kM2lRp / 2; ++q) {
-        const double2 v = *reinterpret_cast<const double2*>(B + kk * kM2lBs + 16 * q + 2 * tx);
-        b[2 * q] = v.x;
-        b[2 * q + 1] = v.y;
-      }
-#pragma unroll
-      for (int i = 0; i < S::kRg; ++i) av[i] = A[kk * kNg + ty + S::kTy * i];
-#pragma unroll
-      for (int i = 0; i < S::kRg; ++i)
-#pragma unroll
-        for (int j = 0; j < kM2lRp; ++j) acc[i][j] = fma(av[i], b[j], acc[i][j]);
-    }
-    if (chunk == kChunks - 1) {
-#pragma unroll
-      for (int j = 0; j < kM2lRp; ++j) {
-        const int e = pe[tile * kM2lTileP + 16 * (j >> 1) + 2 * tx + (j & 1)];
-#pragma unroll
-        for (int i = 0; i < S::kRg; ++i) {
-          const int g = ty + S::kTy * i;
-          if (e >= 0 && g < kNm) out[static_cast<size_t>(e - e0) * kNm + g] = acc[i][j] * rowf[g];
-          acc[i][j] = 0.0;
-        }
-      }
-    }
-  }
-  cp_async_wait<0>();
+AMK_M2L_MMA(1, 1, 8, 4)
+AMK_M2L_MMA(2, 2, 4, 12)
+AMK_M2L_MMA(3, 3, 4, 20)
+AMK_M2L_MMA(4, 5, 4, 12)
+AMK_M2L_MMA(5, 7, 4, 8)
+AMK_M2L_MMA(6, 11, 2, 12)
+AMK_M2L_MMA(7, 5, 4, 12)
+AMK_M2L_MMA(8, 7, 4, 12)
+#undef AMK_M2L_MMA
+
+template <int P>
+size_t m2l_mma_smem() {
+  using S = M2lMma<P>;
+  return sizeof(double) * (static_cast<size_t>(kM2lStages) * S::kKc * kM2lBs + S::kNd + S::kNg + S::kNk) +
+         sizeof(short) * static_cast<size_t>(S::kNk) * S::kNg + 2 * kM2lUnitPairs * sizeof(int) + 16;
 }
 
-// Pairs outside the classes: a warp per pair, the derivative tensor by the
-// recurrence, the product written in the rescaled form Lh = h_t^{|g|+1} L.
+__device__ __forceinline__ void mma_f64(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// Persistent blocks: the index map is built once per block, then units are
+// taken from a counter; within a tile, warps skip the 8-pair column blocks
+// past the tile's last pair, so a class of a few pairs costs a fraction of a
+// tile.
+template <int P>
+__global__ void __launch_bounds__(M2lMma<P>::kThreads)
+m2l_class_mma_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter,
+                     const int* __restrict__ unit_cls, const int* __restrict__ unit_pos,
+                     const int* __restrict__ cls_code, const int* __restrict__ cls_end,
+                     const int* __restrict__ perm, const int* __restrict__ src, const double* __restrict__ Mh,
+                     const double* __restrict__ table, const unsigned long long* __restrict__ keys, long e0,
+                     double* __restrict__ out) {
+  using S = M2lMma<P>;
+  constexpr int kNm = S::kNm, kNg = S::kNg, kNk = S::kNk, kKc = S::kKc, kTh = S::kThreads;
+  constexpr int kChunks = kNk / kKc;
+  extern __shared__ __align__(16) unsigned char mma_smem[];
+  double* Bs = reinterpret_cast<double*>(mma_smem);  // [kM2lStages][kKc][kM2lBs]
+  double* Ds = Bs + kM2lStages * kKc * kM2lBs;        // [kNd]
+  double* rowf = Ds + S::kNd;                         // [kNg]
+  double* colf = rowf + kNg;                          // [kNk]
+  int* pe = reinterpret_cast<int*>(colf + kNk);       // [kM2lUnitPairs]
+  int* ps = pe + kM2lUnitPairs;                       // [kM2lUnitPairs]
+  short* idx = reinterpret_cast<short*>(ps + kM2lUnitPairs);  // [kNk][kNg]
+  __shared__ int s_unit;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wr = warp % S::kWarpsR, wc = warp / S::kWarpsR;
+  const int lr = lane >> 2, lc = lane & 3;  // fragment row / column within a tile
+  const int g_base = 8 * S::kWr * wr + lr, p_base = 8 * S::kWc * wc + lr;
+  for (int x = tid; x < kNk * kNg; x += kTh) {
+    const int a = x / kNg, g = x - a * kNg;
+    idx[x] = (a < kNm && g < kNm) ? T.m2l_index_t[a * kNm + g] : 0;
+  }
+  for (;;) {
+    if (tid == 0) s_unit = atomicAdd(unit_counter, 1);
+    __syncthreads();  // also: the previous unit is done with the shared arrays
+    const int unit = s_unit;
+    if (unit >= n_units) break;
+    const int cls = unit_cls[unit], pos0 = unit_pos[unit];
+    const int np = min(kM2lUnitPairs, cls_end[cls] - pos0);
+    const int n_tiles = (np + kM2lTileP - 1) / kM2lTileP, n_steps = n_tiles * kChunks;
+    const int dd = m2l_key_dd(keys[cls_code[cls]]);
+    const int et = dd < 0 ? -dd : 0, es = dd > 0 ? dd : 0;  // log2(h_t / u), log2(h_s / u)
+    for (int k = tid; k < S::kNd; k += kTh) Ds[k] = table[static_cast<size_t>(cls) * S::kNd + k];
+    for (int g = tid; g < kNg; g += kTh) rowf[g] = g < kNm ? ldexp(T.inv_fact[g], (T.multi[g].w + 1) * et) : 0.0;
+    for (int a = tid; a < kNk; a += kTh) colf[a] = a < kNm ? ldexp(1.0, T.multi[a].w * es) : 0.0;
+    for (int p = tid; p < n_tiles * kM2lTileP; p += kTh) {
+      const int e = p < np ? perm[pos0 + p] : -1;
+      pe[p] = e;
+      ps[p] = e >= 0 ? src[e] : -1;
+    }
+    __syncthreads();
+    auto issue = [&](int step) {
+      if (step < n_steps) {
+        const int tile = step / kChunks, chunk = step - tile * kChunks;
+        const int live = min(kM2lTileP, np - tile * kM2lTileP);
+        double* B = Bs + (step % kM2lStages) * kKc * kM2lBs;
+        for (int x = tid; x < kKc * kM2lTileP; x += kTh) {
+          const int p = x / kKc, kk = x - p * kKc, a = chunk * kKc + kk;
+          if (p >= ((live + 7) & ~7)) continue;  // column blocks no warp reads
+          const int sp = ps[tile * kM2lTileP + p];
+          const bool ok = sp >= 0 && a < kNm;
+          cp_async8(B + kk * kM2lBs + p, ok ? Mh + static_cast<size_t>(sp) * kNm + a : Mh, ok);
+        }
+      }
+      cp_async_commit();
+    };
+    for (int st = 0; st < kM2lStages - 1; ++st) issue(st);
+    double acc[S::kWr][S::kWc][2];
+#pragma unroll
+    for (int i = 0; i < S::kWr; ++i)
+#pragma unroll
+      for (int j = 0; j < S::kWc; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll 1
+    for (int step = 0; step < n_steps; ++step) {
+      const int tile = step / kChunks, chunk = step - tile * kChunks;
+      const int live = min(kM2lTileP, np - tile * kM2lTileP);  // pairs in this tile
+      const int jn = min(S::kWc, max(0, (live - 8 * S::kWc * wc + 7) / 8));  // this warp's live column blocks
+      cp_async_wait<kM2lStages - 2>();
+      __syncthreads();
+      issue(step + kM2lStages - 1);
+      if (jn > 0) {
+        const double* B = Bs + (step % kM2lStages) * kKc * kM2lBs;
+#pragma unroll
+        for (int ks = 0; ks < kKc / 4; ++ks) {
+          const int a = chunk * kKc + 4 * ks + lc;
+          const double cf = colf[a];
+          const short* irow = idx + a * kNg + g_base;
+          double af[S::kWr], bf[S::kWc];
+#pragma unroll
+          for (int i = 0; i < S::kWr; ++i) af[i] = Ds[irow[8 * i]] * cf;
+#pragma unroll
+          for (int j = 0; j < S::kWc; ++j)
+            if (j < jn) bf[j] = B[(4 * ks + lc) * kM2lBs + p_base + 8 * j];
+#pragma unroll
+          for (int j = 0; j < S::kWc; ++j)
+            if (j < jn)
+#pragma unroll
+              for (int i = 0; i < S::kWr; ++i) mma_f64(acc[i][j], af[i], bf[j]);
+        }
+      }
+      if (chunk == kChunks - 1) {
+#pragma unroll
+        for (int j = 0; j < S::kWc; ++j)
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const int e = pe[tile * kM2lTileP + 8 * S::kWc * wc + 8 * j + 2 * lc + h];
+#pragma unroll
+            for (int i = 0; i < S::kWr; ++i) {
+              const int g = 8 * S::kWr * wr + 8 * i + lr;
+              if (e >= 0 && g < kNm) out[static_cast<size_t>(e - e0) * kNm + g] = acc[i][j][h] * rowf[g];
+              acc[i][j][h] = 0.0;
+            }
+          }
+      }
+    }
+    cp_async_wait<0>();
+  }
+}
+
+// Pairs outside the classes: a warp per pair (persistent blocks), the
+// derivative tensor by the recurrence, the product through the transposed
+// index map staged once per block, written in the rescaled form
+// Lh = h_t^{|g|+1} L.
 __global__ void __launch_bounds__(32 * kFmmWarps)
 m2l_pair_kernel(const Octree t, FmmDevTables T, const int* __restrict__ list, int n, const int* __restrict__ tgt,
                 const int* __restrict__ src, const double* __restrict__ M, long e0, double* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char pair_smem[];
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  double* D = reinterpret_cast<double*>(pair_smem) + static_cast<size_t>(w) * (T.n_d + T.n_m);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nm = T.n_m;
+  double* D = reinterpret_cast<double*>(pair_smem) + static_cast<size_t>(w) * (T.n_d + nm);
   double* Ms = D + T.n_d;
-  const int k = blockIdx.x * kFmmWarps + w;
-  if (k >= n) return;
-  const int e = list[k], ti = tgt[e], si = src[e];
-  const double4 tc = t.center[ti], sc = t.center[si];
-  for (int a = lane; a < T.n_m; a += 32) Ms[a] = T.sign[a] * M[static_cast<size_t>(si) * T.n_m + a];
-  const double xs[3] = {tc.x - sc.x, tc.y - sc.y, tc.z - sc.z};
-  m2l_derivatives(T, lane, xs, D);
-  for (int g = lane; g < T.n_m; g += 32) {
-    double s = 0.0;
-    for (int a = 0; a < T.n_m; ++a) s += Ms[a] * D[T.m2l_index[g * T.n_m + a]];
-    double f = T.inv_fact[g];
-    for (int d = 0; d <= T.multi[g].w; ++d) f *= tc.w;
-    out[static_cast<size_t>(e - e0) * T.n_m + g] = s * f;
+  short* idx = reinterpret_cast<short*>(reinterpret_cast<double*>(pair_smem) +
+                                        static_cast<size_t>(kFmmWarps) * (T.n_d + nm));  // [a][g]
+  for (int x = threadIdx.x; x < nm * nm; x += blockDim.x) idx[x] = T.m2l_index_t[x];
+  __syncthreads();
+  for (int k = blockIdx.x * kFmmWarps + w; k < n; k += gridDim.x * kFmmWarps) {
+    const int e = list[k], ti = tgt[e], si = src[e];
+    const double4 tc = t.center[ti], sc = t.center[si];
+    for (int a = lane; a < nm; a += 32) Ms[a] = T.sign[a] * M[static_cast<size_t>(si) * nm + a];
+    const double xs[3] = {tc.x - sc.x, tc.y - sc.y, tc.z - sc.z};
+    m2l_derivatives(T, lane, xs, D);  // ends with __syncwarp
+    for (int g = lane; g < nm; g += 32) {
+      double s = 0.0;
+      for (int a = 0; a < nm; ++a) s += Ms[a] * D[idx[a * nm + g]];
+      double f = T.inv_fact[g];
+      for (int d = 0; d <= T.multi[g].w; ++d) f *= tc.w;
+      out[static_cast<size_t>(e - e0) * nm + g] = s * f;
+    }
+    __syncwarp();
   }
 }
 
@@ -878,23 +893,30 @@ int m2l_reduce(amk_ctx* c, cudaStream_t stream, const Octree& t, const FmmDevTab
 }
 
 template <int P>
-int launch_class_product(amk_ctx* c, const FmmDevTables& T, int n_units, const int* unit_cls, const int* unit_pos,
+int launch_class_product(amk_ctx* c, const FmmDevTables& T, int n_units, int* unit_counter, const int* unit_cls, const int* unit_pos,
                          const int* cls_code, const int* cls_end, const int* perm, const int* src, const double* Mh,
                          const double* table, const unsigned long long* keys, long e0, double* out) {
-  const size_t smem = m2l_product_smem<P>();
-  AMK_CUDA_TRY(cudaFuncSetAttribute(m2l_class_product_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  const size_t smem = m2l_mma_smem<P>();
+  AMK_CUDA_TRY(cudaFuncSetAttribute(m2l_class_mma_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
-  m2l_class_product_kernel<P><<<n_units, M2lShape<P>::kThreads, smem, c->stream>>>(
-      T, unit_cls, unit_pos, cls_code, cls_end, perm, src, Mh, table, keys, e0, out);
-  return check_launch(c, "m2l_class_product_kernel");
+  int per_sm = 0;
+  AMK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m2l_class_mma_kernel<P>, M2lMma<P>::kThreads,
+                                                             smem));
+  int sms = 0;
+  AMK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+  const int grid = std::max(1, std::min(n_units, std::max(1, per_sm) * sms));
+  AMK_CUDA_TRY(cudaMemsetAsync(unit_counter, 0, sizeof(int), c->stream));
+  m2l_class_mma_kernel<P><<<grid, M2lMma<P>::kThreads, smem, c->stream>>>(
+      T, n_units, unit_counter, unit_cls, unit_pos, cls_code, cls_end, perm, src, Mh, table, keys, e0, out);
+  return check_launch(c, "m2l_class_mma_kernel");
 }
 
-int class_product(amk_ctx* c, int order, const FmmDevTables& T, int n_units, const int* unit_cls,
+int class_product(amk_ctx* c, int order, const FmmDevTables& T, int n_units, int* unit_counter, const int* unit_cls,
                   const int* unit_pos, const int* cls_code, const int* cls_end, const int* perm, const int* src,
                   const double* Mh, const double* table, const unsigned long long* keys, long e0, double* out) {
 #define AMK_M2L_CASE(P)                                                                                         \
   case P:                                                                                                     \
-    return launch_class_product<P>(c, T, n_units, unit_cls, unit_pos, cls_code, cls_end, perm, src, Mh, table, \
+    return launch_class_product<P>(c, T, n_units, unit_counter, unit_cls, unit_pos, cls_code, cls_end, perm, src, Mh, table, \
                                    keys, e0, out);
   switch (order) {
     AMK_M2L_CASE(1)
@@ -1021,15 +1043,19 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
       m2l_table_kernel<<<(n_cls + kFmmWarps - 1) / kFmmWarps, 32 * kFmmWarps, tsm, c->stream>>>(T, cls_code, n_cls,
                                                                                               keys, table);
       AMK_TRY(check_launch(c, "m2l_table_kernel"));
-      AMK_TRY(class_product(c, order, T, n_units, unit_cls, unit_pos, cls_code, cls_end, perm, gm.src, Mh, table,
+      AMK_TRY(class_product(c, order, T, n_units, counters + 4, unit_cls, unit_pos, cls_code, cls_end, perm, gm.src, Mh, table,
                             keys, e0, out));
     }
     if (n_fb > 0) {
-      const size_t psm = static_cast<size_t>(kFmmWarps) * (T.n_d + T.n_m) * sizeof(double);
+      const size_t psm = static_cast<size_t>(kFmmWarps) * (T.n_d + T.n_m) * sizeof(double) +
+                         static_cast<size_t>(T.n_m) * T.n_m * sizeof(short);
       AMK_CUDA_TRY(cudaFuncSetAttribute(m2l_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(psm)));
-      m2l_pair_kernel<<<(n_fb + kFmmWarps - 1) / kFmmWarps, 32 * kFmmWarps, psm, c->stream>>>(t, T, fallback, n_fb,
-                                                                                            tgt, gm.src, M, e0, out);
+      int per_sm = 0, sms = 0;
+      AMK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m2l_pair_kernel, 32 * kFmmWarps, psm));
+      AMK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+      const int grid = std::max(1, std::min((n_fb + kFmmWarps - 1) / kFmmWarps, std::max(1, per_sm) * sms));
+      m2l_pair_kernel<<<grid, 32 * kFmmWarps, psm, c->stream>>>(t, T, fallback, n_fb, tgt, gm.src, M, e0, out);
       AMK_TRY(check_launch(c, "m2l_pair_kernel"));
     }
     // per-target sums on the side stream, in chunk order
