@@ -37,7 +37,7 @@ SPECIES = {"antiproton": 0, "positron": 1, "antihydrogen": 2, "electron": 3,
            "proton": 4, "antihelium": 5}
 
 PHASES = ["stage", "allpairs", "cutoff", "sort", "tree", "bh_walk", "fmm_up", "fmm_lists",
-          "fmm_m2l", "fmm_down", "fmm_p2p", "mlp", "push", "annihilation", "energy"]
+          "fmm_m2l", "fmm_down", "fmm_p2p", "mlp", "push", "annihilation", "energy", "fmm_m2l_products"]
 
 
 class AmkError(RuntimeError):
@@ -116,6 +116,7 @@ def lib():
         "amk_set_charge_mass": (C.c_int, [vp, _dp, _dp]),
         "amk_update_state": (C.c_int, [vp, vp, vp, vp, vp, vp, vp]),
         "amk_measure_fp32_peak": (C.c_int, [vp, _dp, _dp]),
+        "amk_measure_fp64_peak": (C.c_int, [vp, _dp, _dp]),
         "amk_init_particles": (C.c_int, [vp]),
         "amk_get_particles": (C.c_int, [vp, _dp, _dp, _dp, _dp, _dp, _dp, _u8p]),
         "amk_get_particles_device": (C.c_int, [vp, vp, vp, vp, vp, vp, vp, vp]),
@@ -320,6 +321,12 @@ class Simulation:
         check(lib().amk_measure_fp32_peak(self._h, C.byref(t), C.byref(ms)), "amk_measure_fp32_peak")
         return t.value
 
+    def measure_fp64_peak(self):
+        """FP64 tensor-pipe throughput in TFLOP/s (probe kernel)."""
+        t, ms = C.c_double(), C.c_double()
+        check(lib().amk_measure_fp64_peak(self._h, C.byref(t), C.byref(ms)), "amk_measure_fp64_peak")
+        return t.value
+
     def set_charge_mass(self, charge=None, mass=None):
         q = None if charge is None else _f64(charge)
         m = None if mass is None else _f64(mass)
@@ -437,10 +444,10 @@ class Simulation:
         return (fx, fy, fz, phi) if want_phi else (fx, fy, fz)
 
     def fmm_stats(self):
-        out = (C.c_long * 8)()
-        check(lib().amk_fmm_stats(self._h, out, 8))
+        out = (C.c_long * 11)()
+        check(lib().amk_fmm_stats(self._h, out, 11))
         keys = ("cells", "leaves", "m2l_pairs", "p2p_leaf_pairs", "p2p_particle_pairs", "depth",
-                "sources", "order")
+                "sources", "order", "m2l_class_pairs", "m2l_classes", "m2l_chunks")
         return dict(zip(keys, list(out)))
 
     # -- learned FMM correction

@@ -1,6 +1,7 @@
-// FP32 FMA-pipe peak probe: the roofline denominator for the FP32-bound
-// pair kernels (no driver-measured FP32 figure exists). Every thread runs
-// eight independent FFMA chains; the grid fills every SM.
+// Peak probes: the FP32 FMA pipe (roofline denominator of the FP32-bound
+// pair kernels) and the FP64 tensor pipe (the FMM's M2L class products); no
+// driver-measured figure exists for either. Every thread runs independent
+// chains; the grid fills every SM.
 #include "amk_internal.cuh"
 
 namespace amk {
@@ -21,34 +22,77 @@ __global__ void __launch_bounds__(256) ffma_probe_kernel(int iters, float seed, 
   if (s == 12345.678f) out[0] = s;  // keeps the chains live
 }
 
+__global__ void __launch_bounds__(256) dmma_probe_kernel(int iters, double seed, double* out) {
+  const double a = seed + 1e-3 * threadIdx.x, b = 0.5;
+  double d[8][2];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) d[i][0] = d[i][1] = 0.0;
+  for (int k = 0; k < iters; ++k) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+      asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                   : "+d"(d[i][0]), "+d"(d[i][1])
+                   : "d"(a), "d"(b));
+  }
+  double s = 0.0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) s += d[i][0] + d[i][1];
+  if (s == 12345.678) out[0] = s;  // keeps the chains live
+}
+
+int time_probe(amk_ctx* c, bool fp64, int iters, float* ms) {
+  int sms = 0;
+  AMK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+  int rc = AMK_OK;
+  double* out = slot<double>(c, kSlotStatus, 8, &rc);
+  AMK_TRY(rc);
+  const int blocks = sms * 8, threads = 256;
+  cudaEvent_t a, b;
+  AMK_CUDA_TRY(cudaEventCreate(&a));
+  AMK_CUDA_TRY(cudaEventCreate(&b));
+  for (int rep = 0; rep < 2; ++rep) {  // warm-up, then timed
+    if (rep == 1) AMK_CUDA_TRY(cudaEventRecord(a, c->stream));
+    if (fp64)
+      dmma_probe_kernel<<<blocks, threads, 0, c->stream>>>(rep ? iters : iters / 8, 1.0, out);
+    else
+      ffma_probe_kernel<<<blocks, threads, 0, c->stream>>>(rep ? iters : iters / 8, 1.f,
+                                                           reinterpret_cast<float*>(out));
+    AMK_TRY(check_launch(c, fp64 ? "dmma_probe_kernel" : "ffma_probe_kernel"));
+  }
+  AMK_CUDA_TRY(cudaEventRecord(b, c->stream));
+  AMK_CUDA_TRY(cudaEventSynchronize(b));
+  AMK_CUDA_TRY(cudaEventElapsedTime(ms, a, b));
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return AMK_OK;
+}
+
 }  // namespace
 }  // namespace amk
 
 using namespace amk;
 
+extern "C" int amk_measure_fp64_peak(amk_ctx* c, double* tflops, double* ms_out) {
+  if (!c || !tflops) return fail(AMK_ERR_INVALID, "null argument");
+  int sms = 0;
+  AMK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+  const int iters = 2048;
+  float ms = 0.f;
+  AMK_TRY(time_probe(c, true, iters, &ms));
+  const double flops = 512.0 * 8.0 * iters * (sms * 8.0) * (256 / 32);
+  *tflops = flops / (ms * 1e-3) / 1e12;
+  if (ms_out) *ms_out = ms;
+  return AMK_OK;
+}
+
 extern "C" int amk_measure_fp32_peak(amk_ctx* c, double* tflops, double* ms_out) {
   if (!c || !tflops) return fail(AMK_ERR_INVALID, "null argument");
   int sms = 0;
   AMK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-  int rc = AMK_OK;
-  float* out = slot<float>(c, kSlotStatus, 8, &rc);
-  AMK_TRY(rc);
-  const int blocks = sms * 8, threads = 256, iters = 4096;
-  cudaEvent_t a, b;
-  AMK_CUDA_TRY(cudaEventCreate(&a));
-  AMK_CUDA_TRY(cudaEventCreate(&b));
-  ffma_probe_kernel<<<blocks, threads, 0, c->stream>>>(iters / 8, 1.f, out);  // warm-up
-  AMK_TRY(check_launch(c, "ffma_probe_kernel"));
-  AMK_CUDA_TRY(cudaEventRecord(a, c->stream));
-  ffma_probe_kernel<<<blocks, threads, 0, c->stream>>>(iters, 1.f, out);
-  AMK_TRY(check_launch(c, "ffma_probe_kernel"));
-  AMK_CUDA_TRY(cudaEventRecord(b, c->stream));
-  AMK_CUDA_TRY(cudaEventSynchronize(b));
+  const int iters = 4096;
   float ms = 0.f;
-  AMK_CUDA_TRY(cudaEventElapsedTime(&ms, a, b));
-  cudaEventDestroy(a);
-  cudaEventDestroy(b);
-  const double flops = 2.0 * 8.0 * 16.0 * static_cast<double>(iters) * blocks * threads;
+  AMK_TRY(time_probe(c, false, iters, &ms));
+  const double flops = 2.0 * 8.0 * 16.0 * static_cast<double>(iters) * (sms * 8.0) * 256;
   *tflops = flops / (ms * 1e-3) / 1e12;
   if (ms_out) *ms_out = ms;
   return AMK_OK;

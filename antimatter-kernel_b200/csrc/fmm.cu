@@ -27,6 +27,7 @@
 #include <array>
 #include <map>
 #include <memory>
+#include <type_traits>
 #include <vector>
 
 #include "amk_internal.cuh"
@@ -171,7 +172,7 @@ struct Fmm {
   cudaStream_t side = nullptr;
   cudaEvent_t products_done[2] = {nullptr, nullptr}, sums_done[2] = {nullptr, nullptr};
   // statistics of the last evaluation (amk_fmm_stats)
-  long stats[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  long stats[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   ~Fmm() {
     for (auto& kv : tables) delete kv.second.first;
     for (int i = 0; i < 2; ++i) {
@@ -649,8 +650,8 @@ AMK_M2L_MMA(3, 3, 4, 20)
 AMK_M2L_MMA(4, 5, 4, 12)
 AMK_M2L_MMA(5, 7, 4, 8)
 AMK_M2L_MMA(6, 11, 2, 12)
-AMK_M2L_MMA(7, 5, 4, 12)
-AMK_M2L_MMA(8, 7, 4, 12)
+AMK_M2L_MMA(7, 5, 4, 24)
+AMK_M2L_MMA(8, 7, 4, 24)
 #undef AMK_M2L_MMA
 
 template <int P>
@@ -746,16 +747,22 @@ m2l_class_mma_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter
       cp_async_wait<kM2lStages - 2>();
       __syncthreads();
       issue(step + kM2lStages - 1);
-      if (jn > 0) {
+      // k chunk: A fragments from D(v) (scaled by the source factor when the
+      // source is the larger cell), B fragments from the staged rows
+      auto chunk_products = [&](auto scaled) {
         const double* B = Bs + (step % kM2lStages) * kKc * kM2lBs;
 #pragma unroll
         for (int ks = 0; ks < kKc / 4; ++ks) {
           const int a = chunk * kKc + 4 * ks + lc;
-          const double cf = colf[a];
           const short* irow = idx + a * kNg + g_base;
           double af[S::kWr], bf[S::kWc];
 #pragma unroll
-          for (int i = 0; i < S::kWr; ++i) af[i] = Ds[irow[8 * i]] * cf;
+          for (int i = 0; i < S::kWr; ++i) af[i] = Ds[irow[8 * i]];
+          if (decltype(scaled)::value) {
+            const double cf = colf[a];
+#pragma unroll
+            for (int i = 0; i < S::kWr; ++i) af[i] *= cf;
+          }
 #pragma unroll
           for (int j = 0; j < S::kWc; ++j)
             if (j < jn) bf[j] = B[(4 * ks + lc) * kM2lBs + p_base + 8 * j];
@@ -765,6 +772,12 @@ m2l_class_mma_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter
 #pragma unroll
               for (int i = 0; i < S::kWr; ++i) mma_f64(acc[i][j], af[i], bf[j]);
         }
+      };
+      if (jn > 0) {
+        if (es > 0)
+          chunk_products(std::true_type());
+        else
+          chunk_products(std::false_type());
       }
       if (chunk == kChunks - 1) {
 #pragma unroll
@@ -1032,6 +1045,9 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
     AMK_CUDA_TRY(cudaMemcpyAsync(tr + 1, tgt + e1 - 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
     const int n_cls = h[1], n_units = h[2], n_fb = h[3];
+    f->stats[8] += ne - n_fb;
+    f->stats[9] += n_cls;
+    f->stats[10] += 1;
     // the sums of the chunk before the previous one still read this buffer
     if (chunk >= 2) AMK_CUDA_TRY(cudaStreamWaitEvent(c->stream, f->sums_done[buf], 0));
     if (n_cls > 0) {
@@ -1043,8 +1059,10 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
       m2l_table_kernel<<<(n_cls + kFmmWarps - 1) / kFmmWarps, 32 * kFmmWarps, tsm, c->stream>>>(T, cls_code, n_cls,
                                                                                               keys, table);
       AMK_TRY(check_launch(c, "m2l_table_kernel"));
-      AMK_TRY(class_product(c, order, T, n_units, counters + 4, unit_cls, unit_pos, cls_code, cls_end, perm, gm.src, Mh, table,
-                            keys, e0, out));
+      AMK_TRY(phase_begin(c, AMK_PHASE_FMM_M2L_PRODUCTS));
+      AMK_TRY(class_product(c, order, T, n_units, counters + 4, unit_cls, unit_pos, cls_code, cls_end, perm, gm.src,
+                            Mh, table, keys, e0, out));
+      AMK_TRY(phase_end(c, AMK_PHASE_FMM_M2L_PRODUCTS));
     }
     if (n_fb > 0) {
       const size_t psm = static_cast<size_t>(kFmmWarps) * (T.n_d + T.n_m) * sizeof(double) +
@@ -1428,6 +1446,7 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
     AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
     long* st = c->fmm->stats;
     st[0] = nn;
+    st[8] = st[9] = st[10] = 0;  // filled by the M2L products
     st[1] = static_cast<long>(h[1]);
     st[2] = n_m2l;
     st[3] = n_p2p;
@@ -1804,7 +1823,7 @@ int fmm_audit(amk_ctx* c, const View& v, int order, double theta, bool learned, 
 // [6] sources, [7] order.
 extern "C" int amk_fmm_stats(amk_ctx* c, long* out, int n) {
   if (!c || !out) return amk::fail(AMK_ERR_INVALID, "null argument");
-  for (int k = 0; k < n && k < 8; ++k) out[k] = c->fmm ? c->fmm->stats[k] : 0;
+  for (int k = 0; k < n && k < 11; ++k) out[k] = c->fmm ? c->fmm->stats[k] : 0;
   return AMK_OK;
 }
 

@@ -137,9 +137,24 @@ TREE_METHODS = [
     ("barnes-hut theta=0.7", dict(coulomb_method="barnes-hut", barnes_hut_theta=0.7)),
     ("fmm p=4 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=4, fast_multipole_theta=0.5)),
     ("fmm p=6 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=6, fast_multipole_theta=0.5)),
+    ("fmm p=7 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=7, fast_multipole_theta=0.5)),
+    ("fmm p=8 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=8, fast_multipole_theta=0.5)),
     ("learned p=2 + MLP theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=2,
                                         fast_multipole_theta=0.5, fmm_learned=1, learned_audit_interval=0)),
 ]
+
+
+# DRAM traffic (read + write) per launch of the FMM's M2L class-product kernel,
+# by order: from ncu captures of one launch (one chunk of at most 4 GiB of
+# per-pair products; launches at N = 1,048,576 process chunks of the same size).
+FMM_PRODUCT_TRAFFIC = {
+    7: (5.18e9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of m2l_class_mma_kernel<7>, mean of two launches "
+                "of 4.47 M pairs each (0.89 / 1.10 GB read + 4.18 GB written: the per-pair products), "
+                "profiles/m2l_class_mma_kernel_tree1m.md"),
+    8: (5.17e9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of m2l_class_mma_kernel<8>, mean of two launches "
+                "of 3.25 M pairs each (0.92 GB read + 4.26 GB written: the per-pair products), "
+                "profiles/m2l_class_mma_kernel_tree1m.md"),
+}
 
 
 # ------------------------------------------------------------------ clocks
@@ -523,7 +538,7 @@ def run_reference_tree(args):
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    pos, _, _ = tree_cloud()
+    pos, _, _ = tree_cloud(args.tree_n)
     n = len(pos)
     x, y, z = pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy()
     q = np.full(n, E)
@@ -585,12 +600,15 @@ def run_tree(args):
     world, rank, local = dist_setup()
     device = torch.device("cuda", local)
     torch.cuda.set_device(device)
-    pos, vel, sp = tree_cloud()
+    pos, vel, sp = tree_cloud(args.tree_n)
     n = len(pos)
     steps = max(1, min(args.steps, 5))
     results = {}
     best = None
-    for name, over in TREE_METHODS:
+    methods = [m for m in TREE_METHODS if not args.tree_methods or m[0] in args.tree_methods.split(",")]
+    if not methods:
+        raise SystemExit(f"--tree-methods: none of {[m[0] for m in TREE_METHODS]}")
+    for name, over in methods:
         kw = dict(seed=42, b0=1.0, trap_voltage=10.0, z0=0.01, rho0=0.01, num_steps=500,
                   populations={"positron": n}, temperatures={"positron": 5.0}, cloud_radii=(1e-4, 1e-4, 3e-4),
                   bath_temperature=0.0, cooling_scale=0.0, cooling_enabled=0, coulomb_forces_enabled=1,
@@ -629,7 +647,7 @@ def run_tree(args):
             best = name
         sim.close()
     # the winner again: roofline of its dominant kernel, e2e through the C ABI
-    name = best if best is not None else "allpairs"
+    name = best if best is not None else methods[0][0]
     over = dict(TREE_METHODS)[name]
     kw = dict(seed=42, b0=1.0, trap_voltage=10.0, populations={"positron": n}, cooling_enabled=0,
               energy_method="allpairs", annihilation_enabled=0)
@@ -670,6 +688,31 @@ def run_tree(args):
                     "peak_source": "measured in this run: FFMA probe kernel over all SMs (2 flop/FFMA)",
                     "flop_convention": "20 flop per pair interaction x N(N-1) pairs",
                     "avg_launch_ms": ap_ms / ap_n}
+    elif over["coulomb_method"] == "fast-multipole" and not over.get("fmm_learned"):
+        sim.set_profiling(True)
+        sim.reset_phase_times()
+        sim.step(1)
+        sim.synchronize()
+        ph = sim.phase_times()
+        sim.set_profiling(False)
+        prod_ms, prod_n = ph["fmm_m2l_products"]
+        st = sim.fmm_stats()
+        p_ = st["order"]
+        nm = (p_ + 1) * (p_ + 2) * (p_ + 3) // 6
+        peak = sim.measure_fp64_peak()
+        achieved = 2.0 * nm * nm * st["m2l_class_pairs"] / (prod_ms * 1e-3) / 1e12
+        traffic = FMM_PRODUCT_TRAFFIC.get(p_)
+        roofline = {"bound": "fp64 tensor", "kernel": f"m2l_class_mma_kernel<{p_}>", "achieved": achieved,
+                    "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                    "traffic": None if traffic is None else traffic[0],
+                    "traffic_source": None if traffic is None else traffic[1],
+                    "peak_source": "measured in this run: mma.m8n8k4 FP64 probe kernel over all SMs "
+                                   "(512 flop per warp instruction)",
+                    "flop_convention": f"2 n_m^2 flop (n_m = {nm}) per M2L pair evaluated as a class product "
+                                       f"({st['m2l_class_pairs']:,} of {st['m2l_pairs']:,} pairs; the rest take "
+                                       "the per-pair path)",
+                    "avg_launch_ms": prod_ms / max(1, prod_n), "launches_per_step": prod_n,
+                    "m2l_phase_ms": ph["fmm_m2l"][0], "classes": st["m2l_classes"]}
     host = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in ("x", "y", "z", "vx", "vy", "vz")}
     alive = torch.empty(n, dtype=torch.uint8, pin_memory=True)
     order = ("x", "y", "z", "vx", "vy", "vz")
@@ -704,7 +747,7 @@ def run_tree(args):
             "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "fp32" if over["coulomb_method"] == "allpairs" else "f64",
             "data": "synthetic (seeded Gaussian cloud)",
-            "config": {"workload": "tree solvers at N=1,048,576 positrons, Gaussian sigma 1e-4 x 1e-4 x 3e-4 m, "
+            "config": {"workload": f"tree solvers at N={n:,} positrons, Gaussian sigma 1e-4 x 1e-4 x 3e-4 m, "
                                    "5 K Maxwellian, b0=1 T, U=10 V; value = fastest method within 1e-5 RMS "
                                    "relative force error vs the FP64 exact sum (1,024 audited particles)",
                        "chosen": name, "methods": results,
@@ -886,6 +929,9 @@ def main():
                     help="steps of the one-at-a-time comparison (sweep workload)")
     ap.add_argument("--instances", type=int, default=512,
                     help="trap instances of the sweep workload (the first k of the 512-instance sweep)")
+    ap.add_argument("--tree-n", type=int, default=1 << 20, help="particles of the tree workload")
+    ap.add_argument("--tree-methods", default="",
+                    help="comma-separated subset of the tree workload's methods (default: all)")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)  # at least three untimed warm-up steps
     if args.impl == "reference":

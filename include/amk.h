@@ -276,7 +276,9 @@ long amk_bh_tree_dump(amk_ctx* ctx, long n, const double* x, const double* y, co
 /* Interaction counts of the context's last FMM evaluation: out[0] cells,
  * [1] leaves, [2] M2L pairs, [3] P2P leaf pairs, [4] P2P particle pairs,
  * [5] tree depth, [6] sources, [7] order (the quantities the reference's
- * phases scale with, fast-multipole.cc:484-661). */
+ * phases scale with, fast-multipole.cc:484-661); [8] M2L pairs evaluated as
+ * class products, [9] displacement classes (summed over pair chunks),
+ * [10] pair chunks. n <= 11. */
 int amk_fmm_stats(amk_ctx* ctx, long* out, int n);
 
 /* ------------------------------------------------------------ learned correction */
@@ -440,7 +442,8 @@ int amk_coulomb_standard_noalloc(const double* x, const double* y, const double*
 #define AMK_PHASE_PUSH 12
 #define AMK_PHASE_ANNIHILATION 13
 #define AMK_PHASE_ENERGY 14
-#define AMK_NUM_PHASES 15
+#define AMK_PHASE_FMM_M2L_PRODUCTS 15 /* the class-product kernels inside FMM_M2L */
+#define AMK_NUM_PHASES 16
 int amk_set_profiling(amk_ctx* ctx, int enabled);
 int amk_phase_times(amk_ctx* ctx, double* ms_out, long* launches_out, int n);
 int amk_reset_phase_times(amk_ctx* ctx);
@@ -450,6 +453,10 @@ long amk_kernel_launches(const amk_ctx* ctx);
  * FFMA), measured by a short probe kernel on the context stream: the
  * roofline denominator of the FP32-bound pair kernels. */
 int amk_measure_fp32_peak(amk_ctx* ctx, double* tflops, double* ms);
+/* FP64 tensor-pipe throughput (mma.m8n8k4 with FP64 operands, 512 flops
+ * per warp instruction) in TFLOP/s: the roofline denominator of the FMM's
+ * M2L class products. */
+int amk_measure_fp64_peak(amk_ctx* ctx, double* tflops, double* ms);
 
 #ifdef __cplusplus
 }
