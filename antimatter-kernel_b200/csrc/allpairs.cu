@@ -16,8 +16,10 @@
 //     |r_ij| (Sterbenz) -- 18 FP32 ops per pair; the self pair and exact
 //     duplicates give r = 0 exactly;
 //   * far pairs: each source carries its FP32 offset u_j from its sub-tile
-//     centre and each target forms a_i = x_i - c_sub once per sub-tile, so
-//     r_ij = a_i - u_j costs one FADD per component -- 12 FP32 ops per pair.
+//     centre (stored negated) and each target forms a_i = x_i - c_sub once
+//     per sub-tile, so r_ij = a_i + (-u_j) costs one FADD per component --
+//     12 FP32 ops per pair, issued as packed FP32x2 operations over a lane's
+//     two targets (one instruction per two pairs, two MUFU.RSQ);
 //     Its relative error is at most eps (1 + 1.5 / 0.25) = 7 eps of |r_ij|
 //     for the closest far pairs (gap >= 0.25 (|h_w| + |h_s|)) and ~eps for
 //     the bulk; about 5 % of the sub-tile pairs of a 65,536-particle cloud
@@ -153,9 +155,9 @@ ap_stage_kernel(View v, const uint32_t* __restrict__ perm, double inv_l, float4*
     l.x = __double2float_rn(xs - static_cast<double>(h.x));
     l.y = __double2float_rn(ys - static_cast<double>(h.y));
     l.z = __double2float_rn(zs - static_cast<double>(h.z));
-    u.x = __double2float_rn(xs - cx);
-    u.y = __double2float_rn(ys - cy);
-    u.z = __double2float_rn(zs - cz);
+    u.x = -__double2float_rn(xs - cx);  // negated: the far loop adds it
+    u.y = -__double2float_rn(ys - cy);
+    u.z = -__double2float_rn(zs - cz);
     u.w = h.w;
   }
   if (k < v.n) {
@@ -188,7 +190,7 @@ __device__ __forceinline__ long unit_start(long c, long units, long grid) { retu
 // Target block tb = sorted targets [512 tb, 512 tb + 512); warp w owns
 // [512 tb + 64 w, + 64): lane l holds targets +l (r = 0) and +32+l (r = 1).
 template <bool kPhi>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, 3)
 allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, const float4* __restrict__ rel,
                 const TileBox* __restrict__ boxes, int n, int n_tiles, int n_tb, int n_split,
                 int tiles_per_chunk, float eps2, float4* __restrict__ part) {
@@ -313,31 +315,43 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, co
             }
           }
         } else {
-          float ax[kR], ay[kR], az[kR];
-#pragma unroll
-          for (int r = 0; r < kR; ++r) {
-            ax[r] = (tx[r] - sbx.c.x) + (ux[r] - sbx.cl.x);
-            ay[r] = (ty[r] - sbx.c.y) + (uy[r] - sbx.cl.y);
-            az[r] = (tz[r] - sbx.c.z) + (uz[r] - sbx.cl.z);
-          }
+          // far: the warp's two targets per lane in the two halves of packed
+          // FP32x2 operations (same operations and association as the
+          // scalar form, half the issue slots)
+          static_assert(kR == 2, "packed far path holds two targets per lane");
+          float2 ax, ay, az;
+          ax.x = (tx[0] - sbx.c.x) + (ux[0] - sbx.cl.x);
+          ax.y = (tx[1] - sbx.c.x) + (ux[1] - sbx.cl.x);
+          ay.x = (ty[0] - sbx.c.y) + (uy[0] - sbx.cl.y);
+          ay.y = (ty[1] - sbx.c.y) + (uy[1] - sbx.cl.y);
+          az.x = (tz[0] - sbx.c.z) + (uz[0] - sbx.cl.z);
+          az.y = (tz[1] - sbx.c.z) + (uz[1] - sbx.cl.z);
+          const float2 e2 = make_float2(eps2, eps2);
+          float2 fx = make_float2(px[0], px[1]), fy = make_float2(py[0], py[1]),
+                 fz = make_float2(pz[0], pz[1]), fp = make_float2(pp[0], pp[1]);
 #pragma unroll 8
           for (int k = 0; k < kSub; ++k) {
-            const float4 s = sc[base + k];
-#pragma unroll
-            for (int r = 0; r < kR; ++r) {
-              const float dx = ax[r] - s.x;
-              const float dy = ay[r] - s.y;
-              const float dz = az[r] - s.z;
-              const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-              const float rinv = rsqrtf(d2);
-              const float qr = s.w * rinv;
-              const float w = qr * (rinv * rinv);
-              px[r] = fmaf(w, dx, px[r]);
-              py[r] = fmaf(w, dy, py[r]);
-              pz[r] = fmaf(w, dz, pz[r]);
-              if (kPhi) pp[r] += qr;
-            }
+            const float4 s = sc[base + k];  // -u_j, q_j
+            const float2 dx = __fadd2_rn(ax, make_float2(s.x, s.x));
+            const float2 dy = __fadd2_rn(ay, make_float2(s.y, s.y));
+            const float2 dz = __fadd2_rn(az, make_float2(s.z, s.z));
+            const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
+            const float2 rinv = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+            const float2 qr = __fmul2_rn(make_float2(s.w, s.w), rinv);
+            const float2 w = __fmul2_rn(qr, __fmul2_rn(rinv, rinv));
+            fx = __ffma2_rn(w, dx, fx);
+            fy = __ffma2_rn(w, dy, fy);
+            fz = __ffma2_rn(w, dz, fz);
+            if (kPhi) fp = __fadd2_rn(fp, qr);
           }
+          px[0] = fx.x;
+          px[1] = fx.y;
+          py[0] = fy.x;
+          py[1] = fy.y;
+          pz[0] = fz.x;
+          pz[1] = fz.y;
+          pp[0] = fp.x;
+          pp[1] = fp.y;
         }
       }
 #pragma unroll
