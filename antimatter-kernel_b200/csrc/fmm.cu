@@ -347,38 +347,67 @@ fmm_m2m_kernel(const Octree t, FmmDevTables T, int depth, double* __restrict__ M
 }
 
 // ------------------------------------------------------------ dual traversal
-// One level of the reference's stack recursion (fast-multipole.cc:484-526)
-// for every pending (target, source) pair.
+// One level of the dual-tree recursion (fast-multipole.cc:484-526): each
+// pair is accepted for M2L, kept for P2P, or split into its children. The
+// emissions of a warp are reserved with one atomic per list (ballot / warp
+// prefix sums); the order of the lists is irrelevant, they are sorted after.
 __global__ void fmm_traverse_kernel(const Octree t, const double* __restrict__ radius, double theta2,
                                     const int2* __restrict__ cur, int n_cur, int2* __restrict__ next,
                                     int2* __restrict__ m2l, int2* __restrict__ p2p, int* counters) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_cur) return;
-  const int2 pr = cur[i];
-  const int ti = pr.x, si = pr.y;
-  const double4 tc = t.center[ti], sc = t.center[si];
-  const double dx = tc.x - sc.x, dy = tc.y - sc.y, dz = tc.z - sc.z;
-  const double dist2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-  const double rt = radius[ti], rs = radius[si];
-  const double rsum = rt + rs;
-  if (__dmul_rn(rsum, rsum) < __dmul_rn(theta2, dist2)) {
-    m2l[atomicAdd(&counters[0], 1)] = pr;
-    return;
-  }
-  const bool tleaf = t.meta[ti].y, sleaf = t.meta[si].y;
-  if (tleaf && sleaf) {
-    p2p[atomicAdd(&counters[1], 1)] = pr;
-    return;
-  }
-  const bool split_target = sleaf || (!tleaf && rt >= rs);
-  const int node = split_target ? ti : si;
+  const int lane = threadIdx.x & 31;
+  const unsigned below = (1u << lane) - 1u;
+  int2 pr = make_int2(0, 0);
+  int kind = -1;  // 0 M2L, 1 P2P, 2 split
   int kids[8], nk = 0;
-  for (int o = 0; o < 8; ++o) {
-    const int ch = t.child[8 * node + o];
-    if (ch >= 0) kids[nk++] = ch;
+  bool split_target = false;
+  if (i < n_cur) {
+    pr = cur[i];
+    const int ti = pr.x, si = pr.y;
+    const double4 tc = t.center[ti], sc = t.center[si];
+    const double dx = tc.x - sc.x, dy = tc.y - sc.y, dz = tc.z - sc.z;
+    const double dist2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+    const double rt = radius[ti], rs = radius[si];
+    const double rsum = rt + rs;
+    if (__dmul_rn(rsum, rsum) < __dmul_rn(theta2, dist2)) {
+      kind = 0;
+    } else {
+      const bool tleaf = t.meta[ti].y, sleaf = t.meta[si].y;
+      if (tleaf && sleaf) {
+        kind = 1;
+      } else {
+        kind = 2;
+        split_target = sleaf || (!tleaf && rt >= rs);
+        const int node = split_target ? ti : si;
+        for (int o = 0; o < 8; ++o) {
+          const int ch = t.child[8 * node + o];
+          if (ch >= 0) kids[nk++] = ch;
+        }
+      }
+    }
   }
-  const int base = atomicAdd(&counters[2], nk);
-  for (int k = 0; k < nk; ++k) next[base + k] = split_target ? make_int2(kids[k], si) : make_int2(ti, kids[k]);
+  // M2L and P2P: one slot per lane
+  for (int list = 0; list < 2; ++list) {
+    const unsigned m = __ballot_sync(0xffffffffu, kind == list);
+    if (m == 0) continue;
+    int base = 0;
+    if (lane == __ffs(m) - 1) base = atomicAdd(&counters[list], __popc(m));
+    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+    if (kind == list) (list == 0 ? m2l : p2p)[base + __popc(m & below)] = pr;
+  }
+  // children: a warp prefix sum of the counts
+  int incl = nk;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  const int total = __shfl_sync(0xffffffffu, incl, 31);
+  if (total == 0) return;
+  int base = 0;
+  if (lane == 31) base = atomicAdd(&counters[2], total);
+  base = __shfl_sync(0xffffffffu, base, 31) + incl - nk;
+  for (int k = 0; k < nk; ++k) next[base + k] = split_target ? make_int2(kids[k], pr.y) : make_int2(pr.x, kids[k]);
 }
 
 // Group pairs by target: pack (target, source) into one key and radix-sort
@@ -393,13 +422,19 @@ __global__ void pair_pack_kernel(const int2* __restrict__ pairs, int n, int bits
   vals[i] = static_cast<uint32_t>(i);
 }
 
+// Sorted keys: a warp's lanes with the same target add their count once.
 __global__ void pair_unpack_kernel(const uint64_t* __restrict__ keys, int n, int bits, int* __restrict__ src,
                                    int* __restrict__ count) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const uint64_t k = keys[i];
-  src[i] = static_cast<int>(k & ((1ull << bits) - 1ull));
-  atomicAdd(&count[static_cast<int>(k >> bits)], 1);
+  const int lane = threadIdx.x & 31;
+  int target = -1;
+  if (i < n) {
+    const uint64_t k = keys[i];
+    src[i] = static_cast<int>(k & ((1ull << bits) - 1ull));
+    target = static_cast<int>(k >> bits);
+  }
+  const unsigned same = __match_any_sync(0xffffffffu, target);
+  if (target >= 0 && lane == __ffs(same) - 1) atomicAdd(&count[target], __popc(same));
 }
 
 struct Grouped {
