@@ -190,7 +190,7 @@ __device__ __forceinline__ long unit_start(long c, long units, long grid) { retu
 // Target block tb = sorted targets [512 tb, 512 tb + 512); warp w owns
 // [512 tb + 64 w, + 64): lane l holds targets +l (r = 0) and +32+l (r = 1).
 template <bool kPhi>
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kThreads, 2)
 allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, const float4* __restrict__ rel,
                 const TileBox* __restrict__ boxes, int n, int n_tiles, int n_tb, int n_split,
                 int tiles_per_chunk, float eps2, float4* __restrict__ part) {
@@ -329,7 +329,7 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, co
           const float2 e2 = make_float2(eps2, eps2);
           float2 fx = make_float2(px[0], px[1]), fy = make_float2(py[0], py[1]),
                  fz = make_float2(pz[0], pz[1]), fp = make_float2(pp[0], pp[1]);
-#pragma unroll 8
+#pragma unroll 16
           for (int k = 0; k < kSub; ++k) {
             const float4 s = sc[base + k];  // -u_j, q_j
             const float2 dx = __fadd2_rn(ax, make_float2(s.x, s.x));
