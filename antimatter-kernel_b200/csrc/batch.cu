@@ -154,7 +154,8 @@ batch_tile_stage_kernel(const int2* __restrict__ units, const InstanceDev* __res
     h = make_float4(__double2float_rn(xs), __double2float_rn(ys), __double2float_rn(zs), __double2float_rn(qe));
     l = make_float4(__double2float_rn(xs - static_cast<double>(h.x)), __double2float_rn(ys - static_cast<double>(h.y)),
                     __double2float_rn(zs - static_cast<double>(h.z)), 0.f);
-    u = make_float4(__double2float_rn(xs - cx), __double2float_rn(ys - cy), __double2float_rn(zs - cz), h.w);
+    u = make_float4(-__double2float_rn(xs - cx), -__double2float_rn(ys - cy), -__double2float_rn(zs - cz),
+                    h.w);  // negated offsets: the far loop adds them
   }
   if (k < e) {
     hq[k] = h;
@@ -181,7 +182,7 @@ batch_tile_stage_kernel(const int2* __restrict__ units, const InstanceDev* __res
 // (r_i - r_j) / |r_i - r_j|^3 in scaled units, written to the particle's
 // original index. Warp w of a unit owns targets [64 w, 64 w + 64) of the
 // block: lane l holds +l (r = 0) and +32+l (r = 1).
-__global__ void __launch_bounds__(kBT)
+__global__ void __launch_bounds__(kBT, 4)
 batch_allpairs_kernel(const int2* __restrict__ units, int n_units, const InstanceDev* __restrict__ inst,
                       const float4* __restrict__ hq, const float4* __restrict__ lo, const float4* __restrict__ rel,
                       const TileBox* __restrict__ boxes, const uint32_t* __restrict__ perm,
@@ -284,29 +285,37 @@ batch_allpairs_kernel(const int2* __restrict__ units, int n_units, const Instanc
             }
           }
         } else {
-          float ax[kBR], ay[kBR], az[kBR];
-#pragma unroll
-          for (int r = 0; r < kBR; ++r) {
-            ax[r] = (tx[r] - sbx.c.x) + (ux[r] - sbx.cl.x);
-            ay[r] = (ty[r] - sbx.c.y) + (uy[r] - sbx.cl.y);
-            az[r] = (tz[r] - sbx.c.z) + (uz[r] - sbx.cl.z);
-          }
-#pragma unroll 8
+          // far: a lane's two targets in the halves of packed FP32x2
+          // operations (same operations and association as the scalar form)
+          static_assert(kBR == 2, "packed far path holds two targets per lane");
+          float2 ax, ay, az;
+          ax.x = (tx[0] - sbx.c.x) + (ux[0] - sbx.cl.x);
+          ax.y = (tx[1] - sbx.c.x) + (ux[1] - sbx.cl.x);
+          ay.x = (ty[0] - sbx.c.y) + (uy[0] - sbx.cl.y);
+          ay.y = (ty[1] - sbx.c.y) + (uy[1] - sbx.cl.y);
+          az.x = (tz[0] - sbx.c.z) + (uz[0] - sbx.cl.z);
+          az.y = (tz[1] - sbx.c.z) + (uz[1] - sbx.cl.z);
+          const float2 e2 = make_float2(eps2, eps2);
+          float2 fx2 = make_float2(px[0], px[1]), fy2 = make_float2(py[0], py[1]), fz2 = make_float2(pz[0], pz[1]);
+#pragma unroll 16
           for (int k = 0; k < kBSub; ++k) {
-            const float4 sr = sc[base + k];
-#pragma unroll
-            for (int r = 0; r < kBR; ++r) {
-              const float dx = ax[r] - sr.x;
-              const float dy = ay[r] - sr.y;
-              const float dz = az[r] - sr.z;
-              const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-              const float rinv = rsqrtf(d2);
-              const float w = (sr.w * rinv) * (rinv * rinv);
-              px[r] = fmaf(w, dx, px[r]);
-              py[r] = fmaf(w, dy, py[r]);
-              pz[r] = fmaf(w, dz, pz[r]);
-            }
+            const float4 sr = sc[base + k];  // -u_j, q_j
+            const float2 dx = __fadd2_rn(ax, make_float2(sr.x, sr.x));
+            const float2 dy = __fadd2_rn(ay, make_float2(sr.y, sr.y));
+            const float2 dz = __fadd2_rn(az, make_float2(sr.z, sr.z));
+            const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
+            const float2 rinv = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+            const float2 w = __fmul2_rn(__fmul2_rn(make_float2(sr.w, sr.w), rinv), __fmul2_rn(rinv, rinv));
+            fx2 = __ffma2_rn(w, dx, fx2);
+            fy2 = __ffma2_rn(w, dy, fy2);
+            fz2 = __ffma2_rn(w, dz, fz2);
           }
+          px[0] = fx2.x;
+          px[1] = fx2.y;
+          py[0] = fy2.x;
+          py[1] = fy2.y;
+          pz[0] = fz2.x;
+          pz[1] = fz2.y;
         }
       }
 #pragma unroll
