@@ -413,6 +413,10 @@ namespace {
 
 constexpr long kNoAllocMaxParticles = 65536;
 constexpr long kNoAllocSortTile = 4096;  // the sort's tile (256 threads x 16)
+// radix_sort_pairs_buffers scans its digit histogram (256 counters per tile)
+// with one CTA, which handles at most 65,536 counters
+static_assert(256 * ((kNoAllocMaxParticles + kNoAllocSortTile - 1) / kNoAllocSortTile) <= 65536,
+              "the allocation-free sort's histogram exceeds the one-CTA scan");
 constexpr size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 constexpr size_t kNaBbox = 0;
 constexpr size_t kNaKeys = align256(kNaBbox + 8 * sizeof(unsigned long long));

@@ -487,14 +487,22 @@ __device__ __forceinline__ int m2l_key_v(unsigned long long k, int axis) {
   return static_cast<int>((k >> (38 - 19 * axis)) & ((1u << 19) - 1)) - kM2lVBias;
 }
 
-// Class key of a pair, kM2lEmpty = off the lattice or out of reach.
+// Class key of a pair, kM2lEmpty = off the lattice or out of reach. The
+// centres are sums of power-of-two fractions of the root half edge, rounded
+// to FP64 at every level, so a lattice offset v carries a rounding error of
+// a few dozen ulp of max|c| / u; the acceptance tolerance tracks that bound
+// (256 ulp), and a pair further off the lattice takes the per-pair path,
+// where D is built from the actual centres as in the reference.
 __device__ __forceinline__ unsigned long long m2l_class_key(const Octree& t, int ti, int si, int reach) {
   const double4 tc = t.center[ti], sc = t.center[si];
   const int dd = static_cast<int>(t.meta[ti].x) - static_cast<int>(t.meta[si].x);
   const double u = fmin(tc.w, sc.w);
   const double vx = (tc.x - sc.x) / u, vy = (tc.y - sc.y) / u, vz = (tc.z - sc.z) / u;
   const double rx = rint(vx), ry = rint(vy), rz = rint(vz);
-  if (fabs(vx - rx) > 1e-6 || fabs(vy - ry) > 1e-6 || fabs(vz - rz) > 1e-6) return kM2lEmpty;
+  const double cmax = fmax(fmax(fmax(fabs(tc.x), fabs(tc.y)), fmax(fabs(tc.z), fabs(sc.x))),
+                           fmax(fabs(sc.y), fabs(sc.z)));
+  const double tol = 256.0 * 2.220446049250313e-16 * (cmax / u + fabs(rx) + fabs(ry) + fabs(rz) + 1.0);
+  if (fabs(vx - rx) > tol || fabs(vy - ry) > tol || fabs(vz - rz) > tol) return kM2lEmpty;
   if (fabs(rx) > reach || fabs(ry) > reach || fabs(rz) > reach) return kM2lEmpty;
   return m2l_key(dd, static_cast<int>(rx), static_cast<int>(ry), static_cast<int>(rz));
 }

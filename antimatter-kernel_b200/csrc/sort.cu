@@ -14,6 +14,9 @@ constexpr int kSortThreads = 256;
 constexpr int kItems = 16;
 constexpr int kTile = kSortThreads * kItems;
 constexpr int kWarps = kSortThreads / 32;
+// counters the one-CTA scan_kernel handles (64 per thread); larger digit
+// histograms take the multi-CTA scan
+constexpr long kSingleScanCounters = 65536;
 
 __global__ void __launch_bounds__(kSortThreads)
 hist_kernel(const uint64_t* __restrict__ keys, long n, int shift, int nb, uint32_t* __restrict__ hist) {
@@ -127,7 +130,7 @@ int radix_sort_pairs(amk_ctx* c, const uint64_t* keys_in, const uint32_t* vals_i
     const int shift = 8 * p;
     hist_kernel<<<nb, kSortThreads, 0, c->stream>>>(ksrc, n, shift, nb, hist);
     AMK_TRY(check_launch(c, "hist_kernel"));
-    if (static_cast<long>(256) * nb > 65536) {
+    if (static_cast<long>(256) * nb > kSingleScanCounters) {
       // many tiles: the multi-CTA scan (in place; counts stay below 2^31)
       AMK_TRY(exclusive_scan_int(c, reinterpret_cast<const int*>(hist), static_cast<long>(256) * nb,
                                  reinterpret_cast<int*>(hist), total));
@@ -148,13 +151,17 @@ int radix_sort_pairs(amk_ctx* c, const uint64_t* keys_in, const uint32_t* vals_i
 namespace amk {
 
 // The same sort on caller-provided buffers (no context, no allocation):
-// ktmp/vtmp hold n elements, hist holds 256 * ceil(n / 4096) counters.
+// ktmp/vtmp hold n elements, hist holds 256 * ceil(n / 4096) counters. The
+// digit scan is the one-CTA scan_kernel, so 256 * ceil(n / 4096) must stay
+// within kSingleScanCounters (n <= 1,048,576): larger n is refused with
+// cudaErrorInvalidValue before anything is launched.
 cudaError_t radix_sort_pairs_buffers(cudaStream_t stream, const uint64_t* keys_in, const uint32_t* vals_in,
                                      uint64_t* keys_out, uint32_t* vals_out, uint64_t* ktmp, uint32_t* vtmp,
                                      uint32_t* hist, long n, int key_bits) {
   if (n <= 0) return cudaSuccess;
   const int passes = std::max(1, (key_bits + 7) / 8);
   const int nb = static_cast<int>((n + kTile - 1) / kTile);
+  if (static_cast<long>(256) * nb > kSingleScanCounters) return cudaErrorInvalidValue;
   const uint64_t* ksrc = keys_in;
   const uint32_t* vsrc = vals_in;
   for (int p = 0; p < passes; ++p) {

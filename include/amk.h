@@ -417,7 +417,10 @@ int amk_batch_info(const amk_ctx* ctx, long* n_instances, long* work_units, int*
  * n <= AMK_NOALLOC_MAX_PARTICLES, else AMK_ERR_LIMIT. The first call on a
  * device looks up the array's address; make it during set-up, before any
  * stream capture. Calls share the array: calls that overlap on the GPU
- * race. */
+ * race. Every one of the n force entries is written: particles that are
+ * dead (alive[i] == 0), neutral, or at a non-finite position get a zero
+ * force (the reference's drivers leave an annihilated agent's slot
+ * untouched instead). cutoff_radius <= 0 writes zero forces for all. */
 #define AMK_NOALLOC_MAX_PARTICLES 65536
 int amk_coulomb_standard_noalloc(const double* x, const double* y, const double* z,
                                  const double* q, const uint8_t* alive, long n,

@@ -142,3 +142,17 @@ def test_fmm_high_orders_match_reference(sim, order):
     (rx, ry, rz), _ = O.ref_fmm(x, y, z, q, order, 0.5, 32)
     rel, _ = rel_errors(f, (rx, ry, rz))
     assert np.max(rel) < FMM_TOL, np.max(rel)
+
+
+def test_fmm_off_origin_cloud_at_order_8(sim):
+    # a cloud centred far from the origin (1e3 sigma): the unit-cube frame
+    # subtracts the box centre, and lattice classes must not accept pairs
+    # whose centres are off the lattice by more than their rounding
+    if not O.ref_available():
+        pytest.skip("reference library not built")
+    x, y, z, q = gaussian_cloud(3000, 44)
+    x, y, z = x + 0.1, y - 0.1, z + 0.3
+    f = sim.solve_fmm(x, y, z, q, 8, 0.5)
+    (rx, ry, rz), _ = O.ref_fmm(x, y, z, q, 8, 0.5, 32)
+    rel, _ = rel_errors(f, (rx, ry, rz))
+    assert np.max(rel) < FMM_TOL, np.max(rel)

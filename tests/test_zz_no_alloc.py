@@ -14,6 +14,7 @@ import numpy as np
 import pytest
 
 import amk
+import oracle_lib as O
 from conftest import gaussian_cloud
 
 pytestmark = pytest.mark.gpu
@@ -62,6 +63,23 @@ def test_noalloc_matches_cutoff_entry_point_twice(sim):
     ref = sim.solve_cutoff(x[live], y[live], z[live], q[live], 3e-5)
     _close(tuple(g[live] for g in got), ref)
     assert all(np.all(g[~live] == 0.0) for g in got)
+
+
+def test_noalloc_at_its_maximum_size_and_against_the_oracle(sim):
+    # n = 65,536 fills every region of the static array (16 sort tiles, the
+    # full digit histogram); a small case is also held to the FP64 oracle
+    x, y, z, q = gaussian_cloud(65536, 73)
+    _close(_call(x, y, z, q, 1e-5), sim.solve_cutoff(x, y, z, q, 1e-5))
+    x, y, z, q = gaussian_cloud(700, 74)
+    _close(_call(x, y, z, q, 4e-5), O.cutoff(x, y, z, q, 4e-5))
+
+
+def test_noalloc_zero_radius_and_empty_input():
+    x, y, z, q = gaussian_cloud(500, 75)
+    got = _call(x, y, z, q, 0.0)  # cutoff_radius <= 0: every force is zero
+    assert all(np.all(g == 0.0) for g in got)
+    vp = C.c_void_p(1)
+    assert _fn()(vp, vp, vp, vp, None, 0, 1e-5, vp, vp, vp, None) == 0  # n = 0: nothing to do
 
 
 def test_noalloc_rejects_sizes_beyond_its_maximum():
