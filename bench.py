@@ -1,30 +1,39 @@
 #!/usr/bin/env python
 """Benchmark of the B200 particle path; prints ONE JSON line on rank 0.
 
-Workload (default ``direct65k``): the plain direct all-pairs Coulomb run --
-N = 65,536 (32,768 positrons + 32,768 antiprotons, real charges and masses),
-uniform ellipsoidal cloud with radii 2e-4 x 2e-4 x 5e-4 m drawn by the
-reference's own generator (seed 42), Maxwellian velocities at 10 K, b0 = 3 T,
-trap_voltage = 50 V, z0 = rho0 = 0.01 m, dt from the reference's rule
-(2.977e-12 s), FP32 pair arithmetic with compensated accumulation and FP64
-state, cooling and annihilation off. One bench step = one simulation step
-(all-pairs force -> Boris push) of the whole cloud.
+Default workload ``tree1m`` -- the 1M-particle solver comparison: N =
+1,048,576 positrons in a Gaussian cloud (sigma 1e-4 x 1e-4 x 3e-4 m, numpy
+default_rng(42)), 5 K Maxwellian velocities, b0 = 1 T, trap_voltage = 10 V,
+z0 = rho0 = 0.01 m, dt from the reference's rule (8.931e-12 s), cooling and
+annihilation off. One bench step = one simulation step of the whole cloud
+(Coulomb force -> Boris push). Every method (all-pairs, Barnes-Hut theta 0.7,
+FMM p = 4/6/7/8 at theta 0.5, learned p = 2 + MLP) is audited against the
+FP64 exact sum on 4,096 evenly spaced particles and timed; ``value`` is the
+fastest method whose RMS relative force error is <= 1e-5, timed for exactly
+``--steps`` steps after ``--warmup`` untimed ones. The same line carries every
+method's error and time, the learned / plain p = 6 ratio and the batched /
+one-at-a-time ratio of the 512-instance sweep (measured in the same run).
 
-``value`` is particle-steps/s over all ranks with the state resident in HBM
-(device-timed with CUDA events on the library's stream, L2 flushed by a
-256 MiB write between steps, the flush outside the per-step events). ``e2e``
-is the same metric through the C ABI with host buffers: every step uploads
-x, v from pinned host memory (amk_update_state), steps, and reads x, v and
-the alive flags back (amk_get_particles).
+``value`` is particle-steps/s with the state resident in HBM (device-timed
+with CUDA events on the library's stream, L2 flushed by a 256 MiB write
+between steps, the flush outside the per-step events). ``e2e`` is the same
+metric through the C ABI with host buffers: every step uploads x, v from
+pinned host memory (amk_update_state), steps, and reads x, v and the alive
+flags back (amk_get_particles).
 
-``--impl reference`` times the reference's own CPU code for the same step on
-the host cores (its Barnes-Hut tree at theta = 0, i.e. the exact all-pairs
-sum, compiled from the reference sources into oracle/_ref, plus the FP64
-push restatement), on a bounded sample of targets per step.
+``--impl reference`` times the reference's own CPU code on the host cores:
+its FMM (fast-multipole.cc, compiled from the reference sources into
+oracle/_ref) at p = 6, theta = 0.5 -- the reference method nearest the 1e-5
+error bar -- plus the FP64 Boris push, for whole steps on a bounded sample of
+the same cloud (its first 65,536 particles). Nothing of this repository's
+CUDA library is imported on that arm.
 
-Multi-GPU: the single-instance run does not shard (replicas only); under
-torchrun every rank runs its own replica and ``value`` sums them over the
-slowest rank's time.
+Other workloads: ``direct65k`` (65,536-particle all-pairs run) and
+``sweep512`` (the 512-instance batched sweep, partitioned across ranks by a
+cost model under torchrun).
+
+Multi-GPU: a single instance does not shard (replicas only; ``value`` sums
+the replicas over the slowest rank's time); the sweep shards by instance.
 """
 from __future__ import annotations
 
@@ -46,32 +55,602 @@ sys.path.insert(0, os.path.join(ROOT, "antimatter-kernel_b200"))
 METRIC = "particle-steps/s at ≤1e-5 force err vs FP64 direct: learned/batched vs plain"
 UNIT = "particle-steps/s"
 E = 1.602176634e-19
+KB = 1.380649e-23
+MASS = {0: 1.67262192369e-27, 1: 9.1093837015e-31, 3: 9.1093837015e-31, 4: 1.67262192369e-27}
+ERROR_BUDGET = 1e-5
+FLUSH_BYTES = 256 * 1024 * 1024
 
 
-def workload_direct65k():
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.rows = []
+        self.proc = None
+        self.device_index = device_index
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.device_index)],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+        time.sleep(0.3)
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [s.strip() for s in line.split(",")]
+            if len(parts) >= 9:
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            for k, name in enumerate(names):
+                if r[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------------ helpers
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def init_nccl(world, local):
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+
+def finish_dist(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def max_over_ranks(value, world, device):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _dp(ptr):
+    return C.cast(C.c_void_p(ptr), C.POINTER(C.c_double))
+
+
+def _oracle():
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_lib as O
+    return O
+
+
+class Flusher:
+    """Writes 256 MiB (twice the L2) on the library's stream between steps."""
+
+    def __init__(self, device, stream):
+        import torch
+        self.torch = torch
+        self.buf = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+        self.stream = stream
+        self.k = 0
+
+    def __call__(self):
+        with self.torch.cuda.stream(self.stream):
+            self.buf.fill_(float(self.k))
+        self.k += 1
+
+
+def timed_steps(sim, stream, flusher, k, step_fn=None):
+    """k steps, CUDA events around each (on the library's stream), L2 flushed
+    between steps outside the events. Returns the summed milliseconds."""
+    import torch
+    step_fn = step_fn or (lambda: sim.step(1))
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
+    for i in range(k):
+        starts[i].record(stream)
+        step_fn()
+        ends[i].record(stream)
+        flusher()
+    torch.cuda.synchronize()
+    return sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+
+
+def e2e_through_abi(sim, stream, n, steps, step_fn=None):
+    """`steps` steps through the C ABI with pinned host buffers: upload x, v,
+    step, read x, v and alive back, every step. Returns (ms, h2d, d2h)."""
+    import torch
     import amk
-    p = amk.make_params(
+    L = amk.lib()
+    step_fn = step_fn or (lambda: sim.step(1))
+    order = ("x", "y", "z", "vx", "vy", "vz")
+    host = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in order}
+    alive = torch.empty(n, dtype=torch.uint8, pin_memory=True)
+    ptr = {k: v.data_ptr() for k, v in host.items()}
+    alive_p = C.cast(C.c_void_p(alive.data_ptr()), C.POINTER(C.c_uint8))
+    amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k]) for k in order], alive_p))
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        sim.update_state(*[ptr[k] for k in order])
+        step_fn()
+        amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k]) for k in order], alive_p))
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1), 6 * 8 * n, 6 * 8 * n + n
+
+
+# ================================================================== tree1m
+TREE_METHODS = [
+    ("allpairs", dict(coulomb_method="allpairs")),
+    ("barnes-hut theta=0.7", dict(coulomb_method="barnes-hut", barnes_hut_theta=0.7)),
+    ("fmm p=4 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=4, fast_multipole_theta=0.5)),
+    ("fmm p=6 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=6, fast_multipole_theta=0.5)),
+    ("fmm p=7 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=7, fast_multipole_theta=0.5)),
+    ("fmm p=8 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=8, fast_multipole_theta=0.5)),
+    ("learned p=2 + MLP theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=2,
+                                        fast_multipole_theta=0.5, fmm_learned=1, learned_audit_interval=0)),
+]
+PLAIN_P6 = "fmm p=6 theta=0.5"
+LEARNED = "learned p=2 + MLP theta=0.5"
+
+# DRAM traffic (read + write) per launch of the FMM's M2L class-product kernel,
+# by order, from ncu captures of one launch (launches at N = 1,048,576 process
+# chunks of the same bounded size).
+FMM_PRODUCT_TRAFFIC = {
+    7: (5.18e9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of m2l_class_mma_kernel<7>, mean of two launches "
+                "of 4.47 M pairs each (0.89 / 1.10 GB read + 4.18 GB written: the per-pair products), "
+                "profiles/m2l_class_mma_kernel_tree1m.md"),
+    8: (5.17e9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of m2l_class_mma_kernel<8>, mean of two launches "
+                "of 3.25 M pairs each (0.92 GB read + 4.26 GB written: the per-pair products), "
+                "profiles/m2l_class_mma_kernel_tree1m.md"),
+}
+
+
+def tree_cloud(n=1 << 20, seed=42):
+    """N positrons, Gaussian cloud sigma 1e-4, 1e-4, 3e-4 m, 5 K Maxwellian."""
+    rng = np.random.default_rng(seed)
+    pos = rng.normal(0.0, 1.0, (n, 3)) * np.array([1e-4, 1e-4, 3e-4])
+    vel = rng.normal(0.0, 1.0, (n, 3)) * np.sqrt(KB * 5.0 / MASS[1])
+    return pos, vel, np.ones(n, np.uint8)
+
+
+def tree_config(n, world):
+    """The workload description; both arms print exactly this dict."""
+    return {"workload": (f"tree solvers on N={n:,} positrons: Gaussian cloud sigma 1e-4 x 1e-4 x 3e-4 m, "
+                         "5 K Maxwellian, b0=1 T, U=10 V, z0=rho0=0.01 m, dt=8.931e-12 s, cooling and "
+                         "annihilation off; one step = Coulomb force + Boris push of the whole cloud"),
+            "n_particles": n, "seed": 42,
+            "methods": [name for name, _ in TREE_METHODS],
+            "selection": "value = fastest method whose RMS relative force error vs the FP64 exact sum "
+                         "is <= 1e-5 (4,096 evenly spaced audited particles)",
+            "error_budget": ERROR_BUDGET,
+            "l2": "flushed between timed steps by a 256 MiB write (outside the per-step events)",
+            "parallelism": f"replicas x{world} (a single instance does not shard)"}
+
+
+def tree_params(n, over):
+    import amk
+    kw = dict(seed=42, b0=1.0, trap_voltage=10.0, z0=0.01, rho0=0.01, num_steps=500,
+              populations={"positron": n}, temperatures={"positron": 5.0}, cloud_radii=(1e-4, 1e-4, 3e-4),
+              bath_temperature=0.0, cooling_scale=0.0, cooling_enabled=0, coulomb_forces_enabled=1,
+              energy_method="allpairs", annihilation_enabled=0)
+    kw.update(over)
+    return amk.make_params(**kw)
+
+
+def cpu_tree_step(x, y, z, vx, vy, vz, order=6, theta=0.5):
+    """One reference CPU step on the sample: the reference's own FMM
+    (fast-multipole.cc via oracle/_ref, OpenMP on all host cores) for the
+    Coulomb force, then the FP64 Boris push of the sample. Returns seconds."""
+    O = _oracle()
+    n = len(x)
+    q = np.full(n, E)
+    m = np.full(n, MASS[1])
+    t0 = time.perf_counter()
+    (fx, fy, fz), _ = O.ref_fmm(x, y, z, q, order, theta)
+    state = dict(x=x, y=y, z=z, vx=vx, vy=vy, vz=vz, q=q, m=m, alive=np.ones(n, np.uint8))
+    O.boris_push(state, fx, fy, fz, 1.0, 10.0, 0.01, 0.01, 8.930966882e-12, False)
+    return time.perf_counter() - t0
+
+
+def cpu_tree_baseline(pos, vel, n_sample, warm, steps):
+    O = _oracle()
+    if not O.ref_available():
+        raise SystemExit("oracle/_ref/libamkref.so is missing: build it with `make -C oracle ref`")
+    x, y, z = (np.ascontiguousarray(pos[:n_sample, k]) for k in range(3))
+    vx, vy, vz = (np.ascontiguousarray(vel[:n_sample, k]) for k in range(3))
+    times = []
+    for k in range(warm + steps):
+        t = cpu_tree_step(x, y, z, vx, vy, vz)
+        if k >= warm:
+            times.append(t)
+    total = float(sum(times))
+    return {"value": n_sample * steps / total, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+            "sample": (f"first {n_sample:,} particles of the same cloud; per step the reference's own FMM "
+                       f"(fast-multipole.cc, p=6, theta=0.5, leaf 32, OpenMP on all host cores) + FP64 Boris "
+                       f"push of the sample; {steps} timed steps after {warm} untimed; the reference FMM's "
+                       "cost per particle at this size is within 15% of its cost at 1,048,576 particles"),
+            "ms_per_step": 1e3 * total / steps}
+
+
+def run_reference_tree(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    pos, vel, _ = tree_cloud(args.tree_n)
+    n_s = min(args.ref_sample, len(pos))
+    cpu = cpu_tree_baseline(pos, vel, n_s, args.warmup, args.steps)
+    line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": cpu["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Gaussian cloud, numpy default_rng(42))",
+            "config": tree_config(len(pos), world),
+            "cpu_baseline": {k: v for k, v in cpu.items() if k != "ms_per_step"},
+            "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def tree_method_entry(sim, name, over, args, stream, flusher):
+    """Audit and time one method on a fresh context holding the cloud."""
+    entry = {}
+    if over.get("fmm_learned"):
+        t0 = time.perf_counter()
+        loss, samples = sim.fmm_train_correction(0.5, sample_leaves=4096, steps=2000, batch=4096, lr=1e-3)
+        entry["training"] = {"seconds": round(time.perf_counter() - t0, 2), "samples": samples,
+                             "final_loss": loss}
+    sim.coulomb()
+    rms, mx = sim.force_error(args.audit_samples)
+    entry.update({"rms_rel": rms, "max_rel": mx, "meets_1e-5": bool(rms <= ERROR_BUDGET)})
+    sim.step(2)
+    sim.synchronize()
+    k = max(1, min(args.steps, args.method_steps))
+    ms = timed_steps(sim, stream, flusher, k) / k
+    entry.update(ms_per_step=ms, value=sim.num_particles() / (ms * 1e-3), steps=k)
+    sim.set_profiling(True)
+    sim.reset_phase_times()
+    sim.step(1)
+    sim.synchronize()
+    entry["phase_ms"] = {kk: round(v[0], 3) for kk, v in sim.phase_times().items() if v[1]}
+    sim.set_profiling(False)
+    return entry
+
+
+def tree_roofline(sim, over, n):
+    if over["coulomb_method"] == "allpairs":
+        sim.set_profiling(True)
+        sim.reset_phase_times()
+        sim.step(1)
+        sim.synchronize()
+        ap_ms, ap_n = sim.phase_times()["allpairs"]
+        sim.set_profiling(False)
+        peak = sim.measure_fp32_peak()
+        achieved = 20.0 * n * (n - 1) / (ap_ms / ap_n * 1e-3) / 1e12
+        return {"bound": "fp32", "kernel": "allpairs_kernel", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": 3.276e6 * n / 65536,
+                "traffic_source": "ncu capture at N = 65,536 (profiles/allpairs_kernel_direct65k.md), scaled by N",
+                "peak_source": "measured in this run: FFMA probe kernel over all SMs (2 flop/FFMA)",
+                "flop_convention": "20 flop per pair interaction x N(N-1) pairs",
+                "avg_launch_ms": ap_ms / ap_n}
+    if over["coulomb_method"] == "fast-multipole" and not over.get("fmm_learned"):
+        sim.set_profiling(True)
+        sim.reset_phase_times()
+        sim.step(1)
+        sim.synchronize()
+        ph = sim.phase_times()
+        sim.set_profiling(False)
+        prod_ms, prod_n = ph["fmm_m2l_products"]
+        st = sim.fmm_stats()
+        p_ = st["order"]
+        nm = (p_ + 1) * (p_ + 2) * (p_ + 3) // 6
+        peak = sim.measure_fp64_peak()
+        achieved = 2.0 * nm * nm * st["m2l_class_pairs"] / (prod_ms * 1e-3) / 1e12
+        traffic = FMM_PRODUCT_TRAFFIC.get(p_)
+        return {"bound": "fp64 tensor", "kernel": f"m2l_class_mma_kernel<{p_}>", "achieved": achieved,
+                "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None if traffic is None else traffic[0],
+                "traffic_source": None if traffic is None else traffic[1],
+                "peak_source": "measured in this run: mma.m8n8k4 FP64 probe kernel over all SMs "
+                               "(512 flop per warp instruction); the driver's peak file has no FP64 figure",
+                "flop_convention": f"2 n_m^2 flop (n_m = {nm}) per M2L pair evaluated as a class product "
+                                   f"({st['m2l_class_pairs']:,} of {st['m2l_pairs']:,} pairs; the rest take "
+                                   "the per-pair path)",
+                "avg_launch_ms": prod_ms / max(1, prod_n), "launches_per_step": prod_n,
+                "m2l_phase_ms": ph["fmm_m2l"][0], "classes": st["m2l_classes"]}
+    return None
+
+
+def run_tree(args):
+    import torch
+    import amk
+    world, rank, local = dist_setup()
+    init_nccl(world, local)
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    pos, vel, sp = tree_cloud(args.tree_n)
+    n = len(pos)
+    methods = [m for m in TREE_METHODS if not args.tree_methods or m[0] in args.tree_methods.split(",")]
+    if not methods:
+        raise SystemExit(f"--tree-methods: none of {[m[0] for m in TREE_METHODS]}")
+
+    def new_sim(over):
+        sim = amk.Simulation(tree_params(n, over), device=local)
+        sim.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
+        stream = torch.cuda.ExternalStream(sim.stream(), device=device)
+        return sim, stream
+
+    results, best = {}, None
+    for name, over in methods:
+        sim, stream = new_sim(over)
+        entry = tree_method_entry(sim, name, over, args, stream, Flusher(device, stream))
+        results[name] = entry
+        if entry["meets_1e-5"] and (best is None or entry["value"] > results[best]["value"]):
+            best = name
+        sim.close()
+
+    # ---- the chosen method: W untimed steps, exactly K timed steps
+    name = best if best is not None else methods[0][0]
+    over = dict(TREE_METHODS)[name]
+    sim, stream = new_sim(over)
+    flusher = Flusher(device, stream)
+    if over.get("fmm_learned"):
+        sim.fmm_train_correction(0.5, sample_leaves=4096, steps=2000, batch=4096, lr=1e-3)
+    for _ in range(args.warmup):
+        sim.step(1)
+        flusher()
+    sim.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    launches0 = sim.kernel_launches()
+    total_ms = timed_steps(sim, stream, flusher, args.steps)
+    if world > 1:
+        torch.distributed.barrier()
+    launches = sim.kernel_launches() - launches0
+    clocks = sampler.stop()
+    total_ms = max_over_ranks(total_ms, world, device)
+    value = world * n * args.steps / (total_ms * 1e-3)
+    roofline = tree_roofline(sim, over, n)
+    e2e_ms, h2d, d2h = e2e_through_abi(sim, stream, n, args.steps)
+    e2e_ms = max_over_ranks(e2e_ms, world, device)
+    e2e = {"value": world * n * args.steps / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "steps": args.steps,
+           "api": "amk_update_state + amk_step + amk_get_particles (pinned host buffers)"}
+    sim.close()
+
+    learned_vs_p6 = None
+    if LEARNED in results and PLAIN_P6 in results:
+        a, b = results[LEARNED], results[PLAIN_P6]
+        learned_vs_p6 = {"ratio": a["value"] / b["value"], "learned_rms": a["rms_rel"], "p6_rms": b["rms_rel"],
+                         "both_within_budget": bool(a["meets_1e-5"] and b["meets_1e-5"]),
+                         "target": ">= 3x at <= 1e-5 RMS"}
+
+    sweep = None
+    if args.sweep_ratio and world == 1:
+        sweep = measure_sweep(args, 1, 0, local, device, ratio_only=True)
+
+    cpu = None
+    if rank == 0 and world == 1 and args.cpu_baseline:
+        cpu = cpu_tree_baseline(pos, vel, min(args.ref_sample, n), 1, 3)
+        cpu.pop("ms_per_step")
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "fp32" if over["coulomb_method"] == "allpairs" else "f64",
+                "data": "synthetic (seeded Gaussian cloud, numpy default_rng(42))",
+                "config": tree_config(n, world), "chosen": name, "methods": results,
+                "learned_vs_plain_p6": learned_vs_p6, "sweep_batched_vs_one_at_a_time": sweep,
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clocks}
+        print(json.dumps(line), flush=True)
+    finish_dist(world)
+    return 0
+
+
+# ================================================================== direct65k
+DIRECT_POPS = {"antiproton": 32768, "positron": 32768}
+
+
+def direct_config(world):
+    return {"workload": "direct all-pairs Coulomb + Boris push, N=65,536 (32,768 e+ + 32,768 pbar), uniform "
+                        "ellipsoid 2e-4 x 2e-4 x 5e-4 m, 10 K Maxwellian, b0=3 T, U=50 V, z0=rho0=0.01 m, "
+                        "dt=2.977e-12 s",
+            "n_particles": 65536, "seed": 42, "cooling": False, "annihilation": False,
+            "state_precision": "fp64 positions/velocities",
+            "l2": "flushed between steps by a 256 MiB write (inputs 6.5 MB < L2)",
+            "parallelism": f"replicas x{world} (a single instance does not shard)"}
+
+
+def direct_params():
+    import amk
+    return amk.make_params(
         seed=42, b0=3.0, trap_voltage=50.0, z0=0.01, rho0=0.01, num_steps=1000,
-        populations={"antiproton": 32768, "positron": 32768},
-        temperatures={"antiproton": 10.0, "positron": 10.0},
+        populations=dict(DIRECT_POPS), temperatures={"antiproton": 10.0, "positron": 10.0},
         cloud_radii=(2e-4, 2e-4, 5e-4), bath_temperature=0.0, cooling_scale=0.0,
         cooling_enabled=0, coulomb_forces_enabled=1, coulomb_method="allpairs",
         energy_method="allpairs", annihilation_enabled=0)
-    config = {"workload": "direct all-pairs Coulomb + Boris push, N=65,536 "
-                          "(32,768 e+ + 32,768 pbar), uniform ellipsoid 2e-4 x 2e-4 x 5e-4 m, "
-                          "10 K Maxwellian, b0=3 T, U=50 V, z0=rho0=0.01 m, dt=2.977e-12 s",
-              "n_particles": 65536, "solver": "allpairs (tiled FP32, double-float positions, "
-                                                  "compensated accumulation)",
-              "state_precision": "fp64 positions/velocities", "cooling": False,
-              "annihilation": False, "seed": 42,
-              "l2": "flushed between steps by a 256 MiB write (inputs 6.5 MB < L2)"}
-    return p, config
 
 
-KB = 1.380649e-23
-MASS = {0: 1.67262192369e-27, 1: 9.1093837015e-31, 3: 9.1093837015e-31, 4: 1.67262192369e-27}
+def cpu_direct_step_time(x, y, z, q, m, n_sample, seed=0):
+    """Reference CPU step on a bounded sample: the reference's Barnes-Hut tree
+    at theta = 0 (exact all-pairs) over all N sources walked for n_sample
+    targets, plus the FP64 push of those targets. Returns (seconds,
+    targets, forces)."""
+    O = _oracle()
+    n = len(x)
+    rng = np.random.default_rng(seed)
+    targets = np.sort(rng.choice(n, n_sample, replace=False))
+    t0 = time.perf_counter()
+    f = O.ref_bh_forces_subset(x, y, z, q, 0.0, targets, 8)
+    state = dict(x=x[targets].copy(), y=y[targets].copy(), z=z[targets].copy(), vx=np.zeros(n_sample),
+                 vy=np.zeros(n_sample), vz=np.zeros(n_sample), q=q[targets], m=m[targets],
+                 alive=np.ones(n_sample, np.uint8))
+    O.boris_push(state, f[0], f[1], f[2], 3.0, 50.0, 0.01, 0.01, 2.977e-12, False)
+    return time.perf_counter() - t0, targets, f
 
 
+def direct_cloud():
+    O = _oracle()
+    pos = O.initial_positions(DIRECT_POPS, [2e-4, 2e-4, 5e-4], 42)
+    sp = O.species_column(DIRECT_POPS)
+    m, q = O.species_props(sp)
+    return pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy(), q, m
+
+
+def run_reference_direct(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return 0
+    x, y, z, q, m = direct_cloud()
+    times = []
+    for k in range(args.warmup + args.steps):
+        t, _, _ = cpu_direct_step_time(x, y, z, q, m, args.ref_sample_direct, seed=k)
+        if k >= args.warmup:
+            times.append(t)
+    total = float(sum(times))
+    value = args.ref_sample_direct * args.steps / total
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (reference initial-condition generator, seed 42)", "config": direct_config(world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                             "sample": f"per step: the reference's exact (theta=0) Barnes-Hut tree over all "
+                                       f"65,536 sources walked for {args.ref_sample_direct} random targets + FP64 "
+                                       "push of those targets; value counts the targets processed"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_direct(args):
+    import torch
+    import amk
+    world, rank, local = dist_setup()
+    init_nccl(world, local)
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    sim = amk.Simulation(direct_params(), device=local)
+    sim.init_particles()
+    n = sim.num_particles()
+    stream = torch.cuda.ExternalStream(sim.stream(), device=device)
+    flusher = Flusher(device, stream)
+    for _ in range(args.warmup):
+        sim.step(1)
+        flusher()
+    sim.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    launches0 = sim.kernel_launches()
+    total_ms = timed_steps(sim, stream, flusher, args.steps)
+    if world > 1:
+        torch.distributed.barrier()
+    launches = sim.kernel_launches() - launches0
+    clocks = sampler.stop()
+    total_ms = max_over_ranks(total_ms, world, device)
+    value = world * n * args.steps / (total_ms * 1e-3)
+
+    prof_steps = min(args.steps, 50)
+    sim.set_profiling(True)
+    sim.reset_phase_times()
+    for _ in range(prof_steps):
+        sim.step(1)
+        flusher()
+    sim.synchronize()
+    phases = sim.phase_times()
+    sim.set_profiling(False)
+    ap_ms, ap_launches = phases["allpairs"]
+    ap_avg_ms = ap_ms / max(ap_launches, 1)
+    flops_per_launch = 20.0 * n * (n - 1)
+    achieved = flops_per_launch / (ap_avg_ms * 1e-3) / 1e12
+    peak = sim.measure_fp32_peak()
+    roofline = {"bound": "fp32", "kernel": "allpairs_kernel", "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": 3.276e6,
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one allpairs_kernel "
+                                  "launch of this workload (profiles/allpairs_kernel_direct65k.md)",
+                "peak_source": "measured in this run: FFMA probe kernel over all SMs "
+                               "(2 flop/FFMA); no FP32 figure in the driver's peak file",
+                "flops_per_launch": flops_per_launch,
+                "flop_convention": "20 flop per pair interaction x N(N-1) pairs",
+                "avg_launch_ms": ap_avg_ms,
+                "phase_ms_per_step": {k: v[0] / max(prof_steps, 1) for k, v in phases.items() if v[1]}}
+    e2e_ms, h2d, d2h = e2e_through_abi(sim, stream, n, args.steps)
+    e2e_ms = max_over_ranks(e2e_ms, world, device)
+    e2e = {"value": world * n * args.steps / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h, "steps": args.steps,
+           "api": "amk_update_state + amk_step + amk_get_particles (pinned host buffers)"}
+    cpu = err = None
+    if rank == 0 and world == 1 and args.cpu_baseline:
+        st = sim.get_particles()
+        sim.coulomb_allpairs()
+        fx, fy, fz = sim.get_forces()
+        _, _, _, q, m = direct_cloud()
+        t, targets, fref = cpu_direct_step_time(st["x"], st["y"], st["z"], q, m, args.cpu_sample)
+        cpu = {"value": args.cpu_sample / t, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+               "sample": f"the reference's exact (theta=0) Barnes-Hut tree over all {n} sources walked for "
+                         f"{args.cpu_sample} random targets + FP64 push of those targets; OpenMP on all host "
+                         "cores; value counts the targets processed"}
+        num = np.sqrt((fx[targets] - fref[0]) ** 2 + (fy[targets] - fref[1]) ** 2 + (fz[targets] - fref[2]) ** 2)
+        den = np.sqrt(fref[0] ** 2 + fref[1] ** 2 + fref[2] ** 2)
+        rel = num / den
+        err = {"rms_rel": float(np.sqrt(np.mean(rel ** 2))), "max_rel": float(np.max(rel)),
+               "targets": int(len(targets)), "against": "the reference's FP64 exact sum"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
+                "data": "synthetic (reference initial-condition generator, seed 42)",
+                "config": direct_config(world), "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": launches, "clocks": clocks, "force_error_vs_fp64": err}
+        print(json.dumps(line), flush=True)
+    sim.close()
+    finish_dist(world)
+    return 0
+
+
+# ================================================================== sweep512
 def make_sweep(n_inst=512, seed=2024, method_split=8192, order=4):
     """The batched sweep: n_inst independent trap instances, populations
     log-uniform in [1e2, 1e5] (even, 1:1 species pairs e-/e+ or e+/pbar per
@@ -121,250 +700,33 @@ def load_sweep(sim, insts):
     return pos, vel, sp, offsets
 
 
-WORKLOADS = {"direct65k": workload_direct65k, "sweep512": None, "tree1m": None}
+def sweep_share(insts, world, rank):
+    """This rank's instances of the sweep (LPT on the per-instance cost model)."""
+    from amk import partition
+    costs = [partition.instance_cost(len(i[0]), int(i[3].coulomb_method)) for i in insts]
+    parts = partition.partition_lpt(costs, world)
+    return parts[rank], partition.imbalance(costs, parts)
 
 
-def tree_cloud(n=1 << 20, seed=42):
-    """N positrons, Gaussian cloud sigma 1e-4, 1e-4, 3e-4 m, 5 K Maxwellian."""
-    rng = np.random.default_rng(seed)
-    pos = rng.normal(0.0, 1.0, (n, 3)) * np.array([1e-4, 1e-4, 3e-4])
-    vel = rng.normal(0.0, 1.0, (n, 3)) * np.sqrt(KB * 5.0 / MASS[1])
-    return pos, vel, np.ones(n, np.uint8)
-
-
-TREE_METHODS = [
-    ("allpairs", dict(coulomb_method="allpairs")),
-    ("barnes-hut theta=0.7", dict(coulomb_method="barnes-hut", barnes_hut_theta=0.7)),
-    ("fmm p=4 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=4, fast_multipole_theta=0.5)),
-    ("fmm p=6 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=6, fast_multipole_theta=0.5)),
-    ("fmm p=7 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=7, fast_multipole_theta=0.5)),
-    ("fmm p=8 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=8, fast_multipole_theta=0.5)),
-    ("learned p=2 + MLP theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=2,
-                                        fast_multipole_theta=0.5, fmm_learned=1, learned_audit_interval=0)),
-]
-
-
-# DRAM traffic (read + write) per launch of the FMM's M2L class-product kernel,
-# by order: from ncu captures of one launch (one chunk of at most 4 GiB of
-# per-pair products; launches at N = 1,048,576 process chunks of the same size).
-FMM_PRODUCT_TRAFFIC = {
-    7: (5.18e9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of m2l_class_mma_kernel<7>, mean of two launches "
-                "of 4.47 M pairs each (0.89 / 1.10 GB read + 4.18 GB written: the per-pair products), "
-                "profiles/m2l_class_mma_kernel_tree1m.md"),
-    8: (5.17e9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of m2l_class_mma_kernel<8>, mean of two launches "
-                "of 3.25 M pairs each (0.92 GB read + 4.26 GB written: the per-pair products), "
-                "profiles/m2l_class_mma_kernel_tree1m.md"),
-}
-
-
-# ------------------------------------------------------------------ clocks
-class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
-
-    def __init__(self, device_index):
-        self.rows = []
-        self.proc = None
-        self.device_index = device_index
-
-    def start(self):
-        try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200", "-i", str(self.device_index)],
-                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-        except (OSError, ValueError):
-            self.proc = None
-            return
-        self.thread = threading.Thread(target=self._read, daemon=True)
-        self.thread.start()
-
-    def _read(self):
-        for line in self.proc.stdout:
-            parts = [s.strip() for s in line.split(",")]
-            if len(parts) >= 9:
-                self.rows.append(parts)
-
-    def stop(self):
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        time.sleep(0.25)
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        reasons = set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in self.rows:
-            for k, name in enumerate(names):
-                if r[5 + k].lower().startswith("active"):
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(self.rows)}
-
-
-# ------------------------------------------------------------------ helpers
-def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
-
-
-def max_over_ranks(value, world, device):
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device=device)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def _dp(ptr):
-    return C.cast(C.c_void_p(ptr), C.POINTER(C.c_double))
-
-
-# ------------------------------------------------------------------ CPU legs
-def cpu_reference_step_time(x, y, z, q, m, n_sample, seed=0):
-    """Reference CPU step on a bounded sample: the reference's Barnes-Hut tree
-    at theta = 0 (exact all-pairs) over all N sources, walked for n_sample
-    targets and extrapolated to N, plus the FP64 push of all N particles.
-    Returns (seconds per full step, kind, sampled target ids, sampled forces)."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle_lib as O
-    n = len(x)
-    rng = np.random.default_rng(seed)
-    targets = np.sort(rng.choice(n, n_sample, replace=False))
-    if O.ref_available():
-        kind = "reference"
-        t0 = time.perf_counter()
-        O.ref_bh_forces_subset(x, y, z, q, 0.0, targets[:1], 8)
-        t_build = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        f = O.ref_bh_forces_subset(x, y, z, q, 0.0, targets, 8)
-        t_walk = max(time.perf_counter() - t0 - t_build, 1e-9)
-    else:
-        kind = "port"
-        t_build = 0.0
-        t0 = time.perf_counter()
-        f = O.allpairs_subset(x, y, z, q, targets)
-        t_walk = time.perf_counter() - t0
-    state = dict(x=x.copy(), y=y.copy(), z=z.copy(), vx=np.zeros(n), vy=np.zeros(n), vz=np.zeros(n),
-                 q=q, m=m, alive=np.ones(n, np.uint8))
-    t0 = time.perf_counter()
-    O.boris_push(state, np.zeros(n), np.zeros(n), np.zeros(n), 3.0, 50.0, 0.01, 0.01, 2.977e-12, True)
-    t_push = time.perf_counter() - t0
-    return t_build + t_walk * n / n_sample + t_push, kind, targets, f
-
-
-def run_reference(args):
-    world, rank, _ = dist_setup()
-    if rank != 0:
-        return 0
-    import amk
-    p, config = WORKLOADS[args.workload]()
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle_lib as O
-    pops = {"antiproton": 32768, "positron": 32768}
-    pos = O.initial_positions(pops, [2e-4, 2e-4, 5e-4], 42)
-    sp = O.species_column(pops)
-    m, q = O.species_props(sp)
-    x, y, z = pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy()
-    sample = args.ref_sample
-    times = []
-    kind = "reference"
-    for k in range(args.warmup + args.steps):
-        t, kind, _, _ = cpu_reference_step_time(x, y, z, q, m, sample, seed=k)
-        if k >= args.warmup:
-            times.append(t)
-    t_step = float(np.mean(times))
-    value = len(x) / t_step
-    cores = os.cpu_count()
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (reference initial-condition generator, seed 42)", "config": config,
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-                             "sample": f"per step: tree over all {len(x)} sources, theta=0 walks for "
-                                       f"{sample} sampled targets extrapolated to {len(x)}, FP64 "
-                                       f"push of all {len(x)}"},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
-    return 0
-
-
-# ------------------------------------------------------------------ batched sweep
-def cpu_sweep_step_time(insts, n_sample=64):
-    """Reference CPU step of every instance on a bounded sample: the
-    reference's Barnes-Hut tree at theta = 0 (exact all-pairs) built over
-    each instance's sources and walked for up to n_sample targets,
-    extrapolated to the instance, plus the FP64 push of every particle."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle_lib as O
-    total = 0.0
-    kind = "reference" if O.ref_available() else "port"
-    for pos, vel, sp, p in insts:
-        n = len(pos)
-        m, q = O.species_props(sp)
-        x, y, z = pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy()
-        k = min(n, n_sample)
-        targets = np.arange(k) * (n // k)
-        t_build = 0.0
-        if kind == "reference":
-            t0 = time.perf_counter()
-            O.ref_bh_forces_subset(x, y, z, q, 0.0, targets[:1], 8)  # tree build + one walk
-            t_build = time.perf_counter() - t0
-            t0 = time.perf_counter()
-            O.ref_bh_forces_subset(x, y, z, q, 0.0, targets, 8)
-            t_walk = max(time.perf_counter() - t0 - t_build, 1e-9)
-        else:
-            t0 = time.perf_counter()
-            O.allpairs_subset(x, y, z, q, targets)
-            t_walk = time.perf_counter() - t0
-        state = dict(x=x, y=y, z=z, vx=vel[:, 0].copy(), vy=vel[:, 1].copy(), vz=vel[:, 2].copy(),
-                     q=q, m=m, alive=np.ones(n, np.uint8))
-        t0 = time.perf_counter()
-        O.boris_push(state, np.zeros(n), np.zeros(n), np.zeros(n), p.b0, p.trap_voltage, p.z0, p.rho0,
-                     p.dt, True)
-        t_push = time.perf_counter() - t0
-        total += t_build + t_walk * n / k + t_push
-    return total, kind
-
-
-def run_sweep(args):
-    """Batched 512-instance sweep: batched step (one persistent all-pairs
-    launch, CUDA-graph chunks) against the same instances stepped one at a
-    time with the single-instance kernels."""
+def measure_sweep(args, world, rank, local, device, ratio_only=False):
+    """Batched sweep (one persistent all-pairs launch, CUDA-graph chunks) on
+    this rank's share of the instances, against the same instances stepped one
+    at a time with the single-instance kernels. Returns a dict of results."""
     import torch
     import amk
-    world, rank, local = dist_setup()
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    device = torch.device("cuda", local)
-    torch.cuda.set_device(device)
-    # every rank runs its own sweep of 512 instances (seeded by rank): the
-    # instances are independent, so the sweep shards with no collective
-    insts = make_sweep(n_inst=args.instances, seed=2024 + rank, method_split=None)
+    all_insts = make_sweep(n_inst=args.instances, seed=2024, method_split=None)
+    mine, imb = sweep_share(all_insts, world, rank)
+    insts = [all_insts[i] for i in mine]
     n_total = int(sum(len(i[0]) for i in insts))
     sim = amk.Simulation(device=local)
     load_sweep(sim, insts)
-    # per-instance method by measurement under the 1e-5 RMS force-error budget
     t0 = time.perf_counter()
-    methods = sim.batch_autotune(error_budget=1e-5, samples=256)
+    methods = sim.batch_autotune(error_budget=ERROR_BUDGET, samples=256)
     tune_s = time.perf_counter() - t0
     names = {-1: "none", 0: "cutoff", 1: "barnes-hut", 2: "fmm", 3: "allpairs"}
     method_counts = {names[int(m)]: int((methods == m).sum()) for m in np.unique(methods)}
-    chunk = min(100, args.steps)
+    steps = args.sweep_steps if ratio_only else args.steps
+    chunk = min(100, steps)
 
     def barrier():
         if world > 1:
@@ -373,12 +735,7 @@ def run_sweep(args):
     def live():
         return int(sim.batch_status()["alive"].sum())
 
-    def live_rate(ms, steps, before, after):
-        # particle-steps/s over the live particles (annihilated ones do no work)
-        return world * 0.5 * (before + after) * steps / (ms * 1e-3)
-
     def timed(fn):
-        # events on the stream of the context in use (contexts are replaced below)
         st = torch.cuda.ExternalStream(sim.stream(), device=device)
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
@@ -391,6 +748,13 @@ def run_sweep(args):
         barrier()
         return ev0.elapsed_time(ev1)
 
+    def live_sum(v):  # live particles summed over ranks
+        if world == 1:
+            return float(v)
+        t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+        torch.distributed.all_reduce(t)
+        return float(t.item())
+
     # warm-up: plain steps (the first is the staggered one), then one chunk to
     # capture and instantiate the graph outside the timed region
     sim.batch_step(args.warmup)
@@ -399,15 +763,28 @@ def run_sweep(args):
     sampler = ClockSampler(local)
     sampler.start()
     launches0 = sim.kernel_launches()
-    live0 = live()
-    ms = timed(lambda: sim.batch_step(args.steps, graph_chunk=chunk))
-    live1 = live()
+    live0 = live_sum(live())
+    ms = timed(lambda: sim.batch_step(steps, graph_chunk=chunk))
+    live1 = live_sum(live())
     launches = sim.kernel_launches() - launches0
     clocks = sampler.stop()
     ms = max_over_ranks(ms, world, device)
-    value = live_rate(ms, args.steps, live0, live1)
+    value = 0.5 * (live0 + live1) * steps / (ms * 1e-3)
 
-    # per-phase device time (profiling runs plain steps, no graph)
+    serial_steps = max(1, min(steps, args.serial_steps))
+    sim.batch_step(1, serial=True)  # untimed: grows the single-instance scratch to its largest size
+    s_live0 = live_sum(live())
+    serial_ms = max_over_ranks(timed(lambda: sim.batch_step(serial_steps, serial=True)), world, device)
+    serial_value = 0.5 * (s_live0 + live_sum(live())) * serial_steps / (serial_ms * 1e-3)
+    out = {"batched_value": value, "one_at_a_time_value": serial_value, "ratio": value / serial_value,
+           "target": ">= 5x", "instances": len(insts), "particles": n_total, "steps": steps,
+           "one_at_a_time_steps": serial_steps, "graph_chunk": chunk,
+           "autotune": {"methods": method_counts, "seconds": round(tune_s, 2)},
+           "rate_counts": "live (not yet annihilated) particles, mean of the timed window's start and end"}
+    if ratio_only:
+        sim.close()
+        return out
+
     prof_steps = 2
     sim.set_profiling(True)
     sim.reset_phase_times()
@@ -421,145 +798,117 @@ def run_sweep(args):
     pairs = float(sum(a * (a - 1) for a, m in zip(alive_i, methods) if m == 3))
     peak = sim.measure_fp32_peak()
     achieved = 20.0 * pairs / (ap_avg * 1e-3) / 1e12
-    roofline = {"bound": "fp32", "kernel": "batch_allpairs_kernel", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": 116.2e6 * n_total / 1380664,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of batch_allpairs_kernel "
-                                  "on the 64-instance case (116.2 MB for 1,380,664 particles, "
-                                  "profiles/batch_allpairs_kernel_sweep.md), scaled by particle count (the "
-                                  "staged particle data read once plus the force writes)",
-                "peak_source": "measured in this run: FFMA probe kernel over all SMs (2 flop/FFMA)",
-                "flops_per_launch": 20.0 * pairs,
-                "flop_convention": "20 flop per pair interaction x sum_i A_i(A_i-1), A_i the live "
-                                   "particles of all-pairs instance i",
-                "avg_launch_ms": ap_avg,
-                "phase_ms_per_step": {k: v[0] / prof_steps for k, v in phases.items() if v[1]}}
+    out["roofline"] = {
+        "bound": "fp32", "kernel": "batch_allpairs_kernel", "achieved": achieved, "peak": peak,
+        "unit": "TFLOP/s", "frac": achieved / peak, "traffic": 116.2e6 * n_total / 1380664,
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of batch_allpairs_kernel on the "
+                          "64-instance case (116.2 MB for 1,380,664 particles, "
+                          "profiles/batch_allpairs_kernel_sweep.md), scaled by particle count",
+        "peak_source": "measured in this run: FFMA probe kernel over all SMs (2 flop/FFMA)",
+        "flops_per_launch": 20.0 * pairs,
+        "flop_convention": "20 flop per pair interaction x sum_i A_i(A_i-1), A_i the live particles of "
+                           "all-pairs instance i",
+        "avg_launch_ms": ap_avg,
+        "phase_ms_per_step": {k: v[0] / prof_steps for k, v in phases.items() if v[1]}}
 
-    # baseline: the same instances one at a time with the single-instance kernels
-    serial_steps = max(1, min(args.steps, args.serial_steps))
-    sim.batch_step(1, serial=True)  # untimed: grows the single-instance scratch to its largest size
-    s_live0 = live()
-    serial_ms = max_over_ranks(timed(lambda: sim.batch_step(serial_steps, serial=True)), world, device)
-    serial_value = live_rate(serial_ms, serial_steps, s_live0, live())
-    sim.close()
-    # the sweep's own method split (FMM p=4 from 8,192 particles), both ways
-    split = make_sweep(n_inst=args.instances, seed=2024 + rank, method_split=8192, order=4)
-    sim = amk.Simulation(device=local)
-    load_sweep(sim, split)
-    sim.batch_step(args.warmup)
-    p_live0 = live()
-    split_ms = max_over_ranks(timed(lambda: sim.batch_step(serial_steps)), world, device)
-    split_value = live_rate(split_ms, serial_steps, p_live0, live())
-    sim.batch_step(1, serial=True)
-    p_live0 = live()
-    split_serial_ms = max_over_ranks(timed(lambda: sim.batch_step(serial_steps, serial=True)), world, device)
-    split_serial_value = live_rate(split_serial_ms, serial_steps, p_live0, live())
-
-    # end to end through the C ABI with host buffers (one step per call)
-    L = amk.lib()
+    e2e_steps = max(1, min(steps, 10))
     sim.close()
     sim = amk.Simulation(device=local)
     load_sweep(sim, insts)
     sim.batch_step(args.warmup)
-    host = {k: torch.empty(n_total, dtype=torch.float64, pin_memory=True) for k in
-            ("x", "y", "z", "vx", "vy", "vz")}
-    alive = torch.empty(n_total, dtype=torch.uint8, pin_memory=True)
-    order = ("x", "y", "z", "vx", "vy", "vz")
-    ptr = {k: v.data_ptr() for k, v in host.items()}
-    amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k]) for k in order],
-                                  C.cast(C.c_void_p(alive.data_ptr()), C.POINTER(C.c_uint8))))
-    e2e_steps = max(1, min(args.steps, 10))
-
-    def e2e_loop():
-        for _ in range(e2e_steps):
-            sim.update_state(*[ptr[k2] for k2 in order])
-            sim.batch_step(1)
-            amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k2]) for k2 in order],
-                                          C.cast(C.c_void_p(alive.data_ptr()), C.POINTER(C.c_uint8))))
-    e_live0 = live()
-    e2e_ms = max_over_ranks(timed(e2e_loop), world, device)
-    e2e = {"value": live_rate(e2e_ms, e2e_steps, e_live0, live()), "unit": UNIT,
-           "h2d_bytes_per_step": 6 * 8 * n_total, "d2h_bytes_per_step": 6 * 8 * n_total + n_total,
-           "steps": e2e_steps,
-           "api": "amk_update_state + amk_batch_step + amk_get_particles (pinned host buffers)"}
+    st = torch.cuda.ExternalStream(sim.stream(), device=device)
+    e_live0 = live_sum(live())
+    barrier()
+    e2e_ms, h2d, d2h = e2e_through_abi(sim, st, n_total, e2e_steps, step_fn=lambda: sim.batch_step(1))
+    e2e_ms = max_over_ranks(e2e_ms, world, device)
+    out["e2e"] = {"value": 0.5 * (e_live0 + live_sum(live())) * e2e_steps / (e2e_ms * 1e-3), "unit": UNIT,
+                  "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h, "steps": e2e_steps,
+                  "api": "amk_update_state + amk_batch_step + amk_get_particles (pinned host buffers)"}
+    # one host gather of per-instance results (live count, total energy) in instance order
+    from amk import partition
     status = sim.batch_status()
+    energies = sim.batch_energy()
+    rows = [(int(a), float(e["total"])) for a, e in zip(status["alive"], energies)]
+    gathered = partition.gather_instance_rows(mine, rows, len(all_insts), world, rank)
+    out["per_instance"] = None if gathered is None else {
+        "instances": len(gathered), "alive_total": int(sum(r[0] for r in gathered))}
+    out.update(value=value, ms=ms, launches=launches, clocks=clocks, imbalance=imb,
+               contact_overflow=bool(status["overflow"]), insts=insts, n_total=n_total)
     sim.close()
+    return out
 
+
+def cpu_sweep_baseline(insts, pair_budget):
+    """The reference's CPU code on a bounded sample of the sweep: instances in
+    index order (a random sample: instance parameters are drawn independently)
+    until their N_i^2 pair counts reach `pair_budget`; each instance the
+    reference's exact (theta=0) Barnes-Hut tree over all its sources walked
+    for all its particles, plus the FP64 push. Returns (instances, particles
+    processed, seconds)."""
+    O = _oracle()
+    total, parts, pairs, k = 0.0, 0, 0.0, 0
+    for pos, vel, sp, p in insts:
+        n = len(pos)
+        if k > 0 and pairs + float(n) * n > pair_budget:
+            continue
+        m, q = O.species_props(sp)
+        x, y, z = pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy()
+        t0 = time.perf_counter()
+        f = O.ref_bh_forces(x, y, z, q, 0.0, 8)
+        state = dict(x=x, y=y, z=z, vx=vel[:, 0].copy(), vy=vel[:, 1].copy(), vz=vel[:, 2].copy(),
+                     q=q, m=m, alive=np.ones(n, np.uint8))
+        O.boris_push(state, f[0], f[1], f[2], p.b0, p.trap_voltage, p.z0, p.rho0, p.dt, False)
+        total += time.perf_counter() - t0
+        parts += n
+        pairs += float(n) * n
+        k += 1
+    return k, parts, total
+
+
+def sweep_config(args, world):
+    return {"workload": f"batched sweep: {args.instances} trap instances, N_i log-uniform 1e2..1e5, e-/e+ or "
+                        "e+/pbar 1:1, T 4..1e4 K, b0 1..5 T, U 5..50 V, radii 5e-5..5e-4 m, cooling (4 K) and "
+                        "annihilation (5e-6 m, p=0.5) on",
+            "instances": args.instances, "seed": 2024,
+            "solver": "per-instance method chosen by amk_batch_autotune under a 1e-5 RMS force-error budget; "
+                      "all-pairs instances share one persistent launch (cost-ordered work queue); FP64 state",
+            "l2": "not flushed: state of about 8 M particles (> 700 MB) exceeds L2",
+            "parallelism": f"dp{world}: the instances partitioned across ranks (LPT on a per-instance cost "
+                           "model), no per-step collective, one host gather at the end"}
+
+
+def run_sweep(args):
+    import torch
+    world, rank, local = dist_setup()
+    init_nccl(world, local)
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    r = measure_sweep(args, world, rank, local, device)
     cpu = None
-    if rank == 0 and world == 1:
-        t_cpu, kind = cpu_sweep_step_time(insts)
-        cpu = {"value": n_total / t_cpu, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
-               "sample": "per instance: reference Barnes-Hut theta=0 tree over all its sources walked "
-                         "for 64 evenly spaced targets (extrapolated), + FP64 push of all particles; "
-                         "all instances, OpenMP on all host cores"}
+    if rank == 0 and world == 1 and args.cpu_baseline:
+        k, parts, secs = cpu_sweep_baseline(r["insts"], args.ref_pairs)
+        cpu = {"value": parts / secs, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+               "sample": f"{k} instances of this rank's share in index order, up to {args.ref_pairs:.0e} "
+                         "particle pairs (instances that would exceed it are skipped): per instance the reference's exact (theta=0) Barnes-Hut tree walked "
+                         "for all its particles + FP64 push; value counts the particles processed"}
     if rank == 0:
-        sizes = np.array([len(i[0]) for i in insts])
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
-                "data": "synthetic (seeded sweep generator)",
-                "config": {"workload": f"batched sweep: {len(insts)} trap instances, N_i log-uniform 1e2..1e5 "
-                                       f"(total {n_total:,}), e-/e+ or e+/pbar 1:1, T 4..1e4 K, b0 1..5 T, "
-                                       "U 5..50 V, radii 5e-5..5e-4 m, cooling (4 K) and annihilation "
-                                       "(5e-6 m, p=0.5) on",
-                           "solver": "per-instance method chosen by amk_batch_autotune under a 1e-5 "
-                                     "RMS force-error budget; all-pairs instances share one persistent "
-                                     "launch (cost-ordered work queue); FP64 state",
-                           "autotune": {"methods": method_counts, "seconds": round(tune_s, 2)},
-                           "graph_chunk": chunk, "instances": len(insts), "n_particles": n_total,
-                           "live_particles_timed": [live0, live1],
-                           "rate_counts": "live (not yet annihilated) particles, mean of the timed "
-                                          "window's start and end",
-                           "instance_sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)),
-                                              "max": int(sizes.max())},
-                           "l2": "not flushed: state of 7.4 M particles (> 700 MB) exceeds L2",
-                           "parallelism": f"dp{world}: one {len(insts)}-instance sweep per GPU, no collective"},
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clocks,
-                "one_at_a_time": {"value": serial_value, "steps": serial_steps,
-                                  "ms_per_step": serial_ms / serial_steps,
-                                  "speedup_batched": value / serial_value,
-                                  "api": "amk_batch_step(serial=1): each instance through the "
-                                         "single-instance kernels, one after another"},
-                "method_split_8192_fmm_p4": {
-                    "batched_value": split_value,
-                    "one_at_a_time_value": split_serial_value,
-                    "note": "all-pairs below 8,192 particles, FMM p=4 theta=0.5 above (RMS error "
-                            "about 7e-5, above the 1e-5 bar); per-instance FMM calls synchronise "
-                            "with the host, so no graphs"},
-                "contact_overflow": bool(status["overflow"])}
+        sizes = np.array([len(i[0]) for i in r["insts"]])
+        line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms"] / args.steps, "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "fp32",
+                "data": "synthetic (seeded sweep generator)", "config": sweep_config(args, world),
+                "rank0_share": {"instances": r["instances"], "particles": r["particles"],
+                                "sizes": {"min": int(sizes.min()), "median": int(np.median(sizes)),
+                                          "max": int(sizes.max())},
+                                "load_imbalance": r["imbalance"]},
+                "roofline": r["roofline"], "cpu_baseline": cpu, "e2e": r["e2e"], "gpu_launches": r["launches"],
+                "clocks": r["clocks"],
+                "one_at_a_time": {"value": r["one_at_a_time_value"], "steps": r["one_at_a_time_steps"],
+                                  "speedup_batched": r["ratio"]},
+                "autotune": r["autotune"], "per_instance_gather": r["per_instance"],
+                "contact_overflow": r["contact_overflow"]}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
-    return 0
-
-
-def run_reference_tree(args):
-    world, rank, _ = dist_setup()
-    if rank != 0:
-        return 0
-    pos, _, _ = tree_cloud(args.tree_n)
-    n = len(pos)
-    x, y, z = pos[:, 0].copy(), pos[:, 1].copy(), pos[:, 2].copy()
-    q = np.full(n, E)
-    m = np.full(n, MASS[1])
-    times = []
-    kind = "reference"
-    for k in range(args.warmup + args.steps):
-        t, kind, _, _ = cpu_reference_step_time(x, y, z, q, m, args.ref_sample, seed=k)
-        if k >= args.warmup:
-            times.append(t)
-    t_step = float(np.mean(times))
-    value = n / t_step
-    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Gaussian cloud)",
-            "config": {"workload": f"tree solvers at N={n:,} positrons (exact force)"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
-                             "sample": f"per step: theta=0 tree over all {n} sources, {args.ref_sample} targets "
-                                       f"walked (extrapolated), FP64 push of all"},
-            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    finish_dist(world)
     return 0
 
 
@@ -567,384 +916,92 @@ def run_reference_sweep(args):
     world, rank, _ = dist_setup()
     if rank != 0:
         return 0
-    insts = make_sweep(n_inst=args.instances, seed=2024, method_split=None)
-    n_total = int(sum(len(i[0]) for i in insts))
-    times = []
-    kind = "reference"
+    insts = sweep_instances_numpy(args.instances)
+    times, parts, k_inst = [], 0, 0
     for k in range(args.warmup + args.steps):
-        t, kind = cpu_sweep_step_time(insts, n_sample=16)
+        k_inst, p, t = cpu_sweep_baseline(insts, args.ref_pairs)
         if k >= args.warmup:
             times.append(t)
-    t_step = float(np.mean(times))
-    value = n_total / t_step
+            parts = p
+    total = float(sum(times))
+    value = parts * args.steps / total
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded sweep generator)",
-            "config": {"workload": f"batched sweep: {len(insts)} trap instances, {n_total:,} particles"},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
-                             "sample": "per instance and step: theta=0 tree over all sources, 16 "
-                                       "targets walked (extrapolated), FP64 push of all"},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded sweep generator)", "config": sweep_config(args, world),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                             "sample": f"per step {k_inst} instances in index order, up to {args.ref_pairs:.0e} "
+                                       "particle pairs (instances that would exceed it are skipped): the reference's exact (theta=0) Barnes-Hut tree walked "
+                                       "for all their particles + FP64 push; value counts the particles processed"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
 
 
-# ------------------------------------------------------------------ tree solvers at 1M
-def run_tree(args):
-    """N = 1,048,576 positrons: every Coulomb method timed per step (force +
-    push) and audited against the FP64 exact sum; `value` is the fastest
-    method whose RMS relative force error is within 1e-5."""
-    import torch
-    import amk
-    world, rank, local = dist_setup()
-    device = torch.device("cuda", local)
-    torch.cuda.set_device(device)
-    pos, vel, sp = tree_cloud(args.tree_n)
-    n = len(pos)
-    steps = max(1, min(args.steps, 5))
-    results = {}
-    best = None
-    methods = [m for m in TREE_METHODS if not args.tree_methods or m[0] in args.tree_methods.split(",")]
-    if not methods:
-        raise SystemExit(f"--tree-methods: none of {[m[0] for m in TREE_METHODS]}")
-    for name, over in methods:
-        kw = dict(seed=42, b0=1.0, trap_voltage=10.0, z0=0.01, rho0=0.01, num_steps=500,
-                  populations={"positron": n}, temperatures={"positron": 5.0}, cloud_radii=(1e-4, 1e-4, 3e-4),
-                  bath_temperature=0.0, cooling_scale=0.0, cooling_enabled=0, coulomb_forces_enabled=1,
-                  energy_method="allpairs", annihilation_enabled=0)
-        kw.update(over)
-        sim = amk.Simulation(amk.make_params(**kw), device=local)
-        sim.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
-        entry = {}
-        if over.get("fmm_learned"):
-            t0 = time.perf_counter()
-            loss, samples = sim.fmm_train_correction(0.5, sample_leaves=4096, steps=2000, batch=4096, lr=1e-3)
-            entry["training"] = {"seconds": round(time.perf_counter() - t0, 2), "samples": samples,
-                                 "final_loss": loss}
-        sim.coulomb()
-        rms, mx = sim.force_error(1024)
-        entry.update({"rms_rel": rms, "max_rel": mx, "meets_1e-5": bool(rms <= 1e-5)})
-        stream = torch.cuda.ExternalStream(sim.stream(), device=device)
-        sim.step(max(1, args.warmup))
-        sim.synchronize()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        sim.step(steps)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        ms = ev0.elapsed_time(ev1) / steps
-        entry.update(ms_per_step=ms, value=n / (ms * 1e-3), steps=steps)
-        sim.set_profiling(True)
-        sim.reset_phase_times()
-        sim.step(1)
-        sim.synchronize()
-        entry["phase_ms"] = {k: round(v[0], 3) for k, v in sim.phase_times().items() if v[1]}
-        sim.set_profiling(False)
-        results[name] = entry
-        if entry["meets_1e-5"] and (best is None or entry["value"] > results[best]["value"]):
-            best = name
-        sim.close()
-    # the winner again: roofline of its dominant kernel, e2e through the C ABI
-    name = best if best is not None else methods[0][0]
-    over = dict(TREE_METHODS)[name]
-    kw = dict(seed=42, b0=1.0, trap_voltage=10.0, populations={"positron": n}, cooling_enabled=0,
-              energy_method="allpairs", annihilation_enabled=0)
-    kw.update(over)
-    sim = amk.Simulation(amk.make_params(**kw), device=local)
-    sim.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
-    sim.step(1)
-    sampler = ClockSampler(local)
-    sampler.start()
-    launches0 = sim.kernel_launches()
-    stream = torch.cuda.ExternalStream(sim.stream(), device=device)
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    ev0.record(stream)
-    sim.step(steps)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    launches = sim.kernel_launches() - launches0
-    clocks = sampler.stop()
-    ms = ev0.elapsed_time(ev1) / steps
-    value = n / (ms * 1e-3)
-    roofline = None
-    if over["coulomb_method"] == "allpairs":
-        sim.set_profiling(True)
-        sim.reset_phase_times()
-        sim.step(1)
-        sim.synchronize()
-        ap_ms, ap_n = sim.phase_times()["allpairs"]
-        sim.set_profiling(False)
-        peak = sim.measure_fp32_peak()
-        achieved = 20.0 * n * (n - 1) / (ap_ms / ap_n * 1e-3) / 1e12
-        roofline = {"bound": "fp32", "kernel": "allpairs_kernel", "achieved": achieved, "peak": peak,
-                    "unit": "TFLOP/s", "frac": achieved / peak, "traffic": 3.276e6 * n / 65536,
-                    "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of allpairs_kernel at "
-                                      "N = 65,536 (3.276 MB, profiles/allpairs_kernel_direct65k.md), scaled by N "
-                                      "(sources are read from DRAM once per launch and re-read from L2)",
-                    "peak_source": "measured in this run: FFMA probe kernel over all SMs (2 flop/FFMA)",
-                    "flop_convention": "20 flop per pair interaction x N(N-1) pairs",
-                    "avg_launch_ms": ap_ms / ap_n}
-    elif over["coulomb_method"] == "fast-multipole" and not over.get("fmm_learned"):
-        sim.set_profiling(True)
-        sim.reset_phase_times()
-        sim.step(1)
-        sim.synchronize()
-        ph = sim.phase_times()
-        sim.set_profiling(False)
-        prod_ms, prod_n = ph["fmm_m2l_products"]
-        st = sim.fmm_stats()
-        p_ = st["order"]
-        nm = (p_ + 1) * (p_ + 2) * (p_ + 3) // 6
-        peak = sim.measure_fp64_peak()
-        achieved = 2.0 * nm * nm * st["m2l_class_pairs"] / (prod_ms * 1e-3) / 1e12
-        traffic = FMM_PRODUCT_TRAFFIC.get(p_)
-        roofline = {"bound": "fp64 tensor", "kernel": f"m2l_class_mma_kernel<{p_}>", "achieved": achieved,
-                    "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                    "traffic": None if traffic is None else traffic[0],
-                    "traffic_source": None if traffic is None else traffic[1],
-                    "peak_source": "measured in this run: mma.m8n8k4 FP64 probe kernel over all SMs "
-                                   "(512 flop per warp instruction)",
-                    "flop_convention": f"2 n_m^2 flop (n_m = {nm}) per M2L pair evaluated as a class product "
-                                       f"({st['m2l_class_pairs']:,} of {st['m2l_pairs']:,} pairs; the rest take "
-                                       "the per-pair path)",
-                    "avg_launch_ms": prod_ms / max(1, prod_n), "launches_per_step": prod_n,
-                    "m2l_phase_ms": ph["fmm_m2l"][0], "classes": st["m2l_classes"]}
-    host = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in ("x", "y", "z", "vx", "vy", "vz")}
-    alive = torch.empty(n, dtype=torch.uint8, pin_memory=True)
-    order = ("x", "y", "z", "vx", "vy", "vz")
-    ptr = {k: v.data_ptr() for k, v in host.items()}
-    L = amk.lib()
-    amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k]) for k in order],
-                                  C.cast(C.c_void_p(alive.data_ptr()), C.POINTER(C.c_uint8))))
-    torch.cuda.synchronize()
-    ev0.record(stream)
-    for _ in range(steps):
-        sim.update_state(*[ptr[k] for k in order])
-        sim.step(1)
-        amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k]) for k in order],
-                                      C.cast(C.c_void_p(alive.data_ptr()), C.POINTER(C.c_uint8))))
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = ev0.elapsed_time(ev1)
-    e2e = {"value": n * steps / (e2e_ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": 48 * n,
-           "d2h_bytes_per_step": 49 * n, "steps": steps,
-           "api": "amk_update_state + amk_step + amk_get_particles (pinned host buffers)"}
-    st = sim.get_particles()
-    sim.close()
-    cpu = None
-    if rank == 0 and world == 1:
-        q = np.full(n, E)
-        m = np.full(n, MASS[1])
-        t_step, kind, _, _ = cpu_reference_step_time(st["x"], st["y"], st["z"], q, m, args.cpu_sample)
-        cpu = {"value": n / t_step, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
-               "sample": f"reference Barnes-Hut theta=0 (exact all-pairs) tree over all {n} sources walked for "
-                         f"{args.cpu_sample} sampled targets, extrapolated to {n}, + FP64 push of all {n}"}
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": args.warmup,
-            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "fp32" if over["coulomb_method"] == "allpairs" else "f64",
-            "data": "synthetic (seeded Gaussian cloud)",
-            "config": {"workload": f"tree solvers at N={n:,} positrons, Gaussian sigma 1e-4 x 1e-4 x 3e-4 m, "
-                                   "5 K Maxwellian, b0=1 T, U=10 V; value = fastest method within 1e-5 RMS "
-                                   "relative force error vs the FP64 exact sum (1,024 audited particles)",
-                       "chosen": name, "methods": results,
-                       "l2": "not flushed: state of 1 M particles (> 100 MB) exceeds L2",
-                       "parallelism": "replicas x1 (single instance)"},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    return 0
+class _SweepParams:
+    """The few per-instance parameters the CPU sweep leg reads."""
+
+    def __init__(self, b0, volt, species):
+        O = _oracle()
+        self.b0, self.trap_voltage, self.z0, self.rho0 = b0, volt, 0.01, 0.01
+        self.dt = O.dt_for(list(species), b0)
 
 
-# ------------------------------------------------------------------ GPU arm
-def run_amk(args):
-    import torch
-    import amk
-    world, rank, local = dist_setup()
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
-    device = torch.device("cuda", local)
-    torch.cuda.set_device(device)
-    p, config = WORKLOADS[args.workload]()
-    sim = amk.Simulation(p, device=local)
-    sim.init_particles()
-    n = sim.num_particles()
-    stream = torch.cuda.ExternalStream(sim.stream(), device=device)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
-
-    def flush_l2(k):
-        with torch.cuda.stream(stream):
-            flush.fill_(float(k))
-
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-
-    # ---------------- warm-up
-    for k in range(args.warmup):
-        sim.step(1)
-        flush_l2(k)
-    sim.synchronize()
-
-    # ---------------- timed region (resident state)
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    sampler = ClockSampler(local)
-    sampler.start()
-    barrier()
-    torch.cuda.synchronize()
-    launches0 = sim.kernel_launches()
-    for k in range(args.steps):
-        starts[k].record(stream)
-        sim.step(1)
-        ends[k].record(stream)
-        flush_l2(k)
-    torch.cuda.synchronize()
-    barrier()
-    launches = sim.kernel_launches() - launches0
-    clocks = sampler.stop()
-    total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
-    total_ms = max_over_ranks(total_ms, world, device)
-    value = world * n * args.steps / (total_ms * 1e-3)
-
-    # ---------------- roofline of the dominant kernel (live phase events)
-    prof_steps = min(args.steps, 50)
-    sim.set_profiling(True)
-    sim.reset_phase_times()
-    for k in range(prof_steps):
-        sim.step(1)
-        flush_l2(k)
-    sim.synchronize()
-    phases = sim.phase_times()
-    sim.set_profiling(False)
-    ap_ms, ap_launches = phases["allpairs"]
-    ap_avg_ms = ap_ms / max(ap_launches, 1)
-    flops_per_launch = 20.0 * n * (n - 1)
-    achieved = flops_per_launch / (ap_avg_ms * 1e-3) / 1e12
-    peak = sim.measure_fp32_peak()
-    roofline = {"bound": "fp32", "kernel": "allpairs_kernel", "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": 3.276e6,
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one allpairs_kernel "
-                                  "launch of this workload (profiles/allpairs_kernel_direct65k.md)",
-                "peak_source": "measured in this run: FFMA probe kernel over all SMs "
-                               "(2 flop/FFMA); no FP32 figure in the driver's peak file",
-                "flops_per_launch": flops_per_launch,
-                "flop_convention": "20 flop per pair interaction x N(N-1) pairs",
-                "avg_launch_ms": ap_avg_ms,
-                "phase_ms_per_step": {k: v[0] / max(prof_steps, 1) for k, v in phases.items() if v[1]}}
-
-    # ---------------- end to end through the C ABI with host buffers
-    L = amk.lib()
-    host = {k: torch.empty(n, dtype=torch.float64, pin_memory=True) for k in
-            ("x", "y", "z", "vx", "vy", "vz")}
-    alive = torch.empty(n, dtype=torch.uint8, pin_memory=True)
-    ptr = {k: v.data_ptr() for k, v in host.items()}
-    order = ("x", "y", "z", "vx", "vy", "vz")
-    amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k]) for k in order],
-                                  C.cast(C.c_void_p(alive.data_ptr()), C.POINTER(C.c_uint8))))
-    e2e_steps = args.steps
-    barrier()
-    torch.cuda.synchronize()
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    for k in range(e2e_steps):
-        sim.update_state(*[ptr[k2] for k2 in order])
-        sim.step(1)
-        amk.check(L.amk_get_particles(sim.handle, *[_dp(ptr[k2]) for k2 in order],
-                                      C.cast(C.c_void_p(alive.data_ptr()), C.POINTER(C.c_uint8))))
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(ev0.elapsed_time(ev1), world, device)
-    e2e_value = world * n * e2e_steps / (e2e_ms * 1e-3)
-    e2e = {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 6 * 8 * n,
-           "d2h_bytes_per_step": 6 * 8 * n + n, "steps": e2e_steps,
-           "api": "amk_update_state + amk_step + amk_get_particles (pinned host buffers)"}
-
-    # ---------------- CPU baseline + force check (rank 0, one GPU only)
-    cpu = None
-    err = None
-    if rank == 0 and world == 1:
-        st = sim.get_particles()
-        sim.coulomb_allpairs()
-        fx, fy, fz = sim.get_forces()
-        q = np.where(np.asarray(_species(sim, p)) == 1, E, -E)
-        m = np.where(np.asarray(_species(sim, p)) == 1, 9.1093837015e-31, 1.67262192369e-27)
-        t_step, kind, targets, fref = cpu_reference_step_time(st["x"], st["y"], st["z"], q, m,
-                                                              args.cpu_sample)
-        cpu = {"value": n / t_step, "unit": UNIT, "cores": os.cpu_count(), "kind": kind,
-               "sample": f"reference Barnes-Hut theta=0 (exact all-pairs) tree over all {n} "
-                         f"sources walked for {args.cpu_sample} sampled targets, extrapolated to "
-                         f"{n}, + FP64 push of all {n}; OpenMP on all host cores"}
-        num = np.sqrt((fx[targets] - fref[0]) ** 2 + (fy[targets] - fref[1]) ** 2 +
-                      (fz[targets] - fref[2]) ** 2)
-        den = np.sqrt(fref[0] ** 2 + fref[1] ** 2 + fref[2] ** 2)
-        rel = num / den
-        err = {"rms_rel": float(np.sqrt(np.mean(rel ** 2))), "max_rel": float(np.max(rel)),
-               "targets": int(len(targets)), "against": f"{kind} FP64 exact sum"}
-
-    if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
-                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "fp32",
-                "data": "synthetic (reference initial-condition generator, seed 42)",
-                "config": dict(config, parallelism=f"replicas x{world} (single instance does not shard)"),
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
-                "clocks": clocks, "force_error_vs_fp64": err}
-        print(json.dumps(line), flush=True)
-    sim.close()
-    if world > 1:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
-    return 0
-
-
-def _species(sim, p):
-    # species in creation order: populations in enum order (antiproton, positron)
+def sweep_instances_numpy(n_inst, seed=2024):
+    """make_sweep's instances for the CPU arm, drawn with the same generator
+    calls but without the CUDA library's parameter struct."""
+    rng = np.random.default_rng(seed)
     out = []
-    for i in sorted(range(p.n_species), key=lambda k: p.species[k]):
-        out += [p.species[i]] * p.populations[i]
+    for i in range(n_inst):
+        n = max(2, int(round(10 ** rng.uniform(2.0, 5.0))) // 2 * 2)
+        pair = (3, 1) if rng.random() < 0.5 else (1, 0)
+        temp = 10 ** rng.uniform(np.log10(4.0), 4.0)
+        b0 = rng.uniform(1.0, 5.0)
+        volt = rng.uniform(5.0, 50.0)
+        radii = rng.uniform(5e-5, 5e-4, 3)
+        d = rng.normal(size=(n, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        pos = d * rng.random((n, 1)) ** (1.0 / 3.0) * radii
+        sp = np.repeat(np.array(pair, np.uint8), n // 2)
+        m = np.array([MASS[int(k)] for k in pair]).repeat(n // 2)
+        vel = rng.normal(size=(n, 3)) * np.sqrt(KB * temp / m)[:, None]
+        out.append((pos, vel, sp, _SweepParams(b0, volt, pair)))
     return out
 
 
-def main():
+# ================================================================== main
+WORKLOADS = {"tree1m": (run_tree, run_reference_tree), "direct65k": (run_direct, run_reference_direct),
+             "sweep512": (run_sweep, run_reference_sweep)}
+
+
+def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=1000)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["amk", "reference"], default="amk")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="direct65k")
-    ap.add_argument("--cpu-sample", type=int, default=8192,
-                    help="targets walked by the CPU baseline leg")
-    ap.add_argument("--ref-sample", type=int, default=256,
-                    help="targets walked per step by the reference arm")
-    ap.add_argument("--serial-steps", type=int, default=3,
-                    help="steps of the one-at-a-time comparison (sweep workload)")
-    ap.add_argument("--instances", type=int, default=512,
-                    help="trap instances of the sweep workload (the first k of the 512-instance sweep)")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="tree1m")
+    ap.add_argument("--cpu-baseline", type=int, default=1, help="time the reference's CPU leg (rank 0, N=1)")
+    ap.add_argument("--cpu-sample", type=int, default=8192, help="targets of the direct workload's CPU leg")
+    ap.add_argument("--ref-sample", type=int, default=65536,
+                    help="particles of the tree workload's reference sample (the cloud's first ones)")
+    ap.add_argument("--ref-sample-direct", type=int, default=512,
+                    help="targets per step of the direct workload's reference arm")
+    ap.add_argument("--ref-pairs", type=float, default=2e9,
+                    help="particle pairs per step of the sweep workload's reference sample")
+    ap.add_argument("--audit-samples", type=int, default=4096, help="particles audited against FP64")
+    ap.add_argument("--method-steps", type=int, default=5, help="timed steps of each method in the table")
+    ap.add_argument("--sweep-ratio", type=int, default=1,
+                    help="tree workload: also measure the sweep's batched / one-at-a-time ratio")
+    ap.add_argument("--sweep-steps", type=int, default=20, help="batched steps of the sweep ratio")
+    ap.add_argument("--serial-steps", type=int, default=3, help="steps of the one-at-a-time comparison")
+    ap.add_argument("--instances", type=int, default=512, help="trap instances of the sweep")
     ap.add_argument("--tree-n", type=int, default=1 << 20, help="particles of the tree workload")
-    ap.add_argument("--tree-methods", default="",
-                    help="comma-separated subset of the tree workload's methods (default: all)")
-    args = ap.parse_args()
+    ap.add_argument("--tree-methods", default="", help="comma-separated subset of the tree workload's methods")
+    args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)  # at least three untimed warm-up steps
-    if args.impl == "reference":
-        if args.workload == "sweep512":
-            return run_reference_sweep(args)
-        if args.workload == "tree1m":
-            return run_reference_tree(args)
-        return run_reference(args)
-    if args.workload == "sweep512":
-        return run_sweep(args)
-    if args.workload == "tree1m":
-        return run_tree(args)
-    return run_amk(args)
+    amk_fn, ref_fn = WORKLOADS[args.workload]
+    return (ref_fn if args.impl == "reference" else amk_fn)(args)
 
 
 if __name__ == "__main__":

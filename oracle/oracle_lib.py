@@ -23,7 +23,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libamkref.so")
-REFERENCE_TREE = "/root/reference"
+REFERENCE_TREE = os.environ.get("AMK_REFERENCE_TREE", "/root/reference")
 
 _dp = C.POINTER(C.c_double)
 _u8p = C.POINTER(C.c_uint8)
