@@ -262,15 +262,7 @@ double orc_cooling_time(double charge, double mass, double b_mag) {
 
 // Three N(0,1) draws for particle `id` at step `step` (philox.h stream rule).
 void orc_cooling_normals(uint32_t seed, uint32_t id, uint64_t step, double* out3) {
-  const orc::U32x4 w = orc::Philox4x32(seed, orc::kTagCooling, id, static_cast<uint32_t>(step),
-                                       static_cast<uint32_t>(step >> 32), 0u);
-  const double u1 = orc::U01(w.v[0]), u2 = orc::U01(w.v[1]);
-  const double u3 = orc::U01(w.v[2]), u4 = orc::U01(w.v[3]);
-  const double r1 = std::sqrt(-2.0 * std::log(u1));
-  const double r2 = std::sqrt(-2.0 * std::log(u3));
-  out3[0] = r1 * std::cos(2.0 * kPi * u2);
-  out3[1] = r1 * std::sin(2.0 * kPi * u2);
-  out3[2] = r2 * std::cos(2.0 * kPi * u4);
+  orc::CoolingNormals(seed, id, step, out3);
 }
 
 // CyclotronCooling::Run, forces/cooling.cc:24-66 with B = (0, 0, b0). The

@@ -306,3 +306,76 @@ def ref_fmm(x, y, z, q, order, theta, leaf_capacity=32, forces=True, energy=Fals
                      C.c_double(theta), C.c_long(leaf_capacity), _ptr(fx), _ptr(fy), _ptr(fz),
                      C.byref(e) if energy else None)
     return (fx, fy, fz), (e.value if energy else None)
+
+
+# ----------------------------------------------------------------- reference behaviours
+class RefWorld:
+    """The reference's own per-agent code (lorentz.cc, cooling.cc,
+    annihilation.cc, coulomb_interaction.cc via oracle/_ref) on stand-in
+    agents: uid = index; each step runs the behaviours phase by phase over
+    agents in ascending uid order, with the stand-in Random replaying the CUDA
+    library's Philox draws (see ref_behaviours.cc)."""
+
+    def __init__(self, pos, vel, species, b0, voltage, z0, rho0, dt, cooling_scale=0.0, bath_temp=0.0,
+                 annihilation=False, contact_radius=0.0, probability=0.0, seed=0):
+        R = ref()
+        R.amkref_world_create.restype = C.c_void_p
+        R.amkref_world_behaviours.restype = C.c_long
+        R.amkref_world_behaviours.argtypes = [C.c_void_p, C.c_uint64, C.c_int, C.c_int, C.c_int]
+        R.amkref_world_destroy.argtypes = [C.c_void_p]
+        R.amkref_cooling_time.restype = C.c_double
+        pos = np.ascontiguousarray(pos, np.float64)
+        vel = np.ascontiguousarray(vel, np.float64)
+        self.n = len(pos)
+        x, y, z = (np.ascontiguousarray(pos[:, k]) for k in range(3))
+        vx, vy, vz = (np.ascontiguousarray(vel[:, k]) for k in range(3))
+        sp = np.ascontiguousarray(species, np.uint8)
+        self._h = R.amkref_world_create(
+            C.c_long(self.n), _ptr(x), _ptr(y), _ptr(z), _ptr(vx), _ptr(vy), _ptr(vz), _ptr(sp, _u8p),
+            C.c_double(b0), C.c_double(voltage), C.c_double(z0), C.c_double(rho0), C.c_double(dt),
+            C.c_double(cooling_scale), C.c_double(bath_temp), C.c_int(1 if annihilation else 0),
+            C.c_double(contact_radius), C.c_double(probability), C.c_uint32(seed))
+        self.h = C.c_void_p(self._h)
+
+    def close(self):
+        if self._h:
+            ref().amkref_world_destroy(self.h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_alive(self, alive):
+        a = np.ascontiguousarray(alive, np.uint8)
+        ref().amkref_world_set_alive(self.h, _ptr(a, _u8p))
+
+    def set_forces(self, fx, fy, fz):
+        fx, fy, fz = map(_f64, (fx, fy, fz))
+        ref().amkref_world_set_forces(self.h, _ptr(fx), _ptr(fy), _ptr(fz))
+
+    def coulomb_standard(self, cutoff):
+        ref().amkref_world_coulomb_standard(self.h, C.c_double(cutoff))
+
+    def behaviours(self, step, lorentz=True, cooling=True, annihilation=True):
+        return ref().amkref_world_behaviours(self.h, int(step), int(lorentz), int(cooling), int(annihilation))
+
+    def state(self):
+        n = self.n
+        arr = {k: np.zeros(n) for k in ("x", "y", "z", "vx", "vy", "vz", "fx", "fy", "fz")}
+        alive = np.zeros(n, np.uint8)
+        ref().amkref_world_get(self.h, *[_ptr(arr[k]) for k in ("x", "y", "z", "vx", "vy", "vz")],
+                               _ptr(alive, _u8p), *[_ptr(arr[k]) for k in ("fx", "fy", "fz")])
+        arr["alive"] = alive
+        return arr
+
+
+def ref_cooling_time(charge, mass, b_mag):
+    ref().amkref_cooling_time.restype = C.c_double
+    return ref().amkref_cooling_time(C.c_double(charge), C.c_double(mass), C.c_double(b_mag))
+
+
+def ref_is_antiparticle_pair(a, b):
+    return bool(ref().amkref_is_antiparticle_pair(int(a), int(b)))

@@ -10,6 +10,7 @@
 //             -> first word -> uniform in (0,1)
 #ifndef AMK_ORACLE_PHILOX_H_
 #define AMK_ORACLE_PHILOX_H_
+#include <cmath>
 #include <cstdint>
 
 namespace orc {
@@ -44,6 +45,28 @@ inline U32x4 Philox4x32(uint32_t k0, uint32_t k1, uint32_t c0, uint32_t c1, uint
 
 // Uniform in the open interval (0, 1) from one 32-bit word.
 inline double U01(uint32_t w) { return (static_cast<double>(w) + 0.5) * 2.3283064365386963e-10; }
+
+// The cooling stream's three N(0,1) draws for particle `id` at `step`:
+// Box-Muller on the four uniforms of one Philox block.
+inline void CoolingNormals(uint32_t seed, uint32_t id, uint64_t step, double* out3) {
+  const double two_pi = 2.0 * 3.14159265358979323846;
+  const U32x4 w = Philox4x32(seed, kTagCooling, id, static_cast<uint32_t>(step),
+                             static_cast<uint32_t>(step >> 32), 0u);
+  const double u1 = U01(w.v[0]), u2 = U01(w.v[1]);
+  const double u3 = U01(w.v[2]), u4 = U01(w.v[3]);
+  const double r1 = std::sqrt(-2.0 * std::log(u1));
+  const double r2 = std::sqrt(-2.0 * std::log(u3));
+  out3[0] = r1 * std::cos(two_pi * u2);
+  out3[1] = r1 * std::sin(two_pi * u2);
+  out3[2] = r2 * std::cos(two_pi * u4);
+}
+
+// The annihilation stream's uniform for the ordered pair owner -> partner.
+inline double AnnihilationUniform(uint32_t seed, uint32_t owner, uint32_t partner, uint64_t step) {
+  const U32x4 w = Philox4x32(seed, kTagAnnihilation, owner, partner, static_cast<uint32_t>(step),
+                             static_cast<uint32_t>(step >> 32));
+  return U01(w.v[0]);
+}
 
 }  // namespace orc
 #endif

@@ -15,6 +15,17 @@ Fixtures (all inputs seeded, all outputs from the reference's code):
                   theta 0) on the same cloud
   fmm_n4000_err.json  the reference's RMS relative force error against the
                   exact sum for p = 2, 4, 6 at theta 0.5 (N = 4,000 Gaussian)
+  readme_steps_ref.npz  the README-scale run (params of the README: cutoff
+                  1e-5 m, cooling at 4 K, annihilation 5e-6 m with p = 1,
+                  seed 42) stepped 40 times by the reference's own per-step
+                  code: ComputeStandardCoulombForces, then LorentzForce,
+                  CyclotronCooling and AnnihilationInteraction on every agent
+                  (coulomb_interaction.cc, lorentz.cc, cooling.cc,
+                  annihilation.cc via oracle/ref_behaviours.cc, whose Random
+                  stand-in replays the CUDA library's Philox draws); positions,
+                  velocities and alive flags after every step
+
+`python tests/golden/make_golden.py readme_steps` regenerates only the last.
 """
 import json
 import os
@@ -95,5 +106,29 @@ def main():
     print(json.dumps(err))
 
 
+def readme_steps(steps=40):
+    O.build(ref=True)
+    g = np.load(os.path.join(OUT, "readme_ic.npz"))
+    sp = g["species"]
+    dt = O.dt_for([1, 3], 1.0)
+    w = O.RefWorld(g["pos"], g["vel"], sp, b0=1.0, voltage=10.0, z0=0.01, rho0=0.01, dt=dt,
+                   cooling_scale=1.0, bath_temp=4.0, annihilation=True, contact_radius=5e-6,
+                   probability=1.0, seed=42)
+    out = {k: [] for k in ("x", "y", "z", "vx", "vy", "vz", "alive")}
+    for step in range(1, steps + 1):
+        w.coulomb_standard(1e-5)
+        w.behaviours(step)
+        st = w.state()
+        for k in out:
+            out[k].append(st[k])
+    np.savez_compressed(os.path.join(OUT, "readme_steps_ref.npz"), dt=dt,
+                        **{k: np.array(v) for k, v in out.items()})
+    print("readme_steps: alive after", steps, "steps:", int(out["alive"][-1].sum()))
+
+
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["readme_steps"]:
+        readme_steps()
+    else:
+        main()
+        readme_steps()

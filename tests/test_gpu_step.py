@@ -148,3 +148,57 @@ def test_readme_run_energy_and_population():
         assert np.isfinite(e1["total"])
         # annihilation removes kinetic energy; the total cannot grow much
         assert e1["total"] < e0["total"] * 1.05
+
+
+def test_readme_steps_match_the_reference_code_fixture():
+    # 40 full steps (cutoff forces, Boris push, cooling at 4 K, annihilation
+    # at 5e-6 m with p = 1) against the fixture the reference's own
+    # coulomb_interaction.cc / lorentz.cc / cooling.cc / annihilation.cc
+    # produced (tests/golden/make_golden.py): the annihilated set bit-exact
+    # every step, positions and velocities to 1e-9
+    ref = np.load(os.path.join(GOLD, "readme_steps_ref.npz"))
+    with amk.Simulation(readme_params()) as s:
+        s.init_particles()
+        for step in range(ref["x"].shape[0]):
+            s.step(1)
+            st = s.get_particles()
+            assert np.array_equal(st["alive"], ref["alive"][step]), step
+            for k in ("x", "y", "z", "vx", "vy", "vz"):
+                a, b = st[k], ref[k][step]
+                assert np.max(np.abs(a - b)) <= 1e-9 * np.max(np.abs(b)), (step, k)
+    assert ref["alive"][-1].sum() < 200
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference library not built")
+def test_push_cooling_annihilation_match_the_reference_world():
+    # a denser two-species cloud stepped by the library and by the
+    # reference's own per-agent code, same forces each step
+    n = 2400
+    rng = np.random.default_rng(21)
+    pos = rng.normal(0, 3e-5, (n, 3))
+    vel = rng.normal(0, 2e4, (n, 3))
+    sp = np.where(rng.random(n) < 0.5, 1, 3).astype(np.uint8)
+    p = readme_params(contact_radius=1.5e-6, annihilation_probability=0.5, cooling_scale=1e-8,
+                      bath_temperature=20.0, seed=5, cutoff_radius=4e-6)
+    w = O.RefWorld(pos, vel, sp, b0=p.b0, voltage=p.trap_voltage, z0=p.z0, rho0=p.rho0, dt=p.dt,
+                   cooling_scale=p.cooling_scale, bath_temp=p.bath_temperature, annihilation=True,
+                   contact_radius=p.contact_radius, probability=p.annihilation_probability, seed=p.seed)
+    with amk.Simulation(p) as s:
+        s.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
+        marked = 0
+        for step in range(1, 9):
+            s.coulomb_standard(p.cutoff_radius)
+            w.coulomb_standard(p.cutoff_radius)
+            f = s.get_forces()
+            r = w.state()
+            live = r["alive"].astype(bool)
+            for a, b in zip(f, (r["fx"], r["fy"], r["fz"])):
+                assert np.max(np.abs(a[live] - b[live])) <= 1e-10 * max(np.max(np.abs(b)), 1e-300)
+            s.push()
+            s.annihilate()
+            marked += w.behaviours(step)
+            st, r = s.get_particles(), w.state()
+            assert np.array_equal(st["alive"], r["alive"]), step
+            for k in ("x", "y", "z", "vx", "vy", "vz"):
+                assert np.max(np.abs(st[k] - r[k])) <= 1e-10 * np.max(np.abs(r[k])), (step, k)
+        assert marked > 0
