@@ -542,6 +542,16 @@ class Simulation:
         check(lib().amk_batch_info(self._h, C.byref(n), C.byref(u), C.byref(g)), "amk_batch_info")
         return {"instances": n.value, "work_units": u.value, "graphable": bool(g.value)}
 
+    # -- checkpoint / export
+    def checkpoint_save(self, path: str):
+        check(lib().amk_checkpoint_save(self._h, os.fsencode(path)), "amk_checkpoint_save")
+
+    def checkpoint_load(self, path: str):
+        check(lib().amk_checkpoint_load(self._h, os.fsencode(path)), "amk_checkpoint_load")
+
+    def export_vtk(self, path: str, binary: bool = True):
+        check(lib().amk_export_vtk(self._h, os.fsencode(path), 1 if binary else 0), "amk_export_vtk")
+
     # -- learned correction (MLP)
     def mlp_params(self):
         n = lib().amk_mlp_num_params()
@@ -677,3 +687,31 @@ def compute_barnes_hut_coulomb_forces(sim: Simulation, theta: float):
 def compute_fast_multipole_coulomb_forces(sim: Simulation, order: int, theta: float):
     """ComputeFastMultipoleCoulombForces(rm, order, theta), fast-multipole.h:73."""
     sim.coulomb_fmm(order, theta)
+
+
+def checkpoint_info(path: str):
+    """(particles, step, Params) of a checkpoint file; needs no GPU."""
+    n, st, p = C.c_long(), C.c_long(), Params()
+    check(lib().amk_checkpoint_info(os.fsencode(path), C.byref(n), C.byref(st), C.byref(p)),
+          "amk_checkpoint_info")
+    return n.value, st.value, p
+
+
+def write_vtu(path: str, x, y, z, species, vx=None, vy=None, vz=None, alive=None, ids=None, time=0.0,
+              binary=True):
+    """VTK XML UnstructuredGrid of host particle arrays (amk_write_vtu); no GPU."""
+    x, y, z = map(_f64, (x, y, z))
+    v = [None if a is None else _f64(a) for a in (vx, vy, vz)]
+    sp = np.ascontiguousarray(species, np.uint8)
+    al = None if alive is None else np.ascontiguousarray(alive, np.uint8)
+    ii = None if ids is None else np.ascontiguousarray(ids, np.uint32)
+    check(lib().amk_write_vtu(os.fsencode(path), len(x), _d(x), _d(y), _d(z), *[_d(a) for a in v],
+                              sp.ctypes.data_as(_u8p), None if al is None else al.ctypes.data_as(_u8p),
+                              None if ii is None else ii.ctypes.data_as(C.POINTER(C.c_uint32)),
+                              C.c_double(time), 1 if binary else 0), "amk_write_vtu")
+
+
+def write_pvd(path: str, files, times):
+    arr = (C.c_char_p * len(files))(*[os.fsencode(f) for f in files])
+    t = _f64(times)
+    check(lib().amk_write_pvd(os.fsencode(path), len(files), arr, _d(t)), "amk_write_pvd")

@@ -404,6 +404,36 @@ int amk_batch_energy(amk_ctx* ctx, int time_centre, amk_energy_out* out);
  * whether the batch can run as CUDA graphs. */
 int amk_batch_info(const amk_ctx* ctx, long* n_instances, long* work_units, int* graphable);
 
+/* ------------------------------------------------------------ checkpoint / export */
+/* Checkpoint/resume, in place of BioDynaMo's backup and restore of the
+ * simulation (the reference runs inside BioDynaMo, which provides them;
+ * bdm.toml:1-4). amk_checkpoint_save writes the context's parameters,
+ * step counter, Boris back-stagger flag, energy time-centring history,
+ * learned-correction state and network, the all-pairs Morton order and the
+ * full particle state (x, v, force slots, q, m, species, alive, ids) to
+ * `path` (written to path.tmp, then renamed), with an FNV-1a checksum;
+ * amk_checkpoint_load replaces the context's parameters and state with the
+ * file's, so the restored context continues bit for bit like the saved one.
+ * A context holding a batch is refused (AMK_ERR_STATE). Corrupt, truncated
+ * or foreign files: AMK_ERR_INVALID. amk_checkpoint_info reads a file's
+ * header (particles, step, parameters) without a GPU. */
+int amk_checkpoint_save(amk_ctx* ctx, const char* path);
+int amk_checkpoint_load(amk_ctx* ctx, const char* path);
+int amk_checkpoint_info(const char* path, long* n, long* step, amk_params* params);
+/* Headless particle export in place of BioDynaMo's ParaView export
+ * (bdm.toml:6-13: ChargedAntiparticle agents, additional data member
+ * species_id): a VTK XML UnstructuredGrid (.vtu) of the live particles as
+ * vertex cells, point data species_id (Int32), velocity (Float64 x 3) and
+ * id (UInt32), the simulated time (step * dt) as field data TimeValue;
+ * binary != 0 appends the arrays as raw little-endian data, 0 writes ASCII.
+ * amk_write_vtu does the same from host arrays (alive and ids may be NULL)
+ * without a GPU; amk_write_pvd writes a ParaView collection of n files. */
+int amk_export_vtk(amk_ctx* ctx, const char* path, int binary);
+int amk_write_vtu(const char* path, long n, const double* x, const double* y, const double* z,
+                  const double* vx, const double* vy, const double* vz, const uint8_t* species,
+                  const uint8_t* alive, const uint32_t* ids, double time, int binary);
+int amk_write_pvd(const char* path, long n, const char* const* files, const double* times);
+
 /* ------------------------------------------------------------ allocation-free */
 /* No counterpart in the reference. The cutoff Coulomb solver (same results
  * as amk_coulomb_standard / amk_solve_cutoff) for callers that cannot let a
