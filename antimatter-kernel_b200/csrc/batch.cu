@@ -647,10 +647,10 @@ int batch_annihilate(amk_ctx* c, Batch& B, bool sync) {
     AMK_TRY(B.reserve_contacts(static_cast<long>(m + m / 4 + 65536), n));
     AMK_CUDA_TRY(cudaMemsetAsync(B.contact_count(), 0, sizeof(unsigned long long), c->stream));
   }
-  match_kernel<<<1, 1024, 0, c->stream>>>(B.contacts.as<Contact>(), B.contact_cap, B.contact_count(),
-                                          B.best.as<unsigned long long>(), B.flags.as<uint8_t>(),
-                                          B.flags.as<uint8_t>() + n, c->alive.as<uint8_t>(), B.match_result());
-  AMK_TRY(check_launch(c, "match_kernel"));
+  unsigned long long* best = B.best.as<unsigned long long>();
+  AMK_TRY(queue_matching(c, c->stream, B.contacts.as<Contact>(), B.contact_cap, B.contact_count(), best, best + n,
+                         B.flags.as<uint8_t>(), B.flags.as<uint8_t>() + n, c->alive.as<uint8_t>(),
+                         reinterpret_cast<MatchState*>(best + 2 * n), B.match_result()));
   batch_overflow_kernel<<<1, 1, 0, c->stream>>>(B.contact_count(), B.contact_cap, B.overflow());
   AMK_TRY(check_launch(c, "batch_overflow_kernel"));
   return phase_end(c, AMK_PHASE_ANNIHILATION);
@@ -825,7 +825,7 @@ extern "C" int amk_batch_set(amk_ctx* c, int n_inst, const amk_params* params, c
   AMK_TRY(B->units.reserve(std::max<size_t>(1, hu.size()) * sizeof(int2)));
   AMK_TRY(B->counters.reserve(64));
   AMK_TRY(B->reserve_contacts(std::max<long>(65536, n / 8), n));
-  AMK_TRY(B->best.reserve(nn * sizeof(unsigned long long)));
+  AMK_TRY(B->best.reserve((2 * nn + sizeof(MatchState) / 8 + 1) * sizeof(unsigned long long)));  // two arrays + state
   AMK_TRY(B->keys.reserve(nn * sizeof(uint64_t)));
   AMK_TRY(B->vals.reserve(nn * sizeof(uint32_t)));
   AMK_TRY(B->skeys.reserve(nn * sizeof(uint64_t)));

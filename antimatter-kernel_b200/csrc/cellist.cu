@@ -354,13 +354,14 @@ int annihilate_view(amk_ctx* c, const View& v, const uint8_t* species, const uin
       continue;
     }
     if (m == 0) break;
-    unsigned long long* best = slot<unsigned long long>(c, kSlotAnnBest, static_cast<size_t>(v.n), &rc);
+    // two per-particle priority arrays, then the matching state
+    unsigned long long* best = slot<unsigned long long>(
+        c, kSlotAnnBest, 2 * static_cast<size_t>(v.n) + sizeof(MatchState) / 8 + 1, &rc);
     AMK_TRY(rc);
     uint8_t* flags = slot<uint8_t>(c, kSlotAuxState1, static_cast<size_t>(v.n) + static_cast<size_t>(m) + 16, &rc);
     AMK_TRY(rc);
-    match_kernel<<<1, 1024, 0, c->stream>>>(edges, static_cast<long>(m), nullptr, best, flags, flags + v.n, v.alive,
-                                            counters + 2);
-    AMK_TRY(check_launch(c, "match_kernel"));
+    AMK_TRY(queue_matching(c, c->stream, edges, static_cast<long>(m), nullptr, best, best + v.n, flags, flags + v.n,
+                           v.alive, reinterpret_cast<MatchState*>(best + 2 * v.n), counters + 2));
     unsigned long long res[2] = {0, 0};
     AMK_CUDA_TRY(cudaMemcpyAsync(res, counters + 2, sizeof(res), cudaMemcpyDeviceToHost, c->stream));
     AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));

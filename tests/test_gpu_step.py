@@ -202,3 +202,26 @@ def test_push_cooling_annihilation_match_the_reference_world():
             for k in ("x", "y", "z", "vx", "vy", "vz"):
                 assert np.max(np.abs(st[k] - r[k])) <= 1e-10 * np.max(np.abs(r[k])), (step, k)
         assert marked > 0
+
+
+@pytest.mark.parametrize("grid_min", [None, "1"])
+def test_annihilation_grid_matcher_bit_exact_vs_oracle(monkeypatch, grid_min):
+    # tens of thousands of contacts: the grid-wide matching rounds (and, with
+    # AMK_MATCH_GRID_MIN=1, the same rounds on every contact set, followed
+    # by the one-CTA finish) give the sequential greedy pass's set
+    if grid_min is not None:
+        monkeypatch.setenv("AMK_MATCH_GRID_MIN", grid_min)
+    n = 20000
+    rng = np.random.default_rng(31)
+    pos = rng.uniform(-5e-5, 5e-5, (n, 3))
+    sp = rng.choice(np.array([0, 1, 3, 4], np.uint8), n)
+    p = readme_params(annihilation_probability=0.7, contact_radius=3e-6, seed=3, coulomb_forces_enabled=0,
+                      populations={"positron": n // 2, "electron": n - n // 2})
+    with amk.Simulation(p) as s:
+        s.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], np.zeros(n), np.zeros(n), np.zeros(n), sp)
+        ref = oracle_state(pos, np.zeros((n, 3)), sp)
+        for step in (1, 2):
+            marked = s.annihilate()
+            mo = O.annihilation(ref, p.contact_radius, p.annihilation_probability, p.seed, 1)
+            assert marked == mo and (step == 2 or mo > 1000)
+            assert np.array_equal(s.get_particles()["alive"], ref["alive"])
