@@ -36,6 +36,7 @@ METHOD = {"standard": 0, "barnes-hut": 1, "barnes_hut": 1, "fast-multipole": 2,
 SPECIES = {"antiproton": 0, "positron": 1, "antihydrogen": 2, "electron": 3,
            "proton": 4, "antihelium": 5}
 
+CLOUD = {"uniform": 0, "gaussian": 1}
 PHASES = ["stage", "allpairs", "cutoff", "sort", "tree", "bh_walk", "fmm_up", "fmm_lists",
           "fmm_m2l", "fmm_down", "fmm_p2p", "mlp", "push", "annihilation", "energy", "fmm_m2l_products"]
 
@@ -334,6 +335,18 @@ class Simulation:
 
     def init_particles(self):
         check(lib().amk_init_particles(self._h), "amk_init_particles")
+
+    def init_particles_gpu(self, distribution: str = "uniform"):
+        """The context's cloud generated on the GPU ("uniform" ellipsoid or
+        "gaussian"); Philox draws, not the reference's std:: streams."""
+        check(lib().amk_init_particles_gpu(self._h, CLOUD[distribution]), "amk_init_particles_gpu")
+
+    def batch_init(self, params, distribution: str = "uniform"):
+        """Generates every instance's cloud on the GPU and sets the batch."""
+        arr = (Params * len(params))(*params)
+        check(lib().amk_batch_init_particles(self._h, len(params), arr, CLOUD[distribution]),
+              "amk_batch_init_particles")
+        self._batch_n = len(params)
 
     def num_particles(self) -> int:
         return int(lib().amk_num_particles(self._h))

@@ -179,6 +179,23 @@ int amk_set_charge_mass(amk_ctx* ctx, const double* charge, const double* mass);
  * std::mt19937(seed) per species) and loads it. */
 int amk_init_particles(amk_ctx* ctx);
 
+/* The reference's cloud generators restated on the GPU for large clouds and
+ * sweeps (penning_trap.cc:51-160): species in the reference's order,
+ * positions uniform in the ellipsoid of radii cloud_radii
+ * (AMK_CLOUD_UNIFORM_ELLIPSOID, the reference's shape) or Gaussian with
+ * those standard deviations (AMK_CLOUD_GAUSSIAN), Maxwellian velocities per
+ * species with the reference's drift removal and sqrt(n/(n-1)) rescale.
+ * Draws come from Philox keyed by (seed, particle index), not from the
+ * reference's std:: engines (amk_init_particles reproduces those), so the
+ * cloud is deterministic and independent of the GPU's scheduling.
+ * amk_batch_init_particles generates every instance of a sweep (instance
+ * i from params[i], each identical to the same instance generated alone)
+ * and sets the batch (amk_batch_set with the implied offsets). */
+#define AMK_CLOUD_UNIFORM_ELLIPSOID 0
+#define AMK_CLOUD_GAUSSIAN 1
+int amk_init_particles_gpu(amk_ctx* ctx, int distribution);
+int amk_batch_init_particles(amk_ctx* ctx, int n_inst, const amk_params* params, int distribution);
+
 /* Copies the state back. Any pointer may be NULL. alive[i] = 0 once
  * annihilated. */
 int amk_get_particles(amk_ctx* ctx, double* x, double* y, double* z, double* vx,
