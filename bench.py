@@ -28,9 +28,11 @@ error bar -- plus the FP64 Boris push, for whole steps on a bounded sample of
 the same cloud (its first 65,536 particles). Nothing of this repository's
 CUDA library is imported on that arm.
 
-Other workloads: ``direct65k`` (65,536-particle all-pairs run) and
+Other workloads: ``direct65k`` (65,536-particle all-pairs run),
 ``sweep512`` (the 512-instance batched sweep, partitioned across ranks by a
-cost model under torchrun).
+cost model under torchrun) and ``long4m`` (4,194,304 particles with cooling
+and annihilation, learned p = 2 with fallback against plain p = 6, FP64
+energy drift every 100 steps).
 
 Multi-GPU: a single instance does not shard (replicas only; ``value`` sums
 the replicas over the slowest rank's time); the sweep shards by instance.
@@ -969,9 +971,115 @@ def sweep_instances_numpy(n_inst, seed=2024):
     return out
 
 
+# ================================================================== long4m
+def long_params(learned, n_half=2097152):
+    """The long run at scale: 2 x n_half particles (positrons + antiprotons),
+    uniform ellipsoid 5e-4 x 5e-4 x 2e-3 m, 100 K, b0 = 5 T, U = 100 V,
+    z0 = rho0 = 0.02 m, cooling at 4 K with cooling_scale 10, annihilation at
+    1e-6 m with p = 1, FMM energies. learned: the p = 2 FMM plus the learned
+    correction with a direct-sum audit every 100 steps and plain p = 6 after
+    a failed audit; else plain p = 6."""
+    import amk
+    kw = dict(seed=42, b0=5.0, trap_voltage=100.0, z0=0.02, rho0=0.02, num_steps=10000,
+              populations={"positron": n_half, "antiproton": n_half},
+              temperatures={"positron": 100.0, "antiproton": 100.0}, cloud_radii=(5e-4, 5e-4, 2e-3),
+              bath_temperature=4.0, cooling_scale=10.0, cooling_enabled=1, coulomb_forces_enabled=1,
+              coulomb_method="fast-multipole", fast_multipole_order=6, fast_multipole_theta=0.5,
+              energy_method="fast-multipole", annihilation_enabled=1, contact_radius=1e-6,
+              annihilation_probability=1.0, fmm_learned=1 if learned else 0, learned_fallback_order=6,
+              learned_error_budget=ERROR_BUDGET, learned_audit_interval=100, learned_audit_samples=1024)
+    return amk.make_params(**kw)
+
+
+def long_run(sim, stream, steps, log_every):
+    """Steps in chunks of log_every, the FP64 total energy after each chunk
+    (outside the timed events); returns (ms, live particle-steps, drift rows)."""
+    import torch
+    e0 = sim.energy()
+    depth = E * 100.0  # the reference's drift scale: the trap depth e |U| (antimatter-kernel.cc:137-142)
+    rows = [{"step": 0, "total_J": e0["total"], "fractional_drift": 0.0, "alive": e0["num_active"]}]
+    ms, work, done = 0.0, 0.0, 0
+    while done < steps:
+        k = min(log_every, steps - done)
+        a0 = sim.num_alive()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        sim.step(k)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        ms += ev0.elapsed_time(ev1)
+        done += k
+        e = sim.energy()
+        work += 0.5 * (a0 + e["num_active"]) * k
+        rows.append({"step": done, "total_J": e["total"], "fractional_drift": (e["total"] - e0["total"]) / depth,
+                     "alive": e["num_active"]})
+    return ms, work, rows
+
+
+def run_long(args):
+    import torch
+    import amk
+    world, rank, local = dist_setup()
+    init_nccl(world, local)
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    n_half = args.long_n // 2
+    out = {}
+    for name, learned in (("learned p=2 + MLP, fallback p=6", True), ("plain p=6", False)):
+        sim = amk.Simulation(long_params(learned, n_half), device=local)
+        sim.init_particles_gpu("uniform")
+        stream = torch.cuda.ExternalStream(sim.stream(), device=device)
+        entry = {}
+        if learned:
+            t0 = time.perf_counter()
+            loss, samples = sim.fmm_train_correction(0.5, sample_leaves=4096, steps=2000, batch=4096, lr=1e-3)
+            entry["training"] = {"seconds": round(time.perf_counter() - t0, 2), "samples": samples,
+                                 "final_loss": loss}
+        sampler = ClockSampler(local)
+        sampler.start()
+        launches0 = sim.kernel_launches()
+        ms, work, rows = long_run(sim, stream, args.steps, args.log_every)
+        entry.update(value=work / (ms * 1e-3), ms_per_step=ms / args.steps, drift=rows,
+                     gpu_launches=sim.kernel_launches() - launches0, clocks=sampler.stop())
+        if learned:
+            st = sim.fmm_learned_state()
+            entry["learned_state"] = st
+        out[name] = entry
+        sim.close()
+    a, b = out["learned p=2 + MLP, fallback p=6"], out["plain p=6"]
+    gap = max(abs(x["fractional_drift"] - y["fractional_drift"]) for x, y in zip(a["drift"], b["drift"]))
+    if rank == 0:
+        line = {"metric": METRIC, "value": a["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": 0, "ms_per_step": a["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (GPU Philox uniform-ellipsoid cloud, seed 42)",
+                "config": {"workload": f"long run at scale: N={2 * n_half:,} ({n_half:,} e+ + {n_half:,} pbar), "
+                                       "uniform ellipsoid 5e-4 x 5e-4 x 2e-3 m, 100 K, b0=5 T, U=100 V, "
+                                       "z0=rho0=0.02 m, cooling (4 K, scale 10), annihilation (1e-6 m, p=1); "
+                                       f"{args.steps} of the 10,000 steps, FP64 total-energy drift every "
+                                       f"{args.log_every} steps, learned p=2 with p=6 fallback vs plain p=6",
+                           "n_particles": 2 * n_half, "log_every": args.log_every,
+                           "l2": "not flushed: state of 4 M particles exceeds L2",
+                           "parallelism": f"replicas x{world}"},
+                "runs": out, "max_drift_gap": gap, "gpu_launches": a["gpu_launches"], "clocks": a["clocks"],
+                "roofline": None, "cpu_baseline": None,
+                "e2e": None}
+        print(json.dumps(line), flush=True)
+    finish_dist(world)
+    return 0
+
+
+def run_reference_long(args):
+    world, rank, _ = dist_setup()
+    if rank == 0:
+        print(json.dumps({"impl": "reference", "unavailable": "the 4M long run is measured on the GPU arm only; "
+                                                             "the reference's CPU FMM takes minutes per step here"}))
+    return 0
+
+
 # ================================================================== main
 WORKLOADS = {"tree1m": (run_tree, run_reference_tree), "direct65k": (run_direct, run_reference_direct),
-             "sweep512": (run_sweep, run_reference_sweep)}
+             "sweep512": (run_sweep, run_reference_sweep), "long4m": (run_long, run_reference_long)}
 
 
 def main(argv=None):
@@ -998,6 +1106,8 @@ def main(argv=None):
     ap.add_argument("--instances", type=int, default=512, help="trap instances of the sweep")
     ap.add_argument("--tree-n", type=int, default=1 << 20, help="particles of the tree workload")
     ap.add_argument("--tree-methods", default="", help="comma-separated subset of the tree workload's methods")
+    ap.add_argument("--long-n", type=int, default=1 << 22, help="particles of the long run")
+    ap.add_argument("--log-every", type=int, default=100, help="steps between energy logs of the long run")
     args = ap.parse_args(argv)
     args.warmup = max(3, args.warmup)  # at least three untimed warm-up steps
     amk_fn, ref_fn = WORKLOADS[args.workload]
