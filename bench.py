@@ -261,7 +261,8 @@ def tree_config(n, world):
             "n_particles": n, "seed": 42,
             "methods": [name for name, _ in TREE_METHODS],
             "selection": "value = fastest method whose RMS relative force error vs the FP64 exact sum "
-                         "is <= 1e-5 (4,096 evenly spaced audited particles)",
+                         "is <= 1e-5 (4,096 evenly spaced audited particles); the table also holds the FMM "
+                         "order/theta/leaf the library's autotuner picks under that budget",
             "error_budget": ERROR_BUDGET,
             "l2": "flushed between timed steps by a 256 MiB write (outside the per-step events)",
             "parallelism": f"replicas x{world} (a single instance does not shard)"}
@@ -412,8 +413,12 @@ def run_tree(args):
     if not methods:
         raise SystemExit(f"--tree-methods: none of {[m[0] for m in TREE_METHODS]}")
 
+    overs = dict(TREE_METHODS)
+
     def new_sim(over):
-        sim = amk.Simulation(tree_params(n, over), device=local)
+        sim = amk.Simulation(tree_params(n, {k: v for k, v in over.items() if k != "leaf"}), device=local)
+        if "leaf" in over:
+            sim.set_leaf_sizes(fmm_leaf=over["leaf"])
         sim.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
         stream = torch.cuda.ExternalStream(sim.stream(), device=device)
         return sim, stream
@@ -426,10 +431,35 @@ def run_tree(args):
         if entry["meets_1e-5"] and (best is None or entry["value"] > results[best]["value"]):
             best = name
         sim.close()
+    if args.autotune:
+        # the FMM configuration (order 4..8, theta 0.5..0.35, leaf 16/32/64)
+        # the library's autotuner finds fastest within the budget
+        sim, stream = new_sim(overs[PLAIN_P6])
+        t0 = time.perf_counter()
+        try:
+            cands, ch = sim.autotune(ERROR_BUDGET, samples=args.audit_samples, flags=1 | 4)  # FMM only
+        except amk.AmkError:
+            cands, ch = [], -1
+        tune_s = time.perf_counter() - t0
+        sim.close()
+        if ch >= 0:
+            w = cands[ch]
+            name = f"fmm autotuned p={w['order']} theta={w['theta']} leaf={w['leaf']}"
+            overs[name] = dict(coulomb_method="fast-multipole", fast_multipole_order=w["order"],
+                               fast_multipole_theta=w["theta"], leaf=w["leaf"])
+            sim, stream = new_sim(overs[name])
+            entry = tree_method_entry(sim, name, overs[name], args, stream, Flusher(device, stream))
+            sim.close()
+            entry["autotune"] = {"seconds": round(tune_s, 1), "candidates": [
+                [c["order"], c["theta"], c["leaf"], round(c["ms"], 2), c["rms"]] for c in cands if c["ms"] > 0],
+                "columns": ["order", "theta", "leaf", "ms per force call", "rms"]}
+            results[name] = entry
+            if entry["meets_1e-5"] and (best is None or entry["value"] > results[best]["value"]):
+                best = name
 
     # ---- the chosen method: W untimed steps, exactly K timed steps
     name = best if best is not None else methods[0][0]
-    over = dict(TREE_METHODS)[name]
+    over = overs[name]
     sim, stream = new_sim(over)
     flusher = Flusher(device, stream)
     if over.get("fmm_learned"):
@@ -1099,6 +1129,8 @@ def main(argv=None):
                     help="particle pairs per step of the sweep workload's reference sample")
     ap.add_argument("--audit-samples", type=int, default=4096, help="particles audited against FP64")
     ap.add_argument("--method-steps", type=int, default=5, help="timed steps of each method in the table")
+    ap.add_argument("--autotune", type=int, default=1,
+                    help="tree workload: also time the FMM configuration the library's autotuner picks")
     ap.add_argument("--sweep-ratio", type=int, default=1,
                     help="tree workload: also measure the sweep's batched / one-at-a-time ratio")
     ap.add_argument("--sweep-steps", type=int, default=20, help="batched steps of the sweep ratio")
