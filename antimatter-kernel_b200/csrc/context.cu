@@ -525,6 +525,47 @@ extern "C" int amk_set_charge_mass(amk_ctx* c, const double* charge, const doubl
   return AMK_OK;
 }
 
+// Host arrays overwrite the force slots (the agents' coulomb_force_), the
+// stable ids that key the random streams, or the alive flags.
+extern "C" int amk_set_forces(amk_ctx* c, const double* fx, const double* fy, const double* fz) {
+  if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (c->n == 0) return AMK_OK;
+  if (!fx || !fy || !fz) return fail(AMK_ERR_INVALID, "amk_set_forces: null array");
+  const size_t nd = static_cast<size_t>(c->n) * sizeof(double);
+  AMK_CUDA_TRY(cudaMemcpyAsync(c->fx.ptr, fx, nd, cudaMemcpyHostToDevice, c->stream));
+  AMK_CUDA_TRY(cudaMemcpyAsync(c->fy.ptr, fy, nd, cudaMemcpyHostToDevice, c->stream));
+  AMK_CUDA_TRY(cudaMemcpyAsync(c->fz.ptr, fz, nd, cudaMemcpyHostToDevice, c->stream));
+  return AMK_OK;
+}
+
+extern "C" int amk_set_ids(amk_ctx* c, const uint32_t* ids) {
+  if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (c->n == 0) return AMK_OK;
+  if (!ids) return fail(AMK_ERR_INVALID, "amk_set_ids: null array");
+  AMK_CUDA_TRY(cudaMemcpyAsync(c->ids.ptr, ids, static_cast<size_t>(c->n) * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                               c->stream));
+  return AMK_OK;
+}
+
+extern "C" int amk_set_alive(amk_ctx* c, const uint8_t* alive) {
+  if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (c->n == 0) return AMK_OK;
+  if (!alive) return fail(AMK_ERR_INVALID, "amk_set_alive: null array");
+  AMK_CUDA_TRY(cudaMemcpyAsync(c->alive.ptr, alive, static_cast<size_t>(c->n), cudaMemcpyHostToDevice, c->stream));
+  c->stage_dirty = true;
+  return AMK_OK;
+}
+
+// Completed steps (the random streams' step is this + 1 on the next push)
+// and whether the velocities are already staggered to t - dt/2.
+extern "C" int amk_set_step_state(amk_ctx* c, long step, int staggered) {
+  if (!c) return fail(AMK_ERR_INVALID, "null context");
+  if (step < 0) return fail(AMK_ERR_INVALID, "amk_set_step_state: step < 0");
+  c->step = step;
+  c->staggered = staggered != 0;
+  return AMK_OK;
+}
+
 // Reference initial cloud, host side (penning_trap.cc:51-160). The streams are
 // the C++ standard engines the reference uses, so the cloud is bit-identical.
 extern "C" int amk_init_particles(amk_ctx* c) {

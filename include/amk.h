@@ -26,7 +26,7 @@
  *   AnnihilationInteraction::Run      src/interaction/annihilation.h:11-20
  *   ComputeTotalEnergy                src/analysis/energy_analysis.h:35
  *   PhysicsParams/InteractionParams/StochasticParams::LoadParams
- *                                     src/params/*_params.h
+ *                                     src/params/{physics,interaction,stochastic}_params.h
  */
 #ifndef AMK_H_
 #define AMK_H_
@@ -172,6 +172,19 @@ int amk_update_state(amk_ctx* ctx, const double* x, const double* y, const doubl
 /* Overrides per-particle charge and mass (ChargedAntiparticle::SetCharge /
  * SetMass). Either pointer may be NULL. */
 int amk_set_charge_mass(amk_ctx* ctx, const double* charge, const double* mass);
+
+/* Host arrays overwrite per-particle state of the context (n entries each):
+ * the Coulomb-force slots (ChargedAntiparticle::SetCoulombForce), the stable
+ * ids that key the cooling and annihilation random streams (creation order
+ * by default; an adapter passes its agents' uids), the alive flags
+ * (MarkAnnihilated). amk_set_step_state sets the completed-step counter
+ * (the next push and annihilation draw with step + 1) and whether the
+ * velocities are already staggered back by dt/2 (LorentzForce's per-agent
+ * flag, lorentz.h:34). */
+int amk_set_forces(amk_ctx* ctx, const double* fx, const double* fy, const double* fz);
+int amk_set_ids(amk_ctx* ctx, const uint32_t* ids);
+int amk_set_alive(amk_ctx* ctx, const uint8_t* alive);
+int amk_set_step_state(amk_ctx* ctx, long step, int staggered);
 
 /* Builds the reference's initial cloud from the context's parameters
  * (penning_trap.cc:51-160: uniform ellipsoid by rejection sampling with

@@ -1,9 +1,14 @@
 """The BioDynaMo drop-in adapter (antimatter-kernel_b200/adapter/
-amk_bdm_adapter.cc): the reference's three Coulomb drivers with their own
-signatures, compiled against stand-ins of BioDynaMo's agent and resource
-manager types and linked to libamk. Its forces on agents must match the
-reference's own drivers (and the FP64 cutoff oracle), annihilated agents
-must be left untouched and neutral agents get zero force under the FMM."""
+amk_bdm_adapter.cc, .h): the reference's Coulomb drivers, solver classes
+(BarnesHutTree, FastMultipoleSolver), behaviours (LorentzForce,
+CyclotronCooling, AnnihilationInteraction, run through the per-step
+standalone operation) and ComputeTotalEnergy with their own signatures,
+compiled against stand-ins of BioDynaMo's types (tests/bdm_stub) and linked
+to libamk. Forces on agents must match the reference's own drivers (and the
+FP64 cutoff oracle), annihilated agents must be left untouched and neutral
+agents get zero force under the FMM; the classes must match the reference's
+classes; the adapter's step loop must match the reference's own per-agent
+code run by the oracle's harness."""
 import ctypes as C
 import os
 import shutil
@@ -16,6 +21,7 @@ import oracle_lib as O
 from conftest import E, ROOT, gaussian_cloud, rel_errors
 
 ADAPTER = os.path.join(ROOT, "antimatter-kernel_b200", "adapter", "amk_bdm_adapter.cc")
+GOLD = os.path.join(ROOT, "tests", "golden")
 STUB = os.path.join(ROOT, "tests", "bdm_stub")
 LIBDIR = os.path.join(ROOT, "antimatter-kernel_b200")
 
@@ -26,7 +32,7 @@ def build_harness(out_dir):
         pytest.skip("no g++")
     out = os.path.join(out_dir, "libamk_adapter_harness.so")
     cmd = ["g++", "-std=c++17", "-O2", "-fPIC", "-shared", f"-I{STUB}", f"-I{os.path.join(ROOT, 'include')}",
-           ADAPTER, os.path.join(STUB, "harness.cc"), f"-L{LIBDIR}", "-lamk", f"-Wl,-rpath,{LIBDIR}", "-o", out]
+           f"-I{os.path.dirname(ADAPTER)}", ADAPTER, os.path.join(STUB, "harness.cc"), f"-L{LIBDIR}", "-lamk", f"-Wl,-rpath,{LIBDIR}", "-o", out]
     subprocess.run(cmd, check=True, capture_output=True)
     return out
 
@@ -49,6 +55,8 @@ def harness(tmp_path_factory):
     lib.harness_run.restype = C.c_int
 
     def run(method, x, y, z, q, annihilated, param, order=0):
+        if method == "lib":
+            return lib
         n = len(x)
         arrs = [np.ascontiguousarray(a, np.float64) for a in (x, y, z, q)]
         an = np.ascontiguousarray(annihilated, np.uint8)
@@ -98,3 +106,90 @@ def test_barnes_hut_and_fmm_drivers_match_the_reference_drivers(harness):
         assert np.max(rel) < tol, (name, np.max(rel))
         neutral = live & (q == 0)
         assert all(np.all(a[neutral] == 0.0) for a in f)
+
+
+@pytest.mark.gpu
+def test_solver_classes_match_the_reference_classes(harness):
+    lib = harness("lib", None, None, None, None, None, None)
+    dp = C.POINTER(C.c_double)
+    lib.harness_bh_class.restype = C.c_long
+    lib.harness_bh_class.argtypes = [C.c_long, dp, dp, dp, dp, C.c_double, C.c_long, dp, dp, C.c_double, C.c_double,
+                                     C.c_double, C.c_double, dp, dp]
+    lib.harness_fmm_class.argtypes = [C.c_long, dp, dp, dp, dp, C.c_int, C.c_double, dp, dp]
+    x, y, z, q = gaussian_cloud(3000, 5)
+    ptr = [np.ascontiguousarray(a).ctypes.data_as(dp) for a in (x, y, z, q)]
+    for theta in (0.0, 0.5):
+        f, phi, fe, pe = np.zeros(9000), np.zeros(3000), np.zeros(3), np.zeros(1)
+        point = (1e-5, -2e-5, 3e-5)
+        nn = lib.harness_bh_class(3000, *ptr, theta, 8, f.ctypes.data_as(dp), phi.ctypes.data_as(dp), *point,
+                                  2 * E, fe.ctypes.data_as(dp), pe.ctypes.data_as(dp))
+        assert nn > 0
+        if O.ref_available():
+            ref = O.ref_bh_forces(x, y, z, q, theta, 8)
+            rel, _ = rel_errors(f.reshape(-1, 3).T, ref)
+            assert np.max(rel) < 1e-10
+            rphi = O.ref_bh_potentials(x, y, z, q, theta, 8)
+            assert np.max(np.abs(phi - rphi)) <= 1e-10 * np.max(np.abs(rphi))
+            assert nn == len(O.ref_bh_tree(x, y, z, q, 8)[0])
+        if theta == 0.0:  # a point that is not a source: the exact sum
+            d = np.stack([point[0] - x, point[1] - y, point[2] - z])
+            r = np.sqrt((d ** 2).sum(0))
+            exact = 8.9875517923e9 * 2 * E * (q * d / r ** 3).sum(1)
+            assert np.max(np.abs(fe - exact)) <= 1e-10 * np.max(np.abs(exact))
+            assert abs(pe[0] - (q / r).sum()) <= 1e-10 * abs((q / r).sum())
+    f, e = np.zeros(9000), np.zeros(1)
+    assert lib.harness_fmm_class(3000, *ptr, 4, 0.5, f.ctypes.data_as(dp), e.ctypes.data_as(dp)) == 0
+    if O.ref_available():
+        (rx, ry, rz), re = O.ref_fmm(x, y, z, q, 4, 0.5, 32, forces=True, energy=True)
+        rel, _ = rel_errors(f.reshape(-1, 3).T, (rx, ry, rz))
+        assert np.max(rel) < 1e-9
+        assert abs(e[0] - re) <= 1e-10 * abs(re)
+    lib.harness_cooling_time.restype = C.c_double
+    lib.harness_cooling_time.argtypes = [C.c_double] * 3
+    assert lib.harness_cooling_time(E, 9.1093837015e-31, 1.0) == O.cooling_time(E, 9.1093837015e-31, 1.0)
+    assert [lib.harness_is_pair(a, b) for a, b in ((0, 4), (4, 0), (1, 3), (0, 1), (2, 2))] == [1, 1, 1, 0, 0]
+
+
+@pytest.mark.gpu
+def test_behaviour_steps_and_energy_match_the_reference_code(harness):
+    # the reference application's loop on the adapter (standard Coulomb
+    # driver, the three behaviours per agent, the per-step operation, the
+    # energy) against the reference's own coulomb_interaction.cc, lorentz.cc,
+    # cooling.cc and annihilation.cc (oracle/_ref, same Philox draws)
+    if not O.ref_available():
+        pytest.skip("reference library not built")
+    lib = harness("lib", None, None, None, None, None, None)
+    dp, u8 = C.POINTER(C.c_double), C.POINTER(C.c_uint8)
+    lib.harness_steps.argtypes = ([C.c_long] + [dp] * 6 + [u8, dp, dp, u8] + [C.c_double] * 9 +
+                                  [C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, dp])
+    g = np.load(os.path.join(GOLD, "readme_ic.npz"))
+    n = 200
+    rng = np.random.default_rng(4)
+    pos = g["pos"] * 0.4 + rng.normal(0, 1e-7, (n, 3))  # denser: contacts within 30 steps
+    vel = g["vel"].copy()
+    sp = g["species"]
+    m, q = O.species_props(sp)
+    trap = dict(b0=1.0, voltage=10.0, z0=0.01, rho0=0.01)
+    dt, steps, rc, contact = O.dt_for([1, 3], 1.0), 30, 1e-5, 4e-6
+    arr = [np.ascontiguousarray(pos[:, k]) for k in range(3)] + [np.ascontiguousarray(vel[:, k]) for k in range(3)]
+    alive = np.ones(n, np.uint8)
+    energy = np.zeros(8)
+    rc_ = lib.harness_steps(n, *[a.ctypes.data_as(dp) for a in arr], sp.ctypes.data_as(u8), q.ctypes.data_as(dp),
+                            m.ctypes.data_as(dp), alive.ctypes.data_as(u8), trap["b0"], trap["voltage"], trap["z0"],
+                            trap["rho0"], dt, rc, 1.0, 4.0, 1, contact, 1.0, 42, steps, energy.ctypes.data_as(dp))
+    assert rc_ == 0
+    w = O.RefWorld(pos, vel, sp, dt=dt, cooling_scale=1.0, bath_temp=4.0, annihilation=True,
+                   contact_radius=contact, probability=1.0, seed=42, **trap)
+    for step in range(1, steps + 1):
+        w.coulomb_standard(rc)
+        w.behaviours(step)
+    r = w.state()
+    assert np.array_equal(alive, r["alive"]) and alive.sum() < n
+    for a, k in zip(arr, ("x", "y", "z", "vx", "vy", "vz")):
+        assert np.max(np.abs(a - r[k])) <= 1e-9 * np.max(np.abs(r[k])), k
+    # the last two energies: raw, then time-centred with the first
+    st = dict(x=arr[0], y=arr[1], z=arr[2], vx=arr[3], vy=arr[4], vz=arr[5], q=q, m=m, alive=alive)
+    e_last = O.energy_standard(st, trap["voltage"], trap["z0"], trap["rho0"], rc)
+    assert abs(energy[4] - e_last["kinetic"]) <= 1e-12 * e_last["kinetic"]
+    assert energy[7] == e_last["num_active"]
+    assert abs(energy[5] - 0.5 * (energy[1] + e_last["trap_potential"])) <= 1e-12 * abs(e_last["trap_potential"])
