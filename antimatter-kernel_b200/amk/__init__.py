@@ -490,6 +490,11 @@ class Simulation:
         check(lib().amk_force_error(self._h, int(samples), C.byref(r), C.byref(m)), "amk_force_error")
         return r.value, m.value
 
+    def set_fmm_precision(self, mode: str = "fp64"):
+        """M2L class-product arithmetic: "fp64" (the reference's) or "tensor"
+        (split-BF16 tcgen05 products for orders 5-7)."""
+        check(lib().amk_set_fmm_precision(self._h, {"fp64": 0, "tensor": 1}[mode]), "amk_set_fmm_precision")
+
     def set_leaf_sizes(self, fmm_leaf=32, bh_leaf=8):
         check(lib().amk_set_leaf_sizes(self._h, int(fmm_leaf), int(bh_leaf)), "amk_set_leaf_sizes")
 

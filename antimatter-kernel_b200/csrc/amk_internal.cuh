@@ -259,6 +259,7 @@ struct amk_ctx {
   // leaf capacities of the context's own solver calls (the reference's 32 and
   // 8 unless amk_autotune or amk_set_leaf_sizes changed them)
   int fmm_leaf = 32;
+  int fmm_precision = 0;  // AMK_FMM_FP64 or AMK_FMM_TENSOR (M2L class products)
   int bh_leaf = 8;
   // learned FMM correction state
   bool learned_trained = false;

@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "amk_internal.cuh"
+#include "tcgen05.cuh"
 
 namespace amk {
 
@@ -841,13 +842,193 @@ m2l_class_mma_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter
   }
 }
 
+// Split-BF16 tensor-core form of the class product (FMM precision mode
+// AMK_FMM_TENSOR): the product Lh = A Mh of a class runs on the 5th-generation
+// tensor cores. A (the class matrix, rows g padded to 128, K = a padded to a
+// multiple of 16) and B (the tile's 128 rescaled source expansions, K-major)
+// are each split into three BF16 terms, x = x0 + x1 + x2 (24 significant
+// bits), and the six products x0y0 + x0y1 + x1y0 + x0y2 + x1y1 + x2y0
+// accumulate into one FP32 accumulator in tensor memory (tcgen05.mma, M = 128,
+// N = 128, K = 16, issued by one thread, completion through an mbarrier with
+// a bounded wait). The per-pair products are written as FP32 (n_m floats per
+// pair) and summed per target in FP64 by the same reduction as the FP64 path.
+// Relative error of a product: about 2^-22, far below the FMM's truncation
+// error at p >= 5.
+constexpr int kM2lTcN = 128;  // pairs per tensor-core tile (MMA N)
+constexpr int kM2lTcThreads = 256;
+constexpr long kM2lTcWaitLimit = 1L << 26;  // polls before an mbarrier wait gives up
+
+template <int P>
+struct M2lTc {
+  static constexpr int kNm = (P + 1) * (P + 2) * (P + 3) / 6;
+  static constexpr int kNd = (2 * P + 1) * (2 * P + 2) * (2 * P + 3) / 6;
+  static constexpr int kKp = 16 * ((kNm + 15) / 16);
+  static constexpr uint32_t kASplit = 128u * kKp * 2u;
+  static constexpr uint32_t kBSplit = static_cast<uint32_t>(kM2lTcN) * kKp * 2u;
+  static constexpr uint32_t kOffB = 3u * kASplit;
+  static constexpr uint32_t kOffD = kOffB + 3u * kBSplit;              // Ds [kNd] doubles
+  static constexpr uint32_t kOffRow = kOffD + 8u * kNd;                // rowf [128]
+  static constexpr uint32_t kOffCol = kOffRow + 8u * 128u;             // colf [kKp]
+  static constexpr uint32_t kOffPe = kOffCol + 8u * kKp;               // pair ids [kM2lUnitPairs]
+  static constexpr uint32_t kOffPs = kOffPe + 4u * kM2lUnitPairs;      // sources [kM2lUnitPairs]
+  static constexpr uint32_t kOffBar = kOffPs + 4u * kM2lUnitPairs;     // mbarrier, TMEM slot
+  static constexpr uint32_t kSmem = kOffBar + 32u;
+  static_assert(kNm <= 128, "the tensor-core class product covers n_m <= 128 (orders up to 7)");
+  static_assert(kSmem <= 227u * 1024u, "tensor-core class product shared memory");
+};
+
+__device__ __forceinline__ void split3_bf16(double v, __nv_bfloat16* t) {
+  const __nv_bfloat16 a0 = __double2bfloat16(v);
+  const double r1 = v - static_cast<double>(__bfloat162float(a0));
+  const __nv_bfloat16 a1 = __double2bfloat16(r1);
+  const double r2 = r1 - static_cast<double>(__bfloat162float(a1));
+  t[0] = a0;
+  t[1] = a1;
+  t[2] = __double2bfloat16(r2);
+}
+
+template <int P>
+__global__ void __launch_bounds__(kM2lTcThreads, 1)
+m2l_class_tc_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter,
+                    const int* __restrict__ unit_cls, const int* __restrict__ unit_pos,
+                    const int* __restrict__ cls_code, const int* __restrict__ cls_end,
+                    const int* __restrict__ perm, const int* __restrict__ src, const double* __restrict__ Mh,
+                    const double* __restrict__ table, const unsigned long long* __restrict__ keys, long e0,
+                    float* __restrict__ out, int* __restrict__ status) {
+  using S = M2lTc<P>;
+  constexpr int kNm = S::kNm, kKp = S::kKp, kN = kM2lTcN;
+  extern __shared__ __align__(1024) unsigned char tc_smem[];
+  unsigned char* a_img = tc_smem;
+  unsigned char* b_img = tc_smem + S::kOffB;
+  double* Ds = reinterpret_cast<double*>(tc_smem + S::kOffD);
+  double* rowf = reinterpret_cast<double*>(tc_smem + S::kOffRow);
+  double* colf = reinterpret_cast<double*>(tc_smem + S::kOffCol);
+  int* pe = reinterpret_cast<int*>(tc_smem + S::kOffPe);
+  int* ps = reinterpret_cast<int*>(tc_smem + S::kOffPs);
+  uint64_t* mbar = reinterpret_cast<uint64_t*>(tc_smem + S::kOffBar);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + S::kOffBar + 16);
+  __shared__ int s_unit;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc::smem_u32(mbar)));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(tmem_slot)),
+                 "r"(kN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tmem = *tmem_slot;
+  const uint32_t a_base = tc::smem_u32(a_img), b_base = tc::smem_u32(b_img), mbar_a = tc::smem_u32(mbar);
+  const uint32_t idesc = tc::make_idesc(kN);
+  uint32_t phase = 0;
+  bool failed = false;
+  for (;;) {
+    if (tid == 0) s_unit = atomicAdd(unit_counter, 1);
+    __syncthreads();  // also: the previous unit is done with the shared arrays
+    const int unit = s_unit;
+    if (unit >= n_units) break;
+    const int cls = unit_cls[unit], pos0 = unit_pos[unit];
+    const int np = min(kM2lUnitPairs, cls_end[cls] - pos0);
+    const int dd = m2l_key_dd(keys[cls_code[cls]]);
+    const int et = dd < 0 ? -dd : 0, es = dd > 0 ? dd : 0;  // log2(h_t / u), log2(h_s / u)
+    for (int k = tid; k < S::kNd; k += kM2lTcThreads) Ds[k] = table[static_cast<size_t>(cls) * S::kNd + k];
+    for (int g = tid; g < 128; g += kM2lTcThreads) rowf[g] = g < kNm ? ldexp(T.inv_fact[g], (T.multi[g].w + 1) * et) : 0.0;
+    for (int a = tid; a < kKp; a += kM2lTcThreads) colf[a] = a < kNm ? ldexp(1.0, T.multi[a].w * es) : 0.0;
+    for (int p = tid; p < np; p += kM2lTcThreads) {
+      const int e = perm[pos0 + p];
+      pe[p] = e;
+      ps[p] = src[e];
+    }
+    __syncthreads();
+    // A = class matrix, three BF16 splits
+    for (int x = tid; x < 128 * kKp; x += kM2lTcThreads) {
+      const int g = x / kKp, a = x - g * kKp;
+      const double v = (g < kNm && a < kNm) ? Ds[T.m2l_index_t[a * kNm + g]] * colf[a] : 0.0;
+      __nv_bfloat16 t[3];
+      split3_bf16(v, t);
+      const uint32_t o = tc::op_offset(g, a, 128);
+#pragma unroll
+      for (int q = 0; q < 3; ++q) *reinterpret_cast<__nv_bfloat16*>(a_img + q * S::kASplit + o) = t[q];
+    }
+    for (int tile0 = 0; tile0 < np && !failed; tile0 += kN) {
+      const int live = min(kN, np - tile0);
+      // B = the tile's rescaled source expansions ([pair][a]), three BF16 splits
+      for (int x = tid; x < kN * kKp; x += kM2lTcThreads) {
+        const int j = x / kKp, a = x - j * kKp;
+        const double v = (j < live && a < kNm) ? Mh[static_cast<size_t>(ps[tile0 + j]) * kNm + a] : 0.0;
+        __nv_bfloat16 t[3];
+        split3_bf16(v, t);
+        const uint32_t o = tc::op_offset(j, a, kN);
+#pragma unroll
+        for (int q = 0; q < 3; ++q) *reinterpret_cast<__nv_bfloat16*>(b_img + q * S::kBSplit + o) = t[q];
+      }
+      tc::fence_proxy_async();
+      tc::fence_before();
+      __syncthreads();
+      if (tid == 0) {
+        tc::fence_after();
+        constexpr int kCombo[6][2] = {{2, 0}, {1, 1}, {0, 2}, {1, 0}, {0, 1}, {0, 0}};  // small terms first
+        int first = 1;
+        for (int st = 0; st < kKp / 16; ++st)
+#pragma unroll
+          for (int c = 0; c < 6; ++c) {
+            const uint64_t ad = tc::make_sdesc(a_base + kCombo[c][0] * S::kASplit + st * 128 * 32);
+            const uint64_t bd = tc::make_sdesc(b_base + kCombo[c][1] * S::kBSplit + st * kN * 32);
+            tc::mma_bf16(tmem, ad, bd, idesc, first ? 0 : 1);
+            first = 0;
+          }
+        tc::mma_commit(mbar_a);
+      }
+      long spins = 0;
+      bool ok = true;
+      while (!tc::mbar_try_wait(mbar_a, phase)) {
+        if (++spins > kM2lTcWaitLimit) {
+          ok = false;
+          break;
+        }
+      }
+      phase ^= 1u;
+      tc::fence_after();
+      if (!__syncthreads_and(ok)) {
+        failed = true;
+        break;
+      }
+      // epilogue: warp w (< 4) holds accumulator rows g = 32 w + lane
+      if (warp < 4) {
+        const int g = 32 * warp + lane;
+        const double rf = rowf[g];
+        for (int c0 = 0; c0 < kN; c0 += 32) {
+          float v[32];
+          tc::tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + c0, v);
+          if (g < kNm)
+            for (int j = 0; j < 32 && c0 + j < live; ++j)
+              out[static_cast<size_t>(pe[tile0 + c0 + j] - e0) * kNm + g] = static_cast<float>(v[j] * rf);
+        }
+      }
+      tc::fence_before();
+      __syncthreads();  // accumulator read out before the next tile's products
+      tc::fence_after();
+    }
+    if (failed) break;
+  }
+  if (failed && tid == 0) atomicExch(status, 1);
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kN));
+}
+
 // Pairs outside the classes: a warp per pair (persistent blocks), the
 // derivative tensor by the recurrence, the product through the transposed
 // index map staged once per block, written in the rescaled form
 // Lh = h_t^{|g|+1} L.
+template <typename OutT>
 __global__ void __launch_bounds__(32 * kFmmWarps)
 m2l_pair_kernel(const Octree t, FmmDevTables T, const int* __restrict__ list, int n, const int* __restrict__ tgt,
-                const int* __restrict__ src, const double* __restrict__ M, long e0, double* __restrict__ out) {
+                const int* __restrict__ src, const double* __restrict__ M, long e0, OutT* __restrict__ out) {
   extern __shared__ __align__(16) unsigned char pair_smem[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nm = T.n_m;
   double* D = reinterpret_cast<double*>(pair_smem) + static_cast<size_t>(w) * (T.n_d + nm);
@@ -867,7 +1048,7 @@ m2l_pair_kernel(const Octree t, FmmDevTables T, const int* __restrict__ list, in
       for (int a = 0; a < nm; ++a) s += Ms[a] * D[idx[a * nm + g]];
       double f = T.inv_fact[g];
       for (int d = 0; d <= T.multi[g].w; ++d) f *= tc.w;
-      out[static_cast<size_t>(e - e0) * nm + g] = s * f;
+      out[static_cast<size_t>(e - e0) * nm + g] = static_cast<OutT>(s * f);
     }
     __syncwarp();
   }
@@ -876,10 +1057,10 @@ m2l_pair_kernel(const Octree t, FmmDevTables T, const int* __restrict__ list, in
 // L(t) += h_t^{-|g|-1} sum over the target's pairs in [e0, e1) in pair order;
 // a warp per target, lanes over coefficients (R rows of 32), four pairs'
 // rows in flight.
-template <int R>
+template <int R, typename InT>
 __global__ void __launch_bounds__(256)
 m2l_reduce_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, const int* __restrict__ count,
-                  int t_first, int n_targets, long e0, long e1, const double* __restrict__ out,
+                  int t_first, int n_targets, long e0, long e1, const InT* __restrict__ out,
                   double* __restrict__ L) {
   constexpr int kU = 4;
   const int lane = threadIdx.x & 31;
@@ -891,7 +1072,7 @@ m2l_reduce_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, c
   double s[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) s[r] = 0.0;
-  const double* o = out + static_cast<size_t>(b - e0) * nm;
+  const InT* o = out + static_cast<size_t>(b - e0) * nm;
   long e = b;
   for (; e + kU <= end; e += kU, o += kU * nm) {
     double v[kU][R];
@@ -924,25 +1105,26 @@ m2l_reduce_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, c
   }
 }
 
+template <typename InT>
 int m2l_reduce(amk_ctx* c, cudaStream_t stream, const Octree& t, const FmmDevTables& T, const int* off,
-               const int* count, int t_first, int n_targets, long e0, long e1, const double* out, double* L) {
+               const int* count, int t_first, int n_targets, long e0, long e1, const InT* out, double* L) {
   const unsigned grid = static_cast<unsigned>((n_targets + 7) / 8);
   switch ((T.n_m + 31) / 32) {
     case 1:
-      m2l_reduce_kernel<1><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
+      m2l_reduce_kernel<1, InT><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
       break;
     case 2:
-      m2l_reduce_kernel<2><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
+      m2l_reduce_kernel<2, InT><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
       break;
     case 3:
-      m2l_reduce_kernel<3><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
+      m2l_reduce_kernel<3, InT><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
       break;
     case 4:
-      m2l_reduce_kernel<4><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
+      m2l_reduce_kernel<4, InT><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
       break;
     default:
       static_assert((kMaxNm + 31) / 32 == 6, "rows per lane");
-      m2l_reduce_kernel<6><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
+      m2l_reduce_kernel<6, InT><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
       break;
   }
   return check_launch(c, "m2l_reduce_kernel");
@@ -987,6 +1169,47 @@ int class_product(amk_ctx* c, int order, const FmmDevTables& T, int n_units, int
       return fail(AMK_ERR_INVALID, "FMM order %d outside [1, %d]", order, kMaxOrder);
   }
 #undef AMK_M2L_CASE
+}
+
+template <int P>
+int launch_class_tc(amk_ctx* c, const FmmDevTables& T, int n_units, int* unit_counter, const int* unit_cls,
+                    const int* unit_pos, const int* cls_code, const int* cls_end, const int* perm, const int* src,
+                    const double* Mh, const double* table, const unsigned long long* keys, long e0, float* out,
+                    int* status) {
+  const size_t smem = M2lTc<P>::kSmem;
+  AMK_CUDA_TRY(cudaFuncSetAttribute(m2l_class_tc_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(smem)));
+  int sms = 0;
+  AMK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+  const int grid = std::max(1, std::min(n_units, sms));  // one CTA per SM (shared memory and TMEM)
+  AMK_CUDA_TRY(cudaMemsetAsync(unit_counter, 0, sizeof(int), c->stream));
+  m2l_class_tc_kernel<P><<<grid, kM2lTcThreads, smem, c->stream>>>(T, n_units, unit_counter, unit_cls, unit_pos,
+                                                                   cls_code, cls_end, perm, src, Mh, table, keys, e0,
+                                                                   out, status);
+  return check_launch(c, "m2l_class_tc_kernel");
+}
+
+// Orders the tensor-core class product covers (n_m <= 128; below p = 5 the
+// FP64 products are already cheap next to the rest of the evaluation).
+inline bool tc_order(int order) { return order >= 5 && order <= 7; }
+
+int class_tc(amk_ctx* c, int order, const FmmDevTables& T, int n_units, int* unit_counter, const int* unit_cls,
+             const int* unit_pos, const int* cls_code, const int* cls_end, const int* perm, const int* src,
+             const double* Mh, const double* table, const unsigned long long* keys, long e0, float* out,
+             int* status) {
+  switch (order) {
+    case 5:
+      return launch_class_tc<5>(c, T, n_units, unit_counter, unit_cls, unit_pos, cls_code, cls_end, perm, src, Mh,
+                                table, keys, e0, out, status);
+    case 6:
+      return launch_class_tc<6>(c, T, n_units, unit_counter, unit_cls, unit_pos, cls_code, cls_end, perm, src, Mh,
+                                table, keys, e0, out, status);
+    case 7:
+      return launch_class_tc<7>(c, T, n_units, unit_counter, unit_cls, unit_pos, cls_code, cls_end, perm, src, Mh,
+                                table, keys, e0, out, status);
+    default:
+      return fail(AMK_ERR_INVALID, "no tensor-core class product for order %d", order);
+  }
 }
 
 // Class reach; AMK_FMM_M2L_REACH narrows it, which sends the pairs beyond it
@@ -1059,16 +1282,21 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
   AMK_TRY(rc);
   int* unit_pos = slot<int>(c, kSlotM2lTilePos, max_units, &rc);
   AMK_TRY(rc);
+  // the tensor-core products (split BF16) write FP32 per-pair products
+  const bool tc = c->fmm_precision == AMK_FMM_TENSOR && tc_order(order);
+  const size_t esz = tc ? sizeof(float) : sizeof(double);
+  int* tc_status = counters + 6;
+  if (tc) AMK_CUDA_TRY(cudaMemsetAsync(tc_status, 0, sizeof(int), c->stream));
   const int n_buf = n_m2l > cap ? 2 : 1;
   for (int i = 0; i < n_buf; ++i)
-    AMK_TRY(f->m2l_out[i].reserve(static_cast<size_t>(std::min(cap, n_m2l)) * T.n_m * sizeof(double)));
+    AMK_TRY(f->m2l_out[i].reserve(static_cast<size_t>(std::min(cap, n_m2l)) * T.n_m * esz));
   int chunk = 0;
   for (long e0 = 0; e0 < n_m2l; e0 += cap, ++chunk) {
     const long e1 = std::min(n_m2l, e0 + cap), ne = e1 - e0;
     const int buf = chunk & 1;
-    double* out = f->m2l_out[buf].as<double>();
+    void* out = f->m2l_out[buf].ptr;
     AMK_CUDA_TRY(cudaMemsetAsync(hist, 0, n_codes * sizeof(int), c->stream));
-    AMK_CUDA_TRY(cudaMemsetAsync(counters, 0, 8 * sizeof(int), c->stream));
+    AMK_CUDA_TRY(cudaMemsetAsync(counters, 0, 6 * sizeof(int), c->stream));  // [6]: the tensor-core status
     const unsigned ge = static_cast<unsigned>((ne + 255) / 256), gc = static_cast<unsigned>((n_codes + 255) / 256);
     m2l_histogram_kernel<<<ge, 256, 0, c->stream>>>(codes, e0, e1, hist, fallback, counters + 3);
     AMK_TRY(check_launch(c, "m2l_histogram_kernel"));
@@ -1103,30 +1331,50 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
                                                                                               keys, table);
       AMK_TRY(check_launch(c, "m2l_table_kernel"));
       AMK_TRY(phase_begin(c, AMK_PHASE_FMM_M2L_PRODUCTS));
-      AMK_TRY(class_product(c, order, T, n_units, counters + 4, unit_cls, unit_pos, cls_code, cls_end, perm, gm.src,
-                            Mh, table, keys, e0, out));
+      if (tc)
+        AMK_TRY(class_tc(c, order, T, n_units, counters + 4, unit_cls, unit_pos, cls_code, cls_end, perm, gm.src, Mh,
+                         table, keys, e0, static_cast<float*>(out), tc_status));
+      else
+        AMK_TRY(class_product(c, order, T, n_units, counters + 4, unit_cls, unit_pos, cls_code, cls_end, perm,
+                              gm.src, Mh, table, keys, e0, static_cast<double*>(out)));
       AMK_TRY(phase_end(c, AMK_PHASE_FMM_M2L_PRODUCTS));
     }
     if (n_fb > 0) {
       const size_t psm = static_cast<size_t>(kFmmWarps) * (T.n_d + T.n_m) * sizeof(double) +
                          static_cast<size_t>(T.n_m) * T.n_m * sizeof(short);
-      AMK_CUDA_TRY(cudaFuncSetAttribute(m2l_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(psm)));
-      int per_sm = 0, sms = 0;
-      AMK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, m2l_pair_kernel, 32 * kFmmWarps, psm));
-      AMK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-      const int grid = std::max(1, std::min((n_fb + kFmmWarps - 1) / kFmmWarps, std::max(1, per_sm) * sms));
-      m2l_pair_kernel<<<grid, 32 * kFmmWarps, psm, c->stream>>>(t, T, fallback, n_fb, tgt, gm.src, M, e0, out);
-      AMK_TRY(check_launch(c, "m2l_pair_kernel"));
+      auto launch_pairs = [&](auto kernel, auto* dst) -> int {
+        AMK_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(psm)));
+        int per_sm = 0, sms = 0;
+        AMK_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 32 * kFmmWarps, psm));
+        AMK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+        const int grid = std::max(1, std::min((n_fb + kFmmWarps - 1) / kFmmWarps, std::max(1, per_sm) * sms));
+        kernel<<<grid, 32 * kFmmWarps, psm, c->stream>>>(t, T, fallback, n_fb, tgt, gm.src, M, e0, dst);
+        return check_launch(c, "m2l_pair_kernel");
+      };
+      if (tc)
+        AMK_TRY(launch_pairs(m2l_pair_kernel<float>, static_cast<float*>(out)));
+      else
+        AMK_TRY(launch_pairs(m2l_pair_kernel<double>, static_cast<double*>(out)));
     }
     // per-target sums on the side stream, in chunk order
     AMK_CUDA_TRY(cudaEventRecord(f->products_done[buf], c->stream));
     AMK_CUDA_TRY(cudaStreamWaitEvent(f->side, f->products_done[buf], 0));
-    AMK_TRY(m2l_reduce(c, f->side, t, T, gm.off, gm.count, tr[0], tr[1] - tr[0] + 1, e0, e1, out, L));
+    if (tc)
+      AMK_TRY(m2l_reduce(c, f->side, t, T, gm.off, gm.count, tr[0], tr[1] - tr[0] + 1, e0, e1,
+                         static_cast<const float*>(out), L));
+    else
+      AMK_TRY(m2l_reduce(c, f->side, t, T, gm.off, gm.count, tr[0], tr[1] - tr[0] + 1, e0, e1,
+                         static_cast<const double*>(out), L));
     AMK_CUDA_TRY(cudaEventRecord(f->sums_done[buf], f->side));
   }
   // the context stream resumes after the last sums
   AMK_CUDA_TRY(cudaStreamWaitEvent(c->stream, f->sums_done[(chunk - 1) & 1], 0));
+  if (tc) {  // a tensor-core wait that timed out leaves its flag
+    int st = 0;
+    AMK_CUDA_TRY(cudaMemcpyAsync(&st, tc_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (st) return fail(AMK_ERR_TIMEOUT, "tensor-core M2L product: an mbarrier wait timed out");
+  }
   return AMK_OK;
 }
 
@@ -1860,6 +2108,15 @@ int fmm_audit(amk_ctx* c, const View& v, int order, double theta, bool learned, 
 }
 
 }  // namespace amk
+
+extern "C" int amk_set_fmm_precision(amk_ctx* c, int mode) {
+  if (!c) return amk::fail(AMK_ERR_INVALID, "null context");
+  if (mode != AMK_FMM_FP64 && mode != AMK_FMM_TENSOR) return amk::fail(AMK_ERR_INVALID, "unknown FMM precision %d", mode);
+  c->fmm_precision = mode;
+  return AMK_OK;
+}
+
+extern "C" int amk_get_fmm_precision(const amk_ctx* c) { return c ? c->fmm_precision : AMK_ERR_INVALID; }
 
 // Counts of the last FMM evaluation on this context: out[0] cells, [1] leaves,
 // [2] M2L pairs, [3] P2P leaf pairs, [4] P2P particle pairs, [5] depth,

@@ -226,6 +226,10 @@ TREE_METHODS = [
     ("fmm p=6 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=6, fast_multipole_theta=0.5)),
     ("fmm p=7 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=7, fast_multipole_theta=0.5)),
     ("fmm p=8 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=8, fast_multipole_theta=0.5)),
+    ("fmm p=6 theta=0.5 tensor", dict(coulomb_method="fast-multipole", fast_multipole_order=6, fast_multipole_theta=0.5,
+                                      precision="tensor")),
+    ("fmm p=7 theta=0.5 tensor", dict(coulomb_method="fast-multipole", fast_multipole_order=7, fast_multipole_theta=0.5,
+                                      precision="tensor")),
     ("learned p=2 + MLP theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=2,
                                         fast_multipole_theta=0.5, fmm_learned=1, learned_audit_interval=0)),
 ]
@@ -356,6 +360,20 @@ def tree_method_entry(sim, name, over, args, stream, flusher):
     return entry
 
 
+def measured_peak(key, fallback):
+    """A figure of the pool's measured-peaks file (MEASURED_PEAKS.json beside
+    this script) and where it came from, else the stated fallback."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            v = json.load(fh).get(key)
+        if isinstance(v, (int, float)) and v > 0:
+            return float(v), f"of measured ({key} in MEASURED_PEAKS.json)"
+    except (OSError, ValueError):
+        pass
+    return fallback, f"of fallback ({fallback:g}; no {key} in a MEASURED_PEAKS.json)"
+
+
 def tree_roofline(sim, over, n):
     if over["coulomb_method"] == "allpairs":
         sim.set_profiling(True)
@@ -383,8 +401,18 @@ def tree_roofline(sim, over, n):
         st = sim.fmm_stats()
         p_ = st["order"]
         nm = (p_ + 1) * (p_ + 2) * (p_ + 3) // 6
-        peak = sim.measure_fp64_peak()
         achieved = 2.0 * nm * nm * st["m2l_class_pairs"] / (prod_ms * 1e-3) / 1e12
+        if over.get("precision") == "tensor" and 5 <= p_ <= 7:
+            bf16, src = measured_peak("bf16_tflops", 1590.0)
+            return {"bound": "tensor (split BF16)", "kernel": f"m2l_class_tc_kernel<{p_}>", "achieved": achieved,
+                    "peak": bf16 / 6.0, "unit": "TFLOP/s", "frac": achieved / (bf16 / 6.0), "traffic": None,
+                    "peak_source": f"dense BF16 tensor peak {src}, divided by the six BF16 products each "
+                                   "split-BF16 product issues",
+                    "flop_convention": f"2 n_m^2 flop (n_m = {nm}) per M2L pair evaluated as a class product "
+                                       f"({st['m2l_class_pairs']:,} of {st['m2l_pairs']:,} pairs)",
+                    "avg_launch_ms": prod_ms / max(1, prod_n), "launches_per_step": prod_n,
+                    "m2l_phase_ms": ph["fmm_m2l"][0], "classes": st["m2l_classes"]}
+        peak = sim.measure_fp64_peak()
         traffic = FMM_PRODUCT_TRAFFIC.get(p_)
         return {"bound": "fp64 tensor", "kernel": f"m2l_class_mma_kernel<{p_}>", "achieved": achieved,
                 "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
@@ -416,9 +444,12 @@ def run_tree(args):
     overs = dict(TREE_METHODS)
 
     def new_sim(over):
-        sim = amk.Simulation(tree_params(n, {k: v for k, v in over.items() if k != "leaf"}), device=local)
+        sim = amk.Simulation(tree_params(n, {k: v for k, v in over.items() if k not in ("leaf", "precision")}),
+                             device=local)
         if "leaf" in over:
             sim.set_leaf_sizes(fmm_leaf=over["leaf"])
+        if "precision" in over:
+            sim.set_fmm_precision(over["precision"])
         sim.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
         stream = torch.cuda.ExternalStream(sim.stream(), device=device)
         return sim, stream
@@ -432,9 +463,10 @@ def run_tree(args):
             best = name
         sim.close()
     if args.autotune:
-        # the FMM configuration (order 4..8, theta 0.5..0.35, leaf 16/32/64)
-        # the library's autotuner finds fastest within the budget
-        sim, stream = new_sim(overs[PLAIN_P6])
+        # the FMM configuration (order 4..8, theta 0.5..0.35, leaf 16/32/64;
+        # tensor-core M2L products for orders 5-7) the library's autotuner
+        # finds fastest within the budget
+        sim, stream = new_sim(dict(overs[PLAIN_P6], precision="tensor"))
         t0 = time.perf_counter()
         try:
             cands, ch = sim.autotune(ERROR_BUDGET, samples=args.audit_samples, flags=1 | 4)  # FMM only
@@ -445,8 +477,9 @@ def run_tree(args):
         if ch >= 0:
             w = cands[ch]
             name = f"fmm autotuned p={w['order']} theta={w['theta']} leaf={w['leaf']}"
+            name += " tensor" if 5 <= w["order"] <= 7 else ""
             overs[name] = dict(coulomb_method="fast-multipole", fast_multipole_order=w["order"],
-                               fast_multipole_theta=w["theta"], leaf=w["leaf"])
+                               fast_multipole_theta=w["theta"], leaf=w["leaf"], precision="tensor")
             sim, stream = new_sim(overs[name])
             entry = tree_method_entry(sim, name, overs[name], args, stream, Flusher(device, stream))
             sim.close()

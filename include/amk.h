@@ -303,6 +303,20 @@ long amk_bh_tree_dump(amk_ctx* ctx, long n, const double* x, const double* y, co
                       const double* q, long leaf_capacity, long max_nodes, double* node_f64,
                       long* node_i64);
 
+/* Arithmetic of the FMM's M2L class products on this context.
+ * AMK_FMM_FP64 (default): FP64 tensor cores (mma.m8n8k4) and FP64 per-pair
+ * products -- the reference's arithmetic, results within 1e-9 of the
+ * reference's FastMultipoleSolver. AMK_FMM_TENSOR: for orders 5 to 7 the
+ * products run on the 5th-generation tensor cores with split-BF16 operands
+ * (three BF16 terms per operand, six products, FP32 accumulation in tensor
+ * memory) and FP32 per-pair products summed in FP64; relative error of an
+ * M2L term about 2^-22, below the truncation error of those orders. Every
+ * other part of the evaluation is unchanged. */
+#define AMK_FMM_FP64 0
+#define AMK_FMM_TENSOR 1
+int amk_set_fmm_precision(amk_ctx* ctx, int mode);
+int amk_get_fmm_precision(const amk_ctx* ctx);
+
 /* Interaction counts of the context's last FMM evaluation: out[0] cells,
  * [1] leaves, [2] M2L pairs, [3] P2P leaf pairs, [4] P2P particle pairs,
  * [5] tree depth, [6] sources, [7] order (the quantities the reference's

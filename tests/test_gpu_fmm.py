@@ -156,3 +156,41 @@ def test_fmm_off_origin_cloud_at_order_8(sim):
     (rx, ry, rz), _ = O.ref_fmm(x, y, z, q, 8, 0.5, 32)
     rel, _ = rel_errors(f, (rx, ry, rz))
     assert np.max(rel) < FMM_TOL, np.max(rel)
+
+
+@pytest.mark.parametrize("order", [5, 6, 7])
+def test_tensor_core_products_match_the_fp64_path(order):
+    # split-BF16 tcgen05 class products: the forces stay within 2e-6 of the
+    # FP64 products and the error against the exact sum is unchanged
+    import amk
+    x, y, z, q = gaussian_cloud(20000, 45, mixed=False)
+    exact = O.allpairs(x, y, z, q)
+    with amk.Simulation() as s:
+        ref = s.solve_fmm(x, y, z, q, order, 0.5)
+        s.set_fmm_precision("tensor")
+        got = s.solve_fmm(x, y, z, q, order, 0.5)
+        st = s.fmm_stats()
+        assert st["m2l_class_pairs"] > 0
+        again = s.solve_fmm(x, y, z, q, order, 0.5)
+    assert all(np.array_equal(a, b) for a, b in zip(got, again))  # run-to-run deterministic
+    rel, _ = rel_errors(got, ref)
+    assert np.max(rel) < 2e-6, np.max(rel)
+    e_ref = np.sqrt(np.mean(rel_errors(ref, exact)[0] ** 2))
+    e_tc = np.sqrt(np.mean(rel_errors(got, exact)[0] ** 2))
+    assert e_tc <= 1.02 * e_ref + 1e-7, (e_tc, e_ref)
+
+
+def test_tensor_core_products_with_per_pair_path_and_chunk_seams(sim, monkeypatch):
+    # pairs outside the classes (narrowed reach) and chunk seams in the
+    # tensor-core mode, against the reference's FMM at p=6
+    import amk
+    g = np.load(os.path.join(GOLD, "fmm_n2000.npz"))
+    monkeypatch.setenv("AMK_FMM_M2L_REACH", "2")
+    monkeypatch.setenv("AMK_FMM_M2L_CHUNK_PAIRS", "1500")
+    with amk.Simulation() as s:
+        s.set_fmm_precision("tensor")
+        f = s.solve_fmm(g["x"], g["y"], g["z"], g["q"], 6, 0.5)
+    # mixed charges: far fields partly cancel, so the bound is on the global
+    # ratio ||dF|| / ||F|| (per particle on the cancelled ones it is larger)
+    rel, glob = rel_errors(f, g["f_p6_theta0.5"].T)
+    assert glob < 1e-6 and np.max(rel) < 1e-4, (glob, np.max(rel))
