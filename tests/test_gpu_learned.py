@@ -21,17 +21,29 @@ def cloud_sim(n=65536, seed=50, **over):
     return s
 
 
-def test_training_and_measured_gain():
+def test_training_and_measured_gain_on_a_held_out_cloud():
+    # trained on one cloud, audited on a second cloud of the same shape
+    # (another seed); the correction reduces the p=2 error on the cloud it
+    # was trained on and does not increase it on the held-out one -- the
+    # gain is small because the p=2 residual is dominated by the source
+    # cells' dropped moments, which per-particle features cannot see
     with cloud_sim() as s:
         plain = s.fmm_audit(2, 0.5, False, 2048)
         loss, samples = s.fmm_train_correction(0.5, sample_leaves=1024, steps=800, batch=2048, lr=1e-3)
         assert samples > 1000 and np.isfinite(loss)
         learned = s.fmm_audit(2, 0.5, True, 2048)
-        p6 = s.fmm_audit(6, 0.5, False, 2048)
-        print(f"RMS relative force error: p=2 {plain:.3e}, p=2 + MLP {learned:.3e}, p=6 {p6:.3e}")
-        assert np.isfinite(learned)
-        assert learned <= 1.1 * plain   # the correction must not make p=2 worse
         assert s.fmm_learned_state()["trained"]
+        x, y, z, _ = gaussian_cloud(65536, 51, mixed=False)
+        s.set_particles(x, y, z, np.zeros(65536), np.zeros(65536), np.zeros(65536), np.ones(65536, np.uint8))
+        plain_b = s.fmm_audit(2, 0.5, False, 2048)
+        learned_b = s.fmm_audit(2, 0.5, True, 2048)
+        p6_b = s.fmm_audit(6, 0.5, False, 2048)
+    print(f"RMS relative force error, training cloud: p=2 {plain:.3e}, p=2 + MLP {learned:.3e}; "
+          f"held-out cloud: p=2 {plain_b:.3e}, p=2 + MLP {learned_b:.3e}, p=6 {p6_b:.3e}")
+    assert np.isfinite(learned) and np.isfinite(learned_b)
+    assert learned < plain               # a gain on the training cloud
+    assert learned_b <= 1.01 * plain_b   # not worse on the held-out cloud
+    assert p6_b < 1e-2 * plain_b
 
 
 def test_failed_audit_falls_back_to_plain_fmm():
