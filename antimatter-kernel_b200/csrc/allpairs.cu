@@ -13,8 +13,9 @@
 //     pairs (the warp's box and the sub-tile's box closer than a quarter of
 //     their summed half-extent norms) use a float pair (hi, lo):
 //     r_ij = (xi_hi - xj_hi) + (xi_lo - xj_lo), exact to FP32 rounding of
-//     |r_ij| (Sterbenz) -- 18 FP32 ops per pair; the self pair and exact
-//     duplicates give r = 0 exactly;
+//     |r_ij| (Sterbenz) -- 18 FP32 ops per pair, issued as packed FP32x2
+//     operations over a lane's two targets (9 issue slots per pair); the
+//     self pair and exact duplicates give r = 0 exactly;
 //   * far pairs: each source carries its FP32 offset u_j from its sub-tile
 //     centre (stored negated) and each target forms a_i = x_i - c_sub once
 //     per sub-tile, so r_ij = a_i + (-u_j) costs one FADD per component --
@@ -295,25 +296,45 @@ allpairs_kernel(const float4* __restrict__ hq, const float4* __restrict__ lo, co
         const float lim = kNearFactor * (wh.w + sbx.h.w);
         const int base = q * kSub;
         if (gx * gx + gy * gy + gz * gz <= lim * lim) {
+          // near: double-float differences (t_hi - s_hi) + (t_lo - s_lo) for
+          // the lane's two targets in the two halves of packed FP32x2
+          // operations; t - s is formed as fma(s, -1, t), the same rounding
+          // as the subtraction, so the sums equal the scalar form bit for bit
+          const float2 m1 = make_float2(-1.f, -1.f), e2 = make_float2(eps2, eps2);
+          const float2 thx = make_float2(tx[0], tx[1]), thy = make_float2(ty[0], ty[1]),
+                       thz = make_float2(tz[0], tz[1]);
+          const float2 tlx = make_float2(ux[0], ux[1]), tly = make_float2(uy[0], uy[1]),
+                       tlz = make_float2(uz[0], uz[1]);
+          float2 fx = make_float2(px[0], px[1]), fy = make_float2(py[0], py[1]),
+                 fz = make_float2(pz[0], pz[1]);
 #pragma unroll 8
           for (int k = 0; k < kSub; ++k) {
             const float4 s = sa[base + k];
             const float4 l = sb[base + k];
-#pragma unroll
-            for (int r = 0; r < kR; ++r) {
-              const float dx = (tx[r] - s.x) + (ux[r] - l.x);
-              const float dy = (ty[r] - s.y) + (uy[r] - l.y);
-              const float dz = (tz[r] - s.z) + (uz[r] - l.z);
-              const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-              const float rinv = rsqrtf(d2);
-              const float qr = s.w * rinv;
-              const float w = qr * (rinv * rinv);
-              px[r] = fmaf(w, dx, px[r]);
-              py[r] = fmaf(w, dy, py[r]);
-              pz[r] = fmaf(w, dz, pz[r]);
-              if (kPhi) pp[r] += (d2 >= self_cut) ? qr : 0.0f;
+            const float2 dx = __fadd2_rn(__ffma2_rn(make_float2(s.x, s.x), m1, thx),
+                                         __ffma2_rn(make_float2(l.x, l.x), m1, tlx));
+            const float2 dy = __fadd2_rn(__ffma2_rn(make_float2(s.y, s.y), m1, thy),
+                                         __ffma2_rn(make_float2(l.y, l.y), m1, tly));
+            const float2 dz = __fadd2_rn(__ffma2_rn(make_float2(s.z, s.z), m1, thz),
+                                         __ffma2_rn(make_float2(l.z, l.z), m1, tlz));
+            const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
+            const float2 rinv = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+            const float2 qr = __fmul2_rn(make_float2(s.w, s.w), rinv);
+            const float2 w = __fmul2_rn(qr, __fmul2_rn(rinv, rinv));
+            fx = __ffma2_rn(w, dx, fx);
+            fy = __ffma2_rn(w, dy, fy);
+            fz = __ffma2_rn(w, dz, fz);
+            if (kPhi) {
+              pp[0] += (d2.x >= self_cut) ? qr.x : 0.0f;
+              pp[1] += (d2.y >= self_cut) ? qr.y : 0.0f;
             }
           }
+          px[0] = fx.x;
+          px[1] = fx.y;
+          py[0] = fy.x;
+          py[1] = fy.y;
+          pz[0] = fz.x;
+          pz[1] = fz.y;
         } else {
           // far: the warp's two targets per lane in the two halves of packed
           // FP32x2 operations (same operations and association as the

@@ -268,22 +268,37 @@ batch_allpairs_kernel(const int2* __restrict__ units, int n_units, const Instanc
         const float lim = kBNearFactor * (wh.w + sbx.h.w);
         const int base = qd * kBSub;
         if (gx * gx + gy * gy + gz * gz <= lim * lim) {
+          // near: double-float differences for the lane's two targets in
+          // packed FP32x2 operations (t - s as fma(s, -1, t): the scalar
+          // form's rounding, so the sums are bit-identical to it)
+          const float2 m1 = make_float2(-1.f, -1.f), e2 = make_float2(eps2, eps2);
+          const float2 thx = make_float2(tx[0], tx[1]), thy = make_float2(ty[0], ty[1]),
+                       thz = make_float2(tz[0], tz[1]);
+          const float2 tlx = make_float2(ux[0], ux[1]), tly = make_float2(uy[0], uy[1]),
+                       tlz = make_float2(uz[0], uz[1]);
+          float2 fx2 = make_float2(px[0], px[1]), fy2 = make_float2(py[0], py[1]), fz2 = make_float2(pz[0], pz[1]);
 #pragma unroll 8
           for (int k = 0; k < kBSub; ++k) {
             const float4 sh = sa[base + k], sl = sb[base + k];
-#pragma unroll
-            for (int r = 0; r < kBR; ++r) {
-              const float dx = (tx[r] - sh.x) + (ux[r] - sl.x);
-              const float dy = (ty[r] - sh.y) + (uy[r] - sl.y);
-              const float dz = (tz[r] - sh.z) + (uz[r] - sl.z);
-              const float d2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
-              const float rinv = rsqrtf(d2);
-              const float w = (sh.w * rinv) * (rinv * rinv);
-              px[r] = fmaf(w, dx, px[r]);
-              py[r] = fmaf(w, dy, py[r]);
-              pz[r] = fmaf(w, dz, pz[r]);
-            }
+            const float2 dx = __fadd2_rn(__ffma2_rn(make_float2(sh.x, sh.x), m1, thx),
+                                         __ffma2_rn(make_float2(sl.x, sl.x), m1, tlx));
+            const float2 dy = __fadd2_rn(__ffma2_rn(make_float2(sh.y, sh.y), m1, thy),
+                                         __ffma2_rn(make_float2(sl.y, sl.y), m1, tly));
+            const float2 dz = __fadd2_rn(__ffma2_rn(make_float2(sh.z, sh.z), m1, thz),
+                                         __ffma2_rn(make_float2(sl.z, sl.z), m1, tlz));
+            const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, e2)));
+            const float2 rinv = make_float2(rsqrtf(d2.x), rsqrtf(d2.y));
+            const float2 w = __fmul2_rn(__fmul2_rn(make_float2(sh.w, sh.w), rinv), __fmul2_rn(rinv, rinv));
+            fx2 = __ffma2_rn(w, dx, fx2);
+            fy2 = __ffma2_rn(w, dy, fy2);
+            fz2 = __ffma2_rn(w, dz, fz2);
           }
+          px[0] = fx2.x;
+          px[1] = fx2.y;
+          py[0] = fy2.x;
+          py[1] = fy2.y;
+          pz[0] = fz2.x;
+          pz[1] = fz2.y;
         } else {
           // far: a lane's two targets in the halves of packed FP32x2
           // operations (same operations and association as the scalar form)
