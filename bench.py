@@ -1140,9 +1140,104 @@ def run_reference_long(args):
     return 0
 
 
+# ================================================================== kernels
+def phase_ms(sim, fn, phase, reps):
+    """Device ms per launch of one library phase (CUDA events the library
+    records around it), over `reps` calls of fn after one untimed call."""
+    fn()
+    sim.synchronize()
+    sim.set_profiling(True)
+    sim.reset_phase_times()
+    for _ in range(reps):
+        fn()
+    sim.synchronize()
+    ms, cnt = sim.phase_times()[phase]
+    sim.set_profiling(False)
+    return ms / max(cnt, 1), cnt / reps
+
+
+def run_kernels(args):
+    """The HBM-bound per-particle kernels and the MLP's tensor-core forward,
+    each timed live in its library phase and set against its roofline:
+    the Boris push with cooling (4,194,304 particles), the radix sort and
+    octree build of an FMM evaluation (4,194,304 positrons), the
+    annihilation contact search and matching (4,194,304 particles, 1e-6 m)
+    and the learned correction's MLP forward (1,048,576 samples). This is
+    also the command the kernels' ncu captures run."""
+    import torch
+    import amk
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    hbm, hbm_src = measured_peak("hbm_gbs", 6650.0)
+    bf16, bf16_src = measured_peak("bf16_tflops", 1590.0)
+    n = args.long_n
+    out = {}
+    p = long_params(False, n // 2)
+    with amk.Simulation(p, device=local) as sim:
+        sim.init_particles_gpu("uniform")
+        ms, per = phase_ms(sim, sim.push, "push", args.steps)
+        bytes_ = 165.0 * n  # x, v read and written, F read and zeroed, q, m, id, alive
+        out["push_kernel"] = {"ms": ms, "algorithmic_bytes": bytes_, "achieved_gbs": bytes_ / (ms * 1e-3) / 1e9,
+                              "frac": bytes_ / (ms * 1e-3) / 1e9 / hbm, "launches_per_call": per,
+                              "unit": "165 B per particle-step: x, v read + written (96), F read + zeroed (48), "
+                                      "q, m (16), id (4), alive (1)"}
+        ms, per = phase_ms(sim, lambda: sim.annihilate(), "annihilation", args.steps)
+        bytes_ = (24.0 + 2 + 12 + 32 * 8 + 24 * 27 / 8) * n
+        out["annihilation (cell list, contact_kernel, matching)"] = {
+            "ms": ms, "algorithmic_bytes": bytes_, "achieved_gbs": bytes_ / (ms * 1e-3) / 1e9,
+            "frac": bytes_ / (ms * 1e-3) / 1e9 / hbm,
+            "unit": "per particle: positions (24), species + alive (2), cell key + index written (12), 8 radix "
+                    "passes x 32 B, neighbour positions of the 27 cells read once per 8 particles (81)"}
+    pos, vel, sp = tree_cloud(n)
+    with amk.Simulation(tree_params(n, dict(coulomb_method="fast-multipole", fast_multipole_order=4,
+                                            fast_multipole_theta=0.5)), device=local) as sim:
+        sim.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
+        sim.coulomb()
+        sim.synchronize()
+        sim.set_profiling(True)
+        sim.reset_phase_times()
+        for _ in range(args.steps):
+            sim.coulomb()
+        sim.synchronize()
+        ph = sim.phase_times()
+        sim.set_profiling(False)
+        nodes = sim.fmm_stats()["cells"]
+        sort_ms = ph["sort"][0] / max(ph["sort"][1], 1)
+        tree_ms = ph["tree"][0] / max(ph["tree"][1], 1) - sort_ms  # the tree phase encloses the sort
+        sb = 256.0 * n
+        tb = 100.0 * n + 78.0 * nodes
+        out["radix sort (hist_kernel, scan, scatter_kernel)"] = {
+            "ms": sort_ms, "algorithmic_bytes": sb, "achieved_gbs": sb / (sort_ms * 1e-3) / 1e9,
+            "frac": sb / (sort_ms * 1e-3) / 1e9 / hbm,
+            "unit": "256 B per key: 8 passes of 8 B key read (histogram) + 12 B read + 12 B written (scatter)"}
+        out["octree build (tree_*_kernel)"] = {
+            "ms": tree_ms, "algorithmic_bytes": tb, "achieved_gbs": tb / (tree_ms * 1e-3) / 1e9,
+            "frac": tb / (tree_ms * 1e-3) / 1e9 / hbm, "nodes": nodes,
+            "unit": "100 B per source (keys, key-prefix lengths, leaf depths, counts, gathered position + charge, "
+                    "source written) + 78 B per node (centre, children, range, meta, parent)"}
+    m = 1 << 20
+    with amk.Simulation(tree_params(m, dict(coulomb_method="fast-multipole", fast_multipole_order=2,
+                                            fast_multipole_theta=0.5, fmm_learned=1,
+                                            learned_audit_interval=0)), device=local) as sim:
+        sim.set_particles(pos[:m, 0], pos[:m, 1], pos[:m, 2], vel[:m, 0], vel[:m, 1], vel[:m, 2], sp[:m])
+        sim.fmm_train_correction(0.5, sample_leaves=256, steps=20, batch=1024, lr=1e-3)
+        ms, per = phase_ms(sim, sim.coulomb, "mlp", args.steps)
+        flops = 2.0 * (35 * 128 + 2 * 128 * 128 + 128 * 3) * m
+        out["mlp_forward_tc_kernel"] = {
+            "ms": ms, "algorithmic_flops": flops, "achieved_tflops": flops / (ms * 1e-3) / 1e12,
+            "frac": flops / (ms * 1e-3) / 1e12 / bf16,
+            "unit": "2 (35x128 + 2x128x128 + 128x3) flop per sample (unpadded), 1,048,576 samples"}
+    if rank == 0:
+        print(json.dumps({"workload": "kernels", "steps": args.steps, "peaks": {"hbm_gbs": [hbm, hbm_src],
+                                                                                "bf16_tflops": [bf16, bf16_src]},
+                          "kernels": out}), flush=True)
+    return 0
+
+
 # ================================================================== main
 WORKLOADS = {"tree1m": (run_tree, run_reference_tree), "direct65k": (run_direct, run_reference_direct),
-             "sweep512": (run_sweep, run_reference_sweep), "long4m": (run_long, run_reference_long)}
+             "sweep512": (run_sweep, run_reference_sweep), "long4m": (run_long, run_reference_long),
+             "kernels": (run_kernels, run_reference_long)}
 
 
 def main(argv=None):
