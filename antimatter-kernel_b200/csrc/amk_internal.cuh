@@ -185,6 +185,7 @@ enum ScratchSlot {
   kSlotFmmWork5,
   kSlotP2PWork,
   kSlotP2PPart,
+  kSlotP2PStage,
   kSlotM2lCodes,
   kSlotM2lTarget,
   kSlotM2lHist,

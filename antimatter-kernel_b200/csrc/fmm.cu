@@ -1526,6 +1526,128 @@ fmm_p2p_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, in
   }
 }
 
+// Near field in FP32 (the tensor precision mode): the sorted sources in
+// unit-cube coordinates as double-float pairs x = hi + lo (hi = float(x),
+// lo = float(x - hi)) plus the charge; a pair's difference
+// (x_i,hi - x_j,hi) + (x_i,lo - x_j,lo) is exact to FP32 rounding of |r_ij|
+// for the neighbouring leaves of a P2P list (Sterbenz), so the pair terms
+// carry FP32 relative error. Per-source-leaf partial sums are FP32 and are
+// added to FP64 accumulators once per leaf.
+__global__ void p2p_stage_kernel(const Octree t, float4* __restrict__ hi, float4* __restrict__ lo) {
+  const long k = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (k >= t.m) return;
+  const double4 s = t.src[k];
+  const float hx = static_cast<float>(s.x), hy = static_cast<float>(s.y), hz = static_cast<float>(s.z);
+  hi[k] = make_float4(hx, hy, hz, static_cast<float>(s.w));
+  lo[k] = make_float4(static_cast<float>(s.x - hx), static_cast<float>(s.y - hy), static_cast<float>(s.z - hz),
+                      0.f);
+}
+
+__global__ void __launch_bounds__(32 * kFmmWarps)
+fmm_p2p32_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, int n_work,
+                 const int* __restrict__ off, const int* __restrict__ count, const int* __restrict__ src,
+                 const int* __restrict__ pbase, const double* __restrict__ L, double min_sq, bool want_phi,
+                 const float4* __restrict__ shi, const float4* __restrict__ slo, double4* __restrict__ part) {
+  __shared__ double4 red[kFmmWarps][32];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int wi = blockIdx.x * kFmmWarps + w;
+  if (wi >= n_work) return;
+  const int2 item = work[wi];
+  const int ti = item.x, chunk = item.y;
+  const double4 tc = t.center[ti];
+  const int2 tr = t.range[ti];
+  const int nt_all = tr.y - tr.x;
+  const int sb = off[ti] + chunk * kP2PChunk;
+  const int se = min(off[ti] + count[ti], sb + kP2PChunk);
+  double4* out = part + pbase[ti] + static_cast<size_t>(chunk) * nt_all;
+  const float min_sq32 = static_cast<float>(min_sq);
+  for (int base = tr.x; base < tr.y; base += 32) {
+    const int nt = min(32, tr.y - base);
+    const int groups = 32 / nt;
+    const int g = lane / nt, tl = lane - g * nt;
+    const bool active = g < groups;
+    const int i = base + tl;
+    double pot = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
+    float4 mh = make_float4(0.f, 0.f, 0.f, 0.f), ml = mh;
+    if (active) {
+      mh = shi[i];
+      ml = slo[i];
+    }
+    if (active && g == 0 && chunk == 0) {  // L2P in FP64, once per target
+      const double4 me = t.src[i];
+      const double* l = L + static_cast<size_t>(ti) * T.n_m;
+      double px[kMaxOrder + 1], py[kMaxOrder + 1], pz[kMaxOrder + 1];
+      powers(T.p, me.x - tc.x, me.y - tc.y, me.z - tc.z, px, py, pz);
+      if (want_phi)
+        for (int gg = 0; gg < T.n_m; ++gg) {
+          const int4 m = T.multi[gg];
+          pot += l[gg] * (px[m.x] * py[m.y] * pz[m.z]);
+        }
+      double gx = 0.0, gy = 0.0, gz = 0.0;
+      for (int gg = 1; gg < T.n_m; ++gg) {
+        const int4 m = T.multi[gg];
+        const int g0 = T.grad[3 * gg], g1 = T.grad[3 * gg + 1], g2 = T.grad[3 * gg + 2];
+        if (g0 >= 0) {
+          const int4 q = T.multi[g0];
+          gx += m.x * l[gg] * (px[q.x] * py[q.y] * pz[q.z]);
+        }
+        if (g1 >= 0) {
+          const int4 q = T.multi[g1];
+          gy += m.y * l[gg] * (px[q.x] * py[q.y] * pz[q.z]);
+        }
+        if (g2 >= 0) {
+          const int4 q = T.multi[g2];
+          gz += m.z * l[gg] * (px[q.x] * py[q.y] * pz[q.z]);
+        }
+      }
+      fx = -gx;
+      fy = -gy;
+      fz = -gz;
+    }
+    if (active) {
+      for (int e = sb; e < se; ++e) {
+        const int2 sr = t.range[src[e]];
+        float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
+        for (int j = sr.x + g; j < sr.y; j += groups) {
+          const float4 s = shi[j];
+          if (j == i || s.w == 0.f) continue;
+          const float4 sl = slo[j];
+          const float rx = (mh.x - s.x) + (ml.x - sl.x);
+          const float ry = (mh.y - s.y) + (ml.y - sl.y);
+          const float rz = (mh.z - s.z) + (ml.z - sl.z);
+          const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+          if (r2 < min_sq32) continue;
+          const float inv_r = rsqrtf(r2);
+          const float qr = s.w * inv_r;
+          const float f = qr * (inv_r * inv_r);
+          ax = fmaf(rx, f, ax);
+          ay = fmaf(ry, f, ay);
+          az = fmaf(rz, f, az);
+          ap += qr;
+        }
+        fx += ax;
+        fy += ay;
+        fz += az;
+        pot += ap;
+      }
+    }
+    red[w][lane] = make_double4(fx, fy, fz, pot);
+    __syncwarp();
+    if (active && g == 0) {
+      double4 a = red[w][tl];
+      for (int gg = 1; gg < groups; ++gg) {
+        const double4 b = red[w][gg * nt + tl];
+        a.x += b.x;
+        a.y += b.y;
+        a.z += b.z;
+        a.w += b.w;
+      }
+      out[i - tr.x] = a;
+    }
+    __syncwarp();
+  }
+}
+
 // Per particle: item partials in chunk order.
 __global__ void fmm_p2p_reduce_kernel(const Octree t, const int* __restrict__ leaf_of, const int* __restrict__ items,
                                       const int* __restrict__ pbase, const double4* __restrict__ part,
@@ -1801,9 +1923,20 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
     AMK_TRY(rc);
     p2p_items_fill_kernel<<<gn, 256, 0, c->stream>>>(t, items, ibase, work, leaf_of);
     AMK_TRY(check_launch(c, "p2p_items_fill_kernel"));
-      fmm_p2p_kernel<<<static_cast<unsigned>((ht[0] + kFmmWarps - 1) / kFmmWarps), 32 * kFmmWarps, 0, c->stream>>>(
-        t, T, work, ht[0], gp.off, gp.count, gp.src, pbase, Lx, min_sq, want_phi, part);
-    AMK_TRY(check_launch(c, "fmm_p2p_kernel"));
+    const unsigned gwork = static_cast<unsigned>((ht[0] + kFmmWarps - 1) / kFmmWarps);
+    if (c->fmm_precision == AMK_FMM_TENSOR) {
+      float4* stage = slot<float4>(c, kSlotP2PStage, 2 * static_cast<size_t>(t.m), &rc);
+      AMK_TRY(rc);
+      p2p_stage_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, c->stream>>>(t, stage, stage + t.m);
+      AMK_TRY(check_launch(c, "p2p_stage_kernel"));
+      fmm_p2p32_kernel<<<gwork, 32 * kFmmWarps, 0, c->stream>>>(t, T, work, ht[0], gp.off, gp.count, gp.src, pbase,
+                                                                Lx, min_sq, want_phi, stage, stage + t.m, part);
+      AMK_TRY(check_launch(c, "fmm_p2p32_kernel"));
+    } else {
+      fmm_p2p_kernel<<<gwork, 32 * kFmmWarps, 0, c->stream>>>(t, T, work, ht[0], gp.off, gp.count, gp.src, pbase,
+                                                              Lx, min_sq, want_phi, part);
+      AMK_TRY(check_launch(c, "fmm_p2p_kernel"));
+    }
     fmm_p2p_reduce_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, c->stream>>>(t, leaf_of, items, pbase,
                                                                                           part, ef);
     AMK_TRY(check_launch(c, "fmm_p2p_reduce_kernel"));

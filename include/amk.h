@@ -310,8 +310,10 @@ long amk_bh_tree_dump(amk_ctx* ctx, long n, const double* x, const double* y, co
  * products run on the 5th-generation tensor cores with split-BF16 operands
  * (three BF16 terms per operand, six products, FP32 accumulation in tensor
  * memory) and FP32 per-pair products summed in FP64; relative error of an
- * M2L term about 2^-22, below the truncation error of those orders. Every
- * other part of the evaluation is unchanged. */
+ * M2L term about 2^-22, below the truncation error of those orders. The
+ * near field (P2P) then runs in FP32 on double-float positions (pair
+ * differences exact to FP32 rounding, FP64 sums per source leaf). Tree,
+ * expansions, L2L and L2P stay FP64. */
 #define AMK_FMM_FP64 0
 #define AMK_FMM_TENSOR 1
 int amk_set_fmm_precision(amk_ctx* ctx, int mode);
