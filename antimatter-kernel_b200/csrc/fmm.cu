@@ -36,8 +36,26 @@
 namespace amk {
 
 // ------------------------------------------------------------ tables
-// FmmTables, fast-multipole.cc:41-178 (multi-indices sorted by degree,
-// within a degree by a then b descending).
+// The expansion tables (the reference keeps the same quantities in its
+// FmmTables, fast-multipole.cc:41-178), generated here from their
+// definitions.
+//
+// Multi-indices (a, b, c) of degree d = a + b + c <= 2p are numbered in
+// graded order -- by degree, then a descending, then b descending -- with
+// the closed form
+//   pos(a, b, c) = d(d+1)(d+2)/6 + e(e+1)/2 + (e - b),   e = d - a,
+// where the first term counts the multi-indices of lower degree and the
+// second those of degree d with a larger first component. The first
+// n_m = (p+1)(p+2)(p+3)/6 positions are the expansion coefficients.
+__host__ __device__ constexpr int graded_index(int a, int b, int c) {
+  return (a < 0 || b < 0 || c < 0)
+             ? -1
+             : (a + b + c) * (a + b + c + 1) * (a + b + c + 2) / 6 + (b + c) * (b + c + 1) / 2 + c;
+}
+static_assert(graded_index(0, 0, 0) == 0 && graded_index(1, 0, 0) == 1 && graded_index(0, 0, 1) == 3 &&
+                  graded_index(2, 0, 0) == 4 && graded_index(0, 2, 0) == 7 && graded_index(0, 0, 2) == 9,
+              "graded order");
+
 struct FmmHostTables {
   int p = 0, n_m = 0, n_d = 0;
   std::vector<int4> multi;  // a, b, c, degree
@@ -52,87 +70,88 @@ struct FmmHostTables {
   std::vector<int> grad;                     // 3 per g, -1 none
 
   explicit FmmHostTables(int order) : p(order) {
-    const int size = 2 * p + 1, maxdeg = 2 * p;
-    std::vector<int> lookup(static_cast<size_t>(size) * size * size, -1);
-    auto index = [&](int a, int b, int c) {
-      if (a < 0 || b < 0 || c < 0 || a >= size || b >= size || c >= size) return -1;
-      return lookup[(a * size + b) * size + c];
+    const int dmax = 2 * p;
+    n_d = graded_index(0, 0, dmax) + 1;
+    n_m = graded_index(0, 0, p) + 1;
+    auto pos = [](const int m[3]) { return graded_index(m[0], m[1], m[2]); };
+    multi.resize(n_d);
+    for (int d = 0; d <= dmax + 1; ++d) deg_start.push_back(d * (d + 1) * (d + 2) / 6);
+    for (int d = 0; d <= dmax; ++d)
+      for (int a = 0; a <= d; ++a)
+        for (int b = 0; a + b <= d; ++b) multi[graded_index(a, b, d - a - b)] = make_int4(a, b, d - a - b, d);
+    auto factorial = [](int n) {
+      double f = 1.0;
+      for (int i = 2; i <= n; ++i) f *= i;
+      return f;
     };
-    for (int deg = 0; deg <= maxdeg; ++deg) {
-      deg_start.push_back(static_cast<int>(multi.size()));
-      for (int a = deg; a >= 0; --a)
-        for (int b = deg - a; b >= 0; --b) {
-          const int c = deg - a - b;
-          lookup[(a * size + b) * size + c] = static_cast<int>(multi.size());
-          multi.push_back(make_int4(a, b, c, deg));
-        }
-    }
-    deg_start.push_back(static_cast<int>(multi.size()));
-    n_d = static_cast<int>(multi.size());
-    n_m = (p + 1) * (p + 2) * (p + 3) / 6;
-    std::vector<double> factorial(maxdeg + 1, 1.0);
-    for (int i = 1; i <= maxdeg; ++i) factorial[i] = factorial[i - 1] * i;
-    for (int k = 0; k < n_d; ++k) {
-      const int4 m = multi[k];
-      fact.push_back(factorial[m.x] * factorial[m.y] * factorial[m.z]);
+    for (const int4& m : multi) {
+      fact.push_back(factorial(m.x) * factorial(m.y) * factorial(m.z));
       inv_fact.push_back(1.0 / fact.back());
-      sign.push_back(((m.x + m.y + m.z) % 2 == 0) ? 1.0 : -1.0);
+      sign.push_back(m.w % 2 == 0 ? 1.0 : -1.0);
     }
+    // Derivatives of 1/r by r^2 d_k f = -(...) along one axis i with k_i >= 1:
+    // the axis with the largest component (lowest index among equals); each
+    // entry lists k_j and the positions of k - e_j and k - 2 e_j per axis.
     rec_axis.assign(n_d, 0);
     rec_delta.assign(3 * n_d, 0);
     rec_m1.assign(3 * n_d, -1);
     rec_m2.assign(3 * n_d, -1);
     for (int k = 1; k < n_d; ++k) {
       const int m[3] = {multi[k].x, multi[k].y, multi[k].z};
-      rec_axis[k] = m[0] > 0 ? 0 : (m[1] > 0 ? 1 : 2);
+      int axis = 0;
+      for (int j = 1; j < 3; ++j)
+        if (m[j] > m[axis]) axis = j;
+      rec_axis[k] = axis;
       for (int j = 0; j < 3; ++j) {
         rec_delta[3 * k + j] = m[j];
         int t[3] = {m[0], m[1], m[2]};
-        if (m[j] >= 1) {
-          t[j] -= 1;
-          rec_m1[3 * k + j] = index(t[0], t[1], t[2]);
-        }
-        if (m[j] >= 2) {
-          t[j] -= 1;
-          rec_m2[3 * k + j] = index(t[0], t[1], t[2]);
-        }
+        t[j] -= 1;
+        if (m[j] >= 1) rec_m1[3 * k + j] = pos(t);
+        t[j] -= 1;
+        if (m[j] >= 2) rec_m2[3 * k + j] = pos(t);
       }
     }
+    // M2L: D_{g+a}; transposed copy for the class products
     m2l_index.resize(static_cast<size_t>(n_m) * n_m);
+    m2l_index_t.resize(static_cast<size_t>(n_m) * n_m);
     for (int g = 0; g < n_m; ++g)
-      for (int a = 0; a < n_m; ++a)
-        m2l_index[static_cast<size_t>(g) * n_m + a] =
-            index(multi[a].x + multi[g].x, multi[a].y + multi[g].y, multi[a].z + multi[g].z);
-    m2l_index_t.assign(static_cast<size_t>(n_m) * n_m, 0);
-    for (int a = 0; a < n_m; ++a)
-      for (int g = 0; g < n_m; ++g)
-        m2l_index_t[static_cast<size_t>(a) * n_m + g] = static_cast<short>(m2l_index[static_cast<size_t>(g) * n_m + a]);
+      for (int a = 0; a < n_m; ++a) {
+        const int s3[3] = {multi[g].x + multi[a].x, multi[g].y + multi[a].y, multi[g].z + multi[a].z};
+        m2l_index[static_cast<size_t>(g) * n_m + a] = pos(s3);
+        m2l_index_t[static_cast<size_t>(a) * n_m + g] = static_cast<short>(pos(s3));
+      }
+    // M2M (child -> parent): M_a += M_b * d^(a-b) / (a-b)! over b <= a;
+    // L2L (parent -> child): L_a += L_b * (b!/a!) d^(b-a) / (b-a)! over b >= a
+    // with |b| <= p. Both enumerated componentwise.
     m2m_off.push_back(0);
     l2l_off.push_back(0);
     for (int a = 0; a < n_m; ++a) {
-      for (int b = 0; b < n_m; ++b) {
-        if (multi[b].x <= multi[a].x && multi[b].y <= multi[a].y && multi[b].z <= multi[a].z) {
-          m2m_b.push_back(b);
-          m2m_c.push_back(index(multi[a].x - multi[b].x, multi[a].y - multi[b].y, multi[a].z - multi[b].z));
-        }
-        if (multi[a].x <= multi[b].x && multi[a].y <= multi[b].y && multi[a].z <= multi[b].z) {
-          l2l_b.push_back(b);
-          l2l_c.push_back(index(multi[b].x - multi[a].x, multi[b].y - multi[a].y, multi[b].z - multi[a].z));
-        }
-      }
+      const int4 ma = multi[a];
+      for (int b0 = 0; b0 <= ma.x; ++b0)
+        for (int b1 = 0; b1 <= ma.y; ++b1)
+          for (int b2 = 0; b2 <= ma.z; ++b2) {
+            m2m_b.push_back(graded_index(b0, b1, b2));
+            m2m_c.push_back(graded_index(ma.x - b0, ma.y - b1, ma.z - b2));
+          }
       m2m_off.push_back(static_cast<int>(m2m_b.size()));
+      for (int c = 0; c < n_m; ++c) {
+        const int4 mc = multi[c];
+        if (ma.w + mc.w > p) break;  // graded order: every later c has a higher degree
+        l2l_b.push_back(graded_index(ma.x + mc.x, ma.y + mc.y, ma.z + mc.z));
+        l2l_c.push_back(c);
+      }
       l2l_off.push_back(static_cast<int>(l2l_b.size()));
     }
+    // gradient of the local expansion: d/dx_k of x^g is g_k x^(g - e_k)
     grad.assign(3 * n_m, -1);
     for (int g = 0; g < n_m; ++g) {
       const int m[3] = {multi[g].x, multi[g].y, multi[g].z};
-      for (int k = 0; k < 3; ++k) {
-        int t[3] = {m[0], m[1], m[2]};
-        if (t[k] >= 1) {
+      for (int k = 0; k < 3; ++k)
+        if (m[k] >= 1) {
+          int t[3] = {m[0], m[1], m[2]};
           t[k] -= 1;
-          grad[3 * g + k] = index(t[0], t[1], t[2]);
+          grad[3 * g + k] = pos(t);
         }
-      }
     }
   }
 };
