@@ -488,7 +488,9 @@ struct Grouped {
 constexpr int kM2lTileP = 64;      // pairs per product tile
 constexpr int kM2lUnitTiles = 8;   // tiles of one class per block
 constexpr int kM2lUnitPairs = kM2lUnitTiles * kM2lTileP;
-constexpr int kM2lMinClass = 4;    // classes below this size take the per-pair path
+constexpr int kM2lMinClass = 4;    // FP64 mode: classes below this size take the per-pair path
+// (the tensor-core product costs about as much per class unit as the
+// per-pair path per pair, so in that mode every lattice class takes it)
 constexpr size_t kM2lChunkBytes = size_t(4) << 30;  // per-pair products of one chunk
 constexpr int kM2lHashBits = 21;
 constexpr long kM2lHashSlots = 1L << kM2lHashBits;
@@ -588,26 +590,28 @@ __global__ void m2l_histogram_kernel(const int* __restrict__ codes, long e0, lon
     fallback[atomicAdd(n_fallback, 1)] = static_cast<int>(e);
 }
 
-// Classes of fewer than kM2lMinClass pairs go the per-pair path.
-__global__ void m2l_code_flags_kernel(const int* __restrict__ hist, long n_codes, int* __restrict__ used,
-                                      int* __restrict__ units) {
+// Classes of fewer than min_class pairs go the per-pair path.
+__global__ void m2l_code_flags_kernel(const int* __restrict__ hist, long n_codes, int min_class,
+                                      int* __restrict__ used, int* __restrict__ units) {
   const long code = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
   if (code >= n_codes) return;
   const int n = hist[code];
-  used[code] = n >= kM2lMinClass;
-  units[code] = n >= kM2lMinClass ? (n + kM2lUnitPairs - 1) / kM2lUnitPairs : 0;
+  const bool take = n > 0 && n >= min_class;
+  used[code] = take;
+  units[code] = take ? (n + kM2lUnitPairs - 1) / kM2lUnitPairs : 0;
 }
 
 // Class list and product units (<= 8 tiles of one class) from the scanned
 // per-code counts.
 __global__ void m2l_class_fill_kernel(const int* __restrict__ hist, const int* __restrict__ start,
                                       const int* __restrict__ cls_index, const int* __restrict__ unit_start,
-                                      long n_codes, int* __restrict__ cls_code, int* __restrict__ cls_end,
-                                      int* __restrict__ unit_cls, int* __restrict__ unit_pos) {
+                                      long n_codes, const int* __restrict__ used, int* __restrict__ cls_code,
+                                      int* __restrict__ cls_end, int* __restrict__ unit_cls,
+                                      int* __restrict__ unit_pos) {
   const long code = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
   if (code >= n_codes) return;
   const int n = hist[code];
-  if (n < kM2lMinClass) return;
+  if (!used[code]) return;
   const int cls = cls_index[code];
   cls_code[cls] = static_cast<int>(code);
   cls_end[cls] = start[code] + n;
@@ -1320,12 +1324,12 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
     m2l_histogram_kernel<<<ge, 256, 0, c->stream>>>(codes, e0, e1, hist, fallback, counters + 3);
     AMK_TRY(check_launch(c, "m2l_histogram_kernel"));
     AMK_TRY(exclusive_scan_int(c, hist, n_codes, start, counters));
-    m2l_code_flags_kernel<<<gc, 256, 0, c->stream>>>(hist, n_codes, used, nunit);
+    m2l_code_flags_kernel<<<gc, 256, 0, c->stream>>>(hist, n_codes, tc ? 1 : kM2lMinClass, used, nunit);
     AMK_TRY(check_launch(c, "m2l_code_flags_kernel"));
     AMK_TRY(exclusive_scan_int(c, used, n_codes, cls_index, counters + 1));
     AMK_TRY(exclusive_scan_int(c, nunit, n_codes, unit_start, counters + 2));
-    m2l_class_fill_kernel<<<gc, 256, 0, c->stream>>>(hist, start, cls_index, unit_start, n_codes, cls_code, cls_end,
-                                                     unit_cls, unit_pos);
+    m2l_class_fill_kernel<<<gc, 256, 0, c->stream>>>(hist, start, cls_index, unit_start, n_codes, used, cls_code,
+                                                     cls_end, unit_cls, unit_pos);
     AMK_TRY(check_launch(c, "m2l_class_fill_kernel"));
     m2l_scatter_kernel<<<ge, 256, 0, c->stream>>>(codes, e0, e1, start, used, hist, perm, fallback, counters + 3);
     AMK_TRY(check_launch(c, "m2l_scatter_kernel"));
