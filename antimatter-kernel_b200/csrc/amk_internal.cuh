@@ -203,6 +203,7 @@ enum ScratchSlot {
   kSlotM2lTilePos,
   kSlotM2lTable,
   kSlotM2lHash,
+  kSlotM2lSplit,
   kNumSlots
 };
 static_assert(kNumSlots <= 96, "scratch slots");

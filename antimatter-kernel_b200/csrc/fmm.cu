@@ -868,16 +868,23 @@ m2l_class_mma_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter
 // Split-BF16 tensor-core form of the class product (FMM precision mode
 // AMK_FMM_TENSOR): the product Lh = A Mh of a class runs on the 5th-generation
 // tensor cores. A (the class matrix, rows g padded to 128, K = a padded to a
-// multiple of 16) and B (the tile's 128 rescaled source expansions, K-major)
-// are each split into three BF16 terms, x = x0 + x1 + x2 (24 significant
-// bits), and the six products x0y0 + x0y1 + x1y0 + x0y2 + x1y1 + x2y0
-// accumulate into one FP32 accumulator in tensor memory (tcgen05.mma, M = 128,
-// N = 128, K = 16, issued by one thread, completion through an mbarrier with
-// a bounded wait). The per-pair products are written as FP32 (n_m floats per
+// multiple of 16) and B (the tile's rescaled source expansions, K-major) are
+// each split into three BF16 terms, x = x0 + x1 + x2 (24 significant bits),
+// and the six products x0y0 + x0y1 + x1y0 + x0y2 + x1y1 + x2y0 accumulate
+// into one FP32 accumulator in tensor memory (tcgen05.mma, M = 128, N = 64,
+// K = 16, issued by one thread, completion through an mbarrier with a
+// bounded wait). The per-pair products are written as FP32 (n_m floats per
 // pair) and summed per target in FP64 by the same reduction as the FP64 path.
 // Relative error of a product: about 2^-22, far below the FMM's truncation
 // error at p >= 5.
-constexpr int kM2lTcN = 128;  // pairs per tensor-core tile (MMA N)
+//
+// Data movement: the cells' rescaled expansions are split once per
+// evaluation into BF16 rows of kKp elements (m2l_split_kernel), so a tile's B
+// operand is 16-byte core-matrix rows copied with cp.async straight into the
+// canonical layout; the next tile's copies are in flight (second buffer)
+// while the current tile's products and write-back run. A is built in shared
+// memory once per unit (one class, up to 8 tiles).
+constexpr int kM2lTcN = 64;  // pairs per tensor-core tile (MMA N)
 constexpr int kM2lTcThreads = 256;
 constexpr long kM2lTcWaitLimit = 1L << 26;  // polls before an mbarrier wait gives up
 
@@ -888,8 +895,9 @@ struct M2lTc {
   static constexpr int kKp = 16 * ((kNm + 15) / 16);
   static constexpr uint32_t kASplit = 128u * kKp * 2u;
   static constexpr uint32_t kBSplit = static_cast<uint32_t>(kM2lTcN) * kKp * 2u;
-  static constexpr uint32_t kOffB = 3u * kASplit;
-  static constexpr uint32_t kOffD = kOffB + 3u * kBSplit;              // Ds [kNd] doubles
+  static constexpr uint32_t kBBuf = 3u * kBSplit;
+  static constexpr uint32_t kOffB = 3u * kASplit;                      // two B buffers
+  static constexpr uint32_t kOffD = kOffB + 2u * kBBuf;                // Ds [kNd] doubles
   static constexpr uint32_t kOffRow = kOffD + 8u * kNd;                // rowf [128]
   static constexpr uint32_t kOffCol = kOffRow + 8u * 128u;             // colf [kKp]
   static constexpr uint32_t kOffPe = kOffCol + 8u * kKp;               // pair ids [kM2lUnitPairs]
@@ -897,7 +905,7 @@ struct M2lTc {
   static constexpr uint32_t kOffBar = kOffPs + 4u * kM2lUnitPairs;     // mbarrier, TMEM slot
   static constexpr uint32_t kSmem = kOffBar + 32u;
   static_assert(kNm <= 128, "the tensor-core class product covers n_m <= 128 (orders up to 7)");
-  static_assert(kSmem <= 227u * 1024u, "tensor-core class product shared memory");
+  static_assert(kSmem <= 226u * 1024u, "tensor-core class product shared memory");
 };
 
 __device__ __forceinline__ void split3_bf16(double v, __nv_bfloat16* t) {
@@ -910,16 +918,37 @@ __device__ __forceinline__ void split3_bf16(double v, __nv_bfloat16* t) {
   t[2] = __double2bfloat16(r2);
 }
 
+// Mh3[(cell * 3 + q) * kp + a] = term q of the split of Mh[cell][a] (zero for
+// a >= n_m): each cell's row of a split is kp contiguous BF16 values.
+__global__ void m2l_split_kernel(long n_cells, int nm, int kp, const double* __restrict__ Mh,
+                                 __nv_bfloat16* __restrict__ Mh3) {
+  const long e = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (e >= n_cells * kp) return;
+  const long cell = e / kp;
+  const int a = static_cast<int>(e - cell * kp);
+  __nv_bfloat16 t[3];
+  split3_bf16(a < nm ? Mh[cell * nm + a] : 0.0, t);
+#pragma unroll
+  for (int q = 0; q < 3; ++q) Mh3[(cell * 3 + q) * kp + a] = t[q];
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
+  const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+  const int n = valid ? 16 : 0;  // 0: zero fill, nothing read
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
+}
+
 template <int P>
 __global__ void __launch_bounds__(kM2lTcThreads, 1)
 m2l_class_tc_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter,
                     const int* __restrict__ unit_cls, const int* __restrict__ unit_pos,
                     const int* __restrict__ cls_code, const int* __restrict__ cls_end,
-                    const int* __restrict__ perm, const int* __restrict__ src, const double* __restrict__ Mh,
-                    const double* __restrict__ table, const unsigned long long* __restrict__ keys, long e0,
-                    float* __restrict__ out, int* __restrict__ status) {
+                    const int* __restrict__ perm, const int* __restrict__ src,
+                    const __nv_bfloat16* __restrict__ Mh3, const double* __restrict__ table,
+                    const unsigned long long* __restrict__ keys, long e0, float* __restrict__ out,
+                    int* __restrict__ status) {
   using S = M2lTc<P>;
-  constexpr int kNm = S::kNm, kKp = S::kKp, kN = kM2lTcN;
+  constexpr int kNm = S::kNm, kKp = S::kKp, kN = kM2lTcN, kChunks = kKp / 8;
   extern __shared__ __align__(1024) unsigned char tc_smem[];
   unsigned char* a_img = tc_smem;
   unsigned char* b_img = tc_smem + S::kOffB;
@@ -949,6 +978,19 @@ m2l_class_tc_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter,
   const uint32_t idesc = tc::make_idesc(kN);
   uint32_t phase = 0;
   bool failed = false;
+  // B of the tile starting at pair `tile0` of the unit into buffer `buf`:
+  // 16-byte core-matrix rows of the pre-split expansions (zero past the
+  // unit's last pair)
+  auto load_b = [&](int tile0, int np, int buf) {
+    unsigned char* dst = b_img + buf * S::kBBuf;
+    for (int x = tid; x < kN * 3 * kChunks; x += kM2lTcThreads) {
+      const int j = x / (3 * kChunks), r = x - j * 3 * kChunks, q = r / kChunks, ch = r - q * kChunks;
+      const bool ok = tile0 + j < np;
+      const __nv_bfloat16* sp = ok ? Mh3 + (static_cast<size_t>(ps[tile0 + j]) * 3 + q) * kKp + 8 * ch : Mh3;
+      cp_async16(dst + q * S::kBSplit + tc::op_offset(j, 8 * ch, kN), sp, ok);
+    }
+    cp_async_commit();
+  };
   for (;;) {
     if (tid == 0) s_unit = atomicAdd(unit_counter, 1);
     __syncthreads();  // also: the previous unit is done with the shared arrays
@@ -967,7 +1009,8 @@ m2l_class_tc_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter,
       ps[p] = src[e];
     }
     __syncthreads();
-    // A = class matrix, three BF16 splits
+    load_b(0, np, 0);
+    // A = class matrix, three BF16 splits (built while the first tile's B arrives)
     for (int x = tid; x < 128 * kKp; x += kM2lTcThreads) {
       const int g = x / kKp, a = x - g * kKp;
       const double v = (g < kNm && a < kNm) ? Ds[T.m2l_index_t[a * kNm + g]] * colf[a] : 0.0;
@@ -977,30 +1020,29 @@ m2l_class_tc_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter,
 #pragma unroll
       for (int q = 0; q < 3; ++q) *reinterpret_cast<__nv_bfloat16*>(a_img + q * S::kASplit + o) = t[q];
     }
-    for (int tile0 = 0; tile0 < np && !failed; tile0 += kN) {
+    const int n_tiles = (np + kN - 1) / kN;
+    for (int tile = 0; tile < n_tiles && !failed; ++tile) {
+      const int tile0 = tile * kN, buf = tile & 1;
       const int live = min(kN, np - tile0);
-      // B = the tile's rescaled source expansions ([pair][a]), three BF16 splits
-      for (int x = tid; x < kN * kKp; x += kM2lTcThreads) {
-        const int j = x / kKp, a = x - j * kKp;
-        const double v = (j < live && a < kNm) ? Mh[static_cast<size_t>(ps[tile0 + j]) * kNm + a] : 0.0;
-        __nv_bfloat16 t[3];
-        split3_bf16(v, t);
-        const uint32_t o = tc::op_offset(j, a, kN);
-#pragma unroll
-        for (int q = 0; q < 3; ++q) *reinterpret_cast<__nv_bfloat16*>(b_img + q * S::kBSplit + o) = t[q];
+      if (tile + 1 < n_tiles) {
+        load_b(tile0 + kN, np, buf ^ 1);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
       }
-      tc::fence_proxy_async();
+      tc::fence_proxy_async();  // this thread's A writes and landed copies, for the async proxy
       tc::fence_before();
       __syncthreads();
       if (tid == 0) {
         tc::fence_after();
         constexpr int kCombo[6][2] = {{2, 0}, {1, 1}, {0, 2}, {1, 0}, {0, 1}, {0, 0}};  // small terms first
+        const uint32_t bb = b_base + buf * S::kBBuf;
         int first = 1;
         for (int st = 0; st < kKp / 16; ++st)
 #pragma unroll
           for (int c = 0; c < 6; ++c) {
             const uint64_t ad = tc::make_sdesc(a_base + kCombo[c][0] * S::kASplit + st * 128 * 32);
-            const uint64_t bd = tc::make_sdesc(b_base + kCombo[c][1] * S::kBSplit + st * kN * 32);
+            const uint64_t bd = tc::make_sdesc(bb + kCombo[c][1] * S::kBSplit + st * kN * 32);
             tc::mma_bf16(tmem, ad, bd, idesc, first ? 0 : 1);
             first = 0;
           }
@@ -1024,18 +1066,24 @@ m2l_class_tc_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter,
       if (warp < 4) {
         const int g = 32 * warp + lane;
         const double rf = rowf[g];
+#pragma unroll
         for (int c0 = 0; c0 < kN; c0 += 32) {
           float v[32];
           tc::tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + c0, v);
-          if (g < kNm)
-            for (int j = 0; j < 32 && c0 + j < live; ++j)
-              out[static_cast<size_t>(pe[tile0 + c0 + j] - e0) * kNm + g] = static_cast<float>(v[j] * rf);
+          if (g < kNm) {
+#pragma unroll
+            for (int j = 0; j < 32; ++j)
+              if (c0 + j < live)
+                out[static_cast<size_t>(pe[tile0 + c0 + j] - e0) * kNm + g] = static_cast<float>(v[j] * rf);
+          }
         }
       }
       tc::fence_before();
-      __syncthreads();  // accumulator read out before the next tile's products
+      __syncthreads();  // accumulator read out and buffer free before the next tile's products
       tc::fence_after();
     }
+    cp_async_wait<0>();  // no copy of an abandoned tile left in flight
+    __syncthreads();
     if (failed) break;
   }
   if (failed && tid == 0) atomicExch(status, 1);
@@ -1197,8 +1245,8 @@ int class_product(amk_ctx* c, int order, const FmmDevTables& T, int n_units, int
 template <int P>
 int launch_class_tc(amk_ctx* c, const FmmDevTables& T, int n_units, int* unit_counter, const int* unit_cls,
                     const int* unit_pos, const int* cls_code, const int* cls_end, const int* perm, const int* src,
-                    const double* Mh, const double* table, const unsigned long long* keys, long e0, float* out,
-                    int* status) {
+                    const __nv_bfloat16* Mh, const double* table, const unsigned long long* keys, long e0,
+                    float* out, int* status) {
   const size_t smem = M2lTc<P>::kSmem;
   AMK_CUDA_TRY(cudaFuncSetAttribute(m2l_class_tc_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
@@ -1218,7 +1266,7 @@ inline bool tc_order(int order) { return order >= 5 && order <= 7; }
 
 int class_tc(amk_ctx* c, int order, const FmmDevTables& T, int n_units, int* unit_counter, const int* unit_cls,
              const int* unit_pos, const int* cls_code, const int* cls_end, const int* perm, const int* src,
-             const double* Mh, const double* table, const unsigned long long* keys, long e0, float* out,
+             const __nv_bfloat16* Mh, const double* table, const unsigned long long* keys, long e0, float* out,
              int* status) {
   switch (order) {
     case 5:
@@ -1309,7 +1357,15 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
   const bool tc = c->fmm_precision == AMK_FMM_TENSOR && tc_order(order);
   const size_t esz = tc ? sizeof(float) : sizeof(double);
   int* tc_status = counters + 6;
-  if (tc) AMK_CUDA_TRY(cudaMemsetAsync(tc_status, 0, sizeof(int), c->stream));
+  __nv_bfloat16* Mh3 = nullptr;
+  if (tc) {
+    AMK_CUDA_TRY(cudaMemsetAsync(tc_status, 0, sizeof(int), c->stream));
+    const int kp = 16 * ((T.n_m + 15) / 16);
+    Mh3 = slot<__nv_bfloat16>(c, kSlotM2lSplit, static_cast<size_t>(nn) * 3 * kp, &rc);
+    AMK_TRY(rc);
+    m2l_split_kernel<<<static_cast<unsigned>((nn * kp + 255) / 256), 256, 0, c->stream>>>(nn, T.n_m, kp, Mh, Mh3);
+    AMK_TRY(check_launch(c, "m2l_split_kernel"));
+  }
   const int n_buf = n_m2l > cap ? 2 : 1;
   for (int i = 0; i < n_buf; ++i)
     AMK_TRY(f->m2l_out[i].reserve(static_cast<size_t>(std::min(cap, n_m2l)) * T.n_m * esz));
@@ -1355,7 +1411,7 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
       AMK_TRY(check_launch(c, "m2l_table_kernel"));
       AMK_TRY(phase_begin(c, AMK_PHASE_FMM_M2L_PRODUCTS));
       if (tc)
-        AMK_TRY(class_tc(c, order, T, n_units, counters + 4, unit_cls, unit_pos, cls_code, cls_end, perm, gm.src, Mh,
+        AMK_TRY(class_tc(c, order, T, n_units, counters + 4, unit_cls, unit_pos, cls_code, cls_end, perm, gm.src, Mh3,
                          table, keys, e0, static_cast<float*>(out), tc_status));
       else
         AMK_TRY(class_product(c, order, T, n_units, counters + 4, unit_cls, unit_pos, cls_code, cls_end, perm,

@@ -160,7 +160,7 @@ def test_behaviour_steps_and_energy_match_the_reference_code(harness):
         pytest.skip("reference library not built")
     lib = harness("lib", None, None, None, None, None, None)
     dp, u8 = C.POINTER(C.c_double), C.POINTER(C.c_uint8)
-    lib.harness_steps.argtypes = ([C.c_long] + [dp] * 6 + [u8, dp, dp, u8] + [C.c_double] * 9 +
+    lib.harness_steps.argtypes = ([C.c_long] + [dp] * 6 + [u8, dp, dp, u8] + [C.c_double] * 8 +
                                   [C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, dp])
     g = np.load(os.path.join(GOLD, "readme_ic.npz"))
     n = 200
