@@ -150,27 +150,13 @@ def test_solver_classes_match_the_reference_classes(harness):
     assert [lib.harness_is_pair(a, b) for a, b in ((0, 4), (4, 0), (1, 3), (0, 1), (2, 2))] == [1, 1, 1, 0, 0]
 
 
-@pytest.mark.gpu
-def test_behaviour_steps_and_energy_match_the_reference_code(harness):
-    # the reference application's loop on the adapter (standard Coulomb
-    # driver, the three behaviours per agent, the per-step operation, the
-    # energy) against the reference's own coulomb_interaction.cc, lorentz.cc,
-    # cooling.cc and annihilation.cc (oracle/_ref, same Philox draws)
-    if not O.ref_available():
-        pytest.skip("reference library not built")
+def _adapter_steps(harness, pos, vel, sp, trap, dt, steps, rc, contact):
     lib = harness("lib", None, None, None, None, None, None)
     dp, u8 = C.POINTER(C.c_double), C.POINTER(C.c_uint8)
     lib.harness_steps.argtypes = ([C.c_long] + [dp] * 6 + [u8, dp, dp, u8] + [C.c_double] * 8 +
                                   [C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, dp])
-    g = np.load(os.path.join(GOLD, "readme_ic.npz"))
-    n = 200
-    rng = np.random.default_rng(4)
-    pos = g["pos"] * 0.4 + rng.normal(0, 1e-7, (n, 3))  # denser: contacts within 30 steps
-    vel = g["vel"].copy()
-    sp = g["species"]
+    n = len(pos)
     m, q = O.species_props(sp)
-    trap = dict(b0=1.0, voltage=10.0, z0=0.01, rho0=0.01)
-    dt, steps, rc, contact = O.dt_for([1, 3], 1.0), 30, 1e-5, 4e-6
     arr = [np.ascontiguousarray(pos[:, k]) for k in range(3)] + [np.ascontiguousarray(vel[:, k]) for k in range(3)]
     alive = np.ones(n, np.uint8)
     energy = np.zeros(8)
@@ -178,18 +164,67 @@ def test_behaviour_steps_and_energy_match_the_reference_code(harness):
                             m.ctypes.data_as(dp), alive.ctypes.data_as(u8), trap["b0"], trap["voltage"], trap["z0"],
                             trap["rho0"], dt, rc, 1.0, 4.0, 1, contact, 1.0, 42, steps, energy.ctypes.data_as(dp))
     assert rc_ == 0
+    st = dict(zip(("x", "y", "z", "vx", "vy", "vz"), arr), alive=alive, q=q, m=m)
+    return st, energy
+
+
+def _dense_readme_cloud():
+    g = np.load(os.path.join(GOLD, "readme_ic.npz"))
+    rng = np.random.default_rng(4)
+    pos = g["pos"] * 0.4 + rng.normal(0, 1e-7, (len(g["pos"]), 3))  # denser: contacts within a few steps
+    return pos, g["vel"].copy(), g["species"]
+
+
+@pytest.mark.gpu
+def test_behaviour_steps_equal_the_library_step(harness):
+    # the reference application's loop on the adapter (standard Coulomb
+    # driver, the three behaviours per agent, the per-step operation, the
+    # energy) equals the library's own amk_step on the same particles
+    import amk
+    pos, vel, sp = _dense_readme_cloud()
+    n = len(pos)
+    trap = dict(b0=1.0, voltage=10.0, z0=0.01, rho0=0.01)
+    dt, steps, rc, contact = O.dt_for([1, 3], 1.0), 30, 1e-5, 4e-6
+    st, energy = _adapter_steps(harness, pos, vel, sp, trap, dt, steps, rc, contact)
+    d = np.sqrt(0.01 ** 2 / 2 + 0.01 ** 2 / 4)  # the adapter hands the library z0 = sqrt(2) d, rho0 = 0
+    p = amk.make_params(seed=42, b0=1.0, trap_voltage=10.0, z0=np.sqrt(2.0) * d, rho0=0.0, dt=dt,
+                        populations={"positron": 100, "electron": 100}, coulomb_method="standard",
+                        cutoff_radius=rc, cooling_enabled=1, cooling_scale=1.0, bath_temperature=4.0,
+                        annihilation_enabled=1, contact_radius=contact, annihilation_probability=1.0)
+    with amk.Simulation(p) as s:
+        s.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
+        for _ in range(steps):
+            s.step(1)
+        lib = s.get_particles()
+    assert lib["alive"].sum() < n
+    assert np.array_equal(st["alive"], lib["alive"]), int((st["alive"] != lib["alive"]).sum())
+    for k in ("x", "y", "z", "vx", "vy", "vz"):
+        assert np.array_equal(st[k], lib[k]), (k, np.max(np.abs(st[k] - lib[k])))
+    # the last two energies: raw, then time-centred with the first
+    e_last = O.energy_standard(st, trap["voltage"], trap["z0"], trap["rho0"], rc)
+    assert abs(energy[4] - e_last["kinetic"]) <= 1e-12 * e_last["kinetic"]
+    assert energy[7] == e_last["num_active"]
+    assert abs(energy[5] - 0.5 * (energy[1] + e_last["trap_potential"])) <= 1e-12 * abs(e_last["trap_potential"])
+
+
+@pytest.mark.gpu
+def test_behaviour_steps_match_the_reference_code(harness):
+    # against the reference's own coulomb_interaction.cc, lorentz.cc,
+    # cooling.cc and annihilation.cc (oracle/_ref, same Philox draws) over
+    # the first 10 steps of the dense cloud
+    if not O.ref_available():
+        pytest.skip("reference library not built")
+    pos, vel, sp = _dense_readme_cloud()
+    trap = dict(b0=1.0, voltage=10.0, z0=0.01, rho0=0.01)
+    dt, steps, rc, contact = O.dt_for([1, 3], 1.0), 10, 1e-5, 4e-6
+    st, _ = _adapter_steps(harness, pos, vel, sp, trap, dt, steps, rc, contact)
     w = O.RefWorld(pos, vel, sp, dt=dt, cooling_scale=1.0, bath_temp=4.0, annihilation=True,
                    contact_radius=contact, probability=1.0, seed=42, **trap)
     for step in range(1, steps + 1):
         w.coulomb_standard(rc)
         w.behaviours(step)
     r = w.state()
-    assert np.array_equal(alive, r["alive"]) and alive.sum() < n
-    for a, k in zip(arr, ("x", "y", "z", "vx", "vy", "vz")):
-        assert np.max(np.abs(a - r[k])) <= 1e-9 * np.max(np.abs(r[k])), k
-    # the last two energies: raw, then time-centred with the first
-    st = dict(x=arr[0], y=arr[1], z=arr[2], vx=arr[3], vy=arr[4], vz=arr[5], q=q, m=m, alive=alive)
-    e_last = O.energy_standard(st, trap["voltage"], trap["z0"], trap["rho0"], rc)
-    assert abs(energy[4] - e_last["kinetic"]) <= 1e-12 * e_last["kinetic"]
-    assert energy[7] == e_last["num_active"]
-    assert abs(energy[5] - 0.5 * (energy[1] + e_last["trap_potential"])) <= 1e-12 * abs(e_last["trap_potential"])
+    diff = {k: float(np.max(np.abs(st[k] - r[k])) / np.max(np.abs(r[k]))) for k in ("x", "y", "z", "vx", "vy", "vz")}
+    assert np.array_equal(st["alive"], r["alive"]), (int((st["alive"] != r["alive"]).sum()), diff)
+    assert r["alive"].sum() < len(pos)
+    assert max(diff.values()) <= 1e-9, diff
