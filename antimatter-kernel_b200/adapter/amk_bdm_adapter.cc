@@ -53,6 +53,7 @@
 #include "amk.h"
 #include "core/param/param.h"
 #include "core/resource_manager.h"
+#include "core/scheduler.h"
 #include "core/simulation.h"
 #include "fields/penning_trap.h"
 #include "params/physics_params.h"
@@ -150,7 +151,6 @@ struct Queue {
   std::vector<std::pair<ChargedAntiparticle*, LorentzForce*>> lorentz;
   std::unordered_map<ChargedAntiparticle*, CyclotronCooling*> cooling;
   std::vector<ChargedAntiparticle*> annihilation;
-  long step = 0;  // flushes so far: the random streams' step index
 };
 Queue& TheQueue() {
   static Queue q;
@@ -391,14 +391,15 @@ void AmkRunQueuedBehaviours() {
   std::vector<std::pair<ChargedAntiparticle*, LorentzForce*>> lorentz;
   std::unordered_map<ChargedAntiparticle*, CyclotronCooling*> cooling;
   std::vector<ChargedAntiparticle*> annihilation;
-  long step = 0;
   {
     std::lock_guard<std::mutex> lock(q.mu);
     lorentz.swap(q.lorentz);
     cooling.swap(q.cooling);
     annihilation.swap(q.annihilation);
-    step = ++q.step;
   }
+  // the random streams' step index: the scheduler step being simulated
+  // (GetSimulatedSteps counts the steps completed before it)
+  const long step = static_cast<long>(Simulation::GetActive()->GetScheduler()->GetSimulatedSteps()) + 1;
   const auto* physics = Simulation::GetActive()->GetParam()->Get<PhysicsParams>();
   auto by_uid = [](const ChargedAntiparticle* a, const ChargedAntiparticle* b) { return StableId(a) < StableId(b); };
   amk_ctx* ctx = Context();
@@ -427,11 +428,16 @@ void AmkRunQueuedBehaviours() {
     p.annihilation_enabled = 0;
     p.coulomb_forces_enabled = 0;
     // agents still at v(0) take the one-time back-stagger, the rest do not
+    // (the groups are fixed before either is pushed: a pushed agent's flag
+    // flips, and it must not join the second group of the same step)
+    std::vector<char> was_staggered;
+    for (const auto& e : lorentz) was_staggered.push_back(e.second->velocity_staggered_ ? 1 : 0);
     for (int staggered = 0; staggered < 2; ++staggered) {
       Gathered g;
       std::vector<LorentzForce*> owners;
-      for (const auto& e : lorentz)
-        if (e.second->velocity_staggered_ == (staggered != 0)) {
+      for (size_t k = 0; k < lorentz.size(); ++k)
+        if (was_staggered[k] == staggered) {
+          const auto& e = lorentz[k];
           g.Add(e.first);
           owners.push_back(e.second);
         }

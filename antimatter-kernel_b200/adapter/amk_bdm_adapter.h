@@ -140,8 +140,9 @@ class AnnihilationInteraction : public Behavior {
 // field parameters), then the agents queued by AnnihilationInteraction::Run
 // are matched under the library's deterministic rule (the reference visits
 // agents in parallel with a shared random stream). Random streams are keyed
-// by the agents' uids and a step counter this function advances. Throws
-// std::runtime_error with the library's message on failure.
+// by the agents' uids and the scheduler step being simulated
+// (Scheduler::GetSimulatedSteps() + 1). Throws std::runtime_error with the
+// library's message on failure.
 void AmkRunQueuedBehaviours();
 
 // energy_analysis.h:13-35.

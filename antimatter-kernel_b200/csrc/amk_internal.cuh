@@ -204,6 +204,9 @@ enum ScratchSlot {
   kSlotM2lTable,
   kSlotM2lHash,
   kSlotM2lSplit,
+  kSlotM2lUnitDesc,
+  kSlotM2lPairSrc,
+  kSlotM2lTable3,
   kNumSlots
 };
 static_assert(kNumSlots <= 96, "scratch slots");

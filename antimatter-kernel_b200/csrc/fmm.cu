@@ -866,46 +866,78 @@ m2l_class_mma_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter
 }
 
 // Split-BF16 tensor-core form of the class product (FMM precision mode
-// AMK_FMM_TENSOR): the product Lh = A Mh of a class runs on the 5th-generation
-// tensor cores. A (the class matrix, rows g padded to 128, K = a padded to a
-// multiple of 16) and B (the tile's rescaled source expansions, K-major) are
-// each split into three BF16 terms, x = x0 + x1 + x2 (24 significant bits),
-// and the six products x0y0 + x0y1 + x1y0 + x0y2 + x1y1 + x2y0 accumulate
-// into one FP32 accumulator in tensor memory (tcgen05.mma, M = 128, N = 64,
-// K = 16, issued by one thread, completion through an mbarrier with a
-// bounded wait). The per-pair products are written as FP32 (n_m floats per
-// pair) and summed per target in FP64 by the same reduction as the FP64 path.
-// Relative error of a product: about 2^-22, far below the FMM's truncation
-// error at p >= 5.
+// AMK_FMM_TENSOR). The class matrix A (rows g padded to 128, K = a padded
+// to a multiple of 32) and the tile's rescaled source expansions B (64
+// pairs, K-major) are each split into three BF16 terms, x = x0 + x1 + x2
+// (24 significant bits), and the six products x0y0 + x0y1 + x1y0 + x0y2 +
+// x1y1 + x2y0 accumulate into one FP32 accumulator in tensor memory
+// (tcgen05.mma, M = 128, N = 64, K = 16, A from tensor memory). The
+// per-pair products are written as FP32 (n_m floats per pair) and summed
+// per target in FP64 by the same reduction as the FP64 path. Relative error
+// of a product: about 2^-22, far below the FMM's truncation error at p >= 5.
 //
-// Data movement: the cells' rescaled expansions are split once per
-// evaluation into BF16 rows of kKp elements (m2l_split_kernel), so a tile's B
-// operand is 16-byte core-matrix rows copied with cp.async straight into the
-// canonical layout; the next tile's copies are in flight (second buffer)
-// while the current tile's products and write-back run. A is built in shared
-// memory once per unit (one class, up to 8 tiles).
-constexpr int kM2lTcN = 64;  // pairs per tensor-core tile (MMA N)
-constexpr int kM2lTcThreads = 256;
-constexpr long kM2lTcWaitLimit = 1L << 26;  // polls before an mbarrier wait gives up
+// Before the kernel, per evaluation chunk: the cells' rescaled expansions
+// are split into BF16 rows of kKp elements (m2l_split_kernel), each class's
+// D(v) into packed BF16 terms (m2l_table3_kernel), and every unit gets a
+// descriptor {class, first pair, pairs, depth difference} and every pair its
+// source cell (m2l_tc_prep_kernel), so each role reads one value where it
+// would otherwise follow a chain of dependent loads.
+//
+// Roles (one CTA per SM, units of one class taken in a fixed stride; every
+// role prefetches the next unit's descriptor and the next tile's indices):
+//  - warps 0-3 drain the accumulators (tcgen05.ld, FP32 stores), row g =
+//    TMEM lane of the warp's quarter;
+//  - warps 4-11 build A for the next unit straight into tensor memory
+//    (tcgen05.st, two K halves per lane quarter, A double-buffered) from the
+//    class's split D(v), staged in shared memory by cp.async one unit ahead;
+//  - warps 12-15 stream B: a pair's column is 3 * kKp / 8 16-byte
+//    core-matrix rows copied with cp.async into one of 3-4 stages;
+//  - one thread of warp 16 issues the MMAs into one of two accumulators.
+// The roles meet at mbarriers (stage full / empty, accumulator full /
+// empty, A full / empty). Every wait is bounded in time; a wait that runs out
+// sets an abort flag that ends every other wait at once, the roles run
+// through their loops without work, and the kernel reports the status.
+constexpr int kM2lTcN = 64;          // pairs per tensor-core tile (MMA N)
+constexpr int kM2lTcAcc = 2;         // FP32 accumulators in tensor memory
+constexpr int kM2lTcEpiWarps = 4;    // accumulator readers
+constexpr int kM2lTcBldWarps = 8;    // A builders (two per TMEM lane quarter)
+constexpr int kM2lTcProdWarps = 4;   // B producers
+constexpr int kM2lTcBldThreads = 32 * kM2lTcBldWarps;
+constexpr int kM2lTcProdThreads = 32 * kM2lTcProdWarps;
+constexpr int kM2lTcBld0 = kM2lTcEpiWarps;                      // first builder warp
+constexpr int kM2lTcProd0 = kM2lTcBld0 + kM2lTcBldWarps;        // first producer warp
+constexpr int kM2lTcMmaWarp = kM2lTcProd0 + kM2lTcProdWarps;
+constexpr int kM2lTcThreads = 32 * (kM2lTcMmaWarp + 1);
+constexpr unsigned long long kM2lTcWaitNs = 2000000000ull;  // a wait gives up after 2 s
+constexpr uint32_t kM2lTcCols = 512;                         // TMEM columns the block allocates
 
 template <int P>
 struct M2lTc {
   static constexpr int kNm = (P + 1) * (P + 2) * (P + 3) / 6;
   static constexpr int kNd = (2 * P + 1) * (2 * P + 2) * (2 * P + 3) / 6;
-  static constexpr int kKp = 16 * ((kNm + 15) / 16);
-  static constexpr uint32_t kASplit = 128u * kKp * 2u;
+  static constexpr int kNd3 = (kNd + 2) & ~1;              // packed D row: zero at kNd, 16-byte multiple
+  static constexpr int kKp = 32 * ((kNm + 31) / 32);
+  static constexpr int kChunks = kKp / 8;                  // 16-byte rows of one split of a pair
+  static constexpr uint32_t kACols = kKp / 2;              // TMEM columns of one split of A (2 BF16 per column)
+  static constexpr uint32_t kABuf = 3 * kACols;            // one A buffer
+  static constexpr uint32_t kAccCol = 2 * kABuf;           // first accumulator column
   static constexpr uint32_t kBSplit = static_cast<uint32_t>(kM2lTcN) * kKp * 2u;
-  static constexpr uint32_t kBBuf = 3u * kBSplit;
-  static constexpr uint32_t kOffB = 3u * kASplit;                      // two B buffers
-  static constexpr uint32_t kOffD = kOffB + 2u * kBBuf;                // Ds [kNd] doubles
-  static constexpr uint32_t kOffRow = kOffD + 8u * kNd;                // rowf [128]
-  static constexpr uint32_t kOffCol = kOffRow + 8u * 128u;             // colf [kKp]
-  static constexpr uint32_t kOffPe = kOffCol + 8u * kKp;               // pair ids [kM2lUnitPairs]
-  static constexpr uint32_t kOffPs = kOffPe + 4u * kM2lUnitPairs;      // sources [kM2lUnitPairs]
-  static constexpr uint32_t kOffBar = kOffPs + 4u * kM2lUnitPairs;     // mbarrier, TMEM slot
-  static constexpr uint32_t kSmem = kOffBar + 32u;
+  static constexpr uint32_t kBStage = 3u * kBSplit;
+  static constexpr int kStages = kBStage > 40u * 1024u ? 3 : 4;      // B stages
+  static constexpr int kIdxStride = kKp + 2;  // index-map row pitch: an odd number of words, rows in distinct banks
+  static constexpr uint32_t kOffIdx = kStages * kBStage;             // idx [kNm][kIdxStride] (u16)
+  static constexpr uint32_t kOffD = kOffIdx + ((2u * kNm * kIdxStride + 15u) & ~15u);  // Ds3 [2][kNd3]
+  static constexpr uint32_t kOffCol = kOffD + 2u * 8u * kNd3;        // column scales [2][kKp] (float)
+  static constexpr int kBars = 2 * kStages + 2 * kM2lTcAcc + 5;       // + A full x2, A empty x2, done
+  static constexpr uint32_t kOffBar = kOffCol + 2u * 4u * kKp;
+  static constexpr uint32_t kOffSlot = kOffBar + 8u * kBars;         // TMEM address, abort flag
+  static constexpr uint32_t kUsed = kOffSlot + 16u;
+  // one CTA per SM: the block allocates all of tensor memory
+  static constexpr uint32_t kSmem = kUsed > 120u * 1024u ? kUsed : 120u * 1024u;
   static_assert(kNm <= 128, "the tensor-core class product covers n_m <= 128 (orders up to 7)");
-  static_assert(kSmem <= 226u * 1024u, "tensor-core class product shared memory");
+  static_assert(kAccCol + kM2lTcAcc * kM2lTcN <= kM2lTcCols, "tensor memory columns");
+  static_assert(kUsed <= 226u * 1024u, "tensor-core class product shared memory");
+  static_assert(kKp % 32 == 0 && kNd3 < 65535, "K halves of 16-column chunks; 16-bit derivative indices");
 };
 
 __device__ __forceinline__ void split3_bf16(double v, __nv_bfloat16* t) {
@@ -919,7 +951,7 @@ __device__ __forceinline__ void split3_bf16(double v, __nv_bfloat16* t) {
 }
 
 // Mh3[(cell * 3 + q) * kp + a] = term q of the split of Mh[cell][a] (zero for
-// a >= n_m): each cell's row of a split is kp contiguous BF16 values.
+// a >= n_m): a cell's three rows are 3 * kp contiguous BF16 values.
 __global__ void m2l_split_kernel(long n_cells, int nm, int kp, const double* __restrict__ Mh,
                                  __nv_bfloat16* __restrict__ Mh3) {
   const long e = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
@@ -932,164 +964,364 @@ __global__ void m2l_split_kernel(long n_cells, int nm, int kp, const double* __r
   for (int q = 0; q < 3; ++q) Mh3[(cell * 3 + q) * kp + a] = t[q];
 }
 
+// table3[cls * nd3 + k] = the split of D_k(v) of class cls packed as
+// {t0 | t1 << 16, t2} (zero for k >= n_d).
+__global__ void m2l_table3_kernel(long n_cls, int nd, int nd3, const double* __restrict__ table,
+                                  uint2* __restrict__ table3) {
+  const long e = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (e >= n_cls * nd3) return;
+  const long cls = e / nd3;
+  const int k = static_cast<int>(e - cls * nd3);
+  __nv_bfloat16 t[3];
+  split3_bf16(k < nd ? table[cls * nd + k] : 0.0, t);
+  table3[e] = make_uint2(static_cast<uint32_t>(__bfloat16_as_ushort(t[0])) |
+                             (static_cast<uint32_t>(__bfloat16_as_ushort(t[1])) << 16),
+                         __bfloat16_as_ushort(t[2]));
+}
+
+// Unit descriptors {class, first pair, pairs, depth difference} and the
+// source cell of every class pair.
+__global__ void m2l_tc_prep_kernel(int n_units, const int* __restrict__ unit_cls, const int* __restrict__ unit_pos,
+                                   const int* __restrict__ cls_code, const int* __restrict__ cls_end,
+                                   const unsigned long long* __restrict__ keys, int n_pairs,
+                                   const int* __restrict__ perm, const int* __restrict__ src,
+                                   int4* __restrict__ ud, int* __restrict__ psrc) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x < n_units) {
+    const int cls = unit_cls[x], pos0 = unit_pos[x];
+    ud[x] = make_int4(cls, pos0, min(kM2lUnitPairs, cls_end[cls] - pos0), m2l_key_dd(keys[cls_code[cls]]));
+  }
+  if (x < n_pairs) psrc[x] = src[perm[x]];
+}
+
 __device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
   const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
   const int n = valid ? 16 : 0;  // 0: zero fill, nothing read
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(n) : "memory");
 }
 
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Bounded wait for the phase of parity `parity` of an mbarrier. Returns
+// false (and raises the block's abort flag) when the flag is already up or
+// the wait runs past kM2lTcWaitNs.
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
+  if (*abort_flag) return false;
+  unsigned long long t0 = 0;
+  for (long spins = 1;; ++spins) {
+    if (tc::mbar_try_wait(bar, parity)) return true;
+    if ((spins & 63) == 0) {
+      if (*abort_flag) return false;
+      const unsigned long long now = global_ns();
+      if (t0 == 0) {
+        t0 = now;
+      } else if (now - t0 > kM2lTcWaitNs || spins > (1L << 34)) {
+        *abort_flag = 1;
+        return false;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// One MMA with A in tensor memory and B in shared memory.
+__device__ __forceinline__ void mma_bf16_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t idesc,
+                                            int accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+      :
+      : "r"(tmem_d), "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t (&r)[8]) {
+  asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(r[0]),
+               "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+               : "memory");
+}
+
+// A BF16 value (bit pattern) times 2^s, exact for the exponents of the
+// class matrices (no overflow or subnormal results).
+__device__ __forceinline__ uint32_t bf16_scale(uint32_t bits, float scale) {
+  const float f = __uint_as_float(bits << 16) * scale;
+  return __bfloat16_as_ushort(__float2bfloat16_rn(f));
+}
+
+// The block's units in order: unit = blockIdx.x + k * gridDim.x.
+struct TcUnits {
+  const int4* ud;
+  int n_units;
+  __device__ int4 load(int unit) const { return unit < n_units ? ud[unit] : make_int4(0, 0, 0, 0); }
+};
+
 template <int P>
 __global__ void __launch_bounds__(kM2lTcThreads, 1)
-m2l_class_tc_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter,
-                    const int* __restrict__ unit_cls, const int* __restrict__ unit_pos,
-                    const int* __restrict__ cls_code, const int* __restrict__ cls_end,
-                    const int* __restrict__ perm, const int* __restrict__ src,
-                    const __nv_bfloat16* __restrict__ Mh3, const double* __restrict__ table,
-                    const unsigned long long* __restrict__ keys, long e0, float* __restrict__ out,
-                    int* __restrict__ status) {
+m2l_class_tc_kernel(FmmDevTables T, int n_units, const int4* __restrict__ ud, const int* __restrict__ perm,
+                    const int* __restrict__ psrc, const __nv_bfloat16* __restrict__ Mh3,
+                    const uint2* __restrict__ table3, long e0, float* __restrict__ out, int* __restrict__ status) {
   using S = M2lTc<P>;
-  constexpr int kNm = S::kNm, kKp = S::kKp, kN = kM2lTcN, kChunks = kKp / 8;
+  constexpr int kNm = S::kNm, kKp = S::kKp, kN = kM2lTcN, kSt = S::kStages, kAc = kM2lTcAcc;
   extern __shared__ __align__(1024) unsigned char tc_smem[];
-  unsigned char* a_img = tc_smem;
-  unsigned char* b_img = tc_smem + S::kOffB;
-  double* Ds = reinterpret_cast<double*>(tc_smem + S::kOffD);
-  double* rowf = reinterpret_cast<double*>(tc_smem + S::kOffRow);
-  double* colf = reinterpret_cast<double*>(tc_smem + S::kOffCol);
-  int* pe = reinterpret_cast<int*>(tc_smem + S::kOffPe);
-  int* ps = reinterpret_cast<int*>(tc_smem + S::kOffPs);
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(tc_smem + S::kOffBar);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + S::kOffBar + 16);
-  __shared__ int s_unit;
+  unsigned char* b_img = tc_smem;
+  uint16_t* idx = reinterpret_cast<uint16_t*>(tc_smem + S::kOffIdx);  // [g][a]; kNd where g or a >= n_m
+  uint2* Ds3 = reinterpret_cast<uint2*>(tc_smem + S::kOffD);           // [2][kNd3]: x = t0 | t1 << 16, y = t2
+  float* colsc = reinterpret_cast<float*>(tc_smem + S::kOffCol);       // [2][kKp]
+  const uint32_t bar0 = tc::smem_u32(tc_smem + S::kOffBar);
+  // barrier addresses: full[s], empty[s], accf[b], acce[b], afull[2], aempty[2], done
+  auto full_bar = [&](int s) { return bar0 + 8u * s; };
+  auto empty_bar = [&](int s) { return bar0 + 8u * (kSt + s); };
+  auto accf_bar = [&](int b) { return bar0 + 8u * (2 * kSt + b); };
+  auto acce_bar = [&](int b) { return bar0 + 8u * (2 * kSt + kAc + b); };
+  auto afull_bar = [&](int h) { return bar0 + 8u * (2 * kSt + 2 * kAc + h); };
+  auto aempty_bar = [&](int h) { return bar0 + 8u * (2 * kSt + 2 * kAc + 2 + h); };
+  const uint32_t done_bar = bar0 + 8u * (2 * kSt + 2 * kAc + 4);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(tc_smem + S::kOffSlot);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tc_smem + S::kOffSlot + 4);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int stride = gridDim.x;
+  const TcUnits units{ud, n_units};
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc::smem_u32(mbar)));
+    auto init = [](uint32_t b, int count) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(b), "r"(count));
+    };
+    for (int s = 0; s < kSt; ++s) {
+      init(full_bar(s), kM2lTcProdThreads);
+      init(empty_bar(s), 1);
+    }
+    for (int b = 0; b < kAc; ++b) {
+      init(accf_bar(b), 1);
+      init(acce_bar(b), 32 * kM2lTcEpiWarps);
+    }
+    for (int h = 0; h < 2; ++h) {
+      init(afull_bar(h), kM2lTcBldThreads);
+      init(aempty_bar(h), 1);
+    }
+    init(done_bar, 1);
+    *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
-  if (warp == 0) {
+  if (warp == kM2lTcMmaWarp) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(tmem_slot)),
-                 "r"(kN));
+                 "r"(kM2lTcCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  for (int x = tid; x < kNm * S::kIdxStride; x += kM2lTcThreads) {
+    const int g = x / S::kIdxStride, a = x - g * S::kIdxStride;
+    idx[x] = a < kNm ? static_cast<uint16_t>(T.m2l_index_t[a * kNm + g]) : static_cast<uint16_t>(S::kNd);
   }
   tc::fence_before();
   __syncthreads();
   tc::fence_after();
   const uint32_t tmem = *tmem_slot;
-  const uint32_t a_base = tc::smem_u32(a_img), b_base = tc::smem_u32(b_img), mbar_a = tc::smem_u32(mbar);
-  const uint32_t idesc = tc::make_idesc(kN);
-  uint32_t phase = 0;
-  bool failed = false;
-  // B of the tile starting at pair `tile0` of the unit into buffer `buf`:
-  // 16-byte core-matrix rows of the pre-split expansions (zero past the
-  // unit's last pair)
-  auto load_b = [&](int tile0, int np, int buf) {
-    unsigned char* dst = b_img + buf * S::kBBuf;
-    for (int x = tid; x < kN * 3 * kChunks; x += kM2lTcThreads) {
-      const int j = x / (3 * kChunks), r = x - j * 3 * kChunks, q = r / kChunks, ch = r - q * kChunks;
-      const bool ok = tile0 + j < np;
-      const __nv_bfloat16* sp = ok ? Mh3 + (static_cast<size_t>(ps[tile0 + j]) * 3 + q) * kKp + 8 * ch : Mh3;
-      cp_async16(dst + q * S::kBSplit + tc::op_offset(j, 8 * ch, kN), sp, ok);
-    }
-    cp_async_commit();
-  };
-  for (;;) {
-    if (tid == 0) s_unit = atomicAdd(unit_counter, 1);
-    __syncthreads();  // also: the previous unit is done with the shared arrays
-    const int unit = s_unit;
-    if (unit >= n_units) break;
-    const int cls = unit_cls[unit], pos0 = unit_pos[unit];
-    const int np = min(kM2lUnitPairs, cls_end[cls] - pos0);
-    const int dd = m2l_key_dd(keys[cls_code[cls]]);
-    const int et = dd < 0 ? -dd : 0, es = dd > 0 ? dd : 0;  // log2(h_t / u), log2(h_s / u)
-    for (int k = tid; k < S::kNd; k += kM2lTcThreads) Ds[k] = table[static_cast<size_t>(cls) * S::kNd + k];
-    for (int g = tid; g < 128; g += kM2lTcThreads) rowf[g] = g < kNm ? ldexp(T.inv_fact[g], (T.multi[g].w + 1) * et) : 0.0;
-    for (int a = tid; a < kKp; a += kM2lTcThreads) colf[a] = a < kNm ? ldexp(1.0, T.multi[a].w * es) : 0.0;
-    for (int p = tid; p < np; p += kM2lTcThreads) {
-      const int e = perm[pos0 + p];
-      pe[p] = e;
-      ps[p] = src[e];
-    }
-    __syncthreads();
-    load_b(0, np, 0);
-    // A = class matrix, three BF16 splits (built while the first tile's B arrives)
-    for (int x = tid; x < 128 * kKp; x += kM2lTcThreads) {
-      const int g = x / kKp, a = x - g * kKp;
-      const double v = (g < kNm && a < kNm) ? Ds[T.m2l_index_t[a * kNm + g]] * colf[a] : 0.0;
-      __nv_bfloat16 t[3];
-      split3_bf16(v, t);
-      const uint32_t o = tc::op_offset(g, a, 128);
+
+  if (warp < kM2lTcEpiWarps) {
+    // ---- accumulator readers: row g, all kN pairs of a tile
+    const int g = 32 * warp + lane;
+    const uint32_t lane_addr = static_cast<uint32_t>(32 * warp) << 16;
+    const double ifact = g < kNm ? T.inv_fact[g] : 0.0;
+    const int wg1 = g < kNm ? T.multi[g].w + 1 : 0;
+    long i = 0;
+    int4 u = units.load(blockIdx.x);
+    for (int unit = blockIdx.x; unit < n_units; unit += stride) {
+      const int4 un = units.load(unit + stride);  // next unit, in flight
+      const int pos0 = u.y, np = u.z, et = u.w < 0 ? -u.w : 0;  // log2(h_t / u)
+      const double rf = ldexp(ifact, wg1 * et);
+      int e_lo = lane < np ? perm[pos0 + lane] : 0, e_hi = 32 + lane < np ? perm[pos0 + 32 + lane] : 0;
+      for (int tile0 = 0; tile0 < np; tile0 += kN, ++i) {
+        const int b = static_cast<int>(i % kAc);
+        const int nx = tile0 + kN;  // the next tile's pairs, in flight
+        const int f_lo = nx + lane < np ? perm[pos0 + nx + lane] : 0;
+        const int f_hi = nx + 32 + lane < np ? perm[pos0 + nx + 32 + lane] : 0;
+        const bool ok = tc_wait(accf_bar(b), static_cast<uint32_t>((i / kAc) & 1), abort_flag);
+        tc::fence_after();
+        float v0[32], v1[32];
+        tc::tmem_ld32(tmem + lane_addr + S::kAccCol + b * kN, v0);
+        tc::tmem_ld32(tmem + lane_addr + S::kAccCol + b * kN + 32, v1);
+        tc::fence_before();
+        mbar_arrive(acce_bar(b));
+        const int live = min(kN, np - tile0);
 #pragma unroll
-      for (int q = 0; q < 3; ++q) *reinterpret_cast<__nv_bfloat16*>(a_img + q * S::kASplit + o) = t[q];
+        for (int j = 0; j < 32; ++j) {
+          const int ej = __shfl_sync(0xFFFFFFFFu, e_lo, j);
+          if (ok && j < live && g < kNm) out[static_cast<size_t>(ej - e0) * kNm + g] = static_cast<float>(v0[j] * rf);
+        }
+#pragma unroll
+        for (int j = 0; j < 32; ++j) {
+          const int ej = __shfl_sync(0xFFFFFFFFu, e_hi, j);
+          if (ok && 32 + j < live && g < kNm)
+            out[static_cast<size_t>(ej - e0) * kNm + g] = static_cast<float>(v1[j] * rf);
+        }
+        e_lo = f_lo;
+        e_hi = f_hi;
+      }
+      u = un;
     }
-    const int n_tiles = (np + kN - 1) / kN;
-    for (int tile = 0; tile < n_tiles && !failed; ++tile) {
-      const int tile0 = tile * kN, buf = tile & 1;
-      const int live = min(kN, np - tile0);
-      if (tile + 1 < n_tiles) {
-        load_b(tile0 + kN, np, buf ^ 1);
+  } else if (warp < kM2lTcProd0) {
+    // ---- A builders: row g of A, half c2 of its K range
+    const int bt = tid - 32 * kM2lTcBld0, q4 = warp & 3, c2 = (warp - kM2lTcBld0) >> 2, g = 32 * q4 + lane;
+    const uint32_t lane_addr = static_cast<uint32_t>(32 * q4) << 16;
+    const uint32_t* irow = reinterpret_cast<const uint32_t*>(idx + (g < kNm ? g : 0) * S::kIdxStride);
+    constexpr int kCopies = S::kNd3 * 8 / 16;  // 16-byte copies of one packed D row
+    auto stage_d = [&](int4 uu, int h) {     // the packed D row of unit uu's class into Ds3[h]
+      const unsigned char* srcp = reinterpret_cast<const unsigned char*>(table3 + static_cast<size_t>(uu.x) * S::kNd3);
+      unsigned char* dst = reinterpret_cast<unsigned char*>(Ds3 + h * S::kNd3);
+      for (int x = bt; x < kCopies; x += kM2lTcBldThreads) cp_async16(dst + 16 * x, srcp + 16 * x, true);
+      cp_async_commit();
+    };
+    int4 u = units.load(blockIdx.x);
+    if (blockIdx.x < n_units) stage_d(u, 0);
+    for (int k = 0, unit = blockIdx.x; unit < n_units; ++k, unit += stride) {
+      const int4 un = units.load(unit + stride);
+      const int es = u.w > 0 ? u.w : 0;  // log2(h_s / u)
+      const int h = k & 1;
+      float* cs = colsc + h * kKp;
+      if (es > 0)
+        for (int x = bt; x < kKp; x += kM2lTcBldThreads)
+          cs[x] = x < kNm ? __uint_as_float(static_cast<uint32_t>(127 + T.multi[x].w * es) << 23) : 0.0f;
+      if (unit + stride < n_units) {
+        stage_d(un, h ^ 1);  // the next unit's row: its buffer was released by the barrier ending the last build
         cp_async_wait<1>();
       } else {
         cp_async_wait<0>();
       }
-      tc::fence_proxy_async();  // this thread's A writes and landed copies, for the async proxy
-      tc::fence_before();
-      __syncthreads();
-      if (tid == 0) {
-        tc::fence_after();
-        constexpr int kCombo[6][2] = {{2, 0}, {1, 1}, {0, 2}, {1, 0}, {0, 1}, {0, 0}};  // small terms first
-        const uint32_t bb = b_base + buf * S::kBBuf;
-        int first = 1;
-        for (int st = 0; st < kKp / 16; ++st)
+      asm volatile("bar.sync 1, %0;" ::"n"(kM2lTcBldThreads) : "memory");  // Ds3[h], colsc[h] complete
+      // A buffer h was last read by unit k - 2
+      const bool ok = k < 2 || tc_wait(aempty_bar(h), static_cast<uint32_t>(((k - 2) >> 1) & 1), abort_flag);
+      if (!__any_sync(0xFFFFFFFFu, !ok)) {  // warp-uniform: tcgen05.st is .aligned
+        const uint2* D3 = Ds3 + h * S::kNd3;
+        const uint32_t abase = tmem + lane_addr + h * S::kABuf;
+#pragma unroll 1
+        for (int a0 = c2 * (kKp / 2); a0 < (c2 + 1) * (kKp / 2); a0 += 16) {
+          uint32_t r[3][8];
 #pragma unroll
-          for (int c = 0; c < 6; ++c) {
-            const uint64_t ad = tc::make_sdesc(a_base + kCombo[c][0] * S::kASplit + st * 128 * 32);
-            const uint64_t bd = tc::make_sdesc(bb + kCombo[c][1] * S::kBSplit + st * kN * 32);
-            tc::mma_bf16(tmem, ad, bd, idesc, first ? 0 : 1);
-            first = 0;
+          for (int c = 0; c < 8; ++c) {
+            // two derivative indices per 32-bit load; even k in the low half of a column
+            const uint32_t ip = g < kNm ? irow[(a0 >> 1) + c] : (S::kNd | (S::kNd << 16));
+            uint2 d0 = D3[ip & 0xFFFFu], d1 = D3[ip >> 16];
+            if (es > 0) {
+              const float s0 = cs[a0 + 2 * c], s1 = cs[a0 + 2 * c + 1];
+              d0 = make_uint2(bf16_scale(d0.x & 0xFFFFu, s0) | (bf16_scale(d0.x >> 16, s0) << 16),
+                              bf16_scale(d0.y, s0));
+              d1 = make_uint2(bf16_scale(d1.x & 0xFFFFu, s1) | (bf16_scale(d1.x >> 16, s1) << 16),
+                              bf16_scale(d1.y, s1));
+            }
+            r[0][c] = __byte_perm(d0.x, d1.x, 0x5410);
+            r[1][c] = __byte_perm(d0.x, d1.x, 0x7632);
+            r[2][c] = __byte_perm(d0.y, d1.y, 0x5410);
           }
-        tc::mma_commit(mbar_a);
-      }
-      long spins = 0;
-      bool ok = true;
-      while (!tc::mbar_try_wait(mbar_a, phase)) {
-        if (++spins > kM2lTcWaitLimit) {
-          ok = false;
-          break;
-        }
-      }
-      phase ^= 1u;
-      tc::fence_after();
-      if (!__syncthreads_and(ok)) {
-        failed = true;
-        break;
-      }
-      // epilogue: warp w (< 4) holds accumulator rows g = 32 w + lane
-      if (warp < 4) {
-        const int g = 32 * warp + lane;
-        const double rf = rowf[g];
 #pragma unroll
-        for (int c0 = 0; c0 < kN; c0 += 32) {
-          float v[32];
-          tc::tmem_ld32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + c0, v);
-          if (g < kNm) {
-#pragma unroll
-            for (int j = 0; j < 32; ++j)
-              if (c0 + j < live)
-                out[static_cast<size_t>(pe[tile0 + c0 + j] - e0) * kNm + g] = static_cast<float>(v[j] * rf);
-          }
+          for (int q = 0; q < 3; ++q) tmem_st8(abase + q * S::kACols + a0 / 2, r[q]);
         }
+        asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
       }
       tc::fence_before();
-      __syncthreads();  // accumulator read out and buffer free before the next tile's products
-      tc::fence_after();
+      mbar_arrive(afull_bar(h));
+      asm volatile("bar.sync 1, %0;" ::"n"(kM2lTcBldThreads) : "memory");  // Ds3[h], colsc[h] free
+      u = un;
     }
-    cp_async_wait<0>();  // no copy of an abandoned tile left in flight
-    __syncthreads();
-    if (failed) break;
+    cp_async_wait<0>();
+  } else if (warp < kM2lTcMmaWarp) {
+    // ---- B producers: thread pt copies half of pair j's 3 * kChunks rows
+    const int pt = tid - 32 * kM2lTcProd0, j = pt >> 1, hh = pt & 1;
+    long i = 0;
+    int unit = blockIdx.x, tile0 = 0;
+    int4 u = units.load(unit);
+    int cur = unit < n_units && j < u.z ? psrc[u.y + j] : -1;
+    while (unit < n_units) {
+      // the next tile (possibly of the next unit): its source cell, in flight
+      int nunit = unit, ntile0 = tile0 + kN;
+      int4 nu = u;
+      if (ntile0 >= u.z) {
+        nunit = unit + stride;
+        ntile0 = 0;
+        nu = units.load(nunit);
+      }
+      const int nxt = nunit < n_units && ntile0 + j < nu.z ? psrc[nu.y + ntile0 + j] : -1;
+      const int s = static_cast<int>(i % kSt);
+      const bool ok = i < kSt || tc_wait(empty_bar(s), static_cast<uint32_t>((i / kSt - 1) & 1), abort_flag);
+      if (ok) {
+        const bool live = cur >= 0;
+        const unsigned char* sp =
+            reinterpret_cast<const unsigned char*>(Mh3) + (live ? static_cast<size_t>(cur) * (3u * kKp * 2u) : 0);
+        unsigned char* dst = b_img + s * S::kBStage;
+#pragma unroll 4
+        for (int r = hh; r < 3 * S::kChunks; r += 2) {
+          const int q = r / S::kChunks, ch = r - q * S::kChunks;
+          cp_async16(dst + q * S::kBSplit + tc::op_offset(j, 8 * ch, kN), sp + 16 * r, live);
+        }
+      }
+      cp_async_commit();
+      if (i >= 1) {  // the previous tile's copies have landed: publish them to the tensor core
+        cp_async_wait<1>();
+        tc::fence_proxy_async();
+        mbar_arrive(full_bar(static_cast<int>((i - 1) % kSt)));
+      }
+      ++i;
+      unit = nunit;
+      tile0 = ntile0;
+      u = nu;
+      cur = nxt;
+    }
+    cp_async_wait<0>();
+    if (i >= 1) {
+      tc::fence_proxy_async();
+      mbar_arrive(full_bar(static_cast<int>((i - 1) % kSt)));
+    }
+  } else if (lane == 0) {
+    // ---- MMA issue: six split products per K step of 16, smallest terms first
+    constexpr int kCombo[6][2] = {{2, 0}, {1, 1}, {0, 2}, {1, 0}, {0, 1}, {0, 0}};
+    const uint32_t idesc = tc::make_idesc(kN), b_base = tc::smem_u32(b_img);
+    long i = 0;
+    int4 u = units.load(blockIdx.x);
+    for (int k = 0, unit = blockIdx.x; unit < n_units; ++k, unit += stride) {
+      const int4 un = units.load(unit + stride);
+      const int h = k & 1;
+      const bool a_ok = tc_wait(afull_bar(h), static_cast<uint32_t>((k >> 1) & 1), abort_flag);
+      const uint32_t abuf = tmem + h * S::kABuf;
+      for (int tile0 = 0; tile0 < u.z; tile0 += kN, ++i) {
+        const int s = static_cast<int>(i % kSt), b = static_cast<int>(i % kAc);
+        bool ok = a_ok && tc_wait(full_bar(s), static_cast<uint32_t>((i / kSt) & 1), abort_flag);
+        ok = ok && (i < kAc || tc_wait(acce_bar(b), static_cast<uint32_t>((i / kAc - 1) & 1), abort_flag));
+        tc::fence_after();
+        if (ok) {
+          const uint32_t bb = b_base + s * S::kBStage, d = tmem + S::kAccCol + b * kN;
+          uint64_t bd[3];
+#pragma unroll
+          for (int q = 0; q < 3; ++q) bd[q] = tc::make_sdesc(bb + q * S::kBSplit);
+#pragma unroll
+          for (int st = 0; st < kKp / 16; ++st)
+#pragma unroll
+            for (int c = 0; c < 6; ++c)  // descriptor start address advances by 16-byte units
+              mma_bf16_ts(d, abuf + kCombo[c][0] * S::kACols + st * 8,
+                          bd[kCombo[c][1]] + static_cast<uint64_t>((st * kN * 32) >> 4), idesc, (st | c) != 0);
+        }
+        tc::mma_commit(empty_bar(s));  // arrives once the products above have read the stage
+        tc::mma_commit(accf_bar(b));
+      }
+      tc::mma_commit(aempty_bar(h));  // every product of this unit has read A buffer h
+      u = un;
+    }
+    // every product has completed before tensor memory is released
+    tc::mma_commit(done_bar);
+    const unsigned long long t0 = global_ns();
+    while (!tc::mbar_try_wait(done_bar, 0) && global_ns() - t0 < kM2lTcWaitNs) {
+    }
   }
-  if (failed && tid == 0) atomicExch(status, 1);
+  __syncwarp();
   tc::fence_before();
   __syncthreads();
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kN));
+  tc::fence_after();
+  if (warp == kM2lTcMmaWarp)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kM2lTcCols));
+  if (tid == 0 && *abort_flag) atomicExch(status, 1);
 }
 
 // Pairs outside the classes: a warp per pair (persistent blocks), the
@@ -1243,19 +1475,16 @@ int class_product(amk_ctx* c, int order, const FmmDevTables& T, int n_units, int
 }
 
 template <int P>
-int launch_class_tc(amk_ctx* c, const FmmDevTables& T, int n_units, int* unit_counter, const int* unit_cls,
-                    const int* unit_pos, const int* cls_code, const int* cls_end, const int* perm, const int* src,
-                    const __nv_bfloat16* Mh, const double* table, const unsigned long long* keys, long e0,
-                    float* out, int* status) {
+int launch_class_tc(amk_ctx* c, const FmmDevTables& T, int n_units, const int4* ud, const int* perm,
+                    const int* psrc, const __nv_bfloat16* Mh3, const uint2* table3, long e0, float* out,
+                    int* status) {
   const size_t smem = M2lTc<P>::kSmem;
   AMK_CUDA_TRY(cudaFuncSetAttribute(m2l_class_tc_kernel<P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     static_cast<int>(smem)));
   int sms = 0;
   AMK_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
   const int grid = std::max(1, std::min(n_units, sms));  // one CTA per SM (shared memory and TMEM)
-  AMK_CUDA_TRY(cudaMemsetAsync(unit_counter, 0, sizeof(int), c->stream));
-  m2l_class_tc_kernel<P><<<grid, kM2lTcThreads, smem, c->stream>>>(T, n_units, unit_counter, unit_cls, unit_pos,
-                                                                   cls_code, cls_end, perm, src, Mh, table, keys, e0,
+  m2l_class_tc_kernel<P><<<grid, kM2lTcThreads, smem, c->stream>>>(T, n_units, ud, perm, psrc, Mh3, table3, e0,
                                                                    out, status);
   return check_launch(c, "m2l_class_tc_kernel");
 }
@@ -1264,22 +1493,16 @@ int launch_class_tc(amk_ctx* c, const FmmDevTables& T, int n_units, int* unit_co
 // FP64 products are already cheap next to the rest of the evaluation).
 inline bool tc_order(int order) { return order >= 5 && order <= 7; }
 
-int class_tc(amk_ctx* c, int order, const FmmDevTables& T, int n_units, int* unit_counter, const int* unit_cls,
-             const int* unit_pos, const int* cls_code, const int* cls_end, const int* perm, const int* src,
-             const __nv_bfloat16* Mh, const double* table, const unsigned long long* keys, long e0, float* out,
-             int* status) {
+// Packed D row length of the tensor-core product for an order.
+inline int tc_nd3(int n_d) { return (n_d + 2) & ~1; }
+
+int class_tc(amk_ctx* c, int order, const FmmDevTables& T, int n_units, const int4* ud, const int* perm,
+             const int* psrc, const __nv_bfloat16* Mh3, const uint2* table3, long e0, float* out, int* status) {
   switch (order) {
-    case 5:
-      return launch_class_tc<5>(c, T, n_units, unit_counter, unit_cls, unit_pos, cls_code, cls_end, perm, src, Mh,
-                                table, keys, e0, out, status);
-    case 6:
-      return launch_class_tc<6>(c, T, n_units, unit_counter, unit_cls, unit_pos, cls_code, cls_end, perm, src, Mh,
-                                table, keys, e0, out, status);
-    case 7:
-      return launch_class_tc<7>(c, T, n_units, unit_counter, unit_cls, unit_pos, cls_code, cls_end, perm, src, Mh,
-                                table, keys, e0, out, status);
-    default:
-      return fail(AMK_ERR_INVALID, "no tensor-core class product for order %d", order);
+    case 5: return launch_class_tc<5>(c, T, n_units, ud, perm, psrc, Mh3, table3, e0, out, status);
+    case 6: return launch_class_tc<6>(c, T, n_units, ud, perm, psrc, Mh3, table3, e0, out, status);
+    case 7: return launch_class_tc<7>(c, T, n_units, ud, perm, psrc, Mh3, table3, e0, out, status);
+    default: return fail(AMK_ERR_INVALID, "no tensor-core class product for order %d", order);
   }
 }
 
@@ -1327,7 +1550,10 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
   AMK_CUDA_TRY(cudaMemsetAsync(keys, 0xff, kM2lHashSlots * sizeof(unsigned long long), c->stream));
   m2l_classify_kernel<<<4 * 148, 256, 0, c->stream>>>(t, gm.off, gm.count, gm.src, reach, keys, codes, tgt);
   AMK_TRY(check_launch(c, "m2l_classify_kernel"));
-  long cap = std::max<long>(1L << 20, static_cast<long>(kM2lChunkBytes / (sizeof(double) * T.n_m)));
+  // the tensor-core products (split BF16) write FP32 per-pair products
+  const bool tc = c->fmm_precision == AMK_FMM_TENSOR && tc_order(order);
+  const size_t esz = tc ? sizeof(float) : sizeof(double);
+  long cap = std::max<long>(1L << 20, static_cast<long>(kM2lChunkBytes / (esz * T.n_m)));
   if (const char* env = getenv("AMK_FMM_M2L_CHUNK_PAIRS")) {  // smaller chunks (tests of the chunk seams)
     const long v = atol(env);
     if (v > 0) cap = std::min(cap, v);
@@ -1353,14 +1579,11 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
   AMK_TRY(rc);
   int* unit_pos = slot<int>(c, kSlotM2lTilePos, max_units, &rc);
   AMK_TRY(rc);
-  // the tensor-core products (split BF16) write FP32 per-pair products
-  const bool tc = c->fmm_precision == AMK_FMM_TENSOR && tc_order(order);
-  const size_t esz = tc ? sizeof(float) : sizeof(double);
   int* tc_status = counters + 6;
   __nv_bfloat16* Mh3 = nullptr;
   if (tc) {
     AMK_CUDA_TRY(cudaMemsetAsync(tc_status, 0, sizeof(int), c->stream));
-    const int kp = 16 * ((T.n_m + 15) / 16);
+    const int kp = 32 * ((T.n_m + 31) / 32);  // M2lTc<P>::kKp
     Mh3 = slot<__nv_bfloat16>(c, kSlotM2lSplit, static_cast<size_t>(nn) * 3 * kp, &rc);
     AMK_TRY(rc);
     m2l_split_kernel<<<static_cast<unsigned>((nn * kp + 255) / 256), 256, 0, c->stream>>>(nn, T.n_m, kp, Mh, Mh3);
@@ -1409,10 +1632,31 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
       m2l_table_kernel<<<(n_cls + kFmmWarps - 1) / kFmmWarps, 32 * kFmmWarps, tsm, c->stream>>>(T, cls_code, n_cls,
                                                                                               keys, table);
       AMK_TRY(check_launch(c, "m2l_table_kernel"));
+      int4* ud = nullptr;
+      int* psrc = nullptr;
+      uint2* table3 = nullptr;
+      if (tc) {  // the tensor-core product's inputs: split D rows, unit descriptors, pair sources
+        const int nd3 = tc_nd3(T.n_d);
+        const long n_cp = ne - n_fb;  // pairs in classes: perm[0, n_cp)
+        table3 = slot<uint2>(c, kSlotM2lTable3, static_cast<size_t>(n_cls) * nd3, &rc);
+        AMK_TRY(rc);
+        ud = slot<int4>(c, kSlotM2lUnitDesc, static_cast<size_t>(n_units), &rc);
+        AMK_TRY(rc);
+        psrc = slot<int>(c, kSlotM2lPairSrc, static_cast<size_t>(std::max<long>(1, n_cp)), &rc);
+        AMK_TRY(rc);
+        const long nt = static_cast<long>(n_cls) * nd3;
+        m2l_table3_kernel<<<static_cast<unsigned>((nt + 255) / 256), 256, 0, c->stream>>>(n_cls, T.n_d, nd3, table,
+                                                                                         table3);
+        AMK_TRY(check_launch(c, "m2l_table3_kernel"));
+        const long np_ = std::max<long>(n_units, n_cp);
+        m2l_tc_prep_kernel<<<static_cast<unsigned>((np_ + 255) / 256), 256, 0, c->stream>>>(
+            n_units, unit_cls, unit_pos, cls_code, cls_end, keys, static_cast<int>(n_cp), perm, gm.src, ud, psrc);
+        AMK_TRY(check_launch(c, "m2l_tc_prep_kernel"));
+      }
       AMK_TRY(phase_begin(c, AMK_PHASE_FMM_M2L_PRODUCTS));
       if (tc)
-        AMK_TRY(class_tc(c, order, T, n_units, counters + 4, unit_cls, unit_pos, cls_code, cls_end, perm, gm.src, Mh3,
-                         table, keys, e0, static_cast<float*>(out), tc_status));
+        AMK_TRY(class_tc(c, order, T, n_units, ud, perm, psrc, Mh3, table3, e0, static_cast<float*>(out),
+                         tc_status));
       else
         AMK_TRY(class_product(c, order, T, n_units, counters + 4, unit_cls, unit_pos, cls_code, cls_end, perm,
                               gm.src, Mh, table, keys, e0, static_cast<double*>(out)));
@@ -2082,6 +2326,12 @@ int fmm_forces(amk_ctx* c, const View& v, int order, double theta, long leaf_cap
 // relative far-field error, scaled to order one.
 constexpr int kFeat = 35;
 constexpr double kTargetScale = 100.0;
+// The correction is bounded: a predicted relative error above 20 % of |E|
+// (far beyond the p=2 truncation error) or not finite is scaled back to it,
+// so a network queried outside its training distribution cannot inject an
+// unbounded force. Features are clipped to +-64 for the same reason.
+constexpr double kMaxPred = 0.2 * kTargetScale;
+constexpr float kMaxFeature = 64.0f;
 
 __global__ void fmm_features_kernel(const Octree t, FmmDevTables T, const double* __restrict__ L,
                                     const double* __restrict__ M, const double* __restrict__ radius,
@@ -2130,6 +2380,7 @@ __global__ void fmm_features_kernel(const Octree t, FmmDevTables T, const double
   f[32] = static_cast<float>(radius[leaf] / h);
   f[33] = static_cast<float>(p2p_count[leaf]) / 64.f;
   f[34] = 1.f;
+  for (int i = 0; i < kFeat; ++i) f[i] = isfinite(f[i]) ? fminf(fmaxf(f[i], -kMaxFeature), kMaxFeature) : 0.f;
   scale[s] = se / kTargetScale;
 }
 
@@ -2138,9 +2389,12 @@ __global__ void fmm_correct_kernel(const float* __restrict__ pred, const double*
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= m) return;
   double4 e = ef[k];
-  e.x += scale[k] * pred[3 * k + 0];
-  e.y += scale[k] * pred[3 * k + 1];
-  e.z += scale[k] * pred[3 * k + 2];
+  const double px = pred[3 * k + 0], py = pred[3 * k + 1], pz = pred[3 * k + 2];
+  const double n2 = px * px + py * py + pz * pz;
+  const double lim = n2 <= kMaxPred * kMaxPred ? 1.0 : (isfinite(n2) ? kMaxPred / sqrt(n2) : 0.0);
+  e.x += scale[k] * lim * px;
+  e.y += scale[k] * lim * py;
+  e.z += scale[k] * lim * pz;
   ef[k] = e;
 }
 

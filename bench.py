@@ -222,6 +222,7 @@ def e2e_through_abi(sim, stream, n, steps, step_fn=None):
 TREE_METHODS = [
     ("allpairs", dict(coulomb_method="allpairs")),
     ("barnes-hut theta=0.7", dict(coulomb_method="barnes-hut", barnes_hut_theta=0.7)),
+    ("fmm p=2 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=2, fast_multipole_theta=0.5)),
     ("fmm p=4 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=4, fast_multipole_theta=0.5)),
     ("fmm p=6 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=6, fast_multipole_theta=0.5)),
     ("fmm p=7 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=7, fast_multipole_theta=0.5)),
@@ -234,6 +235,9 @@ TREE_METHODS = [
                                         fast_multipole_theta=0.5, fmm_learned=1, learned_audit_interval=0)),
 ]
 PLAIN_P6 = "fmm p=6 theta=0.5"
+# training of the learned correction: particles of 8,192 sampled leaves,
+# 8,000 Adam steps of 4,096 samples (outside the timed region)
+LEARNED_TRAINING = dict(sample_leaves=8192, steps=8000, batch=4096, lr=5e-4)
 LEARNED = "learned p=2 + MLP theta=0.5"
 
 # DRAM traffic (read + write) per launch of the FMM's M2L class-product kernel,
@@ -340,7 +344,7 @@ def tree_method_entry(sim, name, over, args, stream, flusher):
     entry = {}
     if over.get("fmm_learned"):
         t0 = time.perf_counter()
-        loss, samples = sim.fmm_train_correction(0.5, sample_leaves=4096, steps=2000, batch=4096, lr=1e-3)
+        loss, samples = sim.fmm_train_correction(0.5, **LEARNED_TRAINING)
         entry["training"] = {"seconds": round(time.perf_counter() - t0, 2), "samples": samples,
                              "final_loss": loss}
     sim.coulomb()
@@ -496,7 +500,7 @@ def run_tree(args):
     sim, stream = new_sim(over)
     flusher = Flusher(device, stream)
     if over.get("fmm_learned"):
-        sim.fmm_train_correction(0.5, sample_leaves=4096, steps=2000, batch=4096, lr=1e-3)
+        sim.fmm_train_correction(0.5, **LEARNED_TRAINING)
     for _ in range(args.warmup):
         sim.step(1)
         flusher()
@@ -1096,7 +1100,7 @@ def run_long(args):
         entry = {}
         if learned:
             t0 = time.perf_counter()
-            loss, samples = sim.fmm_train_correction(0.5, sample_leaves=4096, steps=2000, batch=4096, lr=1e-3)
+            loss, samples = sim.fmm_train_correction(0.5, **LEARNED_TRAINING)
             entry["training"] = {"seconds": round(time.perf_counter() - t0, 2), "samples": samples,
                                  "final_loss": loss}
         sampler = ClockSampler(local)

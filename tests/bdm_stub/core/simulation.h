@@ -1,6 +1,8 @@
-// Test stand-in for BioDynaMo's Simulation: the active simulation's Param.
+// Test stand-in for BioDynaMo's Simulation: the active simulation's Param
+// and Scheduler.
 #pragma once
 #include "core/param/param.h"
+#include "core/scheduler.h"
 namespace bdm {
 class Simulation {
  public:
@@ -10,6 +12,8 @@ class Simulation {
     return s;
   }
   static Simulation* GetActive() { return Active(); }
+  Scheduler scheduler;
   const Param* GetParam() const { return &param; }
+  Scheduler* GetScheduler() { return &scheduler; }
 };
 }  // namespace bdm

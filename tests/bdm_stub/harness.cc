@@ -155,6 +155,7 @@ extern "C" int harness_steps(long n, double* x, double* y, double* z, double* vx
     es.cutoff_radius = cutoff;
     bdm::EnergyHistory history;
     for (int s = 1; s <= steps; ++s) {
+      sim.scheduler.simulated_steps = static_cast<uint64_t>(s - 1);  // steps completed before this one
       bdm::ComputeStandardCoulombForces(&a.rm, cutoff);
       for (long i = 0; i < n; ++i)
         if (!a.parts[i]->removed)

@@ -15,7 +15,7 @@ MASS = {0: 1.67262192369e-27, 1: 9.1093837015e-31, 3: 9.1093837015e-31}
 
 
 def params(n_e=60000, n_p=40000, radii=(5e-4, 5e-4, 2e-3), temp=100.0, seed=7):
-    return amk.make_params(seed=seed, b0=5.0, trap_voltage=100.0, z0=0.02, rho0=0.02,
+    return amk.make_params(seed=seed, b0=5.0, trap_voltage=100.0, z0=0.02, rho0=0.02, cutoff_radius=2e-5,
                            populations={"positron": n_e, "antiproton": n_p},
                            temperatures={"positron": temp, "antiproton": temp}, cloud_radii=radii)
 

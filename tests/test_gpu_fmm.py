@@ -160,8 +160,9 @@ def test_fmm_off_origin_cloud_at_order_8(sim):
 
 @pytest.mark.parametrize("order", [5, 6, 7])
 def test_tensor_core_products_match_the_fp64_path(order):
-    # split-BF16 tcgen05 class products: the forces stay within 2e-6 of the
-    # FP64 products and the error against the exact sum is unchanged
+    # split-BF16 tcgen05 class products (FP32 per-pair products): the forces
+    # stay within 1e-6 RMS (1e-5 at worst) of the FP64 products and the error
+    # against the exact sum is unchanged
     import amk
     x, y, z, q = gaussian_cloud(20000, 45, mixed=False)
     exact = O.allpairs(x, y, z, q)
@@ -174,7 +175,7 @@ def test_tensor_core_products_match_the_fp64_path(order):
         again = s.solve_fmm(x, y, z, q, order, 0.5)
     assert all(np.array_equal(a, b) for a, b in zip(got, again))  # run-to-run deterministic
     rel, _ = rel_errors(got, ref)
-    assert np.max(rel) < 2e-6, np.max(rel)
+    assert np.sqrt(np.mean(rel ** 2)) < 1e-6 and np.max(rel) < 1e-5, (np.sqrt(np.mean(rel ** 2)), np.max(rel))
     e_ref = np.sqrt(np.mean(rel_errors(ref, exact)[0] ** 2))
     e_tc = np.sqrt(np.mean(rel_errors(got, exact)[0] ** 2))
     assert e_tc <= 1.02 * e_ref + 1e-7, (e_tc, e_ref)

@@ -22,15 +22,17 @@ def cloud_sim(n=65536, seed=50, **over):
 
 
 def test_training_and_measured_gain_on_a_held_out_cloud():
-    # trained on one cloud, audited on a second cloud of the same shape
-    # (another seed); the correction reduces the p=2 error on the cloud it
-    # was trained on and does not increase it on the held-out one -- the
-    # gain is small because the p=2 residual is dominated by the source
-    # cells' dropped moments, which per-particle features cannot see
+    # trained on one cloud (all of its particles), audited on it and on a
+    # second cloud of the same shape (another seed): the correction must
+    # reduce the p=2 error by at least 10 % on the cloud it was trained on and
+    # by at least 5 % on the held-out one (measured: about 20 % and 11 %). The
+    # gain stays far from the 1e-5 budget because the p=2 residual is
+    # dominated by the source cells' dropped moments, which per-particle
+    # features cannot see; a network that learned nothing fails both bounds.
     with cloud_sim() as s:
         plain = s.fmm_audit(2, 0.5, False, 2048)
-        loss, samples = s.fmm_train_correction(0.5, sample_leaves=1024, steps=800, batch=2048, lr=1e-3)
-        assert samples > 1000 and np.isfinite(loss)
+        loss, samples = s.fmm_train_correction(0.5, sample_leaves=4096, steps=8000, batch=4096, lr=5e-4)
+        assert samples == 65536 and np.isfinite(loss)
         learned = s.fmm_audit(2, 0.5, True, 2048)
         assert s.fmm_learned_state()["trained"]
         x, y, z, _ = gaussian_cloud(65536, 51, mixed=False)
@@ -40,9 +42,8 @@ def test_training_and_measured_gain_on_a_held_out_cloud():
         p6_b = s.fmm_audit(6, 0.5, False, 2048)
     print(f"RMS relative force error, training cloud: p=2 {plain:.3e}, p=2 + MLP {learned:.3e}; "
           f"held-out cloud: p=2 {plain_b:.3e}, p=2 + MLP {learned_b:.3e}, p=6 {p6_b:.3e}")
-    assert np.isfinite(learned) and np.isfinite(learned_b)
-    assert learned < plain               # a gain on the training cloud
-    assert learned_b <= 1.01 * plain_b   # not worse on the held-out cloud
+    assert learned < 0.9 * plain, (learned, plain)
+    assert learned_b < 0.95 * plain_b, (learned_b, plain_b)
     assert p6_b < 1e-2 * plain_b
 
 
