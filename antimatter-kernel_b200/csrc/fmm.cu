@@ -928,8 +928,10 @@ struct M2lTc {
   static constexpr uint32_t kOffIdx = kStages * kBStage;             // idx [kNm][kIdxStride] (u16)
   static constexpr uint32_t kOffD = kOffIdx + ((2u * kNm * kIdxStride + 15u) & ~15u);  // Ds3 [2][kNd3]
   static constexpr uint32_t kOffCol = kOffD + 2u * 8u * kNd3;        // column scales [2][kKp] (float)
+  static constexpr uint32_t kOffStg = kOffCol + 2u * 4u * kKp;       // output staging [kN][kNm] (float)
+  static constexpr uint32_t kOffPe = kOffStg + 4u * kM2lTcN * kNm;    // the tile's pair ids [kN]
   static constexpr int kBars = 2 * kStages + 2 * kM2lTcAcc + 5;       // + A full x2, A empty x2, done
-  static constexpr uint32_t kOffBar = kOffCol + 2u * 4u * kKp;
+  static constexpr uint32_t kOffBar = kOffPe + 4u * kM2lTcN;
   static constexpr uint32_t kOffSlot = kOffBar + 8u * kBars;         // TMEM address, abort flag
   static constexpr uint32_t kUsed = kOffSlot + 16u;
   // one CTA per SM: the block allocates all of tensor memory
@@ -938,6 +940,7 @@ struct M2lTc {
   static_assert(kAccCol + kM2lTcAcc * kM2lTcN <= kM2lTcCols, "tensor memory columns");
   static_assert(kUsed <= 226u * 1024u, "tensor-core class product shared memory");
   static_assert(kKp % 32 == 0 && kNd3 < 65535, "K halves of 16-column chunks; 16-bit derivative indices");
+  static_assert(kNm % 4 == 0, "per-pair product rows are whole 16-byte vectors");
 };
 
 __device__ __forceinline__ void split3_bf16(double v, __nv_bfloat16* t) {
@@ -1123,23 +1126,27 @@ m2l_class_tc_kernel(FmmDevTables T, int n_units, const int4* __restrict__ ud, co
   const uint32_t tmem = *tmem_slot;
 
   if (warp < kM2lTcEpiWarps) {
-    // ---- accumulator readers: row g, all kN pairs of a tile
-    const int g = 32 * warp + lane;
+    // ---- accumulator readers: row g of the accumulator (all kN pairs of a
+    // tile) scaled into the staging tile [pair][g], then whole 16-byte
+    // vectors of the pairs' product rows to global memory
+    const int g = 32 * warp + lane, et_ = tid;  // et_: thread index among the readers
     const uint32_t lane_addr = static_cast<uint32_t>(32 * warp) << 16;
+    float* stg = reinterpret_cast<float*>(tc_smem + S::kOffStg);
+    int* pe_s = reinterpret_cast<int*>(tc_smem + S::kOffPe);
     const double ifact = g < kNm ? T.inv_fact[g] : 0.0;
     const int wg1 = g < kNm ? T.multi[g].w + 1 : 0;
+    constexpr int kVec = kNm / 4;  // 16-byte vectors per pair row
     long i = 0;
     int4 u = units.load(blockIdx.x);
     for (int unit = blockIdx.x; unit < n_units; unit += stride) {
       const int4 un = units.load(unit + stride);  // next unit, in flight
       const int pos0 = u.y, np = u.z, et = u.w < 0 ? -u.w : 0;  // log2(h_t / u)
-      const double rf = ldexp(ifact, wg1 * et);
-      int e_lo = lane < np ? perm[pos0 + lane] : 0, e_hi = 32 + lane < np ? perm[pos0 + 32 + lane] : 0;
+      const float rf = static_cast<float>(ldexp(ifact, wg1 * et));
+      int pe_next = et_ < kN && et_ < np ? perm[pos0 + et_] : 0;
       for (int tile0 = 0; tile0 < np; tile0 += kN, ++i) {
         const int b = static_cast<int>(i % kAc);
-        const int nx = tile0 + kN;  // the next tile's pairs, in flight
-        const int f_lo = nx + lane < np ? perm[pos0 + nx + lane] : 0;
-        const int f_hi = nx + 32 + lane < np ? perm[pos0 + nx + 32 + lane] : 0;
+        const int pe_cur = pe_next;  // this tile's pair id of reader et_ (< kN)
+        pe_next = et_ < kN && tile0 + kN + et_ < np ? perm[pos0 + tile0 + kN + et_] : 0;  // in flight
         const bool ok = tc_wait(accf_bar(b), static_cast<uint32_t>((i / kAc) & 1), abort_flag);
         tc::fence_after();
         float v0[32], v1[32];
@@ -1148,19 +1155,21 @@ m2l_class_tc_kernel(FmmDevTables T, int n_units, const int4* __restrict__ ud, co
         tc::fence_before();
         mbar_arrive(acce_bar(b));
         const int live = min(kN, np - tile0);
+        asm volatile("bar.sync 2, %0;" ::"n"(32 * kM2lTcEpiWarps) : "memory");  // the last tile's rows are out
+        if (et_ < kN) pe_s[et_] = pe_cur;
+        if (g < kNm) {
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int ej = __shfl_sync(0xFFFFFFFFu, e_lo, j);
-          if (ok && j < live && g < kNm) out[static_cast<size_t>(ej - e0) * kNm + g] = static_cast<float>(v0[j] * rf);
-        }
+          for (int j = 0; j < 32; ++j) stg[j * kNm + g] = v0[j] * rf;
 #pragma unroll
-        for (int j = 0; j < 32; ++j) {
-          const int ej = __shfl_sync(0xFFFFFFFFu, e_hi, j);
-          if (ok && 32 + j < live && g < kNm)
-            out[static_cast<size_t>(ej - e0) * kNm + g] = static_cast<float>(v1[j] * rf);
+          for (int j = 0; j < 32; ++j) stg[(32 + j) * kNm + g] = v1[j] * rf;
         }
-        e_lo = f_lo;
-        e_hi = f_hi;
+        asm volatile("bar.sync 2, %0;" ::"n"(32 * kM2lTcEpiWarps) : "memory");
+        if (ok)
+          for (int x = et_; x < live * kVec; x += 32 * kM2lTcEpiWarps) {
+            const int j = x / kVec, cv = x - j * kVec;
+            const float4 val = *reinterpret_cast<const float4*>(stg + j * kNm + 4 * cv);
+            *reinterpret_cast<float4*>(out + static_cast<size_t>(pe_s[j] - e0) * kNm + 4 * cv) = val;
+          }
       }
       u = un;
     }
