@@ -492,6 +492,9 @@ constexpr int kM2lMinClass = 4;    // FP64 mode: classes below this size take th
 // (the tensor-core product costs about as much per class unit as the
 // per-pair path per pair, so in that mode every lattice class takes it)
 constexpr size_t kM2lChunkBytes = size_t(4) << 30;  // per-pair products of one chunk
+// tensor-core mode: larger chunks (a class split across chunks costs one
+// more class-matrix build per chunk; two buffers of this size at most)
+constexpr size_t kM2lTcChunkBytes = size_t(12) << 30;
 constexpr int kM2lHashBits = 21;
 constexpr long kM2lHashSlots = 1L << kM2lHashBits;
 constexpr int kM2lHashProbes = 64;
@@ -891,7 +894,9 @@ m2l_class_mma_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter
 //    (tcgen05.st, two K halves per lane quarter, A double-buffered) from the
 //    class's split D(v), staged in shared memory by cp.async one unit ahead;
 //  - warps 12-15 stream B: a pair's column is 3 * kKp / 8 16-byte
-//    core-matrix rows copied with cp.async into one of 3-4 stages;
+//    core-matrix rows copied with cp.async into one of 3-4 stages, each
+//    thread's arrival on the stage's barrier triggered by the completion of
+//    its copies (cp.async.mbarrier.arrive.noinc);
 //  - one thread of warp 16 issues the MMAs into one of two accumulators.
 // The roles meet at mbarriers (stage full / empty, accumulator full /
 // empty, A full / empty). Every wait is bounded in time; a wait that runs out
@@ -1267,12 +1272,9 @@ m2l_class_tc_kernel(FmmDevTables T, int n_units, const int4* __restrict__ ud, co
           cp_async16(dst + q * S::kBSplit + tc::op_offset(j, 8 * ch, kN), sp + 16 * r, live);
         }
       }
-      cp_async_commit();
-      if (i >= 1) {  // the previous tile's copies have landed: publish them to the tensor core
-        cp_async_wait<1>();
-        tc::fence_proxy_async();
-        mbar_arrive(full_bar(static_cast<int>((i - 1) % kSt)));
-      }
+      // full[s] counts this thread's arrival once all of its copies so far
+      // have landed (the MMA thread orders them for the tensor core)
+      asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(full_bar(s)) : "memory");
       ++i;
       unit = nunit;
       tile0 = ntile0;
@@ -1280,10 +1282,6 @@ m2l_class_tc_kernel(FmmDevTables T, int n_units, const int4* __restrict__ ud, co
       cur = nxt;
     }
     cp_async_wait<0>();
-    if (i >= 1) {
-      tc::fence_proxy_async();
-      mbar_arrive(full_bar(static_cast<int>((i - 1) % kSt)));
-    }
   } else if (lane == 0) {
     // ---- MMA issue: six split products per K step of 16, smallest terms first
     constexpr int kCombo[6][2] = {{2, 0}, {1, 1}, {0, 2}, {1, 0}, {0, 1}, {0, 0}};
@@ -1299,6 +1297,7 @@ m2l_class_tc_kernel(FmmDevTables T, int n_units, const int4* __restrict__ ud, co
         const int s = static_cast<int>(i % kSt), b = static_cast<int>(i % kAc);
         bool ok = a_ok && tc_wait(full_bar(s), static_cast<uint32_t>((i / kSt) & 1), abort_flag);
         ok = ok && (i < kAc || tc_wait(acce_bar(b), static_cast<uint32_t>((i / kAc - 1) & 1), abort_flag));
+        tc::fence_proxy_async();  // the stage's cp.async writes, for the tensor core's reads
         tc::fence_after();
         if (ok) {
           const uint32_t bb = b_base + s * S::kBStage, d = tmem + S::kAccCol + b * kN;
@@ -1417,10 +1416,64 @@ m2l_reduce_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, c
   }
 }
 
+// The same sum over FP32 per-pair products (tensor-core mode, n_m a multiple
+// of 4): lane l holds coefficients 4l..4l+3 and reads them as one 16-byte
+// vector, eight pairs' rows in flight per warp. The sum per coefficient is
+// the FP64 sum in pair order, as in m2l_reduce_kernel.
+__global__ void __launch_bounds__(256)
+m2l_reduce_f4_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, const int* __restrict__ count,
+                     int t_first, int n_targets, long e0, long e1, const float* __restrict__ out,
+                     double* __restrict__ L) {
+  constexpr int kU = 8;
+  const int lane = threadIdx.x & 31;
+  const int k = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (k >= n_targets) return;
+  const int ti = t_first + k, nm = T.n_m, nv = nm >> 2;
+  const long b = max(static_cast<long>(off[ti]), e0), end = min(static_cast<long>(off[ti]) + count[ti], e1);
+  if (b >= end || lane >= nv) return;
+  double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  const float4* o = reinterpret_cast<const float4*>(out + static_cast<size_t>(b - e0) * nm) + lane;
+  long e = b;
+  for (; e + kU <= end; e += kU, o += kU * nv) {
+    float4 v[kU];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) v[u] = o[u * nv];
+#pragma unroll
+    for (int u = 0; u < kU; ++u) {
+      s0 += v[u].x;
+      s1 += v[u].y;
+      s2 += v[u].z;
+      s3 += v[u].w;
+    }
+  }
+  for (; e < end; ++e, o += nv) {
+    const float4 v = *o;
+    s0 += v.x;
+    s1 += v.y;
+    s2 += v.z;
+    s3 += v.w;
+  }
+  const double ih = 1.0 / t.center[ti].w;
+  const double sv[4] = {s0, s1, s2, s3};
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const int g = 4 * lane + c;
+    double f = sv[c];
+    for (int d = 0; d <= T.multi[g].w; ++d) f *= ih;
+    L[static_cast<size_t>(ti) * nm + g] += f;
+  }
+}
+
 template <typename InT>
 int m2l_reduce(amk_ctx* c, cudaStream_t stream, const Octree& t, const FmmDevTables& T, const int* off,
                const int* count, int t_first, int n_targets, long e0, long e1, const InT* out, double* L) {
   const unsigned grid = static_cast<unsigned>((n_targets + 7) / 8);
+  if constexpr (std::is_same<InT, float>::value) {
+    if (T.n_m % 4 == 0 && T.n_m <= 128) {
+      m2l_reduce_f4_kernel<<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
+      return check_launch(c, "m2l_reduce_f4_kernel");
+    }
+  }
   switch ((T.n_m + 31) / 32) {
     case 1:
       m2l_reduce_kernel<1, InT><<<grid, 256, 0, stream>>>(t, T, off, count, t_first, n_targets, e0, e1, out, L);
@@ -1562,7 +1615,7 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
   // the tensor-core products (split BF16) write FP32 per-pair products
   const bool tc = c->fmm_precision == AMK_FMM_TENSOR && tc_order(order);
   const size_t esz = tc ? sizeof(float) : sizeof(double);
-  long cap = std::max<long>(1L << 20, static_cast<long>(kM2lChunkBytes / (esz * T.n_m)));
+  long cap = std::max<long>(1L << 20, static_cast<long>((tc ? kM2lTcChunkBytes : kM2lChunkBytes) / (esz * T.n_m)));
   if (const char* env = getenv("AMK_FMM_M2L_CHUNK_PAIRS")) {  // smaller chunks (tests of the chunk seams)
     const long v = atol(env);
     if (v > 0) cap = std::min(cap, v);
