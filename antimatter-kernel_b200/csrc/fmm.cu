@@ -1928,12 +1928,15 @@ __global__ void p2p_stage_kernel(const Octree t, float4* __restrict__ hi, float4
                       0.f);
 }
 
+constexpr int kP2PStage = 64;  // source particles staged per warp at a time
+
 __global__ void __launch_bounds__(32 * kFmmWarps)
 fmm_p2p32_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, int n_work,
                  const int* __restrict__ off, const int* __restrict__ count, const int* __restrict__ src,
                  const int* __restrict__ pbase, const double* __restrict__ L, double min_sq, bool want_phi,
                  const float4* __restrict__ shi, const float4* __restrict__ slo, double4* __restrict__ part) {
   __shared__ double4 red[kFmmWarps][32];
+  __shared__ float4 stg_hi[kFmmWarps][kP2PStage], stg_lo[kFmmWarps][kP2PStage];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int wi = blockIdx.x * kFmmWarps + w;
   if (wi >= n_work) return;
@@ -1946,6 +1949,8 @@ fmm_p2p32_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, 
   const int se = min(off[ti] + count[ti], sb + kP2PChunk);
   double4* out = part + pbase[ti] + static_cast<size_t>(chunk) * nt_all;
   const float min_sq32 = static_cast<float>(min_sq);
+  float4* sh = stg_hi[w];
+  float4* sl = stg_lo[w];
   for (int base = tr.x; base < tr.y; base += 32) {
     const int nt = min(32, tr.y - base);
     const int groups = 32 / nt;
@@ -1989,32 +1994,44 @@ fmm_p2p32_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, 
       fy = -gy;
       fz = -gz;
     }
-    if (active) {
-      for (int e = sb; e < se; ++e) {
-        const int2 sr = t.range[src[e]];
-        float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
-        for (int j = sr.x + g; j < sr.y; j += groups) {
-          const float4 s = shi[j];
-          if (j == i || s.w == 0.f) continue;
-          const float4 sl = slo[j];
-          const float rx = (mh.x - s.x) + (ml.x - sl.x);
-          const float ry = (mh.y - s.y) + (ml.y - sl.y);
-          const float rz = (mh.z - s.z) + (ml.z - sl.z);
-          const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-          if (r2 < min_sq32) continue;
-          const float inv_r = rsqrtf(r2);
-          const float qr = s.w * inv_r;
-          const float f = qr * (inv_r * inv_r);
-          ax = fmaf(rx, f, ax);
-          ay = fmaf(ry, f, ay);
-          az = fmaf(rz, f, az);
-          ap += qr;
+    // Sources of each leaf in blocks of kP2PStage, staged by the warp in
+    // shared memory (all lanes of a group read the same source: broadcast);
+    // lane group g takes every groups-th source. The pair term is computed
+    // without branches: a pair closer than the minimum distance (the
+    // particle itself included) contributes zero, as does a neutral source.
+    for (int e = sb; e < se; ++e) {
+      const int2 sr = t.range[src[e]];
+      float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
+      for (int s0 = sr.x; s0 < sr.y; s0 += kP2PStage) {
+        const int ns = min(kP2PStage, sr.y - s0);
+        __syncwarp();
+        for (int k = lane; k < ns; k += 32) {
+          sh[k] = shi[s0 + k];
+          sl[k] = slo[s0 + k];
         }
-        fx += ax;
-        fy += ay;
-        fz += az;
-        pot += ap;
+        __syncwarp();
+        if (active) {
+#pragma unroll 4
+          for (int j = g; j < ns; j += groups) {
+            const float4 s = sh[j], q = sl[j];
+            const float rx = (mh.x - s.x) + (ml.x - q.x);
+            const float ry = (mh.y - s.y) + (ml.y - q.y);
+            const float rz = (mh.z - s.z) + (ml.z - q.z);
+            const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+            const float inv_r = (r2 >= min_sq32 && r2 > 0.f) ? rsqrtf(r2) : 0.f;
+            const float qr = s.w * inv_r;
+            const float f = qr * (inv_r * inv_r);
+            ax = fmaf(rx, f, ax);
+            ay = fmaf(ry, f, ay);
+            az = fmaf(rz, f, az);
+            ap += qr;
+          }
+        }
       }
+      fx += ax;
+      fy += ay;
+      fz += az;
+      pot += ap;
     }
     red[w][lane] = make_double4(fx, fy, fz, pot);
     __syncwarp();
