@@ -176,8 +176,8 @@ extern "C" int amk_autotune(amk_ctx* c, double error_budget, long samples, int f
   std::vector<amk_tune_candidate> cand;
   if (!(flags & AMK_TUNE_NO_ALLPAIRS)) cand.push_back({AMK_METHOD_ALLPAIRS, 0, 0.0, 0, 0.0, 0.0, 0});
   if (!(flags & AMK_TUNE_NO_FMM))
-    for (double theta : {0.5, 0.45, 0.4, 0.35})
-      for (int leaf : {16, 32, 64})
+    for (double theta : {0.5, 0.475, 0.45, 0.4})
+      for (int leaf : {16, 32, 64, 128, 256})
         for (int order : {4, 5, 6, 7, 8}) cand.push_back({AMK_METHOD_FAST_MULTIPOLE, order, theta, leaf, 0.0, 0.0, 0});
   if (!(flags & AMK_TUNE_NO_BARNES_HUT))
     for (double theta : {0.5, 0.3, 0.2}) cand.push_back({AMK_METHOD_BARNES_HUT, 0, theta, 8, 0.0, 0.0, 0});

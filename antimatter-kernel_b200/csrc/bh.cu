@@ -13,8 +13,9 @@
 // reference's); accepting lanes add the two monopoles, the others push the
 // children for themselves. Leaves are summed directly, skipping the target
 // itself and q = 0 sources. Pairs closer than 1e-30 m^2 are skipped
-// (barnes-hut.cc:33-41). All arithmetic is FP64; inverse distances use
-// rsqrt where the reference divides by sqrt (an ulp-level difference).
+// (barnes-hut.cc:33-41). All arithmetic is FP64 (leaf sums FP32 in the
+// tensor precision mode, below); inverse distances use rsqrt where the
+// reference divides by sqrt (an ulp-level difference).
 #include <algorithm>
 #include <vector>
 
@@ -110,10 +111,32 @@ __device__ __forceinline__ void add_phi(double tx, double ty, double tz, double 
   *phi += sq * rsqrt(d2);
 }
 
-template <bool kPhi>
+// Leaf sums in FP32 (the tensor precision mode): sources as double-float
+// pairs x = hi + lo (hi = float(x), lo = float(x - hi)) relative to the
+// tree frame; a pair's difference (x_i,hi - x_j,hi) + (x_i,lo - x_j,lo) is
+// exact to FP32 rounding of |r| for particles of neighbouring cells
+// (Sterbenz), the per-leaf sums of q_j r / r^3 are FP32 and are added to the
+// FP64 accumulators once per leaf. The opening test and the node monopoles
+// stay FP64, so the accepted-node sets are the reference's.
+struct BhF32 {
+  const float4* hi;  // (x, y, z, q) hi parts, q as float
+  const float4* lo;  // lo parts
+  double qs;         // charges were divided by this before the float conversion
+};
+
+__global__ void bh_stage_kernel(const Octree t, double qs, float4* __restrict__ hi, float4* __restrict__ lo) {
+  const long k = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (k >= t.m) return;
+  const double4 s = t.src[k];
+  const float hx = static_cast<float>(s.x), hy = static_cast<float>(s.y), hz = static_cast<float>(s.z);
+  hi[k] = make_float4(hx, hy, hz, static_cast<float>(s.w / qs));
+  lo[k] = make_float4(static_cast<float>(s.x - hx), static_cast<float>(s.y - hy), static_cast<float>(s.z - hz), 0.f);
+}
+
+template <bool kPhi, bool kF32>
 __global__ void __launch_bounds__(32 * kWalkWarps)
 bh_walk_kernel(const Octree t, const double4* __restrict__ pos, const double4* __restrict__ neg, double theta2,
-               double* __restrict__ out, int* __restrict__ status) {
+               BhF32 f32, double* __restrict__ out, int* __restrict__ status) {
   __shared__ int s_node[kWalkWarps][kStack];
   __shared__ unsigned s_mask[kWalkWarps][kStack];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -146,14 +169,47 @@ bh_walk_kernel(const Octree t, const double4* __restrict__ pos, const double4* _
     if (t.meta[nd].y) {
       const int2 r = t.range[nd];
       if (act) {
-        for (int j = r.x; j < r.y; ++j) {
-          if (j == k) continue;
-          const double4 s = t.src[j];
-          if (s.w == 0.0) continue;
-          if (kPhi)
-            add_phi(me.x, me.y, me.z, s.x, s.y, s.z, s.w, &phi);
-          else
-            add_point(me.x, me.y, me.z, me.w, s.x, s.y, s.z, s.w, f);
+        if (kF32) {
+          // sum over the leaf of (q_j / qs) r / r^3 (or / r) in FP32
+          const float4 mh = f32.hi[k], ml = f32.lo[k];
+          const float min_sq = 1e-30f;  // kMinSquaredDistance (m^2), a normal float
+          float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
+          for (int j = r.x; j < r.y; ++j) {
+            const float4 s = f32.hi[j], q = f32.lo[j];
+            const float rx = fmaf(s.x, -1.f, mh.x) + fmaf(q.x, -1.f, ml.x);
+            const float ry = fmaf(s.y, -1.f, mh.y) + fmaf(q.y, -1.f, ml.y);
+            const float rz = fmaf(s.z, -1.f, mh.z) + fmaf(q.z, -1.f, ml.z);
+            const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+            // the target itself (r = 0), closer pairs and neutral sources add zero
+            const float inv = (j != k && r2 >= min_sq) ? rsqrtf(r2) : 0.f;
+            const float qr = s.w * inv;
+            if (kPhi) {
+              ap += qr;
+            } else {
+              const float w = qr * (inv * inv);
+              ax = fmaf(rx, w, ax);
+              ay = fmaf(ry, w, ay);
+              az = fmaf(rz, w, az);
+            }
+          }
+          if (kPhi) {
+            phi += f32.qs * static_cast<double>(ap);
+          } else {
+            const double sc = kCoulombConstant * me.w * f32.qs;
+            f[0] += sc * static_cast<double>(ax);
+            f[1] += sc * static_cast<double>(ay);
+            f[2] += sc * static_cast<double>(az);
+          }
+        } else {
+          for (int j = r.x; j < r.y; ++j) {
+            if (j == k) continue;
+            const double4 s = t.src[j];
+            if (s.w == 0.0) continue;
+            if (kPhi)
+              add_phi(me.x, me.y, me.z, s.x, s.y, s.z, s.w, &phi);
+            else
+              add_point(me.x, me.y, me.z, me.w, s.x, s.y, s.z, s.w, f);
+          }
         }
       }
       continue;
@@ -269,11 +325,27 @@ int barnes_hut_forces(amk_ctx* c, const View& v, double theta, long leaf_capacit
   AMK_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), c->stream));
   const unsigned blocks = static_cast<unsigned>((t.m + 32 * kWalkWarps - 1) / (32 * kWalkWarps));
   const double theta2 = theta * theta;  // squared_theta_, barnes-hut.cc:36
+  const bool f32 = c->fmm_precision == AMK_FMM_TENSOR;
+  BhF32 fs{nullptr, nullptr, kElementaryCharge};
+  if (f32) {  // sources as double-float pairs, charges in units of e
+    float4* stage = slot<float4>(c, kSlotP2PStage, 2 * static_cast<size_t>(t.m), &rc);
+    AMK_TRY(rc);
+    bh_stage_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, c->stream>>>(t, fs.qs, stage, stage + t.m);
+    AMK_TRY(check_launch(c, "bh_stage_kernel"));
+    fs.hi = stage;
+    fs.lo = stage + t.m;
+  }
   AMK_TRY(phase_begin(c, AMK_PHASE_BH_WALK));
-  bh_walk_kernel<false><<<blocks, 32 * kWalkWarps, 0, c->stream>>>(t, pos, neg, theta2, fo, status);
+  if (f32)
+    bh_walk_kernel<false, true><<<blocks, 32 * kWalkWarps, 0, c->stream>>>(t, pos, neg, theta2, fs, fo, status);
+  else
+    bh_walk_kernel<false, false><<<blocks, 32 * kWalkWarps, 0, c->stream>>>(t, pos, neg, theta2, fs, fo, status);
   AMK_TRY(check_launch(c, "bh_walk_kernel"));
   if (po) {
-    bh_walk_kernel<true><<<blocks, 32 * kWalkWarps, 0, c->stream>>>(t, pos, neg, theta2, po, status);
+    if (f32)
+      bh_walk_kernel<true, true><<<blocks, 32 * kWalkWarps, 0, c->stream>>>(t, pos, neg, theta2, fs, po, status);
+    else
+      bh_walk_kernel<true, false><<<blocks, 32 * kWalkWarps, 0, c->stream>>>(t, pos, neg, theta2, fs, po, status);
     AMK_TRY(check_launch(c, "bh_walk_kernel"));
   }
   AMK_TRY(phase_end(c, AMK_PHASE_BH_WALK));

@@ -664,10 +664,15 @@ __device__ __forceinline__ void m2l_derivatives(const FmmDevTables& T, int lane,
   }
 }
 
-// D(v) of every class: a warp per class, into table[class * n_d + k].
+__device__ __forceinline__ void split3_bf16(double v, __nv_bfloat16* t);
+
+// D(v) of every class: a warp per class, into table[class * n_d + k], or
+// (tensor-core mode, table3 given) split into three BF16 terms packed as
+// {t0 | t1 << 16, t2} into table3[class * nd3 + k], zero for k >= n_d.
 __global__ void __launch_bounds__(32 * kFmmWarps)
 m2l_table_kernel(FmmDevTables T, const int* __restrict__ cls_code, int n_classes,
-                 const unsigned long long* __restrict__ keys, double* __restrict__ table) {
+                 const unsigned long long* __restrict__ keys, double* __restrict__ table,
+                 uint2* __restrict__ table3, int nd3) {
   extern __shared__ __align__(16) unsigned char tab_smem[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   double* D = reinterpret_cast<double*>(tab_smem) + static_cast<size_t>(w) * T.n_d;
@@ -677,7 +682,18 @@ m2l_table_kernel(FmmDevTables T, const int* __restrict__ cls_code, int n_classes
   const double xs[3] = {static_cast<double>(m2l_key_v(key, 0)), static_cast<double>(m2l_key_v(key, 1)),
                         static_cast<double>(m2l_key_v(key, 2))};
   m2l_derivatives(T, lane, xs, D);
-  for (int k = lane; k < T.n_d; k += 32) table[static_cast<size_t>(cls) * T.n_d + k] = D[k];
+  if (table3 == nullptr) {
+    for (int k = lane; k < T.n_d; k += 32) table[static_cast<size_t>(cls) * T.n_d + k] = D[k];
+    return;
+  }
+  for (int k = lane; k < nd3; k += 32) {
+    __nv_bfloat16 t3[3];
+    split3_bf16(k < T.n_d ? D[k] : 0.0, t3);
+    table3[static_cast<size_t>(cls) * nd3 + k] =
+        make_uint2(static_cast<uint32_t>(__bfloat16_as_ushort(t3[0])) |
+                       (static_cast<uint32_t>(__bfloat16_as_ushort(t3[1])) << 16),
+                   __bfloat16_as_ushort(t3[2]));
+  }
 }
 
 constexpr int kM2lBs = kM2lTileP + 2;   // B row stride (doubles): 16-byte rows, 2-way store conflicts
@@ -881,7 +897,7 @@ m2l_class_mma_kernel(FmmDevTables T, int n_units, int* __restrict__ unit_counter
 //
 // Before the kernel, per evaluation chunk: the cells' rescaled expansions
 // are split into BF16 rows of kKp elements (m2l_split_kernel), each class's
-// D(v) into packed BF16 terms (m2l_table3_kernel), and every unit gets a
+// D(v) into packed BF16 terms (m2l_table_kernel), and every unit gets a
 // descriptor {class, first pair, pairs, depth difference} and every pair its
 // source cell (m2l_tc_prep_kernel), so each role reads one value where it
 // would otherwise follow a chain of dependent loads.
@@ -970,21 +986,6 @@ __global__ void m2l_split_kernel(long n_cells, int nm, int kp, const double* __r
   split3_bf16(a < nm ? Mh[cell * nm + a] : 0.0, t);
 #pragma unroll
   for (int q = 0; q < 3; ++q) Mh3[(cell * 3 + q) * kp + a] = t[q];
-}
-
-// table3[cls * nd3 + k] = the split of D_k(v) of class cls packed as
-// {t0 | t1 << 16, t2} (zero for k >= n_d).
-__global__ void m2l_table3_kernel(long n_cls, int nd, int nd3, const double* __restrict__ table,
-                                  uint2* __restrict__ table3) {
-  const long e = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
-  if (e >= n_cls * nd3) return;
-  const long cls = e / nd3;
-  const int k = static_cast<int>(e - cls * nd3);
-  __nv_bfloat16 t[3];
-  split3_bf16(k < nd ? table[cls * nd + k] : 0.0, t);
-  table3[e] = make_uint2(static_cast<uint32_t>(__bfloat16_as_ushort(t[0])) |
-                             (static_cast<uint32_t>(__bfloat16_as_ushort(t[1])) << 16),
-                         __bfloat16_as_ushort(t[2]));
 }
 
 // Unit descriptors {class, first pair, pairs, depth difference} and the
@@ -1686,30 +1687,30 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
     // the sums of the chunk before the previous one still read this buffer
     if (chunk >= 2) AMK_CUDA_TRY(cudaStreamWaitEvent(c->stream, f->sums_done[buf], 0));
     if (n_cls > 0) {
-      double* table = slot<double>(c, kSlotM2lTable, static_cast<size_t>(n_cls) * T.n_d, &rc);
+      // D(v) per class: FP64 rows for the FP64 product, split BF16 rows for
+      // the tensor-core product
+      const int nd3 = tc_nd3(T.n_d);
+      double* table = nullptr;
+      uint2* table3 = nullptr;
+      if (tc)
+        table3 = slot<uint2>(c, kSlotM2lTable3, static_cast<size_t>(n_cls) * nd3, &rc);
+      else
+        table = slot<double>(c, kSlotM2lTable, static_cast<size_t>(n_cls) * T.n_d, &rc);
       AMK_TRY(rc);
       const size_t tsm = static_cast<size_t>(kFmmWarps) * T.n_d * sizeof(double);
       AMK_CUDA_TRY(cudaFuncSetAttribute(m2l_table_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         static_cast<int>(tsm)));
-      m2l_table_kernel<<<(n_cls + kFmmWarps - 1) / kFmmWarps, 32 * kFmmWarps, tsm, c->stream>>>(T, cls_code, n_cls,
-                                                                                              keys, table);
+      m2l_table_kernel<<<(n_cls + kFmmWarps - 1) / kFmmWarps, 32 * kFmmWarps, tsm, c->stream>>>(
+          T, cls_code, n_cls, keys, table, table3, nd3);
       AMK_TRY(check_launch(c, "m2l_table_kernel"));
       int4* ud = nullptr;
       int* psrc = nullptr;
-      uint2* table3 = nullptr;
-      if (tc) {  // the tensor-core product's inputs: split D rows, unit descriptors, pair sources
-        const int nd3 = tc_nd3(T.n_d);
+      if (tc) {  // the tensor-core product's other inputs: unit descriptors, pair sources
         const long n_cp = ne - n_fb;  // pairs in classes: perm[0, n_cp)
-        table3 = slot<uint2>(c, kSlotM2lTable3, static_cast<size_t>(n_cls) * nd3, &rc);
-        AMK_TRY(rc);
         ud = slot<int4>(c, kSlotM2lUnitDesc, static_cast<size_t>(n_units), &rc);
         AMK_TRY(rc);
         psrc = slot<int>(c, kSlotM2lPairSrc, static_cast<size_t>(std::max<long>(1, n_cp)), &rc);
         AMK_TRY(rc);
-        const long nt = static_cast<long>(n_cls) * nd3;
-        m2l_table3_kernel<<<static_cast<unsigned>((nt + 255) / 256), 256, 0, c->stream>>>(n_cls, T.n_d, nd3, table,
-                                                                                         table3);
-        AMK_TRY(check_launch(c, "m2l_table3_kernel"));
         const long np_ = std::max<long>(n_units, n_cp);
         m2l_tc_prep_kernel<<<static_cast<unsigned>((np_ + 255) / 256), 256, 0, c->stream>>>(
             n_units, unit_cls, unit_pos, cls_code, cls_end, keys, static_cast<int>(n_cp), perm, gm.src, ud, psrc);
@@ -1930,6 +1931,49 @@ __global__ void p2p_stage_kernel(const Octree t, float4* __restrict__ hi, float4
 
 constexpr int kP2PStage = 64;  // source particles staged per warp at a time
 
+// L2P in FP64 for particle i of leaf ti (centre tc): force and potential of
+// the leaf's local expansion at the particle.
+__device__ __forceinline__ double4 l2p_fp64(const Octree& t, const FmmDevTables& T, const double* __restrict__ L,
+                                            int ti, const double4& tc, int i, bool want_phi) {
+  const double4 me = t.src[i];
+  const double* l = L + static_cast<size_t>(ti) * T.n_m;
+  double px[kMaxOrder + 1], py[kMaxOrder + 1], pz[kMaxOrder + 1];
+  powers(T.p, me.x - tc.x, me.y - tc.y, me.z - tc.z, px, py, pz);
+  double pot = 0.0;
+  if (want_phi)
+    for (int gg = 0; gg < T.n_m; ++gg) {
+      const int4 m = T.multi[gg];
+      pot += l[gg] * (px[m.x] * py[m.y] * pz[m.z]);
+    }
+  double gx = 0.0, gy = 0.0, gz = 0.0;
+  for (int gg = 1; gg < T.n_m; ++gg) {
+    const int4 m = T.multi[gg];
+    const int g0 = T.grad[3 * gg], g1 = T.grad[3 * gg + 1], g2 = T.grad[3 * gg + 2];
+    if (g0 >= 0) {
+      const int4 q = T.multi[g0];
+      gx += m.x * l[gg] * (px[q.x] * py[q.y] * pz[q.z]);
+    }
+    if (g1 >= 0) {
+      const int4 q = T.multi[g1];
+      gy += m.y * l[gg] * (px[q.x] * py[q.y] * pz[q.z]);
+    }
+    if (g2 >= 0) {
+      const int4 q = T.multi[g2];
+      gz += m.z * l[gg] * (px[q.x] * py[q.y] * pz[q.z]);
+    }
+  }
+  return make_double4(-gx, -gy, -gz, pot);
+}
+
+// Targets: a full block of 64 runs two targets per lane in the halves of
+// packed FP32x2 operations; a remainder of at most 32 runs one target per
+// lane with the warp's lanes split into groups that take every groups-th
+// source. Sources of each leaf come in blocks of kP2PStage staged by the
+// warp in shared memory (broadcast reads). The pair term is branch-free: a
+// pair closer than the minimum distance (the particle itself included)
+// contributes zero, as does a neutral source; t - s is formed as
+// fma(s, -1, t), the rounding of the subtraction, so both paths give the
+// same pair terms bit for bit.
 __global__ void __launch_bounds__(32 * kFmmWarps)
 fmm_p2p32_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, int n_work,
                  const int* __restrict__ off, const int* __restrict__ count, const int* __restrict__ src,
@@ -1951,72 +1995,93 @@ fmm_p2p32_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, 
   const float min_sq32 = static_cast<float>(min_sq);
   float4* sh = stg_hi[w];
   float4* sl = stg_lo[w];
-  for (int base = tr.x; base < tr.y; base += 32) {
+  auto stage = [&](int s0, int ns) {
+    __syncwarp();
+    for (int k = lane; k < ns; k += 32) {
+      sh[k] = shi[s0 + k];
+      sl[k] = slo[s0 + k];
+    }
+    __syncwarp();
+  };
+  for (int base = tr.x; base < tr.y;) {
+    if (tr.y - base >= 64) {
+      // ---- a full block of 64 targets: two per lane, packed FP32x2
+      const int i0 = base + lane, i1 = base + 32 + lane;
+      double4 a0 = make_double4(0.0, 0.0, 0.0, 0.0), a1 = a0;
+      if (chunk == 0) {
+        a0 = l2p_fp64(t, T, L, ti, tc, i0, want_phi);
+        a1 = l2p_fp64(t, T, L, ti, tc, i1, want_phi);
+      }
+      const float4 h0 = shi[i0], l0 = slo[i0], h1 = shi[i1], l1 = slo[i1];
+      const float2 thx = make_float2(h0.x, h1.x), thy = make_float2(h0.y, h1.y), thz = make_float2(h0.z, h1.z);
+      const float2 tlx = make_float2(l0.x, l1.x), tly = make_float2(l0.y, l1.y), tlz = make_float2(l0.z, l1.z);
+      const float2 m1 = make_float2(-1.f, -1.f);
+      for (int e = sb; e < se; ++e) {
+        const int2 sr = t.range[src[e]];
+        float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax, ap = ax;
+        for (int s0 = sr.x; s0 < sr.y; s0 += kP2PStage) {
+          const int ns = min(kP2PStage, sr.y - s0);
+          stage(s0, ns);
+#pragma unroll 4
+          for (int j = 0; j < ns; ++j) {
+            const float4 s = sh[j], q = sl[j];
+            const float2 rx = __fadd2_rn(__ffma2_rn(make_float2(s.x, s.x), m1, thx),
+                                         __ffma2_rn(make_float2(q.x, q.x), m1, tlx));
+            const float2 ry = __fadd2_rn(__ffma2_rn(make_float2(s.y, s.y), m1, thy),
+                                         __ffma2_rn(make_float2(q.y, q.y), m1, tly));
+            const float2 rz = __fadd2_rn(__ffma2_rn(make_float2(s.z, s.z), m1, thz),
+                                         __ffma2_rn(make_float2(q.z, q.z), m1, tlz));
+            const float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __fmul2_rn(rz, rz)));
+            const float2 inv = make_float2((r2.x >= min_sq32 && r2.x > 0.f) ? rsqrtf(r2.x) : 0.f,
+                                           (r2.y >= min_sq32 && r2.y > 0.f) ? rsqrtf(r2.y) : 0.f);
+            const float2 qr = __fmul2_rn(make_float2(s.w, s.w), inv);
+            const float2 f = __fmul2_rn(qr, __fmul2_rn(inv, inv));
+            ax = __ffma2_rn(rx, f, ax);
+            ay = __ffma2_rn(ry, f, ay);
+            az = __ffma2_rn(rz, f, az);
+            ap = __fadd2_rn(ap, qr);
+          }
+        }
+        a0.x += ax.x;
+        a0.y += ay.x;
+        a0.z += az.x;
+        a0.w += ap.x;
+        a1.x += ax.y;
+        a1.y += ay.y;
+        a1.z += az.y;
+        a1.w += ap.y;
+      }
+      out[i0 - tr.x] = a0;
+      out[i1 - tr.x] = a1;
+      base += 64;
+      continue;
+    }
+    // ---- at most 32 targets: one per lane, lanes in groups over the sources
     const int nt = min(32, tr.y - base);
     const int groups = 32 / nt;
     const int g = lane / nt, tl = lane - g * nt;
     const bool active = g < groups;
     const int i = base + tl;
-    double pot = 0.0, fx = 0.0, fy = 0.0, fz = 0.0;
+    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
     float4 mh = make_float4(0.f, 0.f, 0.f, 0.f), ml = mh;
     if (active) {
       mh = shi[i];
       ml = slo[i];
     }
-    if (active && g == 0 && chunk == 0) {  // L2P in FP64, once per target
-      const double4 me = t.src[i];
-      const double* l = L + static_cast<size_t>(ti) * T.n_m;
-      double px[kMaxOrder + 1], py[kMaxOrder + 1], pz[kMaxOrder + 1];
-      powers(T.p, me.x - tc.x, me.y - tc.y, me.z - tc.z, px, py, pz);
-      if (want_phi)
-        for (int gg = 0; gg < T.n_m; ++gg) {
-          const int4 m = T.multi[gg];
-          pot += l[gg] * (px[m.x] * py[m.y] * pz[m.z]);
-        }
-      double gx = 0.0, gy = 0.0, gz = 0.0;
-      for (int gg = 1; gg < T.n_m; ++gg) {
-        const int4 m = T.multi[gg];
-        const int g0 = T.grad[3 * gg], g1 = T.grad[3 * gg + 1], g2 = T.grad[3 * gg + 2];
-        if (g0 >= 0) {
-          const int4 q = T.multi[g0];
-          gx += m.x * l[gg] * (px[q.x] * py[q.y] * pz[q.z]);
-        }
-        if (g1 >= 0) {
-          const int4 q = T.multi[g1];
-          gy += m.y * l[gg] * (px[q.x] * py[q.y] * pz[q.z]);
-        }
-        if (g2 >= 0) {
-          const int4 q = T.multi[g2];
-          gz += m.z * l[gg] * (px[q.x] * py[q.y] * pz[q.z]);
-        }
-      }
-      fx = -gx;
-      fy = -gy;
-      fz = -gz;
-    }
-    // Sources of each leaf in blocks of kP2PStage, staged by the warp in
-    // shared memory (all lanes of a group read the same source: broadcast);
-    // lane group g takes every groups-th source. The pair term is computed
-    // without branches: a pair closer than the minimum distance (the
-    // particle itself included) contributes zero, as does a neutral source.
+    if (active && g == 0 && chunk == 0) acc = l2p_fp64(t, T, L, ti, tc, i, want_phi);  // once per target
     for (int e = sb; e < se; ++e) {
       const int2 sr = t.range[src[e]];
       float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
       for (int s0 = sr.x; s0 < sr.y; s0 += kP2PStage) {
         const int ns = min(kP2PStage, sr.y - s0);
-        __syncwarp();
-        for (int k = lane; k < ns; k += 32) {
-          sh[k] = shi[s0 + k];
-          sl[k] = slo[s0 + k];
-        }
-        __syncwarp();
+        stage(s0, ns);
         if (active) {
 #pragma unroll 4
           for (int j = g; j < ns; j += groups) {
             const float4 s = sh[j], q = sl[j];
-            const float rx = (mh.x - s.x) + (ml.x - q.x);
-            const float ry = (mh.y - s.y) + (ml.y - q.y);
-            const float rz = (mh.z - s.z) + (ml.z - q.z);
+            const float rx = fmaf(s.x, -1.f, mh.x) + fmaf(q.x, -1.f, ml.x);
+            const float ry = fmaf(s.y, -1.f, mh.y) + fmaf(q.y, -1.f, ml.y);
+            const float rz = fmaf(s.z, -1.f, mh.z) + fmaf(q.z, -1.f, ml.z);
             const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
             const float inv_r = (r2 >= min_sq32 && r2 > 0.f) ? rsqrtf(r2) : 0.f;
             const float qr = s.w * inv_r;
@@ -2028,12 +2093,12 @@ fmm_p2p32_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, 
           }
         }
       }
-      fx += ax;
-      fy += ay;
-      fz += az;
-      pot += ap;
+      acc.x += ax;
+      acc.y += ay;
+      acc.z += az;
+      acc.w += ap;
     }
-    red[w][lane] = make_double4(fx, fy, fz, pot);
+    red[w][lane] = acc;
     __syncwarp();
     if (active && g == 0) {
       double4 a = red[w][tl];
@@ -2047,6 +2112,7 @@ fmm_p2p32_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, 
       out[i - tr.x] = a;
     }
     __syncwarp();
+    base += nt;
   }
 }
 

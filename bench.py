@@ -222,6 +222,7 @@ def e2e_through_abi(sim, stream, n, steps, step_fn=None):
 TREE_METHODS = [
     ("allpairs", dict(coulomb_method="allpairs")),
     ("barnes-hut theta=0.7", dict(coulomb_method="barnes-hut", barnes_hut_theta=0.7)),
+    ("barnes-hut theta=0.7 tensor", dict(coulomb_method="barnes-hut", barnes_hut_theta=0.7, precision="tensor")),
     ("fmm p=2 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=2, fast_multipole_theta=0.5)),
     ("fmm p=4 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=4, fast_multipole_theta=0.5)),
     ("fmm p=6 theta=0.5", dict(coulomb_method="fast-multipole", fast_multipole_order=6, fast_multipole_theta=0.5)),
@@ -467,7 +468,7 @@ def run_tree(args):
             best = name
         sim.close()
     if args.autotune:
-        # the FMM configuration (order 4..8, theta 0.5..0.35, leaf 16/32/64;
+        # the FMM configuration (order 4..8, theta 0.5..0.4, leaf 16..256;
         # tensor-core M2L products for orders 5-7) the library's autotuner
         # finds fastest within the budget
         sim, stream = new_sim(dict(overs[PLAIN_P6], precision="tensor"))

@@ -313,7 +313,9 @@ long amk_bh_tree_dump(amk_ctx* ctx, long n, const double* x, const double* y, co
  * M2L term about 2^-22, below the truncation error of those orders. The
  * near field (P2P) then runs in FP32 on double-float positions (pair
  * differences exact to FP32 rounding, FP64 sums per source leaf). Tree,
- * expansions, L2L and L2P stay FP64. */
+ * expansions, L2L and L2P stay FP64. The mode also selects FP32 leaf sums
+ * (same double-float differences) in the Barnes-Hut walk, whose opening test
+ * and node monopoles stay FP64. */
 #define AMK_FMM_FP64 0
 #define AMK_FMM_TENSOR 1
 int amk_set_fmm_precision(amk_ctx* ctx, int mode);
@@ -389,9 +391,9 @@ typedef struct amk_tune_candidate {
 #define AMK_TUNE_NO_BARNES_HUT 4
 /* Autotuner: on the context's own particles, times (CUDA events, median of
  * 3 after a warm call) and audits (amk_force_error with `samples`) the
- * all-pairs solver, the FMM for orders 4..8 x theta 0.5/0.45/0.4/0.35 x
- * leaf 16/32/64 (higher orders skipped once a lower one meets the budget,
- * up to 61 candidates with the others) and
+ * all-pairs solver, the FMM for orders 4..8 x theta 0.5/0.475/0.45/0.4 x
+ * leaf 16/32/64/128/256 (higher orders skipped once a lower one meets the
+ * budget; up to 104 candidates with the others) and
  * Barnes-Hut for theta 0.5/0.3/0.2, then sets the context's Coulomb method,
  * order, theta and leaf size to the fastest candidate whose RMS error is
  * <= error_budget. out (max_out entries, may be NULL) receives every

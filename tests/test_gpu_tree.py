@@ -110,3 +110,22 @@ def test_context_barnes_hut_skips_annihilated(sim):
         if ref is not None:
             rel, _ = rel_errors(tuple(a[alive] for a in f), ref)
             assert np.max(rel) < BH_TOL
+
+
+def test_bh_fp32_leaf_sums_in_tensor_mode():
+    # tensor precision mode: FP32 leaf sums on double-float differences,
+    # FP64 opening test and monopoles; forces and potentials stay within
+    # FP32 rounding of the FP64 walk (mixed charges, neutral sources)
+    import amk
+    x, y, z, q = gaussian_cloud(20000, 23)
+    q[::11] = 0.0
+    with amk.Simulation() as s:
+        ref = s.solve_barnes_hut(x, y, z, q, 0.6, want_phi=True)
+        s.set_fmm_precision("tensor")
+        got = s.solve_barnes_hut(x, y, z, q, 0.6, want_phi=True)
+        again = s.solve_barnes_hut(x, y, z, q, 0.6, want_phi=True)
+    assert all(np.array_equal(a, b) for a, b in zip(got, again))  # deterministic
+    rel, glob = rel_errors(got[:3], ref[:3])
+    assert glob < 1e-6 and np.sqrt(np.mean(rel ** 2)) < 1e-5, (glob, np.sqrt(np.mean(rel ** 2)))
+    assert np.all(got[0][q == 0.0] == 0.0)
+    assert np.max(np.abs(got[3] - ref[3])) <= 1e-6 * np.max(np.abs(ref[3]))
