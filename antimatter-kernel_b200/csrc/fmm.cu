@@ -1965,6 +1965,8 @@ __device__ __forceinline__ double4 l2p_fp64(const Octree& t, const FmmDevTables&
   return make_double4(-gx, -gy, -gz, pot);
 }
 
+// Near-field pair sums of one work item (target leaf, up to kP2PChunk
+// source leaves); the FP64 L2P runs in fmm_l2p_add_kernel.
 // Targets: a full block of 64 runs two targets per lane in the halves of
 // packed FP32x2 operations; a remainder of at most 32 runs one target per
 // lane with the warp's lanes split into groups that take every groups-th
@@ -1974,11 +1976,11 @@ __device__ __forceinline__ double4 l2p_fp64(const Octree& t, const FmmDevTables&
 // contributes zero, as does a neutral source; t - s is formed as
 // fma(s, -1, t), the rounding of the subtraction, so both paths give the
 // same pair terms bit for bit.
-__global__ void __launch_bounds__(32 * kFmmWarps)
-fmm_p2p32_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, int n_work,
-                 const int* __restrict__ off, const int* __restrict__ count, const int* __restrict__ src,
-                 const int* __restrict__ pbase, const double* __restrict__ L, double min_sq, bool want_phi,
-                 const float4* __restrict__ shi, const float4* __restrict__ slo, double4* __restrict__ part) {
+__global__ void __launch_bounds__(32 * kFmmWarps, 8)  // 8 blocks per SM: latency hiding beats the spills
+fmm_p2p32_kernel(const Octree t, const int2* __restrict__ work, int n_work, const int* __restrict__ off,
+                 const int* __restrict__ count, const int* __restrict__ src, const int* __restrict__ pbase,
+                 double min_sq, const float4* __restrict__ shi, const float4* __restrict__ slo,
+                 double4* __restrict__ part) {
   __shared__ double4 red[kFmmWarps][32];
   __shared__ float4 stg_hi[kFmmWarps][kP2PStage], stg_lo[kFmmWarps][kP2PStage];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1986,13 +1988,15 @@ fmm_p2p32_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, 
   if (wi >= n_work) return;
   const int2 item = work[wi];
   const int ti = item.x, chunk = item.y;
-  const double4 tc = t.center[ti];
   const int2 tr = t.range[ti];
   const int nt_all = tr.y - tr.x;
   const int sb = off[ti] + chunk * kP2PChunk;
   const int se = min(off[ti] + count[ti], sb + kP2PChunk);
   double4* out = part + pbase[ti] + static_cast<size_t>(chunk) * nt_all;
-  const float min_sq32 = static_cast<float>(min_sq);
+  // pairs below the minimum distance (the particle itself included: r = 0)
+  // get r^2 = +inf, so 1/r = 0 without a select on the result
+  const float min_sq32 = fmaxf(static_cast<float>(min_sq), 1.17549435e-38f);
+  const float inf32 = __int_as_float(0x7f800000);
   float4* sh = stg_hi[w];
   float4* sl = stg_lo[w];
   auto stage = [&](int s0, int ns) {
@@ -2008,10 +2012,6 @@ fmm_p2p32_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, 
       // ---- a full block of 64 targets: two per lane, packed FP32x2
       const int i0 = base + lane, i1 = base + 32 + lane;
       double4 a0 = make_double4(0.0, 0.0, 0.0, 0.0), a1 = a0;
-      if (chunk == 0) {
-        a0 = l2p_fp64(t, T, L, ti, tc, i0, want_phi);
-        a1 = l2p_fp64(t, T, L, ti, tc, i1, want_phi);
-      }
       const float4 h0 = shi[i0], l0 = slo[i0], h1 = shi[i1], l1 = slo[i1];
       const float2 thx = make_float2(h0.x, h1.x), thy = make_float2(h0.y, h1.y), thz = make_float2(h0.z, h1.z);
       const float2 tlx = make_float2(l0.x, l1.x), tly = make_float2(l0.y, l1.y), tlz = make_float2(l0.z, l1.z);
@@ -2031,9 +2031,10 @@ fmm_p2p32_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, 
                                          __ffma2_rn(make_float2(q.y, q.y), m1, tly));
             const float2 rz = __fadd2_rn(__ffma2_rn(make_float2(s.z, s.z), m1, thz),
                                          __ffma2_rn(make_float2(q.z, q.z), m1, tlz));
-            const float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __fmul2_rn(rz, rz)));
-            const float2 inv = make_float2((r2.x >= min_sq32 && r2.x > 0.f) ? rsqrtf(r2.x) : 0.f,
-                                           (r2.y >= min_sq32 && r2.y > 0.f) ? rsqrtf(r2.y) : 0.f);
+            float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __fmul2_rn(rz, rz)));
+            r2.x = r2.x >= min_sq32 ? r2.x : inf32;
+            r2.y = r2.y >= min_sq32 ? r2.y : inf32;
+            const float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
             const float2 qr = __fmul2_rn(make_float2(s.w, s.w), inv);
             const float2 f = __fmul2_rn(qr, __fmul2_rn(inv, inv));
             ax = __ffma2_rn(rx, f, ax);
@@ -2068,7 +2069,6 @@ fmm_p2p32_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, 
       mh = shi[i];
       ml = slo[i];
     }
-    if (active && g == 0 && chunk == 0) acc = l2p_fp64(t, T, L, ti, tc, i, want_phi);  // once per target
     for (int e = sb; e < se; ++e) {
       const int2 sr = t.range[src[e]];
       float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
@@ -2083,7 +2083,7 @@ fmm_p2p32_kernel(const Octree t, FmmDevTables T, const int2* __restrict__ work, 
             const float ry = fmaf(s.y, -1.f, mh.y) + fmaf(q.y, -1.f, ml.y);
             const float rz = fmaf(s.z, -1.f, mh.z) + fmaf(q.z, -1.f, ml.z);
             const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-            const float inv_r = (r2 >= min_sq32 && r2 > 0.f) ? rsqrtf(r2) : 0.f;
+            const float inv_r = rsqrtf(r2 >= min_sq32 ? r2 : inf32);
             const float qr = s.w * inv_r;
             const float f = qr * (inv_r * inv_r);
             ax = fmaf(rx, f, ax);
@@ -2134,6 +2134,23 @@ __global__ void fmm_p2p_reduce_kernel(const Octree t, const int* __restrict__ le
     a.z += b.z;
     a.w += b.w;
   }
+  ef[k] = a;
+}
+
+// FP32 near-field path: the FP64 L2P of every particle added to its summed
+// near field (a thread per particle; the table indices are the same on every
+// lane and a leaf's coefficients are shared by its particles' lanes).
+__global__ void fmm_l2p_add_kernel(const Octree t, FmmDevTables T, const int* __restrict__ leaf_of,
+                                   const double* __restrict__ L, bool want_phi, double4* __restrict__ ef) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= t.m) return;
+  const int leaf = leaf_of[k];
+  const double4 l = l2p_fp64(t, T, L, leaf, t.center[leaf], k, want_phi);
+  double4 a = ef[k];
+  a.x += l.x;
+  a.y += l.y;
+  a.z += l.z;
+  a.w += l.w;
   ef[k] = a;
 }
 
@@ -2397,8 +2414,8 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
       AMK_TRY(rc);
       p2p_stage_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, c->stream>>>(t, stage, stage + t.m);
       AMK_TRY(check_launch(c, "p2p_stage_kernel"));
-      fmm_p2p32_kernel<<<gwork, 32 * kFmmWarps, 0, c->stream>>>(t, T, work, ht[0], gp.off, gp.count, gp.src, pbase,
-                                                                Lx, min_sq, want_phi, stage, stage + t.m, part);
+      fmm_p2p32_kernel<<<gwork, 32 * kFmmWarps, 0, c->stream>>>(t, work, ht[0], gp.off, gp.count, gp.src, pbase,
+                                                                min_sq, stage, stage + t.m, part);
       AMK_TRY(check_launch(c, "fmm_p2p32_kernel"));
     } else {
       fmm_p2p_kernel<<<gwork, 32 * kFmmWarps, 0, c->stream>>>(t, T, work, ht[0], gp.off, gp.count, gp.src, pbase,
@@ -2408,6 +2425,11 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
     fmm_p2p_reduce_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, c->stream>>>(t, leaf_of, items, pbase,
                                                                                           part, ef);
     AMK_TRY(check_launch(c, "fmm_p2p_reduce_kernel"));
+    if (c->fmm_precision == AMK_FMM_TENSOR) {  // the FP32 near-field kernel leaves the L2P to this one
+      fmm_l2p_add_kernel<<<static_cast<unsigned>((t.m + 127) / 128), 128, 0, c->stream>>>(t, T, leaf_of, Lx, want_phi,
+                                                                                          ef);
+      AMK_TRY(check_launch(c, "fmm_l2p_add_kernel"));
+    }
     run->leaf_of = leaf_of;
   }
   AMK_TRY(phase_end(c, AMK_PHASE_FMM_P2P));

@@ -244,6 +244,14 @@ LEARNED = "learned p=2 + MLP theta=0.5"
 # DRAM traffic (read + write) per launch of the FMM's M2L class-product kernel,
 # by order, from ncu captures of one launch (launches at N = 1,048,576 process
 # chunks of the same bounded size).
+# DRAM traffic per class pair of the tensor-core product kernel (the FP32
+# per-pair products written, the split expansions read past L2), from one
+# ncu launch at 262,144 particles scaled by the pairs of a launch here.
+TC_PRODUCT_TRAFFIC_PER_PAIR = {
+    7: (570.0, "ncu dram__bytes_read.sum + dram__bytes_write.sum of m2l_class_tc_kernel<7> on 262,144 particles "
+               "(leaf 128, 3,007,536 pairs: 0.315 GB read + 1.399 GB written = 570 B per pair), scaled by this "
+               "launch's class pairs; profiles/m2l_class_tc_kernel_tree262k_leaf128.md"),
+}
 FMM_PRODUCT_TRAFFIC = {
     7: (5.18e9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of m2l_class_mma_kernel<7>, mean of two launches "
                 "of 4.47 M pairs each (0.89 / 1.10 GB read + 4.18 GB written: the per-pair products), "
@@ -409,8 +417,11 @@ def tree_roofline(sim, over, n):
         achieved = 2.0 * nm * nm * st["m2l_class_pairs"] / (prod_ms * 1e-3) / 1e12
         if over.get("precision") == "tensor" and 5 <= p_ <= 7:
             bf16, src = measured_peak("bf16_tflops", 1590.0)
+            per_pair = TC_PRODUCT_TRAFFIC_PER_PAIR.get(p_)
+            traffic = None if per_pair is None else per_pair[0] * st["m2l_class_pairs"] / max(1, prod_n)
             return {"bound": "tensor (split BF16)", "kernel": f"m2l_class_tc_kernel<{p_}>", "achieved": achieved,
-                    "peak": bf16 / 6.0, "unit": "TFLOP/s", "frac": achieved / (bf16 / 6.0), "traffic": None,
+                    "peak": bf16 / 6.0, "unit": "TFLOP/s", "frac": achieved / (bf16 / 6.0), "traffic": traffic,
+                    "traffic_source": None if per_pair is None else per_pair[1],
                     "peak_source": f"dense BF16 tensor peak {src}, divided by the six BF16 products each "
                                    "split-BF16 product issues",
                     "flop_convention": f"2 n_m^2 flop (n_m = {nm}) per M2L pair evaluated as a class product "
@@ -453,6 +464,8 @@ def run_tree(args):
                              device=local)
         if "leaf" in over:
             sim.set_leaf_sizes(fmm_leaf=over["leaf"])
+        elif args.fmm_leaf and over.get("coulomb_method") == "fast-multipole":
+            sim.set_leaf_sizes(fmm_leaf=args.fmm_leaf)
         if "precision" in over:
             sim.set_fmm_precision(over["precision"])
         sim.set_particles(pos[:, 0], pos[:, 1], pos[:, 2], vel[:, 0], vel[:, 1], vel[:, 2], sp)
@@ -1271,6 +1284,8 @@ def main(argv=None):
     ap.add_argument("--instances", type=int, default=512, help="trap instances of the sweep")
     ap.add_argument("--tree-n", type=int, default=1 << 20, help="particles of the tree workload")
     ap.add_argument("--tree-methods", default="", help="comma-separated subset of the tree workload's methods")
+    ap.add_argument("--fmm-leaf", type=int, default=0,
+                    help="leaf capacity of the table's FMM methods (0: the library's default, 32)")
     ap.add_argument("--long-n", type=int, default=1 << 22, help="particles of the long run")
     ap.add_argument("--log-every", type=int, default=100, help="steps between energy logs of the long run")
     args = ap.parse_args(argv)
