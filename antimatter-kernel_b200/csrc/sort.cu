@@ -14,9 +14,13 @@ constexpr int kSortThreads = 256;
 constexpr int kItems = 16;
 constexpr int kTile = kSortThreads * kItems;
 constexpr int kWarps = kSortThreads / 32;
-// counters the one-CTA scan_kernel handles (64 per thread); larger digit
-// histograms take the multi-CTA scan
+// counters the one-CTA scan_kernel handles (64 per thread; the bound of the
+// allocation-free sort, which has no scratch for the multi-CTA scan)
 constexpr long kSingleScanCounters = 65536;
+// the context's sort scans more than this many counters (n > 32,768 keys)
+// with the multi-CTA scan: the one-CTA scan of 65,536 counters takes about
+// 100 us per pass, the multi-CTA one about 15 us
+constexpr long kCtxSingleScanCounters = 2048;
 
 __global__ void __launch_bounds__(kSortThreads)
 hist_kernel(const uint64_t* __restrict__ keys, long n, int shift, int nb, uint32_t* __restrict__ hist) {
@@ -130,7 +134,7 @@ int radix_sort_pairs(amk_ctx* c, const uint64_t* keys_in, const uint32_t* vals_i
     const int shift = 8 * p;
     hist_kernel<<<nb, kSortThreads, 0, c->stream>>>(ksrc, n, shift, nb, hist);
     AMK_TRY(check_launch(c, "hist_kernel"));
-    if (static_cast<long>(256) * nb > kSingleScanCounters) {
+    if (static_cast<long>(256) * nb > kCtxSingleScanCounters) {
       // many tiles: the multi-CTA scan (in place; counts stay below 2^31)
       AMK_TRY(exclusive_scan_int(c, reinterpret_cast<const int*>(hist), static_cast<long>(256) * nb,
                                  reinterpret_cast<int*>(hist), total));
