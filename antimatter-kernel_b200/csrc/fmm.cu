@@ -312,38 +312,83 @@ __global__ void fmm_parent_radius_kernel(const Octree t, int depth, double* __re
 }
 
 // ------------------------------------------------------------ P2M, M2M
-// A warp per leaf; lanes over coefficients (fast-multipole.cc:443-461).
+// P2M (fast-multipole.cc:443-461): M_a = sum_j q_j d_j^a / a!, d_j = x_j - c.
+// A warp per leaf; lanes over particles (up to kP2mPer per lane per round).
+// The multi-indices a are visited in the lexicographic order of three
+// nested loops with running powers, so each monomial of each particle costs
+// one multiply; the lanes' partial sums of a coefficient are added by a
+// shuffle tree (fixed order: run-to-run deterministic) and lane 0 keeps the
+// leaf's sums in shared memory across rounds.
+constexpr int kP2mPer = 4;
+
 __global__ void __launch_bounds__(32 * kFmmWarps)
 fmm_p2m_kernel(const Octree t, FmmDevTables T, double* __restrict__ M) {
-  const int lane = threadIdx.x & 31;
-  const int id = blockIdx.x * kFmmWarps + (threadIdx.x >> 5);
+  __shared__ double acc_s[kFmmWarps][kMaxNm];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int id = blockIdx.x * kFmmWarps + w;
   if (id >= t.n_nodes || !t.meta[id].y) return;
   const double4 c = t.center[id];
   const int2 r = t.range[id];
-  double acc[(kMaxNm + 31) / 32];
-  for (int u = 0; u < (kMaxNm + 31) / 32; ++u) acc[u] = 0.0;
-  double px[kMaxOrder + 1], py[kMaxOrder + 1], pz[kMaxOrder + 1];
-  for (int k = r.x; k < r.y; ++k) {
-    const double4 s = t.src[k];
-    if (s.w == 0.0) continue;
-    powers(T.p, s.x - c.x, s.y - c.y, s.z - c.z, px, py, pz);
-    for (int u = 0, a = lane; a < T.n_m; ++u, a += 32) {
-      const int4 m = T.multi[a];
-      acc[u] += s.w * (px[m.x] * py[m.y] * pz[m.z]) * T.inv_fact[a];
+  const int P = T.p;
+  double* acc = acc_s[w];
+  for (int a = lane; a < T.n_m; a += 32) acc[a] = 0.0;
+  __syncwarp();
+  for (int r0 = r.x; r0 < r.y; r0 += 32 * kP2mPer) {
+    double dx[kP2mPer], dy[kP2mPer], dz[kP2mPer], qx[kP2mPer];
+#pragma unroll
+    for (int u = 0; u < kP2mPer; ++u) {
+      const int k = r0 + lane + 32 * u;
+      const double4 s = k < r.y ? t.src[k] : make_double4(c.x, c.y, c.z, 0.0);
+      dx[u] = s.x - c.x;
+      dy[u] = s.y - c.y;
+      dz[u] = s.z - c.z;
+      qx[u] = s.w;  // q x^i, running
+    }
+    for (int i = 0; i <= P; ++i) {
+      double qy[kP2mPer];
+#pragma unroll
+      for (int u = 0; u < kP2mPer; ++u) qy[u] = qx[u];  // q x^i y^j, running
+      for (int j = 0; i + j <= P; ++j) {
+        double m[kP2mPer];
+#pragma unroll
+        for (int u = 0; u < kP2mPer; ++u) m[u] = qy[u];  // q x^i y^j z^k, running
+        for (int k = 0; i + j + k <= P; ++k) {
+          double v = 0.0;
+#pragma unroll
+          for (int u = 0; u < kP2mPer; ++u) {
+            v += m[u];
+            m[u] *= dz[u];
+          }
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (lane == 0) acc[graded_index(i, j, k)] += v;
+        }
+#pragma unroll
+        for (int u = 0; u < kP2mPer; ++u) qy[u] *= dy[u];
+      }
+#pragma unroll
+      for (int u = 0; u < kP2mPer; ++u) qx[u] *= dx[u];
     }
   }
-  for (int u = 0, a = lane; a < T.n_m; ++u, a += 32) M[static_cast<size_t>(id) * T.n_m + a] = acc[u];
+  __syncwarp();
+  for (int a = lane; a < T.n_m; a += 32) M[static_cast<size_t>(id) * T.n_m + a] = acc[a] * T.inv_fact[a];
 }
 
-// M2M for parents at `depth` (fast-multipole.cc:463-482).
+// M2M for parents at `depth` (fast-multipole.cc:463-482). A warp per
+// parent, lanes over the parent's coefficients; per child the lanes first
+// write the offset's monomials d^c / c! (c over all multi-indices) into
+// shared memory, then each term of coefficient a is one product
+// M_child[b] * mono[a - b] with b and a - b from the table.
 __global__ void __launch_bounds__(32 * kFmmWarps)
 fmm_m2m_kernel(const Octree t, FmmDevTables T, int depth, double* __restrict__ M) {
-  const int lane = threadIdx.x & 31;
-  const int id = blockIdx.x * kFmmWarps + (threadIdx.x >> 5);
+  __shared__ double mono_s[kFmmWarps][kMaxNm];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int id = blockIdx.x * kFmmWarps + w;
   if (id >= t.n_nodes) return;
   const uchar2 mt = t.meta[id];
   if (mt.y || mt.x != depth) return;
   const double4 c = t.center[id];
+  double* mono = mono_s[w];
   double acc[(kMaxNm + 31) / 32];
   for (int u = 0; u < (kMaxNm + 31) / 32; ++u) acc[u] = 0.0;
   double px[kMaxOrder + 1], py[kMaxOrder + 1], pz[kMaxOrder + 1];
@@ -352,14 +397,16 @@ fmm_m2m_kernel(const Octree t, FmmDevTables T, int depth, double* __restrict__ M
     if (ch < 0) continue;
     const double4 cc = t.center[ch];
     powers(T.p, cc.x - c.x, cc.y - c.y, cc.z - c.z, px, py, pz);
+    __syncwarp();  // the previous child's monomials are no longer read
+    for (int a = lane; a < T.n_m; a += 32) {
+      const int4 m = T.multi[a];
+      mono[a] = (px[m.x] * py[m.y] * pz[m.z]) * T.inv_fact[a];
+    }
+    __syncwarp();
     const double* mc = M + static_cast<size_t>(ch) * T.n_m;
     for (int u = 0, a = lane; a < T.n_m; ++u, a += 32) {
       double s = acc[u];
-      for (int e = T.m2m_off[a]; e < T.m2m_off[a + 1]; ++e) {
-        const int cidx = T.m2m_c[e];
-        const int4 m = T.multi[cidx];
-        s += mc[T.m2m_b[e]] * (px[m.x] * py[m.y] * pz[m.z]) * T.inv_fact[cidx];
-      }
+      for (int e = T.m2m_off[a]; e < T.m2m_off[a + 1]; ++e) s += mc[T.m2m_b[e]] * mono[T.m2m_c[e]];
       acc[u] = s;
     }
   }
@@ -1766,10 +1813,14 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
 
 // ------------------------------------------------------------ L2L
 // Children at `depth` receive their parent's expansion (fast-multipole.cc:557-578).
+// A warp per child, lanes over its coefficients; the offset's monomials
+// d^c / c! and the parent's L_b b! are staged in shared memory first, so a
+// term is one product; 1/a! is applied once per coefficient.
 __global__ void __launch_bounds__(32 * kFmmWarps)
 fmm_l2l_kernel(const Octree t, FmmDevTables T, int depth, double* __restrict__ L) {
-  const int lane = threadIdx.x & 31;
-  const int id = blockIdx.x * kFmmWarps + (threadIdx.x >> 5);
+  __shared__ double mono_s[kFmmWarps][kMaxNm], lps_s[kFmmWarps][kMaxNm];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int id = blockIdx.x * kFmmWarps + w;
   if (id >= t.n_nodes) return;
   if (t.meta[id].x != depth) return;
   const int par = t.parent[id];
@@ -1779,14 +1830,18 @@ fmm_l2l_kernel(const Octree t, FmmDevTables T, int depth, double* __restrict__ L
   powers(T.p, c.x - pc.x, c.y - pc.y, c.z - pc.z, px, py, pz);
   const double* lp = L + static_cast<size_t>(par) * T.n_m;
   double* lc = L + static_cast<size_t>(id) * T.n_m;
+  double* mono = mono_s[w];
+  double* lps = lps_s[w];
   for (int a = lane; a < T.n_m; a += 32) {
-    double s = lc[a];
-    for (int e = T.l2l_off[a]; e < T.l2l_off[a + 1]; ++e) {
-      const int bb = T.l2l_b[e], cc = T.l2l_c[e];
-      const int4 m = T.multi[cc];
-      s += lp[bb] * T.fact[bb] * T.inv_fact[a] * T.inv_fact[cc] * (px[m.x] * py[m.y] * pz[m.z]);
-    }
-    lc[a] = s;
+    const int4 m = T.multi[a];
+    mono[a] = (px[m.x] * py[m.y] * pz[m.z]) * T.inv_fact[a];
+    lps[a] = lp[a] * T.fact[a];
+  }
+  __syncwarp();
+  for (int a = lane; a < T.n_m; a += 32) {
+    double s = 0.0;
+    for (int e = T.l2l_off[a]; e < T.l2l_off[a + 1]; ++e) s += lps[T.l2l_b[e]] * mono[T.l2l_c[e]];
+    lc[a] += s * T.inv_fact[a];
   }
 }
 
