@@ -25,6 +25,7 @@
 // rsqrt (the reference divides by sqrt), a difference of an ulp.
 #include <algorithm>
 #include <array>
+#include <functional>
 #include <map>
 #include <memory>
 #include <type_traits>
@@ -191,6 +192,10 @@ struct Fmm {
   // of the next chunk run on the context stream
   cudaStream_t side = nullptr;
   cudaEvent_t products_done[2] = {nullptr, nullptr}, sums_done[2] = {nullptr, nullptr};
+  // FP32 near field (tensor mode): its pair kernel runs on `near` after the
+  // last M2L products, concurrently with the per-target sums and L2L
+  cudaStream_t near = nullptr;
+  cudaEvent_t near_start = nullptr, near_done = nullptr;
   // statistics of the last evaluation (amk_fmm_stats)
   long stats[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   ~Fmm() {
@@ -199,6 +204,9 @@ struct Fmm {
       if (products_done[i]) cudaEventDestroy(products_done[i]);
       if (sums_done[i]) cudaEventDestroy(sums_done[i]);
     }
+    if (near_start) cudaEventDestroy(near_start);
+    if (near_done) cudaEventDestroy(near_done);
+    if (near) cudaStreamDestroy(near);
     if (side) cudaStreamDestroy(side);
   }
 };
@@ -1625,9 +1633,11 @@ int m2l_reach() {
   return r < 0 ? 0 : (r > kM2lMaxReach ? kM2lMaxReach : r);
 }
 
-// All M2L pairs (grouped by target in gm) into L.
+// All M2L pairs (grouped by target in gm) into L. after_products (may be
+// empty) runs once the last chunk's products are enqueued on the context
+// stream, before their per-target sums and the final status read.
 int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, const Grouped& gm, long n_m2l,
-                 const double* M, double* L) {
+                 const double* M, double* L, const std::function<int()>& after_products) {
   int rc = AMK_OK;
   const long nn = t.n_nodes;
   const int reach = m2l_reach();
@@ -1789,6 +1799,7 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
       else
         AMK_TRY(launch_pairs(m2l_pair_kernel<double>, static_cast<double*>(out)));
     }
+    if (e1 >= n_m2l && after_products) AMK_TRY(after_products());
     // per-target sums on the side stream, in chunk order
     AMK_CUDA_TRY(cudaEventRecord(f->products_done[buf], c->stream));
     AMK_CUDA_TRY(cudaStreamWaitEvent(f->side, f->products_done[buf], 0));
@@ -2415,10 +2426,83 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
                       kSlotFmmWork3, &gp));
   AMK_TRY(phase_end(c, AMK_PHASE_FMM_LISTS));
 
+  // ---- near-field set-up: work items (a target leaf and up to kP2PChunk
+  // source leaves of its list) and the per-item partial sums' layout
+  double4* ef = slot<double4>(c, kSlotFmmWork4, t.m, &rc);
+  AMK_TRY(rc);
+  TreeFrame hf;
+  AMK_CUDA_TRY(cudaMemcpyAsync(&hf, t.frame, sizeof(hf), cudaMemcpyDeviceToHost, c->stream));
+  AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  const double min_sq = kMinSquaredDistance / (hf.length * hf.length);
+  const bool f32 = c->fmm_precision == AMK_FMM_TENSOR;
+  AMK_TRY(phase_begin(c, AMK_PHASE_FMM_P2P));
+  int* items = slot<int>(c, kSlotFmmAux2, nn + 1, &rc);
+  AMK_TRY(rc);
+  int* psize = slot<int>(c, kSlotTreeCount, nn + 1, &rc);  // tree build scratch, free again
+  AMK_TRY(rc);
+  int* ibase = slot<int>(c, kSlotTreeBase, nn + 1, &rc);
+  AMK_TRY(rc);
+  int* pbase = slot<int>(c, kSlotTreeL, nn + 1, &rc);
+  AMK_TRY(rc);
+  int* totals = slot<int>(c, kSlotFmmAux1, 8, &rc);
+  AMK_TRY(rc);
+  p2p_items_count_kernel<<<gn, 256, 0, c->stream>>>(t, gp.count, items, psize);
+  AMK_TRY(check_launch(c, "p2p_items_count_kernel"));
+  AMK_TRY(exclusive_scan_int(c, items, nn, ibase, totals));
+  AMK_TRY(exclusive_scan_int(c, psize, nn, pbase, totals + 1));
+  int ht[2] = {0, 0};
+  AMK_CUDA_TRY(cudaMemcpyAsync(ht, totals, sizeof(ht), cudaMemcpyDeviceToHost, c->stream));
+  AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
+  int2* work = slot<int2>(c, kSlotP2PWork, ht[0] + 1, &rc);
+  AMK_TRY(rc);
+  int* leaf_of = slot<int>(c, kSlotTreeLeafDepth, t.m + 1, &rc);
+  AMK_TRY(rc);
+  double4* part = slot<double4>(c, kSlotP2PPart, static_cast<size_t>(ht[1]) + 1, &rc);
+  AMK_TRY(rc);
+  float4* stage = nullptr;
+  if (f32) {
+    stage = slot<float4>(c, kSlotP2PStage, 2 * static_cast<size_t>(t.m), &rc);
+    AMK_TRY(rc);
+  }
+  p2p_items_fill_kernel<<<gn, 256, 0, c->stream>>>(t, items, ibase, work, leaf_of);
+  AMK_TRY(check_launch(c, "p2p_items_fill_kernel"));
+  AMK_TRY(phase_end(c, AMK_PHASE_FMM_P2P));
+  const unsigned gwork = static_cast<unsigned>((ht[0] + kFmmWarps - 1) / kFmmWarps);
+  Fmm* f = c->fmm;
+  // FP32 near field: its pair sums need no expansion, so they run on their
+  // own stream once the last M2L products are enqueued (the product kernel
+  // holds every SM's shared memory), concurrently with the per-target M2L
+  // sums and L2L; the FP64 L2P is added after L2L on the context stream
+  auto launch_near = [&]() -> int {
+    if (!f->near) {
+      AMK_CUDA_TRY(cudaStreamCreateWithFlags(&f->near, cudaStreamNonBlocking));
+      AMK_CUDA_TRY(cudaEventCreateWithFlags(&f->near_start, cudaEventDisableTiming));
+      AMK_CUDA_TRY(cudaEventCreateWithFlags(&f->near_done, cudaEventDisableTiming));
+    }
+    AMK_CUDA_TRY(cudaEventRecord(f->near_start, c->stream));
+    AMK_CUDA_TRY(cudaStreamWaitEvent(f->near, f->near_start, 0));
+    p2p_stage_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, f->near>>>(t, stage, stage + t.m);
+    AMK_TRY(check_launch(c, "p2p_stage_kernel"));
+    fmm_p2p32_kernel<<<gwork, 32 * kFmmWarps, 0, f->near>>>(t, work, ht[0], gp.off, gp.count, gp.src, pbase, min_sq,
+                                                            stage, stage + t.m, part);
+    AMK_TRY(check_launch(c, "fmm_p2p32_kernel"));
+    fmm_p2p_reduce_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, f->near>>>(t, leaf_of, items, pbase,
+                                                                                       part, ef);
+    AMK_TRY(check_launch(c, "fmm_p2p_reduce_kernel"));
+    AMK_CUDA_TRY(cudaEventRecord(f->near_done, f->near));
+    return AMK_OK;
+  };
+  const std::function<int()> no_hook;
+
   // ---- M2L
   AMK_CUDA_TRY(cudaMemsetAsync(Lx, 0, static_cast<size_t>(nn) * T.n_m * sizeof(double), c->stream));
   AMK_TRY(phase_begin(c, AMK_PHASE_FMM_M2L));
-  if (n_m2l > 0) AMK_TRY(m2l_products(c, order, t, T, gm, n_m2l, M, Lx));
+  if (n_m2l > 0) {
+    const std::function<int()> hook(launch_near);
+    AMK_TRY(m2l_products(c, order, t, T, gm, n_m2l, M, Lx, f32 ? hook : no_hook));
+  } else if (f32) {
+    AMK_TRY(launch_near());
+  }
   AMK_TRY(phase_end(c, AMK_PHASE_FMM_M2L));
 
   // ---- L2L
@@ -2430,63 +2514,21 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
   AMK_TRY(phase_end(c, AMK_PHASE_FMM_DOWN));
 
   // ---- L2P + P2P
-  double4* ef = slot<double4>(c, kSlotFmmWork4, t.m, &rc);
-  AMK_TRY(rc);
-  TreeFrame hf;
-  AMK_CUDA_TRY(cudaMemcpyAsync(&hf, t.frame, sizeof(hf), cudaMemcpyDeviceToHost, c->stream));
-  AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  const double min_sq = kMinSquaredDistance / (hf.length * hf.length);
   AMK_TRY(phase_begin(c, AMK_PHASE_FMM_P2P));
-  {
-    int* items = slot<int>(c, kSlotFmmAux2, nn + 1, &rc);
-    AMK_TRY(rc);
-    int* psize = slot<int>(c, kSlotTreeCount, nn + 1, &rc);  // tree build scratch, free again
-    AMK_TRY(rc);
-    int* ibase = slot<int>(c, kSlotTreeBase, nn + 1, &rc);
-    AMK_TRY(rc);
-    int* pbase = slot<int>(c, kSlotTreeL, nn + 1, &rc);
-    AMK_TRY(rc);
-    int* totals = slot<int>(c, kSlotFmmAux1, 8, &rc);
-    AMK_TRY(rc);
-    p2p_items_count_kernel<<<gn, 256, 0, c->stream>>>(t, gp.count, items, psize);
-    AMK_TRY(check_launch(c, "p2p_items_count_kernel"));
-    AMK_TRY(exclusive_scan_int(c, items, nn, ibase, totals));
-    AMK_TRY(exclusive_scan_int(c, psize, nn, pbase, totals + 1));
-    int ht[2] = {0, 0};
-    AMK_CUDA_TRY(cudaMemcpyAsync(ht, totals, sizeof(ht), cudaMemcpyDeviceToHost, c->stream));
-    AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    int2* work = slot<int2>(c, kSlotP2PWork, ht[0] + 1, &rc);
-    AMK_TRY(rc);
-    int* leaf_of = slot<int>(c, kSlotTreeLeafDepth, t.m + 1, &rc);
-    AMK_TRY(rc);
-    double4* part = slot<double4>(c, kSlotP2PPart, static_cast<size_t>(ht[1]) + 1, &rc);
-    AMK_TRY(rc);
-    p2p_items_fill_kernel<<<gn, 256, 0, c->stream>>>(t, items, ibase, work, leaf_of);
-    AMK_TRY(check_launch(c, "p2p_items_fill_kernel"));
-    const unsigned gwork = static_cast<unsigned>((ht[0] + kFmmWarps - 1) / kFmmWarps);
-    if (c->fmm_precision == AMK_FMM_TENSOR) {
-      float4* stage = slot<float4>(c, kSlotP2PStage, 2 * static_cast<size_t>(t.m), &rc);
-      AMK_TRY(rc);
-      p2p_stage_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, c->stream>>>(t, stage, stage + t.m);
-      AMK_TRY(check_launch(c, "p2p_stage_kernel"));
-      fmm_p2p32_kernel<<<gwork, 32 * kFmmWarps, 0, c->stream>>>(t, work, ht[0], gp.off, gp.count, gp.src, pbase,
-                                                                min_sq, stage, stage + t.m, part);
-      AMK_TRY(check_launch(c, "fmm_p2p32_kernel"));
-    } else {
-      fmm_p2p_kernel<<<gwork, 32 * kFmmWarps, 0, c->stream>>>(t, T, work, ht[0], gp.off, gp.count, gp.src, pbase,
-                                                              Lx, min_sq, want_phi, part);
-      AMK_TRY(check_launch(c, "fmm_p2p_kernel"));
-    }
+  if (f32) {  // join the near-field stream, then the FP64 L2P
+    AMK_CUDA_TRY(cudaStreamWaitEvent(c->stream, f->near_done, 0));
+    fmm_l2p_add_kernel<<<static_cast<unsigned>((t.m + 127) / 128), 128, 0, c->stream>>>(t, T, leaf_of, Lx, want_phi,
+                                                                                        ef);
+    AMK_TRY(check_launch(c, "fmm_l2p_add_kernel"));
+  } else {
+    fmm_p2p_kernel<<<gwork, 32 * kFmmWarps, 0, c->stream>>>(t, T, work, ht[0], gp.off, gp.count, gp.src, pbase, Lx,
+                                                            min_sq, want_phi, part);
+    AMK_TRY(check_launch(c, "fmm_p2p_kernel"));
     fmm_p2p_reduce_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, c->stream>>>(t, leaf_of, items, pbase,
                                                                                           part, ef);
     AMK_TRY(check_launch(c, "fmm_p2p_reduce_kernel"));
-    if (c->fmm_precision == AMK_FMM_TENSOR) {  // the FP32 near-field kernel leaves the L2P to this one
-      fmm_l2p_add_kernel<<<static_cast<unsigned>((t.m + 127) / 128), 128, 0, c->stream>>>(t, T, leaf_of, Lx, want_phi,
-                                                                                          ef);
-      AMK_TRY(check_launch(c, "fmm_l2p_add_kernel"));
-    }
-    run->leaf_of = leaf_of;
   }
+  run->leaf_of = leaf_of;
   AMK_TRY(phase_end(c, AMK_PHASE_FMM_P2P));
   run->t = t;
   run->T = T;
