@@ -543,9 +543,10 @@ struct Grouped {
 constexpr int kM2lTileP = 64;      // pairs per product tile
 constexpr int kM2lUnitTiles = 8;   // tiles of one class per block
 constexpr int kM2lUnitPairs = kM2lUnitTiles * kM2lTileP;
-constexpr int kM2lMinClass = 4;    // FP64 mode: classes below this size take the per-pair path
-// (the tensor-core product costs about as much per class unit as the
-// per-pair path per pair, so in that mode every lattice class takes it)
+// classes below this size take the per-pair path in both precision modes (in
+// tensor-core mode a class-matrix build per tiny class costs more than the
+// per-pair path: measured at 1,048,576 particles, leaf 128)
+constexpr int kM2lMinClass = 4;
 constexpr size_t kM2lChunkBytes = size_t(4) << 30;  // per-pair products of one chunk
 // tensor-core mode: larger chunks (a class split across chunks costs one
 // more class-matrix build per chunk; two buffers of this size at most)
@@ -1723,7 +1724,7 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
     m2l_histogram_kernel<<<ge, 256, 0, c->stream>>>(codes, e0, e1, hist, fallback, counters + 3);
     AMK_TRY(check_launch(c, "m2l_histogram_kernel"));
     AMK_TRY(exclusive_scan_int(c, hist, n_codes, start, counters));
-    m2l_code_flags_kernel<<<gc, 256, 0, c->stream>>>(hist, n_codes, tc ? 1 : kM2lMinClass, used, nunit);
+    m2l_code_flags_kernel<<<gc, 256, 0, c->stream>>>(hist, n_codes, kM2lMinClass, used, nunit);
     AMK_TRY(check_launch(c, "m2l_code_flags_kernel"));
     AMK_TRY(exclusive_scan_int(c, used, n_codes, cls_index, counters + 1));
     AMK_TRY(exclusive_scan_int(c, nunit, n_codes, unit_start, counters + 2));
