@@ -649,8 +649,10 @@ __global__ void m2l_histogram_kernel(const int* __restrict__ codes, long e0, lon
     fallback[atomicAdd(n_fallback, 1)] = static_cast<int>(e);
 }
 
-// Classes of fewer than min_class pairs go the per-pair path.
-__global__ void m2l_code_flags_kernel(const int* __restrict__ hist, long n_codes, int min_class,
+// Classes of fewer than min_class pairs go the per-pair path; their counts
+// are cleared, so the scan of hist places the pairs of the classes taken
+// contiguously at the start of the chunk's permutation.
+__global__ void m2l_code_flags_kernel(int* __restrict__ hist, long n_codes, int min_class,
                                       int* __restrict__ used, int* __restrict__ units) {
   const long code = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
   if (code >= n_codes) return;
@@ -658,6 +660,7 @@ __global__ void m2l_code_flags_kernel(const int* __restrict__ hist, long n_codes
   const bool take = n > 0 && n >= min_class;
   used[code] = take;
   units[code] = take ? (n + kM2lUnitPairs - 1) / kM2lUnitPairs : 0;
+  if (!take) hist[code] = 0;
 }
 
 // Class list and product units (<= 8 tiles of one class) from the scanned
@@ -1723,9 +1726,9 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
     const unsigned ge = static_cast<unsigned>((ne + 255) / 256), gc = static_cast<unsigned>((n_codes + 255) / 256);
     m2l_histogram_kernel<<<ge, 256, 0, c->stream>>>(codes, e0, e1, hist, fallback, counters + 3);
     AMK_TRY(check_launch(c, "m2l_histogram_kernel"));
-    AMK_TRY(exclusive_scan_int(c, hist, n_codes, start, counters));
     m2l_code_flags_kernel<<<gc, 256, 0, c->stream>>>(hist, n_codes, kM2lMinClass, used, nunit);
     AMK_TRY(check_launch(c, "m2l_code_flags_kernel"));
+    AMK_TRY(exclusive_scan_int(c, hist, n_codes, start, counters));
     AMK_TRY(exclusive_scan_int(c, used, n_codes, cls_index, counters + 1));
     AMK_TRY(exclusive_scan_int(c, nunit, n_codes, unit_start, counters + 2));
     m2l_class_fill_kernel<<<gc, 256, 0, c->stream>>>(hist, start, cls_index, unit_start, n_codes, used, cls_code,
@@ -1739,6 +1742,9 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
     AMK_CUDA_TRY(cudaMemcpyAsync(tr + 1, tgt + e1 - 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
     const int n_cls = h[1], n_units = h[2], n_fb = h[3];
+    // the classes' pairs fill perm[0, h[0]) and every other pair is on the per-pair list
+    if (static_cast<long>(h[0]) + n_fb != ne)
+      return fail(AMK_ERR_STATE, "M2L chunk: %d class pairs + %d per-pair != %ld", h[0], n_fb, ne);
     f->stats[8] += ne - n_fb;
     f->stats[9] += n_cls;
     f->stats[10] += 1;
