@@ -38,7 +38,8 @@ SPECIES = {"antiproton": 0, "positron": 1, "antihydrogen": 2, "electron": 3,
 
 CLOUD = {"uniform": 0, "gaussian": 1}
 PHASES = ["stage", "allpairs", "cutoff", "sort", "tree", "bh_walk", "fmm_up", "fmm_lists",
-          "fmm_m2l", "fmm_down", "fmm_p2p", "mlp", "push", "annihilation", "energy", "fmm_m2l_products"]
+          "fmm_m2l", "fmm_down", "fmm_p2p", "mlp", "push", "annihilation", "energy", "fmm_m2l_products",
+          "fmm_near"]
 
 
 class AmkError(RuntimeError):

@@ -278,6 +278,9 @@ namespace amk {
 // profiling is enabled (events are read lazily in amk_phase_times).
 int phase_begin(amk_ctx* c, int phase);
 int phase_end(amk_ctx* c, int phase);
+// the same, with the events recorded on another stream of the context
+int phase_begin_on(amk_ctx* c, int phase, cudaStream_t stream);
+int phase_end_on(amk_ctx* c, int phase, cudaStream_t stream);
 
 inline int check_launch(amk_ctx* c, const char* what) {
   c->kernel_launches++;

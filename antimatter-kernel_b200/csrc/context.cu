@@ -121,7 +121,11 @@ int stage_view(amk_ctx* c, const View& v) {
   return check_launch(c, "stage_kernel");
 }
 
-int phase_begin(amk_ctx* c, int phase) {
+int phase_begin(amk_ctx* c, int phase) { return phase_begin_on(c, phase, c->stream); }
+
+int phase_end(amk_ctx* c, int phase) { return phase_end_on(c, phase, c->stream); }
+
+int phase_begin_on(amk_ctx* c, int phase, cudaStream_t stream) {
   if (!c->profiling) return AMK_OK;
   auto& pools = g_events[c];
   if (pools.size() < AMK_NUM_PHASES) pools.resize(AMK_NUM_PHASES);
@@ -134,18 +138,18 @@ int phase_begin(amk_ctx* c, int phase) {
     p.start.push_back(a);
     p.stop.push_back(b);
   }
-  AMK_CUDA_TRY(cudaEventRecord(p.start[p.used], c->stream));
+  AMK_CUDA_TRY(cudaEventRecord(p.start[p.used], stream));
   return AMK_OK;
 }
 
-int phase_end(amk_ctx* c, int phase) {
+int phase_end_on(amk_ctx* c, int phase, cudaStream_t stream) {
   if (!c->profiling) return AMK_OK;
   auto& pools = g_events[c];
   if (pools.size() < AMK_NUM_PHASES) return AMK_OK;
   EventPool& p = pools[phase];
   if (p.open == 0) return AMK_OK;
   if (--p.open > 0) return AMK_OK;
-  AMK_CUDA_TRY(cudaEventRecord(p.stop[p.used], c->stream));
+  AMK_CUDA_TRY(cudaEventRecord(p.stop[p.used], stream));
   p.used++;
   return AMK_OK;
 }

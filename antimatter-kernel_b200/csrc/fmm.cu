@@ -182,6 +182,8 @@ struct FmmDevTables {
 
 struct FmmLists {
   DevBuf cur, next, m2l, p2p;
+  // list lengths the last traversal needed (the next one reserves them)
+  long need_front = 0, need_m2l = 0, need_p2p = 0;
 };
 
 struct Fmm {
@@ -196,6 +198,10 @@ struct Fmm {
   // last M2L products, concurrently with the per-target sums and L2L
   cudaStream_t near = nullptr;
   cudaEvent_t near_start = nullptr, near_done = nullptr;
+  // P2M / M2M run on `up` concurrently with the traversal, which needs only
+  // the cell radii
+  cudaStream_t up = nullptr;
+  cudaEvent_t up_start = nullptr, up_done = nullptr;
   // statistics of the last evaluation (amk_fmm_stats)
   long stats[11] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
   ~Fmm() {
@@ -208,6 +214,9 @@ struct Fmm {
     if (near_done) cudaEventDestroy(near_done);
     if (near) cudaStreamDestroy(near);
     if (side) cudaStreamDestroy(side);
+    if (up_start) cudaEventDestroy(up_start);
+    if (up_done) cudaEventDestroy(up_done);
+    if (up) cudaStreamDestroy(up);
   }
 };
 
@@ -426,63 +435,104 @@ fmm_m2m_kernel(const Octree t, FmmDevTables T, int depth, double* __restrict__ M
 // pair is accepted for M2L, kept for P2P, or split into its children. The
 // emissions of a warp are reserved with one atomic per list (ballot / warp
 // prefix sums); the order of the lists is irrelevant, they are sorted after.
+// The level's pair count is read on the device (lv[0]), the children are
+// counted into lv[1]; a slot past a list's capacity is not written and
+// raises cnt[2], so the host can grow the lists and run the traversal again
+// (counts keep growing past the capacity, and every slot below it is
+// written). A pair that is not a pair of nodes raises cnt[3] and is
+// skipped. Warps stride over the level's pairs, so one grid size serves
+// every level.
+__global__ void fmm_traverse_root_kernel(int2* __restrict__ cur, int* __restrict__ lv) {
+  if (threadIdx.x == 0) {
+    cur[0] = make_int2(0, 0);
+    lv[0] = 1;
+  }
+}
+
+struct TraverseLists {
+  int2* m2l;
+  int2* p2p;
+  long cap_m2l, cap_p2p, cap_front;
+};
+
 __global__ void fmm_traverse_kernel(const Octree t, const double* __restrict__ radius, double theta2,
-                                    const int2* __restrict__ cur, int n_cur, int2* __restrict__ next,
-                                    int2* __restrict__ m2l, int2* __restrict__ p2p, int* counters) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+                                    const int2* __restrict__ cur, int2* __restrict__ next, TraverseLists out,
+                                    int* __restrict__ lv, int* __restrict__ cnt) {
   const int lane = threadIdx.x & 31;
   const unsigned below = (1u << lane) - 1u;
-  int2 pr = make_int2(0, 0);
-  int kind = -1;  // 0 M2L, 1 P2P, 2 split
-  int kids[8], nk = 0;
-  bool split_target = false;
-  if (i < n_cur) {
-    pr = cur[i];
-    const int ti = pr.x, si = pr.y;
-    const double4 tc = t.center[ti], sc = t.center[si];
-    const double dx = tc.x - sc.x, dy = tc.y - sc.y, dz = tc.z - sc.z;
-    const double dist2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-    const double rt = radius[ti], rs = radius[si];
-    const double rsum = rt + rs;
-    if (__dmul_rn(rsum, rsum) < __dmul_rn(theta2, dist2)) {
-      kind = 0;
-    } else {
-      const bool tleaf = t.meta[ti].y, sleaf = t.meta[si].y;
-      if (tleaf && sleaf) {
-        kind = 1;
+  const long n_cur = min(static_cast<long>(lv[0]), out.cap_front);
+  const long warp0 = (blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x) >> 5;
+  const long n_warps = (static_cast<long>(gridDim.x) * blockDim.x) >> 5;
+  for (long base = warp0 * 32; base < n_cur; base += n_warps * 32) {
+    const long i = base + lane;
+    int2 pr = make_int2(0, 0);
+    int kind = -1;  // 0 M2L, 1 P2P, 2 split
+    int kids[8], nk = 0;
+    bool split_target = false;
+    if (i < n_cur) pr = cur[i];
+    if (i < n_cur && (static_cast<unsigned>(pr.x) >= static_cast<unsigned>(t.n_nodes) ||
+                      static_cast<unsigned>(pr.y) >= static_cast<unsigned>(t.n_nodes))) {
+      cnt[3] = 1;  // not a node pair: recorded and skipped
+    } else if (i < n_cur) {
+      const int ti = pr.x, si = pr.y;
+      const double4 tc = t.center[ti], sc = t.center[si];
+      const double dx = tc.x - sc.x, dy = tc.y - sc.y, dz = tc.z - sc.z;
+      const double dist2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+      const double rt = radius[ti], rs = radius[si];
+      const double rsum = rt + rs;
+      if (__dmul_rn(rsum, rsum) < __dmul_rn(theta2, dist2)) {
+        kind = 0;
       } else {
-        kind = 2;
-        split_target = sleaf || (!tleaf && rt >= rs);
-        const int node = split_target ? ti : si;
-        for (int o = 0; o < 8; ++o) {
-          const int ch = t.child[8 * node + o];
-          if (ch >= 0) kids[nk++] = ch;
+        const bool tleaf = t.meta[ti].y, sleaf = t.meta[si].y;
+        if (tleaf && sleaf) {
+          kind = 1;
+        } else {
+          kind = 2;
+          split_target = sleaf || (!tleaf && rt >= rs);
+          const int node = split_target ? ti : si;
+          for (int o = 0; o < 8; ++o) {
+            const int ch = t.child[8 * node + o];
+            if (ch >= 0) kids[nk++] = ch;
+          }
         }
       }
     }
-  }
-  // M2L and P2P: one slot per lane
-  for (int list = 0; list < 2; ++list) {
-    const unsigned m = __ballot_sync(0xffffffffu, kind == list);
-    if (m == 0) continue;
-    int base = 0;
-    if (lane == __ffs(m) - 1) base = atomicAdd(&counters[list], __popc(m));
-    base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
-    if (kind == list) (list == 0 ? m2l : p2p)[base + __popc(m & below)] = pr;
-  }
-  // children: a warp prefix sum of the counts
-  int incl = nk;
+    // M2L and P2P: one slot per lane
+    for (int list = 0; list < 2; ++list) {
+      const unsigned m = __ballot_sync(0xffffffffu, kind == list);
+      if (m == 0) continue;
+      int b = 0;
+      if (lane == __ffs(m) - 1) b = atomicAdd(&cnt[list], __popc(m));
+      b = __shfl_sync(0xffffffffu, b, __ffs(m) - 1);
+      const long slot = static_cast<long>(b) + __popc(m & below);
+      if (kind == list) {
+        if (slot < (list == 0 ? out.cap_m2l : out.cap_p2p))
+          (list == 0 ? out.m2l : out.p2p)[slot] = pr;
+        else
+          cnt[2] = 1;
+      }
+    }
+    // children: a warp prefix sum of the counts
+    int incl = nk;
 #pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const int v = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += v;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, incl, 31);
+    if (total == 0) continue;
+    int b = 0;
+    if (lane == 31) b = atomicAdd(&lv[1], total);
+    const long first = static_cast<long>(__shfl_sync(0xffffffffu, b, 31)) + incl - nk;
+    // every slot below the capacity is written (the reservations are
+    // contiguous), so the next level reads only pairs of this one
+    for (int k = 0; k < nk; ++k) {
+      if (first + k < out.cap_front)
+        next[first + k] = split_target ? make_int2(kids[k], pr.y) : make_int2(pr.x, kids[k]);
+      else
+        cnt[2] = 1;
+    }
   }
-  const int total = __shfl_sync(0xffffffffu, incl, 31);
-  if (total == 0) return;
-  int base = 0;
-  if (lane == 31) base = atomicAdd(&counters[2], total);
-  base = __shfl_sync(0xffffffffu, base, 31) + incl - nk;
-  for (int k = 0; k < nk; ++k) next[base + k] = split_target ? make_int2(kids[k], pr.y) : make_int2(pr.x, kids[k]);
 }
 
 // Group pairs by target: pack (target, source) into one key and radix-sort
@@ -1806,6 +1856,8 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
       else
         AMK_TRY(launch_pairs(m2l_pair_kernel<double>, static_cast<double*>(out)));
     }
+    // after the per-pair products (run concurrently with them, the near
+    // field took longer than both in sequence)
     if (e1 >= n_m2l && after_products) AMK_TRY(after_products());
     // per-target sums on the side stream, in chunk order
     AMK_CUDA_TRY(cudaEventRecord(f->products_done[buf], c->stream));
@@ -1865,7 +1917,7 @@ fmm_l2l_kernel(const Octree t, FmmDevTables T, int depth, double* __restrict__ L
 
 // ------------------------------------------------------------ L2P + P2P
 // Work items = (target leaf, chunk of <= kP2PChunk source leaves of its P2P
-// list); every leaf has at least one item (its L2P). A warp takes one item;
+// list; kP2P32Chunk in the FP32 near field); every leaf has at least one item (its L2P). A warp takes one item;
 // its lanes are split into G = 32 / n_targets groups, group g summing every
 // G-th source particle for all the leaf's targets, so small leaves still
 // fill the warp. Group sums are added in group order and item partials in
@@ -1873,12 +1925,12 @@ fmm_l2l_kernel(const Octree t, FmmDevTables T, int depth, double* __restrict__ L
 // scheduling.
 constexpr int kP2PChunk = 8;
 
-__global__ void p2p_items_count_kernel(const Octree t, const int* __restrict__ count, int* __restrict__ items,
-                                       int* __restrict__ psize) {
+__global__ void p2p_items_count_kernel(const Octree t, const int* __restrict__ count, int chunk,
+                                       int* __restrict__ items, int* __restrict__ psize) {
   const int id = blockIdx.x * blockDim.x + threadIdx.x;
   if (id >= t.n_nodes) return;
   int it = 0;
-  if (t.meta[id].y) it = max(1, (count[id] + kP2PChunk - 1) / kP2PChunk);
+  if (t.meta[id].y) it = max(1, (count[id] + chunk - 1) / chunk);
   const int2 r = t.range[id];
   items[id] = it;
   psize[id] = it * (r.y - r.x);
@@ -2003,6 +2055,7 @@ __global__ void p2p_stage_kernel(const Octree t, float4* __restrict__ hi, float4
 }
 
 constexpr int kP2PStage = 64;  // source particles staged per warp at a time
+constexpr int kP2P32Chunk = 16;  // source leaves per work item of the FP32 near field
 
 // L2P in FP64 for particle i of leaf ti (centre tc): force and potential of
 // the leaf's local expansion at the particle.
@@ -2038,24 +2091,177 @@ __device__ __forceinline__ double4 l2p_fp64(const Octree& t, const FmmDevTables&
   return make_double4(-gx, -gy, -gz, pot);
 }
 
-// Near-field pair sums of one work item (target leaf, up to kP2PChunk
+// Near-field pair sums of one work item (target leaf, up to kP2P32Chunk
 // source leaves); the FP64 L2P runs in fmm_l2p_add_kernel.
-// Targets: a full block of 64 runs two targets per lane in the halves of
-// packed FP32x2 operations; a remainder of at most 32 runs one target per
-// lane with the warp's lanes split into groups that take every groups-th
-// source. Sources of each leaf come in blocks of kP2PStage staged by the
-// warp in shared memory (broadcast reads). The pair term is branch-free: a
-// pair closer than the minimum distance (the particle itself included)
-// contributes zero, as does a neutral source; t - s is formed as
-// fma(s, -1, t), the rounding of the subtraction, so both paths give the
-// same pair terms bit for bit.
-__global__ void __launch_bounds__(32 * kFmmWarps, 8)  // 8 blocks per SM: latency hiding beats the spills
+// The arithmetic is packed over pairs of SOURCES: a lane holds its target's
+// coordinates duplicated in both halves of FP32x2 registers and each packed
+// operation evaluates the pair terms of two consecutive sources, so every
+// pass is packed whatever the leaf's size. The sources of a leaf are staged
+// by the warp in shared memory 64 at a time as pairs {x_hi, y_hi} {z_hi, q}
+// {x_lo, y_lo} {z_lo} of two sources each (broadcast reads; an odd count is
+// padded with a neutral source). Targets: two per lane while more than 32
+// remain, else one per lane, with the lanes split into groups over the source
+// pairs when 16 or fewer remain. A pair term is
+//   r = (t_hi - s_hi) + (t_lo - s_lo)  (t - s formed as fma(s, -1, t)),
+// exact to FP32 rounding of |r| for neighbouring leaves (Sterbenz), and is
+// zero for a pair closer than the minimum distance (r^2 := +inf, so 1/r = 0;
+// the particle itself included) or a neutral source. Each lane keeps FP32
+// sums of its even and odd sources per source leaf, added to FP64 once per
+// leaf in a fixed order, so results do not depend on scheduling.
+struct P2PPairs {
+  float4 a[kP2PStage / 2];  // {x_hi, x_hi'}, {y_hi, y_hi'}
+  float4 b[kP2PStage / 2];  // {z_hi, z_hi'}, {q, q'}
+  float4 c[kP2PStage / 2];  // {x_lo, x_lo'}, {y_lo, y_lo'}
+  float2 d[kP2PStage / 2];  // {z_lo, z_lo'}
+};
+
+struct P2PTarget {
+  float2 hx, hy, hz, lx, ly, lz;  // duplicated in both halves
+  float2 ox, oy, oz;              // offset from a separated source leaf's centre (duplicated)
+  float2 ax, ay, az, ap;          // even / odd source sums of the current leaf
+  double4 acc;
+};
+
+// A source leaf separated from the target leaf: gap between their spheres
+// (centre, radius) of at least half the summed radii. Its pairs use FP32
+// offsets from the source leaf's centre c: r = (x_i - c) + (-(x_j - c)),
+// each offset formed once from the double-float positions. The relative
+// error of r is then at most 2 eps (1 + r_s / |r|) <= 6 eps, and r > 0
+// (no pair below the minimum distance: the spheres are apart).
+struct P2PCentre {
+  float hx, hy, hz, lx, ly, lz;
+};
+
+__device__ __forceinline__ float2 dup2(float v) { return make_float2(v, v); }
+
+__device__ __forceinline__ void p2p32_far_begin(P2PTarget& t, const P2PCentre& c) {
+  t.ox = dup2((t.hx.x - c.hx) + (t.lx.x - c.lx));
+  t.oy = dup2((t.hy.x - c.hy) + (t.ly.x - c.ly));
+  t.oz = dup2((t.hz.x - c.hz) + (t.lz.x - c.lz));
+}
+
+// Far pair term of two sources: a = {-u_x, -u_x'} {-u_y, -u_y'}, b = {-u_z, -u_z'} {q, q'}.
+__device__ __forceinline__ void p2p32_far_term(P2PTarget& t, const float4& a, const float4& b) {
+  const float2 rx = __fadd2_rn(t.ox, make_float2(a.x, a.y));
+  const float2 ry = __fadd2_rn(t.oy, make_float2(a.z, a.w));
+  const float2 rz = __fadd2_rn(t.oz, make_float2(b.x, b.y));
+  const float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __fmul2_rn(rz, rz)));
+  const float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+  const float2 qr = __fmul2_rn(make_float2(b.z, b.w), inv);
+  const float2 f = __fmul2_rn(qr, __fmul2_rn(inv, inv));
+  t.ax = __ffma2_rn(rx, f, t.ax);
+  t.ay = __ffma2_rn(ry, f, t.ay);
+  t.az = __ffma2_rn(rz, f, t.az);
+  t.ap = __fadd2_rn(t.ap, qr);
+}
+
+__device__ __forceinline__ void p2p32_load_target(P2PTarget& t, const float4* __restrict__ shi,
+                                                  const float4* __restrict__ slo, int i) {
+  const float4 h = shi[i], l = slo[i];
+  t.hx = make_float2(h.x, h.x);
+  t.hy = make_float2(h.y, h.y);
+  t.hz = make_float2(h.z, h.z);
+  t.lx = make_float2(l.x, l.x);
+  t.ly = make_float2(l.y, l.y);
+  t.lz = make_float2(l.z, l.z);
+  t.acc = make_double4(0.0, 0.0, 0.0, 0.0);
+}
+
+__device__ __forceinline__ void p2p32_term(P2PTarget& t, const float4& a, const float4& b, const float4& c,
+                                           const float2& d, float min_sq32) {
+  const float2 m1 = make_float2(-1.f, -1.f);
+  const float inf32 = __int_as_float(0x7f800000);
+  const float2 rx = __fadd2_rn(__ffma2_rn(make_float2(a.x, a.y), m1, t.hx), __ffma2_rn(make_float2(c.x, c.y), m1, t.lx));
+  const float2 ry = __fadd2_rn(__ffma2_rn(make_float2(a.z, a.w), m1, t.hy), __ffma2_rn(make_float2(c.z, c.w), m1, t.ly));
+  const float2 rz = __fadd2_rn(__ffma2_rn(make_float2(b.x, b.y), m1, t.hz), __ffma2_rn(d, m1, t.lz));
+  float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __fmul2_rn(rz, rz)));
+  r2.x = r2.x >= min_sq32 ? r2.x : inf32;
+  r2.y = r2.y >= min_sq32 ? r2.y : inf32;
+  const float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+  const float2 qr = __fmul2_rn(make_float2(b.z, b.w), inv);
+  const float2 f = __fmul2_rn(qr, __fmul2_rn(inv, inv));
+  t.ax = __ffma2_rn(rx, f, t.ax);
+  t.ay = __ffma2_rn(ry, f, t.ay);
+  t.az = __ffma2_rn(rz, f, t.az);
+  t.ap = __fadd2_rn(t.ap, qr);
+}
+
+__device__ __forceinline__ void p2p32_leaf_begin(P2PTarget& t) {
+  t.ax = t.ay = t.az = t.ap = make_float2(0.f, 0.f);
+}
+
+__device__ __forceinline__ void p2p32_leaf_end(P2PTarget& t) {
+  t.acc.x += static_cast<double>(t.ax.x) + static_cast<double>(t.ax.y);
+  t.acc.y += static_cast<double>(t.ay.x) + static_cast<double>(t.ay.y);
+  t.acc.z += static_cast<double>(t.az.x) + static_cast<double>(t.az.y);
+  t.acc.w += static_cast<double>(t.ap.x) + static_cast<double>(t.ap.y);
+}
+
+// Stages sources [s0, s0 + ns) (ns <= kP2PStage) as pairs; returns the pairs.
+__device__ __forceinline__ int p2p32_stage(P2PPairs& sp, const float4* __restrict__ shi,
+                                           const float4* __restrict__ slo, int s0, int ns, int lane) {
+  const int np = (ns + 1) >> 1;
+  __syncwarp();
+  if (lane < np) {
+    const int j0 = s0 + 2 * lane;
+    const bool two = 2 * lane + 1 < ns;
+    const float4 h0 = shi[j0], l0 = slo[j0];
+    float4 h1 = h0, l1 = l0;
+    if (two) {
+      h1 = shi[j0 + 1];
+      l1 = slo[j0 + 1];
+    } else {
+      h1.w = 0.f;  // neutral padding source at the same position: a zero term
+    }
+    sp.a[lane] = make_float4(h0.x, h1.x, h0.y, h1.y);
+    sp.b[lane] = make_float4(h0.z, h1.z, h0.w, h1.w);
+    sp.c[lane] = make_float4(l0.x, l1.x, l0.y, l1.y);
+    sp.d[lane] = make_float2(l0.z, l1.z);
+  }
+  __syncwarp();
+  return np;
+}
+
+// Stages sources [s0, s0 + ns) of a separated leaf as negated FP32 offsets
+// from its centre; returns the pairs (padding: a neutral source).
+__device__ __forceinline__ int p2p32_stage_far(P2PPairs& sp, const float4* __restrict__ shi,
+                                               const float4* __restrict__ slo, int s0, int ns, int lane,
+                                               const P2PCentre& c) {
+  const int np = (ns + 1) >> 1;
+  __syncwarp();
+  if (lane < np) {
+    const int j0 = s0 + 2 * lane;
+    const bool two = 2 * lane + 1 < ns;
+    const float4 h0 = shi[j0], l0 = slo[j0];
+    float4 h1 = h0, l1 = l0;
+    if (two) {
+      h1 = shi[j0 + 1];
+      l1 = slo[j0 + 1];
+    } else {
+      h1.w = 0.f;
+    }
+    auto neg_off = [&](const float4& h, const float4& l, float& x, float& y, float& z) {
+      x = -((h.x - c.hx) + (l.x - c.lx));
+      y = -((h.y - c.hy) + (l.y - c.ly));
+      z = -((h.z - c.hz) + (l.z - c.lz));
+    };
+    float x0, y0, z0, x1, y1, z1;
+    neg_off(h0, l0, x0, y0, z0);
+    neg_off(h1, l1, x1, y1, z1);
+    sp.a[lane] = make_float4(x0, x1, y0, y1);
+    sp.b[lane] = make_float4(z0, z1, h0.w, h1.w);
+  }
+  __syncwarp();
+  return np;
+}
+
+__global__ void __launch_bounds__(32 * kFmmWarps, 6)  // 6 blocks per SM (80 registers): measured best of 4-6
 fmm_p2p32_kernel(const Octree t, const int2* __restrict__ work, int n_work, const int* __restrict__ off,
                  const int* __restrict__ count, const int* __restrict__ src, const int* __restrict__ pbase,
                  double min_sq, const float4* __restrict__ shi, const float4* __restrict__ slo,
-                 double4* __restrict__ part) {
+                 const double* __restrict__ radius, double4* __restrict__ part) {
   __shared__ double4 red[kFmmWarps][32];
-  __shared__ float4 stg_hi[kFmmWarps][kP2PStage], stg_lo[kFmmWarps][kP2PStage];
+  __shared__ P2PPairs stg[kFmmWarps];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const int wi = blockIdx.x * kFmmWarps + w;
   if (wi >= n_work) return;
@@ -2063,115 +2269,109 @@ fmm_p2p32_kernel(const Octree t, const int2* __restrict__ work, int n_work, cons
   const int ti = item.x, chunk = item.y;
   const int2 tr = t.range[ti];
   const int nt_all = tr.y - tr.x;
-  const int sb = off[ti] + chunk * kP2PChunk;
-  const int se = min(off[ti] + count[ti], sb + kP2PChunk);
+  const int sb = off[ti] + chunk * kP2P32Chunk;
+  const int se = min(off[ti] + count[ti], sb + kP2P32Chunk);
   double4* out = part + pbase[ti] + static_cast<size_t>(chunk) * nt_all;
-  // pairs below the minimum distance (the particle itself included: r = 0)
-  // get r^2 = +inf, so 1/r = 0 without a select on the result
   const float min_sq32 = fmaxf(static_cast<float>(min_sq), 1.17549435e-38f);
-  const float inf32 = __int_as_float(0x7f800000);
-  float4* sh = stg_hi[w];
-  float4* sl = stg_lo[w];
-  auto stage = [&](int s0, int ns) {
-    __syncwarp();
-    for (int k = lane; k < ns; k += 32) {
-      sh[k] = shi[s0 + k];
-      sl[k] = slo[s0 + k];
-    }
-    __syncwarp();
+  P2PPairs& sp = stg[w];
+  const double4 ct = t.center[ti];
+  const double rt = radius[ti];
+  // whether source leaf sl is separated (warp-uniform), and its centre
+  auto separated = [&](int sl, P2PCentre& c) {
+    const double4 cs = t.center[sl];
+    const double dx = ct.x - cs.x, dy = ct.y - cs.y, dz = ct.z - cs.z;
+    const double rs = radius[sl];
+    const double gap = sqrt(dx * dx + dy * dy + dz * dz) - rt - rs;
+    c.hx = static_cast<float>(cs.x);
+    c.hy = static_cast<float>(cs.y);
+    c.hz = static_cast<float>(cs.z);
+    c.lx = static_cast<float>(cs.x - c.hx);
+    c.ly = static_cast<float>(cs.y - c.hy);
+    c.lz = static_cast<float>(cs.z - c.hz);
+    return gap >= 0.5 * (rt + rs);
   };
   for (int base = tr.x; base < tr.y;) {
-    if (tr.y - base >= 64) {
-      // ---- a full block of 64 targets: two per lane, packed FP32x2
-      const int i0 = base + lane, i1 = base + 32 + lane;
-      double4 a0 = make_double4(0.0, 0.0, 0.0, 0.0), a1 = a0;
-      const float4 h0 = shi[i0], l0 = slo[i0], h1 = shi[i1], l1 = slo[i1];
-      const float2 thx = make_float2(h0.x, h1.x), thy = make_float2(h0.y, h1.y), thz = make_float2(h0.z, h1.z);
-      const float2 tlx = make_float2(l0.x, l1.x), tly = make_float2(l0.y, l1.y), tlz = make_float2(l0.z, l1.z);
-      const float2 m1 = make_float2(-1.f, -1.f);
+    const int rem = tr.y - base;
+    if (rem > 32) {
+      // ---- two targets per lane (the second may be past the leaf: computed, not written)
+      const int i0 = base + lane, i1 = min(base + 32 + lane, tr.y - 1);
+      P2PTarget t0, t1;
+      p2p32_load_target(t0, shi, slo, i0);
+      p2p32_load_target(t1, shi, slo, i1);
       for (int e = sb; e < se; ++e) {
-        const int2 sr = t.range[src[e]];
-        float2 ax = make_float2(0.f, 0.f), ay = ax, az = ax, ap = ax;
-        for (int s0 = sr.x; s0 < sr.y; s0 += kP2PStage) {
-          const int ns = min(kP2PStage, sr.y - s0);
-          stage(s0, ns);
-#pragma unroll 4
-          for (int j = 0; j < ns; ++j) {
-            const float4 s = sh[j], q = sl[j];
-            const float2 rx = __fadd2_rn(__ffma2_rn(make_float2(s.x, s.x), m1, thx),
-                                         __ffma2_rn(make_float2(q.x, q.x), m1, tlx));
-            const float2 ry = __fadd2_rn(__ffma2_rn(make_float2(s.y, s.y), m1, thy),
-                                         __ffma2_rn(make_float2(q.y, q.y), m1, tly));
-            const float2 rz = __fadd2_rn(__ffma2_rn(make_float2(s.z, s.z), m1, thz),
-                                         __ffma2_rn(make_float2(q.z, q.z), m1, tlz));
-            float2 r2 = __ffma2_rn(rx, rx, __ffma2_rn(ry, ry, __fmul2_rn(rz, rz)));
-            r2.x = r2.x >= min_sq32 ? r2.x : inf32;
-            r2.y = r2.y >= min_sq32 ? r2.y : inf32;
-            const float2 inv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-            const float2 qr = __fmul2_rn(make_float2(s.w, s.w), inv);
-            const float2 f = __fmul2_rn(qr, __fmul2_rn(inv, inv));
-            ax = __ffma2_rn(rx, f, ax);
-            ay = __ffma2_rn(ry, f, ay);
-            az = __ffma2_rn(rz, f, az);
-            ap = __fadd2_rn(ap, qr);
+        const int sl = src[e];
+        const int2 sr = t.range[sl];
+        P2PCentre cc;
+        const bool far = separated(sl, cc);
+        p2p32_leaf_begin(t0);
+        p2p32_leaf_begin(t1);
+        if (far) {
+          p2p32_far_begin(t0, cc);
+          p2p32_far_begin(t1, cc);
+          for (int s0 = sr.x; s0 < sr.y; s0 += kP2PStage) {
+            const int np = p2p32_stage_far(sp, shi, slo, s0, min(kP2PStage, sr.y - s0), lane, cc);
+#pragma unroll 2
+            for (int q = 0; q < np; ++q) {
+              const float4 a = sp.a[q], b = sp.b[q];
+              p2p32_far_term(t0, a, b);
+              p2p32_far_term(t1, a, b);
+            }
+          }
+        } else {
+          for (int s0 = sr.x; s0 < sr.y; s0 += kP2PStage) {
+            const int np = p2p32_stage(sp, shi, slo, s0, min(kP2PStage, sr.y - s0), lane);
+#pragma unroll 2
+            for (int q = 0; q < np; ++q) {
+              const float4 a = sp.a[q], b = sp.b[q], c = sp.c[q];
+              const float2 d = sp.d[q];
+              p2p32_term(t0, a, b, c, d, min_sq32);
+              p2p32_term(t1, a, b, c, d, min_sq32);
+            }
           }
         }
-        a0.x += ax.x;
-        a0.y += ay.x;
-        a0.z += az.x;
-        a0.w += ap.x;
-        a1.x += ax.y;
-        a1.y += ay.y;
-        a1.z += az.y;
-        a1.w += ap.y;
+        p2p32_leaf_end(t0);
+        p2p32_leaf_end(t1);
       }
-      out[i0 - tr.x] = a0;
-      out[i1 - tr.x] = a1;
+      out[i0 - tr.x] = t0.acc;
+      if (base + 32 + lane < tr.y) out[base + 32 + lane - tr.x] = t1.acc;
       base += 64;
       continue;
     }
-    // ---- at most 32 targets: one per lane, lanes in groups over the sources
-    const int nt = min(32, tr.y - base);
+    // ---- at most 32 targets: one per lane, lanes in groups over the source pairs
+    const int nt = rem;
     const int groups = 32 / nt;
     const int g = lane / nt, tl = lane - g * nt;
     const bool active = g < groups;
     const int i = base + tl;
-    double4 acc = make_double4(0.0, 0.0, 0.0, 0.0);
-    float4 mh = make_float4(0.f, 0.f, 0.f, 0.f), ml = mh;
-    if (active) {
-      mh = shi[i];
-      ml = slo[i];
-    }
+    P2PTarget t0;
+    p2p32_load_target(t0, shi, slo, active ? i : base);
     for (int e = sb; e < se; ++e) {
-      const int2 sr = t.range[src[e]];
-      float ax = 0.f, ay = 0.f, az = 0.f, ap = 0.f;
-      for (int s0 = sr.x; s0 < sr.y; s0 += kP2PStage) {
-        const int ns = min(kP2PStage, sr.y - s0);
-        stage(s0, ns);
-        if (active) {
-#pragma unroll 4
-          for (int j = g; j < ns; j += groups) {
-            const float4 s = sh[j], q = sl[j];
-            const float rx = fmaf(s.x, -1.f, mh.x) + fmaf(q.x, -1.f, ml.x);
-            const float ry = fmaf(s.y, -1.f, mh.y) + fmaf(q.y, -1.f, ml.y);
-            const float rz = fmaf(s.z, -1.f, mh.z) + fmaf(q.z, -1.f, ml.z);
-            const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
-            const float inv_r = rsqrtf(r2 >= min_sq32 ? r2 : inf32);
-            const float qr = s.w * inv_r;
-            const float f = qr * (inv_r * inv_r);
-            ax = fmaf(rx, f, ax);
-            ay = fmaf(ry, f, ay);
-            az = fmaf(rz, f, az);
-            ap += qr;
+      const int sl = src[e];
+      const int2 sr = t.range[sl];
+      P2PCentre cc;
+      const bool far = separated(sl, cc);
+      p2p32_leaf_begin(t0);
+      if (far) {
+        p2p32_far_begin(t0, cc);
+        for (int s0 = sr.x; s0 < sr.y; s0 += kP2PStage) {
+          const int np = p2p32_stage_far(sp, shi, slo, s0, min(kP2PStage, sr.y - s0), lane, cc);
+          if (active) {
+#pragma unroll 2
+            for (int q = g; q < np; q += groups) p2p32_far_term(t0, sp.a[q], sp.b[q]);
+          }
+        }
+      } else {
+        for (int s0 = sr.x; s0 < sr.y; s0 += kP2PStage) {
+          const int np = p2p32_stage(sp, shi, slo, s0, min(kP2PStage, sr.y - s0), lane);
+          if (active) {
+#pragma unroll 2
+            for (int q = g; q < np; q += groups) p2p32_term(t0, sp.a[q], sp.b[q], sp.c[q], sp.d[q], min_sq32);
           }
         }
       }
-      acc.x += ax;
-      acc.y += ay;
-      acc.z += az;
-      acc.w += ap;
+      p2p32_leaf_end(t0);
     }
-    red[w][lane] = acc;
+    red[w][lane] = t0.acc;
     __syncwarp();
     if (active && g == 0) {
       double4 a = red[w][tl];
@@ -2242,10 +2442,11 @@ __global__ void fmm_output_kernel(const Octree t, const double4* __restrict__ ef
 }
 
 // sum over P2P leaf pairs of |T| * |S| (particle pairs before self/min_sq skips)
-__global__ void p2p_pair_count_kernel(const Octree t, const int2* __restrict__ pairs, int n,
-                                      unsigned long long* out) {
+__global__ void p2p_pair_count_kernel(const Octree t, const int2* __restrict__ pairs, const int* __restrict__ count,
+                                      long cap, unsigned long long* out) {
+  const long n = min(static_cast<long>(*count), cap);
   unsigned long long s = 0;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  for (long i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     const int2 p = pairs[i];
     const int2 a = t.range[p.x], b = t.range[p.y];
     s += static_cast<unsigned long long>(a.y - a.x) * static_cast<unsigned long long>(b.y - b.x);
@@ -2269,18 +2470,6 @@ __global__ void zero_forces_kernel(View v) {
   v.fy[i] = 0.0;
   v.fz[i] = 0.0;
 }
-
-// Growable int2 list that keeps its contents.
-int grow_keep(amk_ctx* c, DevBuf& b, size_t used_bytes, size_t want_bytes) {
-  if (want_bytes <= b.bytes) return AMK_OK;
-  DevBuf nb;
-  AMK_TRY(nb.reserve(want_bytes));
-  if (used_bytes) AMK_CUDA_TRY(cudaMemcpyAsync(nb.ptr, b.ptr, used_bytes, cudaMemcpyDeviceToDevice, c->stream));
-  AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
-  b.swap(nb);
-  return AMK_OK;
-}
-
 
 int group_pairs(amk_ctx* c, const int2* pairs, long n_pairs, long n_nodes, int slot_off, int slot_cnt, int slot_src,
                 int slot_cursor, Grouped* g) {
@@ -2357,7 +2546,14 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
   const unsigned gn = static_cast<unsigned>((nn + 255) / 256);
   const unsigned gw = static_cast<unsigned>((nn + kFmmWarps - 1) / kFmmWarps);
 
-  // ---- upward pass
+  // ---- upward pass: the radii on the context stream, then P2M / M2M on
+  // their own stream while the traversal (radii only) runs
+  Fmm* f = c->fmm;
+  if (!f->up) {
+    AMK_CUDA_TRY(cudaStreamCreateWithFlags(&f->up, cudaStreamNonBlocking));
+    AMK_CUDA_TRY(cudaEventCreateWithFlags(&f->up_start, cudaEventDisableTiming));
+    AMK_CUDA_TRY(cudaEventCreateWithFlags(&f->up_done, cudaEventDisableTiming));
+  }
   AMK_TRY(phase_begin(c, AMK_PHASE_FMM_UP));
   fmm_leaf_radius_kernel<<<gn, 256, 0, c->stream>>>(t, radius);
   AMK_TRY(check_launch(c, "fmm_leaf_radius_kernel"));
@@ -2365,63 +2561,94 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
     fmm_parent_radius_kernel<<<gn, 256, 0, c->stream>>>(t, d, radius);
     AMK_TRY(check_launch(c, "fmm_parent_radius_kernel"));
   }
-  fmm_p2m_kernel<<<gw, 32 * kFmmWarps, 0, c->stream>>>(t, T, M);
+  AMK_CUDA_TRY(cudaEventRecord(f->up_start, c->stream));
+  AMK_CUDA_TRY(cudaStreamWaitEvent(f->up, f->up_start, 0));
+  fmm_p2m_kernel<<<gw, 32 * kFmmWarps, 0, f->up>>>(t, T, M);
   AMK_TRY(check_launch(c, "fmm_p2m_kernel"));
   for (int d = t.max_depth; d >= 0; --d) {
-    fmm_m2m_kernel<<<gw, 32 * kFmmWarps, 0, c->stream>>>(t, T, d, M);
+    fmm_m2m_kernel<<<gw, 32 * kFmmWarps, 0, f->up>>>(t, T, d, M);
     AMK_TRY(check_launch(c, "fmm_m2m_kernel"));
   }
+  AMK_CUDA_TRY(cudaEventRecord(f->up_done, f->up));
   AMK_TRY(phase_end(c, AMK_PHASE_FMM_UP));
 
-  // ---- interaction lists
+  // ---- interaction lists: every level of the traversal is launched without
+  // reading its size back (a pair's depth sum grows by one per level, so
+  // there are at most 2 max_depth + 1 levels); one read-back at the end
+  // checks the capacities, and a traversal that overflowed one runs again
+  // with larger lists
   AMK_TRY(phase_begin(c, AMK_PHASE_FMM_LISTS));
   FmmLists& lists = c->fmm->lists;
-  int* counters = slot<int>(c, kSlotFmmAux0, 4, &rc);
+  const int n_levels = 2 * t.max_depth + 1;
+  const int n_tv = 8 + n_levels + 1;  // m2l, p2p, overflow, -, -, -, -, -, pairs per level
+  int* tv = slot<int>(c, kSlotFmmAux0, n_tv, &rc);
   AMK_TRY(rc);
-  long n_cur = 1, n_m2l = 0, n_p2p = 0;
-  AMK_TRY(grow_keep(c, lists.cur, 0, 64 * sizeof(int2)));
-  const int2 root = make_int2(0, 0);
-  AMK_CUDA_TRY(cudaMemcpyAsync(lists.cur.ptr, &root, sizeof(int2), cudaMemcpyHostToDevice, c->stream));
+  unsigned long long* cnt64 = slot<unsigned long long>(c, kSlotFmmAux1, 4, &rc);
+  AMK_TRY(rc);
   const double theta2 = theta * theta;
-  for (int level = 0; n_cur > 0; ++level) {
-    if (level > 4 * kTreeLevels + 8) return fail(AMK_ERR_TIMEOUT, "FMM traversal did not terminate");
-    AMK_TRY(grow_keep(c, lists.next, 0, static_cast<size_t>(8 * n_cur + 8) * sizeof(int2)));
-    AMK_TRY(grow_keep(c, lists.m2l, n_m2l * sizeof(int2), static_cast<size_t>(n_m2l + n_cur + 8) * sizeof(int2)));
-    AMK_TRY(grow_keep(c, lists.p2p, n_p2p * sizeof(int2), static_cast<size_t>(n_p2p + n_cur + 8) * sizeof(int2)));
-    const int hc[4] = {static_cast<int>(n_m2l), static_cast<int>(n_p2p), 0, 0};
-    AMK_CUDA_TRY(cudaMemcpyAsync(counters, hc, sizeof(hc), cudaMemcpyHostToDevice, c->stream));
-    fmm_traverse_kernel<<<static_cast<unsigned>((n_cur + 255) / 256), 256, 0, c->stream>>>(
-        t, radius, theta2, lists.cur.as<int2>(), static_cast<int>(n_cur), lists.next.as<int2>(), lists.m2l.as<int2>(),
-        lists.p2p.as<int2>(), counters);
-    AMK_TRY(check_launch(c, "fmm_traverse_kernel"));
-    int out[4];
-    AMK_CUDA_TRY(cudaMemcpyAsync(out, counters, sizeof(out), cudaMemcpyDeviceToHost, c->stream));
+  long n_m2l = 0, n_p2p = 0;
+  std::vector<int> hv(n_tv);
+  unsigned long long h64[2] = {0, 0};
+  TreeFrame hf;
+  long want_front = std::max({lists.need_front, 8 * nn, 1024L});
+  long want_m2l = std::max({lists.need_m2l, 64 * nn, 1024L}), want_p2p = std::max({lists.need_p2p, 16 * nn, 1024L});
+  for (int attempt = 0;; ++attempt) {
+    if (attempt > 12) return fail(AMK_ERR_LIMIT, "FMM traversal: interaction lists did not fit");
+    AMK_TRY(lists.cur.reserve(static_cast<size_t>(want_front) * sizeof(int2)));
+    AMK_TRY(lists.next.reserve(static_cast<size_t>(want_front) * sizeof(int2)));
+    AMK_TRY(lists.m2l.reserve(static_cast<size_t>(want_m2l) * sizeof(int2)));
+    AMK_TRY(lists.p2p.reserve(static_cast<size_t>(want_p2p) * sizeof(int2)));
+    TraverseLists tl;
+    tl.m2l = lists.m2l.as<int2>();
+    tl.p2p = lists.p2p.as<int2>();
+    tl.cap_front = static_cast<long>(std::min(lists.cur.bytes, lists.next.bytes) / sizeof(int2));
+    tl.cap_m2l = static_cast<long>(lists.m2l.bytes / sizeof(int2));
+    tl.cap_p2p = static_cast<long>(lists.p2p.bytes / sizeof(int2));
+    AMK_CUDA_TRY(cudaMemsetAsync(tv, 0, n_tv * sizeof(int), c->stream));
+    fmm_traverse_root_kernel<<<1, 32, 0, c->stream>>>(lists.cur.as<int2>(), tv + 8);
+    AMK_TRY(check_launch(c, "fmm_traverse_root_kernel"));
+    const unsigned grid = static_cast<unsigned>(std::min<long>((tl.cap_front + 255) / 256, 148L * 8));
+    for (int level = 0; level < n_levels; ++level) {
+      int2* a = (level & 1) ? lists.next.as<int2>() : lists.cur.as<int2>();
+      int2* b = (level & 1) ? lists.cur.as<int2>() : lists.next.as<int2>();
+      fmm_traverse_kernel<<<grid, 256, 0, c->stream>>>(t, radius, theta2, a, b, tl, tv + 8 + level, tv);
+      AMK_TRY(check_launch(c, "fmm_traverse_kernel"));
+    }
+    // statistics: leaves and P2P particle pairs (before self / min_sq skips)
+    AMK_CUDA_TRY(cudaMemsetAsync(cnt64, 0, 2 * sizeof(unsigned long long), c->stream));
+    p2p_pair_count_kernel<<<148, 256, 0, c->stream>>>(t, tl.p2p, tv + 1, tl.cap_p2p, cnt64);
+    AMK_TRY(check_launch(c, "p2p_pair_count_kernel"));
+    leaf_count_kernel<<<148, 256, 0, c->stream>>>(t, cnt64 + 1);
+    AMK_TRY(check_launch(c, "leaf_count_kernel"));
+    AMK_CUDA_TRY(cudaMemcpyAsync(hv.data(), tv, n_tv * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaMemcpyAsync(h64, cnt64, sizeof(h64), cudaMemcpyDeviceToHost, c->stream));
+    AMK_CUDA_TRY(cudaMemcpyAsync(&hf, t.frame, sizeof(hf), cudaMemcpyDeviceToHost, c->stream));
     AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    n_m2l = out[0];
-    n_p2p = out[1];
-    n_cur = out[2];
-    lists.cur.swap(lists.next);
+    long max_front = 1;
+    for (int level = 0; level <= n_levels; ++level) max_front = std::max<long>(max_front, hv[8 + level]);
+    if (hv[3] != 0) return fail(AMK_ERR_STATE, "FMM traversal: a list entry is not a pair of nodes");
+    if (hv[2] == 0) {
+      if (hv[8 + n_levels] != 0) return fail(AMK_ERR_STATE, "FMM traversal: pairs left after the deepest level");
+      n_m2l = hv[0];
+      n_p2p = hv[1];
+      lists.need_front = max_front;
+      lists.need_m2l = n_m2l;
+      lists.need_p2p = n_p2p;
+      break;
+    }
+    // counts past a capacity keep growing, so they bound the sizes from below
+    want_front = std::max(2 * tl.cap_front, max_front);
+    want_m2l = hv[0] > tl.cap_m2l ? std::max(2 * tl.cap_m2l, static_cast<long>(hv[0])) : tl.cap_m2l;
+    want_p2p = hv[1] > tl.cap_p2p ? std::max(2 * tl.cap_p2p, static_cast<long>(hv[1])) : tl.cap_p2p;
   }
   {  // statistics: nodes, leaves, M2L pairs, P2P leaf pairs, P2P particle pairs, depth
-    unsigned long long* cnt = slot<unsigned long long>(c, kSlotFmmAux1, 4, &rc);
-    AMK_TRY(rc);
-    AMK_CUDA_TRY(cudaMemsetAsync(cnt, 0, 2 * sizeof(unsigned long long), c->stream));
-    if (n_p2p > 0) {
-      p2p_pair_count_kernel<<<148, 256, 0, c->stream>>>(t, lists.p2p.as<int2>(), static_cast<int>(n_p2p), cnt);
-      AMK_TRY(check_launch(c, "p2p_pair_count_kernel"));
-    }
-    leaf_count_kernel<<<148, 256, 0, c->stream>>>(t, cnt + 1);
-    AMK_TRY(check_launch(c, "leaf_count_kernel"));
-    unsigned long long h[2] = {0, 0};
-    AMK_CUDA_TRY(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
-    AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
     long* st = c->fmm->stats;
     st[0] = nn;
     st[8] = st[9] = st[10] = 0;  // filled by the M2L products
-    st[1] = static_cast<long>(h[1]);
+    st[1] = static_cast<long>(h64[1]);
     st[2] = n_m2l;
     st[3] = n_p2p;
-    st[4] = static_cast<long>(h[0]);
+    st[4] = static_cast<long>(h64[0]);
     st[5] = t.max_depth;
     st[6] = t.m;
     st[7] = order;
@@ -2437,9 +2664,6 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
   // source leaves of its list) and the per-item partial sums' layout
   double4* ef = slot<double4>(c, kSlotFmmWork4, t.m, &rc);
   AMK_TRY(rc);
-  TreeFrame hf;
-  AMK_CUDA_TRY(cudaMemcpyAsync(&hf, t.frame, sizeof(hf), cudaMemcpyDeviceToHost, c->stream));
-  AMK_CUDA_TRY(cudaStreamSynchronize(c->stream));
   const double min_sq = kMinSquaredDistance / (hf.length * hf.length);
   const bool f32 = c->fmm_precision == AMK_FMM_TENSOR;
   AMK_TRY(phase_begin(c, AMK_PHASE_FMM_P2P));
@@ -2453,7 +2677,7 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
   AMK_TRY(rc);
   int* totals = slot<int>(c, kSlotFmmAux1, 8, &rc);
   AMK_TRY(rc);
-  p2p_items_count_kernel<<<gn, 256, 0, c->stream>>>(t, gp.count, items, psize);
+  p2p_items_count_kernel<<<gn, 256, 0, c->stream>>>(t, gp.count, f32 ? kP2P32Chunk : kP2PChunk, items, psize);
   AMK_TRY(check_launch(c, "p2p_items_count_kernel"));
   AMK_TRY(exclusive_scan_int(c, items, nn, ibase, totals));
   AMK_TRY(exclusive_scan_int(c, psize, nn, pbase, totals + 1));
@@ -2475,7 +2699,6 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
   AMK_TRY(check_launch(c, "p2p_items_fill_kernel"));
   AMK_TRY(phase_end(c, AMK_PHASE_FMM_P2P));
   const unsigned gwork = static_cast<unsigned>((ht[0] + kFmmWarps - 1) / kFmmWarps);
-  Fmm* f = c->fmm;
   // FP32 near field: its pair sums need no expansion, so they run on their
   // own stream once the last M2L products are enqueued (the product kernel
   // holds every SM's shared memory), concurrently with the per-target M2L
@@ -2490,9 +2713,11 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
     AMK_CUDA_TRY(cudaStreamWaitEvent(f->near, f->near_start, 0));
     p2p_stage_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, f->near>>>(t, stage, stage + t.m);
     AMK_TRY(check_launch(c, "p2p_stage_kernel"));
+    AMK_TRY(phase_begin_on(c, AMK_PHASE_FMM_NEAR, f->near));
     fmm_p2p32_kernel<<<gwork, 32 * kFmmWarps, 0, f->near>>>(t, work, ht[0], gp.off, gp.count, gp.src, pbase, min_sq,
-                                                            stage, stage + t.m, part);
+                                                            stage, stage + t.m, radius, part);
     AMK_TRY(check_launch(c, "fmm_p2p32_kernel"));
+    AMK_TRY(phase_end_on(c, AMK_PHASE_FMM_NEAR, f->near));
     fmm_p2p_reduce_kernel<<<static_cast<unsigned>((t.m + 255) / 256), 256, 0, f->near>>>(t, leaf_of, items, pbase,
                                                                                        part, ef);
     AMK_TRY(check_launch(c, "fmm_p2p_reduce_kernel"));
@@ -2501,7 +2726,8 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
   };
   const std::function<int()> no_hook;
 
-  // ---- M2L
+  // ---- M2L (the multipoles: join the upward pass)
+  AMK_CUDA_TRY(cudaStreamWaitEvent(c->stream, f->up_done, 0));
   AMK_CUDA_TRY(cudaMemsetAsync(Lx, 0, static_cast<size_t>(nn) * T.n_m * sizeof(double), c->stream));
   AMK_TRY(phase_begin(c, AMK_PHASE_FMM_M2L));
   if (n_m2l > 0) {

@@ -252,6 +252,10 @@ TC_PRODUCT_TRAFFIC_PER_PAIR = {
                "(leaf 128, 3,007,536 pairs: 0.315 GB read + 1.399 GB written = 570 B per pair), scaled by this "
                "launch's class pairs; profiles/m2l_class_tc_kernel_tree262k_leaf128.md"),
 }
+NEAR_TRAFFIC_PER_PAIR = (
+    0.0206, "ncu dram__bytes_read.sum + dram__bytes_write.sum of fmm_p2p32_kernel on 262,144 particles (leaf 128, "
+            "1.40 G particle pairs: 12.5 MB read + 16.4 MB written), scaled by this launch's pairs; "
+            "profiles/fmm_p2p32_kernel_tree262k_leaf128.md")
 FMM_PRODUCT_TRAFFIC = {
     7: (5.18e9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of m2l_class_mma_kernel<7>, mean of two launches "
                 "of 4.47 M pairs each (0.89 / 1.10 GB read + 4.18 GB written: the per-pair products), "
@@ -419,15 +423,34 @@ def tree_roofline(sim, over, n):
             bf16, src = measured_peak("bf16_tflops", 1590.0)
             per_pair = TC_PRODUCT_TRAFFIC_PER_PAIR.get(p_)
             traffic = None if per_pair is None else per_pair[0] * st["m2l_class_pairs"] / max(1, prod_n)
-            return {"bound": "tensor (split BF16)", "kernel": f"m2l_class_tc_kernel<{p_}>", "achieved": achieved,
-                    "peak": bf16 / 6.0, "unit": "TFLOP/s", "frac": achieved / (bf16 / 6.0), "traffic": traffic,
-                    "traffic_source": None if per_pair is None else per_pair[1],
-                    "peak_source": f"dense BF16 tensor peak {src}, divided by the six BF16 products each "
-                                   "split-BF16 product issues",
-                    "flop_convention": f"2 n_m^2 flop (n_m = {nm}) per M2L pair evaluated as a class product "
-                                       f"({st['m2l_class_pairs']:,} of {st['m2l_pairs']:,} pairs)",
-                    "avg_launch_ms": prod_ms / max(1, prod_n), "launches_per_step": prod_n,
-                    "m2l_phase_ms": ph["fmm_m2l"][0], "classes": st["m2l_classes"]}
+            products = {"bound": "tensor (split BF16)", "kernel": f"m2l_class_tc_kernel<{p_}>", "achieved": achieved,
+                        "peak": bf16 / 6.0, "unit": "TFLOP/s", "frac": achieved / (bf16 / 6.0), "traffic": traffic,
+                        "traffic_source": None if per_pair is None else per_pair[1],
+                        "peak_source": f"dense BF16 tensor peak {src}, divided by the six BF16 products each "
+                                       "split-BF16 product issues",
+                        "flop_convention": f"2 n_m^2 flop (n_m = {nm}) per M2L pair evaluated as a class product "
+                                           f"({st['m2l_class_pairs']:,} of {st['m2l_pairs']:,} pairs)",
+                        "avg_launch_ms": prod_ms / max(1, prod_n), "launches_per_step": prod_n,
+                        "m2l_phase_ms": ph["fmm_m2l"][0], "classes": st["m2l_classes"]}
+            near_ms, near_n = ph.get("fmm_near", (0.0, 0))
+            if not near_n:
+                return products
+            pairs = st["p2p_particle_pairs"]
+            near_avg = near_ms / near_n
+            peak32 = sim.measure_fp32_peak()
+            ach32 = 20.0 * pairs / (near_avg * 1e-3) / 1e12
+            near = {"bound": "fp32", "kernel": "fmm_p2p32_kernel", "achieved": ach32, "peak": peak32,
+                    "unit": "TFLOP/s", "frac": ach32 / peak32,
+                    "traffic": NEAR_TRAFFIC_PER_PAIR[0] * pairs, "traffic_source": NEAR_TRAFFIC_PER_PAIR[1],
+                    "peak_source": "measured in this run: FFMA probe kernel over all SMs (2 flop/FFMA)",
+                    "flop_convention": f"20 flop per particle pair of the P2P leaf pairs ({pairs:,} pairs, the "
+                                       "particle itself included), as for the all-pairs kernel",
+                    "avg_launch_ms": near_avg, "launches_per_step": near_n,
+                    "timing": "CUDA events on the near-field stream, which it shares with nothing; the kernel "
+                              "runs concurrently with the per-pair M2L products, the per-target M2L sums and L2L"}
+            dominant, other = (near, products) if near_avg >= products["avg_launch_ms"] else (products, near)
+            dominant["other_kernel"] = other
+            return dominant
         peak = sim.measure_fp64_peak()
         traffic = FMM_PRODUCT_TRAFFIC.get(p_)
         return {"bound": "fp64 tensor", "kernel": f"m2l_class_mma_kernel<{p_}>", "achieved": achieved,
@@ -559,7 +582,9 @@ def run_tree(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "fp32" if over["coulomb_method"] == "allpairs" else "f64",
+                "dtype": ("fp32" if over["coulomb_method"] == "allpairs" else
+                          "bf16x3 M2L products, f32 near field, f64 expansions and push"
+                          if over.get("precision") == "tensor" else "f64"),
                 "data": "synthetic (seeded Gaussian cloud, numpy default_rng(42))",
                 "config": tree_config(n, world), "chosen": name, "methods": results,
                 "learned_vs_plain_p6": learned_vs_p6, "sweep_batched_vs_one_at_a_time": sweep,

@@ -525,7 +525,8 @@ int amk_coulomb_standard_noalloc(const double* x, const double* y, const double*
 #define AMK_PHASE_ANNIHILATION 13
 #define AMK_PHASE_ENERGY 14
 #define AMK_PHASE_FMM_M2L_PRODUCTS 15 /* the class-product kernels inside FMM_M2L */
-#define AMK_NUM_PHASES 16
+#define AMK_PHASE_FMM_NEAR 16         /* FP32 near-field pair kernel (tensor mode, its own stream) */
+#define AMK_NUM_PHASES 17
 int amk_set_profiling(amk_ctx* ctx, int enabled);
 int amk_phase_times(amk_ctx* ctx, double* ms_out, long* launches_out, int n);
 int amk_reset_phase_times(amk_ctx* ctx);
