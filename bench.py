@@ -253,9 +253,9 @@ TC_PRODUCT_TRAFFIC_PER_PAIR = {
                "launch's class pairs; profiles/m2l_class_tc_kernel_tree262k_leaf128.md"),
 }
 NEAR_TRAFFIC_PER_PAIR = (
-    0.0206, "ncu dram__bytes_read.sum + dram__bytes_write.sum of fmm_p2p32_kernel on 262,144 particles (leaf 128, "
-            "1.40 G particle pairs: 12.5 MB read + 16.4 MB written), scaled by this launch's pairs; "
-            "profiles/fmm_p2p32_kernel_tree262k_leaf128.md")
+    0.0300, "ncu dram__bytes_read.sum + dram__bytes_write.sum of fmm_p2p32_kernel on 262,144 particles (leaf 128, "
+            "1.374 G particle pairs: 12.9 MB read + 28.4 MB written = 0.030 B per pair), scaled by this launch's "
+            "pairs; profiles/fmm_p2p32_kernel_tree262k_leaf128.md")
 FMM_PRODUCT_TRAFFIC = {
     7: (5.18e9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of m2l_class_mma_kernel<7>, mean of two launches "
                 "of 4.47 M pairs each (0.89 / 1.10 GB read + 4.18 GB written: the per-pair products), "
