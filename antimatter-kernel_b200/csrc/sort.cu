@@ -1,8 +1,10 @@
 // Stable LSD radix sort of (uint64 key, uint32 value) pairs, 8 bits per
 // pass: per-tile digit histograms -> one exclusive scan (digit-major, so the
 // result is stable across tiles) -> scatter with in-tile stable ranks from
-// warp match masks. HBM-bound: each pass reads 12 B and writes 12 B per
-// element plus the key read of the histogram pass.
+// warp match masks (the context's sort stages each tile in digit order in
+// shared memory first, so that a digit's writes are contiguous). HBM-bound:
+// each pass reads 12 B and writes 12 B per element plus the key read of the
+// histogram pass.
 #include <algorithm>
 
 #include "amk_internal.cuh"
@@ -108,6 +110,105 @@ scatter_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vi
   }
 }
 
+// The same scatter with the tile staged in shared memory in digit order, so
+// that the global writes of one digit are contiguous. Warp w ranks the
+// contiguous chunk [w * kWarpChunk, (w + 1) * kWarpChunk) of the tile with
+// counters of its own (match masks per round, no block barrier), which keeps
+// the ranks stable; one block pass then turns the per-warp digit counts into
+// tile positions, the elements are placed in shared memory in sorted order
+// and written out in that order. Element j of the staged tile goes to
+// offs[d][tile] + j - (tile start of digit d).
+constexpr int kWarpChunk = kTile / kWarps;  // 512 consecutive elements per warp
+constexpr size_t kStagedSmem = static_cast<size_t>(kTile) * (sizeof(uint64_t) + sizeof(uint32_t)) +
+                               sizeof(uint32_t) * (kWarps * 256 + 256 + kWarps);
+
+__global__ void __launch_bounds__(kSortThreads)
+scatter_staged_kernel(const uint64_t* __restrict__ kin, const uint32_t* __restrict__ vin, long n, int shift,
+                      int nb, const uint32_t* __restrict__ offs, uint64_t* __restrict__ kout,
+                      uint32_t* __restrict__ vout) {
+  extern __shared__ __align__(16) unsigned char sort_smem[];
+  uint64_t* sk = reinterpret_cast<uint64_t*>(sort_smem);
+  uint32_t* sv = reinterpret_cast<uint32_t*>(sk + kTile);
+  uint32_t* wc = sv + kTile;                 // [kWarps][256]: counts, then tile positions
+  uint32_t* dstart = wc + kWarps * 256;      // [256]
+  uint32_t* wsum = dstart + 256;             // [kWarps]
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const long base = static_cast<long>(blockIdx.x) * kTile;
+  const long wbase = base + static_cast<long>(warp) * kWarpChunk;
+  const uint32_t lt_mask = (1u << lane) - 1u;
+  uint32_t* mine = wc + warp * 256;
+  for (int d = lane; d < 256; d += 32) mine[d] = 0;
+  __syncwarp();
+  uint64_t key[kItems];
+  uint32_t val[kItems], dr[kItems];  // dr: digit | rank in the warp's chunk << 8
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    const long i = wbase + k * 32 + lane;
+    const bool valid = i < n;
+    key[k] = 0;
+    val[k] = 0;
+    dr[k] = 0;
+    const uint32_t active = __ballot_sync(0xffffffffu, valid);
+    if (valid) {
+      key[k] = kin[i];
+      val[k] = vin[i];
+      const int d = static_cast<int>((key[k] >> shift) & 0xFF);
+      const uint32_t peers = __match_any_sync(active, d);
+      const int leader = __ffs(peers) - 1;
+      uint32_t old = lane == leader ? mine[d] : 0u;
+      old = __shfl_sync(active, old, leader);
+      if (lane == leader) mine[d] = old + __popc(peers);
+      dr[k] = static_cast<uint32_t>(d) | ((old + __popc(peers & lt_mask)) << 8);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  // digit d (thread d): the per-warp starts within the digit and the digit's total
+  {
+    const int d = threadIdx.x;
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t c = wc[w * 256 + d];
+      wc[w * 256 + d] = run;
+      run += c;
+    }
+    uint32_t incl = run;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0;
+    for (int w = 0; w < warp; ++w) before += wsum[w];
+    const uint32_t start = before + incl - run;
+    dstart[d] = start;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) wc[w * 256 + d] += start;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < kItems; ++k) {
+    const long i = wbase + k * 32 + lane;
+    if (i < n) {
+      const uint32_t pos = mine[dr[k] & 0xFF] + (dr[k] >> 8);
+      sk[pos] = key[k];
+      sv[pos] = val[k];
+    }
+  }
+  __syncthreads();
+  const int tile_n = static_cast<int>(min(static_cast<long>(kTile), n - base));
+  for (int j = threadIdx.x; j < tile_n; j += kSortThreads) {
+    const uint64_t kk = sk[j];
+    const int d = static_cast<int>((kk >> shift) & 0xFF);
+    const long pos = static_cast<long>(offs[static_cast<long>(d) * nb + blockIdx.x]) + (j - dstart[d]);
+    kout[pos] = kk;
+    vout[pos] = sv[j];
+  }
+}
+
 }  // namespace
 
 int radix_sort_pairs(amk_ctx* c, const uint64_t* keys_in, const uint32_t* vals_in, uint64_t* keys_out,
@@ -125,6 +226,9 @@ int radix_sort_pairs(amk_ctx* c, const uint64_t* keys_in, const uint32_t* vals_i
   AMK_TRY(rc);
   int* total = slot<int>(c, kSlotSortFlags, 8, &rc);
   AMK_TRY(rc);
+  // the staged scatter's shared memory is above the 48 KB default (set per call: per device)
+  AMK_CUDA_TRY(cudaFuncSetAttribute(scatter_staged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    static_cast<int>(kStagedSmem)));
   const uint64_t* ksrc = keys_in;
   const uint32_t* vsrc = vals_in;
   for (int p = 0; p < passes; ++p) {
@@ -142,8 +246,8 @@ int radix_sort_pairs(amk_ctx* c, const uint64_t* keys_in, const uint32_t* vals_i
       scan_kernel<<<1, 1024, 0, c->stream>>>(hist, static_cast<long>(256) * nb);
       AMK_TRY(check_launch(c, "scan_kernel"));
     }
-    scatter_kernel<<<nb, kSortThreads, 0, c->stream>>>(ksrc, vsrc, n, shift, nb, hist, kdst, vdst);
-    AMK_TRY(check_launch(c, "scatter_kernel"));
+    scatter_staged_kernel<<<nb, kSortThreads, kStagedSmem, c->stream>>>(ksrc, vsrc, n, shift, nb, hist, kdst, vdst);
+    AMK_TRY(check_launch(c, "scatter_staged_kernel"));
     ksrc = kdst;
     vsrc = vdst;
   }
