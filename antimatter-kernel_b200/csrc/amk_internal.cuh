@@ -207,6 +207,7 @@ enum ScratchSlot {
   kSlotM2lUnitDesc,
   kSlotM2lPairSrc,
   kSlotM2lTable3,
+  kSlotM2lRefl,
   kNumSlots
 };
 static_assert(kNumSlots <= 96, "scratch slots");

@@ -624,7 +624,8 @@ __device__ __forceinline__ int m2l_key_v(unsigned long long k, int axis) {
 // a few dozen ulp of max|c| / u; the acceptance tolerance tracks that bound
 // (256 ulp), and a pair further off the lattice takes the per-pair path,
 // where D is built from the actual centres as in the reference.
-__device__ __forceinline__ unsigned long long m2l_class_key(const Octree& t, int ti, int si, int reach) {
+__device__ __forceinline__ unsigned long long m2l_class_key(const Octree& t, int ti, int si, int reach, bool fold,
+                                                            int* refl) {
   const double4 tc = t.center[ti], sc = t.center[si];
   const int dd = static_cast<int>(t.meta[ti].x) - static_cast<int>(t.meta[si].x);
   const double u = fmin(tc.w, sc.w);
@@ -635,7 +636,14 @@ __device__ __forceinline__ unsigned long long m2l_class_key(const Octree& t, int
   const double tol = 256.0 * 2.220446049250313e-16 * (cmax / u + fabs(rx) + fabs(ry) + fabs(rz) + 1.0);
   if (fabs(vx - rx) > tol || fabs(vy - ry) > tol || fabs(vz - rz) > tol) return kM2lEmpty;
   if (fabs(rx) > reach || fabs(ry) > reach || fabs(rz) > reach) return kM2lEmpty;
-  return m2l_key(dd, static_cast<int>(rx), static_cast<int>(ry), static_cast<int>(rz));
+  int ix = static_cast<int>(rx), iy = static_cast<int>(ry), iz = static_cast<int>(rz), r = 0;
+  if (fold) {  // the class of |v|; the reflection that maps |v| to v in bits x, y, z
+    if (ix < 0) ix = -ix, r |= 1;
+    if (iy < 0) iy = -iy, r |= 2;
+    if (iz < 0) iz = -iz, r |= 4;
+  }
+  *refl = r;
+  return m2l_key(dd, ix, iy, iz);
 }
 
 // Slot of a key in the class hash (inserted if absent), -1 if no slot
@@ -670,21 +678,57 @@ __global__ void m2l_rescale_kernel(const Octree t, FmmDevTables T, const double*
   Mh[e] = M[e] * f;
 }
 
-// Class slot (-1: per-pair path) and target of every pair (a warp per target).
+// Class slot (-1: per-pair path) and target of every pair (a warp per target);
+// refl (tensor-core mode) is cleared: every pair starts unreflected.
 __global__ void m2l_classify_kernel(const Octree t, const int* __restrict__ off, const int* __restrict__ count,
                                     const int* __restrict__ src, int reach, unsigned long long* __restrict__ keys,
-                                    int* __restrict__ codes, int* __restrict__ tgt) {
+                                    int* __restrict__ codes, int* __restrict__ tgt,
+                                    unsigned char* __restrict__ refl) {
   const int lane = threadIdx.x & 31;
   const long w0 = (blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x) >> 5;
   const long nw = (static_cast<long>(gridDim.x) * blockDim.x) >> 5;
   for (long ti = w0; ti < t.n_nodes; ti += nw) {
     const int b = off[ti], n = count[ti];
     for (int e = b + lane; e < b + n; e += 32) {
-      const unsigned long long key = m2l_class_key(t, static_cast<int>(ti), src[e], reach);
+      int r = 0;
+      const unsigned long long key = m2l_class_key(t, static_cast<int>(ti), src[e], reach, false, &r);
       codes[e] = key == kM2lEmpty ? -1 : m2l_hash_slot(keys, key);
       tgt[e] = static_cast<int>(ti);
+      if (refl) refl[e] = 0;
     }
   }
+}
+
+// Tensor-core mode: a pair of a class smaller than min_class (over all
+// pairs) is moved to the class of |v| with its reflection in refl[e] (bit i:
+// v_i < 0). D is even in each coordinate, D_k(R w) = s^k D_k(w) with
+// s^k = prod_i s_i^k_i, so the class matrix of v is S_g A(|v|) S_a: the
+// source expansion is read with the signs s^a (a sign-flipped copy of its
+// split rows) and the product's row g gets s^g (m2l_refl_sign_kernel).
+// Folding the 8 reflections merges most of the small classes into classes
+// large enough for a class product (or into the class of |v| itself when
+// that one exists), while the pairs of large classes keep their own.
+__global__ void m2l_refold_kernel(const Octree t, const int* __restrict__ hist, int min_class,
+                                  const int* __restrict__ tgt, const int* __restrict__ src, int reach, long n,
+                                  unsigned long long* __restrict__ keys, int* __restrict__ codes,
+                                  unsigned char* __restrict__ refl) {
+  const long e = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (e >= n) return;
+  const int code = codes[e];
+  if (code < 0 || hist[code] >= min_class) return;
+  int r = 0;
+  const unsigned long long key = m2l_class_key(t, tgt[e], src[e], reach, true, &r);
+  if (key == kM2lEmpty || r == 0) return;
+  const int folded = m2l_hash_slot(keys, key);
+  if (folded < 0) return;  // no slot: the pair stays in its own (small) class
+  codes[e] = folded;
+  refl[e] = static_cast<unsigned char>(r);
+}
+
+// Pairs per class code over all pairs (tensor-core mode, before folding).
+__global__ void m2l_code_count_kernel(const int* __restrict__ codes, long n, int* __restrict__ hist) {
+  const long e = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  if (e < n && codes[e] >= 0) atomicAdd(hist + codes[e], 1);
 }
 
 // Pairs per class code in [e0, e1); off-lattice pairs listed for the per-pair path.
@@ -739,15 +783,18 @@ __global__ void m2l_class_fill_kernel(const int* __restrict__ hist, const int* _
 // per-pair list. Consumes hist.
 __global__ void m2l_scatter_kernel(const int* __restrict__ codes, long e0, long e1, const int* __restrict__ start,
                                    const int* __restrict__ used, int* __restrict__ hist, int* __restrict__ perm,
-                                   int* __restrict__ fallback, int* __restrict__ n_fallback) {
+                                   int* __restrict__ fallback, int* __restrict__ n_fallback,
+                                   unsigned char* __restrict__ refl) {
   const long e = e0 + blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
   if (e >= e1) return;
   const int code = codes[e];
   if (code < 0) return;
-  if (used[code])
+  if (used[code]) {
     perm[start[code] + atomicSub(hist + code, 1) - 1] = static_cast<int>(e);
-  else
+  } else {
     fallback[atomicAdd(n_fallback, 1)] = static_cast<int>(e);
+    if (refl) refl[e] = 0;  // the per-pair path works from the actual centres
+  }
 }
 
 // D recurrence (fast-multipole.cc:207-232) for displacement xs into D[0, n_d), one warp.
@@ -1085,16 +1132,24 @@ __device__ __forceinline__ void split3_bf16(double v, __nv_bfloat16* t) {
 
 // Mh3[(cell * 3 + q) * kp + a] = term q of the split of Mh[cell][a] (zero for
 // a >= n_m): a cell's three rows are 3 * kp contiguous BF16 values.
-__global__ void m2l_split_kernel(long n_cells, int nm, int kp, const double* __restrict__ Mh,
-                                 __nv_bfloat16* __restrict__ Mh3) {
+// With copies = 8 (reflection-folded classes), copy R holds the rows with the
+// signs s^a of reflection R: Mh3[((R * n_cells + cell) * 3 + q) * kp + a]
+// (a sign flip of a BF16 term is exact).
+__global__ void m2l_split_kernel(long n_cells, int nm, int kp, const int4* __restrict__ multi, int copies,
+                                 const double* __restrict__ Mh, __nv_bfloat16* __restrict__ Mh3) {
   const long e = blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
   if (e >= n_cells * kp) return;
   const long cell = e / kp;
   const int a = static_cast<int>(e - cell * kp);
   __nv_bfloat16 t[3];
   split3_bf16(a < nm ? Mh[cell * nm + a] : 0.0, t);
+  const int4 ma = a < nm ? multi[a] : make_int4(0, 0, 0, 0);
+  for (int R = 0; R < copies; ++R) {
+    const int odd = ((R & 1) ? ma.x : 0) + ((R & 2) ? ma.y : 0) + ((R & 4) ? ma.z : 0);
+    const size_t row = (static_cast<size_t>(R) * n_cells + cell) * 3;
 #pragma unroll
-  for (int q = 0; q < 3; ++q) Mh3[(cell * 3 + q) * kp + a] = t[q];
+    for (int q = 0; q < 3; ++q) Mh3[(row + q) * kp + a] = (odd & 1) ? __hneg(t[q]) : t[q];
+  }
 }
 
 // Unit descriptors {class, first pair, pairs, depth difference} and the
@@ -1103,13 +1158,17 @@ __global__ void m2l_tc_prep_kernel(int n_units, const int* __restrict__ unit_cls
                                    const int* __restrict__ cls_code, const int* __restrict__ cls_end,
                                    const unsigned long long* __restrict__ keys, int n_pairs,
                                    const int* __restrict__ perm, const int* __restrict__ src,
-                                   int4* __restrict__ ud, int* __restrict__ psrc) {
+                                   const unsigned char* __restrict__ refl, int n_cells, int4* __restrict__ ud,
+                                   int* __restrict__ psrc) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x;
   if (x < n_units) {
     const int cls = unit_cls[x], pos0 = unit_pos[x];
     ud[x] = make_int4(cls, pos0, min(kM2lUnitPairs, cls_end[cls] - pos0), m2l_key_dd(keys[cls_code[cls]]));
   }
-  if (x < n_pairs) psrc[x] = src[perm[x]];
+  if (x < n_pairs) {  // the source's row in the split expansions (its reflected copy when folded)
+    const int e = perm[x];
+    psrc[x] = (refl ? static_cast<int>(refl[e]) * n_cells : 0) + src[e];
+  }
 }
 
 __device__ __forceinline__ void cp_async16(void* dst, const void* src, bool valid) {
@@ -1530,6 +1589,43 @@ m2l_reduce_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, c
 // of 4): lane l holds coefficients 4l..4l+3 and reads them as one 16-byte
 // vector, eight pairs' rows in flight per warp. The sum per coefficient is
 // the FP64 sum in pair order, as in m2l_reduce_kernel.
+// Reflection-folded class pairs (tensor-core mode): the product row of a
+// pair with reflection R gets s^g on coefficient g, in place (refl = 0 for
+// every other pair, the per-pair path's included). A warp takes 32 pairs and
+// rewrites the rows of those with R != 0 together, lane l holding
+// coefficients 4l..4l+3 (n_m a multiple of 4, at most 128).
+__global__ void __launch_bounds__(256)
+m2l_refl_sign_kernel(FmmDevTables T, long e0, long e1, const unsigned char* __restrict__ refl,
+                     float* __restrict__ out) {
+  const int lane = threadIdx.x & 31, nv = T.n_m >> 2;
+  const long e = e0 + blockIdx.x * static_cast<long>(blockDim.x) + threadIdx.x;
+  const uint32_t r = e < e1 ? refl[e] : 0u;
+  uint32_t todo = __ballot_sync(0xffffffffu, r != 0);
+  if (todo == 0) return;
+  uint32_t neg[4] = {0u, 0u, 0u, 0u};  // bit R: s^g = -1 under reflection R, for g = 4 lane + c
+  if (lane < nv)
+    for (int c = 0; c < 4; ++c) {
+      const int4 mg = T.multi[4 * lane + c];
+      for (int R = 1; R < 8; ++R)
+        if ((((R & 1) ? mg.x : 0) + ((R & 2) ? mg.y : 0) + ((R & 4) ? mg.z : 0)) & 1) neg[c] |= 1u << R;
+    }
+  const long warp_e = e - lane;
+  while (todo) {
+    const int src_lane = __ffs(todo) - 1;
+    todo &= todo - 1;
+    const uint32_t rr = __shfl_sync(0xffffffffu, r, src_lane);
+    if (lane < nv) {
+      float4* row = reinterpret_cast<float4*>(out + static_cast<size_t>(warp_e + src_lane - e0) * T.n_m) + lane;
+      float4 v = *row;
+      if ((neg[0] >> rr) & 1u) v.x = -v.x;
+      if ((neg[1] >> rr) & 1u) v.y = -v.y;
+      if ((neg[2] >> rr) & 1u) v.z = -v.z;
+      if ((neg[3] >> rr) & 1u) v.w = -v.w;
+      *row = v;
+    }
+  }
+}
+
 __global__ void __launch_bounds__(256)
 m2l_reduce_f4_kernel(const Octree t, FmmDevTables T, const int* __restrict__ off, const int* __restrict__ count,
                      int t_first, int n_targets, long e0, long e1, const float* __restrict__ out,
@@ -1721,11 +1817,26 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
   const long total = nn * T.n_m;
   m2l_rescale_kernel<<<static_cast<unsigned>((total + 255) / 256), 256, 0, c->stream>>>(t, T, M, Mh);
   AMK_TRY(check_launch(c, "m2l_rescale_kernel"));
-  AMK_CUDA_TRY(cudaMemsetAsync(keys, 0xff, kM2lHashSlots * sizeof(unsigned long long), c->stream));
-  m2l_classify_kernel<<<4 * 148, 256, 0, c->stream>>>(t, gm.off, gm.count, gm.src, reach, keys, codes, tgt);
-  AMK_TRY(check_launch(c, "m2l_classify_kernel"));
-  // the tensor-core products (split BF16) write FP32 per-pair products
+  // the tensor-core products (split BF16) write FP32 per-pair products and
+  // take classes folded over the 8 reflections
   const bool tc = c->fmm_precision == AMK_FMM_TENSOR && tc_order(order);
+  unsigned char* refl = nullptr;
+  if (tc) {
+    refl = slot<unsigned char>(c, kSlotM2lRefl, n_m2l, &rc);
+    AMK_TRY(rc);
+  }
+  AMK_CUDA_TRY(cudaMemsetAsync(keys, 0xff, kM2lHashSlots * sizeof(unsigned long long), c->stream));
+  m2l_classify_kernel<<<4 * 148, 256, 0, c->stream>>>(t, gm.off, gm.count, gm.src, reach, keys, codes, tgt, refl);
+  AMK_TRY(check_launch(c, "m2l_classify_kernel"));
+  if (tc) {  // class sizes over all pairs, then the small classes folded by reflection
+    AMK_CUDA_TRY(cudaMemsetAsync(hist, 0, n_codes * sizeof(int), c->stream));
+    const unsigned ga = static_cast<unsigned>((n_m2l + 255) / 256);
+    m2l_code_count_kernel<<<ga, 256, 0, c->stream>>>(codes, n_m2l, hist);
+    AMK_TRY(check_launch(c, "m2l_code_count_kernel"));
+    m2l_refold_kernel<<<ga, 256, 0, c->stream>>>(t, hist, kM2lMinClass, tgt, gm.src, reach, n_m2l, keys, codes,
+                                                  refl);
+    AMK_TRY(check_launch(c, "m2l_refold_kernel"));
+  }
   const size_t esz = tc ? sizeof(float) : sizeof(double);
   long cap = std::max<long>(1L << 20, static_cast<long>((tc ? kM2lTcChunkBytes : kM2lChunkBytes) / (esz * T.n_m)));
   if (const char* env = getenv("AMK_FMM_M2L_CHUNK_PAIRS")) {  // smaller chunks (tests of the chunk seams)
@@ -1758,9 +1869,10 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
   if (tc) {
     AMK_CUDA_TRY(cudaMemsetAsync(tc_status, 0, sizeof(int), c->stream));
     const int kp = 32 * ((T.n_m + 31) / 32);  // M2lTc<P>::kKp
-    Mh3 = slot<__nv_bfloat16>(c, kSlotM2lSplit, static_cast<size_t>(nn) * 3 * kp, &rc);
+    Mh3 = slot<__nv_bfloat16>(c, kSlotM2lSplit, static_cast<size_t>(8) * nn * 3 * kp, &rc);  // 8 signed copies
     AMK_TRY(rc);
-    m2l_split_kernel<<<static_cast<unsigned>((nn * kp + 255) / 256), 256, 0, c->stream>>>(nn, T.n_m, kp, Mh, Mh3);
+    m2l_split_kernel<<<static_cast<unsigned>((nn * kp + 255) / 256), 256, 0, c->stream>>>(nn, T.n_m, kp, T.multi, 8,
+                                                                                        Mh, Mh3);
     AMK_TRY(check_launch(c, "m2l_split_kernel"));
   }
   const int n_buf = n_m2l > cap ? 2 : 1;
@@ -1784,7 +1896,8 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
     m2l_class_fill_kernel<<<gc, 256, 0, c->stream>>>(hist, start, cls_index, unit_start, n_codes, used, cls_code,
                                                      cls_end, unit_cls, unit_pos);
     AMK_TRY(check_launch(c, "m2l_class_fill_kernel"));
-    m2l_scatter_kernel<<<ge, 256, 0, c->stream>>>(codes, e0, e1, start, used, hist, perm, fallback, counters + 3);
+    m2l_scatter_kernel<<<ge, 256, 0, c->stream>>>(codes, e0, e1, start, used, hist, perm, fallback, counters + 3,
+                                                  refl);
     AMK_TRY(check_launch(c, "m2l_scatter_kernel"));
     int h[4] = {0, 0, 0, 0}, tr[2] = {0, 0};
     AMK_CUDA_TRY(cudaMemcpyAsync(h, counters, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
@@ -1827,7 +1940,8 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
         AMK_TRY(rc);
         const long np_ = std::max<long>(n_units, n_cp);
         m2l_tc_prep_kernel<<<static_cast<unsigned>((np_ + 255) / 256), 256, 0, c->stream>>>(
-            n_units, unit_cls, unit_pos, cls_code, cls_end, keys, static_cast<int>(n_cp), perm, gm.src, ud, psrc);
+            n_units, unit_cls, unit_pos, cls_code, cls_end, keys, static_cast<int>(n_cp), perm, gm.src, refl,
+            static_cast<int>(nn), ud, psrc);
         AMK_TRY(check_launch(c, "m2l_tc_prep_kernel"));
       }
       AMK_TRY(phase_begin(c, AMK_PHASE_FMM_M2L_PRODUCTS));
@@ -1838,6 +1952,11 @@ int m2l_products(amk_ctx* c, int order, const Octree& t, const FmmDevTables& T, 
         AMK_TRY(class_product(c, order, T, n_units, counters + 4, unit_cls, unit_pos, cls_code, cls_end, perm,
                               gm.src, Mh, table, keys, e0, static_cast<double*>(out)));
       AMK_TRY(phase_end(c, AMK_PHASE_FMM_M2L_PRODUCTS));
+      if (tc) {  // the signs s^g of the reflection-folded pairs
+        m2l_refl_sign_kernel<<<static_cast<unsigned>((ne + 255) / 256), 256, 0, c->stream>>>(
+            T, e0, e1, refl, static_cast<float*>(out));
+        AMK_TRY(check_launch(c, "m2l_refl_sign_kernel"));
+      }
     }
     if (n_fb > 0) {
       const size_t psm = static_cast<size_t>(kFmmWarps) * (T.n_d + T.n_m) * sizeof(double) +
