@@ -248,9 +248,9 @@ LEARNED = "learned p=2 + MLP theta=0.5"
 # per-pair products written, the split expansions read past L2), from one
 # ncu launch at 262,144 particles scaled by the pairs of a launch here.
 TC_PRODUCT_TRAFFIC_PER_PAIR = {
-    7: (570.0, "ncu dram__bytes_read.sum + dram__bytes_write.sum of m2l_class_tc_kernel<7> on 262,144 particles "
-               "(leaf 128, 3,007,536 pairs: 0.315 GB read + 1.399 GB written = 570 B per pair), scaled by this "
-               "launch's class pairs; profiles/m2l_class_tc_kernel_tree262k_leaf128.md"),
+    7: (519.0, "ncu dram__bytes_read.sum + dram__bytes_write.sum of m2l_class_tc_kernel<7> on 262,144 particles "
+               "(leaf 128, 2,973,968 class pairs: 0.152 GB read + 1.393 GB written = 519 B per pair), scaled by "
+               "this launch's class pairs; profiles/m2l_class_tc_kernel_tree262k_leaf128.md"),
 }
 NEAR_TRAFFIC_PER_PAIR = (
     0.0300, "ncu dram__bytes_read.sum + dram__bytes_write.sum of fmm_p2p32_kernel on 262,144 particles (leaf 128, "
