@@ -2711,6 +2711,16 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
   TreeFrame hf;
   long want_front = std::max({lists.need_front, 8 * nn, 1024L});
   long want_m2l = std::max({lists.need_m2l, 64 * nn, 1024L}), want_p2p = std::max({lists.need_p2p, 16 * nn, 1024L});
+  if (const char* env = getenv("AMK_FMM_LIST_CAP")) {  // small first capacities (tests of the overflow retry)
+    const long v = atol(env);
+    if (v > 0) {
+      lists.cur.release();
+      lists.next.release();
+      lists.m2l.release();
+      lists.p2p.release();
+      want_front = want_m2l = want_p2p = v;
+    }
+  }
   for (int attempt = 0;; ++attempt) {
     if (attempt > 12) return fail(AMK_ERR_LIMIT, "FMM traversal: interaction lists did not fit");
     AMK_TRY(lists.cur.reserve(static_cast<size_t>(want_front) * sizeof(int2)));

@@ -195,3 +195,34 @@ def test_tensor_core_products_with_per_pair_path_and_chunk_seams(sim, monkeypatc
     # ratio ||dF|| / ||F|| (per particle on the cancelled ones it is larger)
     rel, glob = rel_errors(f, g["f_p6_theta0.5"].T)
     assert glob < 1e-6 and np.max(rel) < 1e-4, (glob, np.max(rel))
+
+
+def test_traversal_overflow_retry_gives_the_same_forces(monkeypatch):
+    # the traversal's lists start at 64 entries, so its first passes overflow
+    # and it runs again with larger lists: the same forces, bit for bit
+    import amk
+    x, y, z, q = gaussian_cloud(20000, 47, mixed=False)
+    with amk.Simulation() as s:
+        base = s.solve_fmm(x, y, z, q, 4, 0.5)
+        st0 = s.fmm_stats()
+        monkeypatch.setenv("AMK_FMM_LIST_CAP", "64")
+        got = s.solve_fmm(x, y, z, q, 4, 0.5)
+        st1 = s.fmm_stats()
+    assert all(np.array_equal(a, b) for a, b in zip(base, got))
+    assert st0["m2l_pairs"] == st1["m2l_pairs"] and st0["p2p_leaf_pairs"] == st1["p2p_leaf_pairs"]
+
+
+def test_tensor_mode_takes_at_least_the_fp64_class_pairs():
+    # the tensor-core mode folds classes below 4 pairs by reflection, so at
+    # least as many pairs are class products as in the FP64 mode, the same
+    # M2L pairs in total
+    import amk
+    x, y, z, q = gaussian_cloud(20000, 45, mixed=False)
+    with amk.Simulation() as s:
+        s.solve_fmm(x, y, z, q, 6, 0.5)
+        fp64 = s.fmm_stats()
+        s.set_fmm_precision("tensor")
+        s.solve_fmm(x, y, z, q, 6, 0.5)
+        tc = s.fmm_stats()
+    assert tc["m2l_pairs"] == fp64["m2l_pairs"]
+    assert tc["m2l_class_pairs"] >= fp64["m2l_class_pairs"], (tc, fp64)

@@ -143,3 +143,46 @@ def test_derivatives_match_closed_forms():
     # Laplace: D_(2,0,0) + D_(0,2,0) + D_(0,0,2) = 0, and likewise one degree up
     assert abs(D[index[(2, 0, 0)]] + D[index[(0, 2, 0)]] + D[index[(0, 0, 2)]]) < 1e-13 / r ** 3
     assert abs(D[index[(3, 1, 0)]] + D[index[(1, 3, 0)]] + D[index[(1, 1, 2)]]) < 1e-12 / r ** 5
+
+
+def test_derivatives_are_even_in_each_coordinate():
+    # D_k(R w) = s^k D_k(w) for a reflection R = diag(s), s^k = prod_i s_i^k_i:
+    # the identity that lets the tensor-core mode fold the 8 reflections of an
+    # offset into one class
+    p = 4
+    mi_d = multi_indices(2 * p)
+    index = {m: k for k, m in enumerate(mi_d)}
+    w = np.array([3.0, 2.0, 5.0])
+    Dw = derivatives(w, 2 * p, index)
+    for R in range(8):
+        s = np.array([-1.0 if (R >> i) & 1 else 1.0 for i in range(3)])
+        sk = np.array([s[0] ** a * s[1] ** b * s[2] ** c for a, b, c in mi_d])
+        np.testing.assert_allclose(derivatives(s * w, 2 * p, index), sk * Dw, rtol=1e-13, atol=0)
+
+
+@pytest.mark.parametrize("p", [3, 5])
+def test_reflected_class_matrix_is_the_signed_class_matrix_of_the_absolute_offset(p):
+    # A(v) = S_g A(|v|) S_a: the product of a folded pair is the class product
+    # of |v| with the source expansion taken with the signs s^a (the split
+    # copy of reflection R) and row g multiplied by s^g afterwards
+    mi_d = multi_indices(2 * p)
+    index = {m: k for k, m in enumerate(mi_d)}
+    n_m = (p + 1) * (p + 2) * (p + 3) // 6
+    mi = mi_d[:n_m]
+    deg = np.array([sum(m) for m in mi])
+    inv_fact = np.array([1.0 / (math.factorial(a) * math.factorial(b) * math.factorial(c)) for a, b, c in mi])
+    gpa = np.array([[index[(g[0] + a[0], g[1] + a[1], g[2] + a[2])] for a in mi] for g in mi])
+    rng = np.random.default_rng(11 + p)
+    for v in ([-3.0, 2.0, 4.0], [5.0, -1.0, -2.0], [-4.0, -4.0, 0.0], [0.0, 0.0, -3.0]):
+        v = np.array(v)
+        R = sum(1 << i for i in range(3) if v[i] < 0)
+        s = np.array([-1.0 if (R >> i) & 1 else 1.0 for i in range(3)])
+        sm = np.array([s[0] ** a * s[1] ** b * s[2] ** c for a, b, c in mi])
+        rt, rs = 2.0, 1.0
+        A_v = (inv_fact * rt ** (deg + 1))[:, None] * (rs ** deg)[None, :] * derivatives(v, 2 * p, index)[gpa]
+        A_w = (inv_fact * rt ** (deg + 1))[:, None] * (rs ** deg)[None, :] * \
+            derivatives(np.abs(v), 2 * p, index)[gpa]
+        Mh = rng.normal(size=n_m)
+        direct = A_v @ Mh
+        folded = sm * (A_w @ (sm * Mh))
+        np.testing.assert_allclose(folded, direct, rtol=1e-12, atol=1e-12 * np.abs(A_v).max())
