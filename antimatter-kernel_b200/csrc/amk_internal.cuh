@@ -108,7 +108,7 @@ struct View {
 
 // ---------------------------------------------------------------- context
 struct Scratch {
-  DevBuf b[96];
+  DevBuf b[128];
 };
 
 enum ScratchSlot {
@@ -208,9 +208,10 @@ enum ScratchSlot {
   kSlotM2lPairSrc,
   kSlotM2lTable3,
   kSlotM2lRefl,
+  kSlotFmmNodeRec,
   kNumSlots
 };
-static_assert(kNumSlots <= 96, "scratch slots");
+static_assert(kNumSlots <= 128, "scratch slots");
 
 struct PhaseClock {
   cudaEvent_t start[AMK_NUM_PHASES] = {};

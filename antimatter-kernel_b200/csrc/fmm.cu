@@ -442,6 +442,18 @@ fmm_m2m_kernel(const Octree t, FmmDevTables T, int depth, double* __restrict__ M
 // written). A pair that is not a pair of nodes raises cnt[3] and is
 // skipped. Warps stride over the level's pairs, so one grid size serves
 // every level.
+// Per node, what the traversal reads of it in one 32-byte record: the
+// centre and the radius, negated for a leaf (a leaf of radius 0 stores -0.0;
+// the sign bit is the leaf flag, the magnitude the radius).
+__global__ void fmm_node_record_kernel(const Octree t, const double* __restrict__ radius,
+                                       double4* __restrict__ rec) {
+  const int id = blockIdx.x * blockDim.x + threadIdx.x;
+  if (id >= t.n_nodes) return;
+  const double4 c = t.center[id];
+  const double r = radius[id];
+  rec[id] = make_double4(c.x, c.y, c.z, t.meta[id].y ? -r : r);
+}
+
 __global__ void fmm_traverse_root_kernel(int2* __restrict__ cur, int* __restrict__ lv) {
   if (threadIdx.x == 0) {
     cur[0] = make_int2(0, 0);
@@ -455,7 +467,7 @@ struct TraverseLists {
   long cap_m2l, cap_p2p, cap_front;
 };
 
-__global__ void fmm_traverse_kernel(const Octree t, const double* __restrict__ radius, double theta2,
+__global__ void fmm_traverse_kernel(const Octree t, const double4* __restrict__ rec, double theta2,
                                     const int2* __restrict__ cur, int2* __restrict__ next, TraverseLists out,
                                     int* __restrict__ lv, int* __restrict__ cnt) {
   const int lane = threadIdx.x & 31;
@@ -475,15 +487,15 @@ __global__ void fmm_traverse_kernel(const Octree t, const double* __restrict__ r
       cnt[3] = 1;  // not a node pair: recorded and skipped
     } else if (i < n_cur) {
       const int ti = pr.x, si = pr.y;
-      const double4 tc = t.center[ti], sc = t.center[si];
+      const double4 tc = rec[ti], sc = rec[si];
       const double dx = tc.x - sc.x, dy = tc.y - sc.y, dz = tc.z - sc.z;
       const double dist2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
-      const double rt = radius[ti], rs = radius[si];
+      const double rt = fabs(tc.w), rs = fabs(sc.w);
       const double rsum = rt + rs;
       if (__dmul_rn(rsum, rsum) < __dmul_rn(theta2, dist2)) {
         kind = 0;
       } else {
-        const bool tleaf = t.meta[ti].y, sleaf = t.meta[si].y;
+        const bool tleaf = signbit(tc.w), sleaf = signbit(sc.w);
         if (tleaf && sleaf) {
           kind = 1;
         } else {
@@ -2705,6 +2717,10 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
   unsigned long long* cnt64 = slot<unsigned long long>(c, kSlotFmmAux1, 4, &rc);
   AMK_TRY(rc);
   const double theta2 = theta * theta;
+  double4* rec = slot<double4>(c, kSlotFmmNodeRec, nn, &rc);
+  AMK_TRY(rc);
+  fmm_node_record_kernel<<<gn, 256, 0, c->stream>>>(t, radius, rec);
+  AMK_TRY(check_launch(c, "fmm_node_record_kernel"));
   long n_m2l = 0, n_p2p = 0;
   std::vector<int> hv(n_tv);
   unsigned long long h64[2] = {0, 0};
@@ -2740,7 +2756,7 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
     for (int level = 0; level < n_levels; ++level) {
       int2* a = (level & 1) ? lists.next.as<int2>() : lists.cur.as<int2>();
       int2* b = (level & 1) ? lists.cur.as<int2>() : lists.next.as<int2>();
-      fmm_traverse_kernel<<<grid, 256, 0, c->stream>>>(t, radius, theta2, a, b, tl, tv + 8 + level, tv);
+      fmm_traverse_kernel<<<grid, 256, 0, c->stream>>>(t, rec, theta2, a, b, tl, tv + 8 + level, tv);
       AMK_TRY(check_launch(c, "fmm_traverse_kernel"));
     }
     // statistics: leaves and P2P particle pairs (before self / min_sq skips)
