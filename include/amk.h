@@ -310,9 +310,11 @@ long amk_bh_tree_dump(amk_ctx* ctx, long n, const double* x, const double* y, co
  * products run on the 5th-generation tensor cores with split-BF16 operands
  * (three BF16 terms per operand, six products, FP32 accumulation in tensor
  * memory) and FP32 per-pair products summed in FP64; relative error of an
- * M2L term about 2^-22, below the truncation error of those orders. The
+ * M2L term about 2^-22, below the truncation error of those orders; classes
+ * of fewer than 4 pairs are folded by reflection into the class of |v|. The
  * near field (P2P) then runs in FP32 on double-float positions (pair
- * differences exact to FP32 rounding, FP64 sums per source leaf). Tree,
+ * differences exact to FP32 rounding for touching leaves, FP32 offsets from
+ * the centre of separated ones, FP64 sums per source leaf). Tree,
  * expansions, L2L and L2P stay FP64. The mode also selects FP32 leaf sums
  * (same double-float differences) in the Barnes-Hut walk, whose opening test
  * and node monopoles stay FP64. */
