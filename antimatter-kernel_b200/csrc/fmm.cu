@@ -2230,9 +2230,9 @@ __device__ __forceinline__ double4 l2p_fp64(const Octree& t, const FmmDevTables&
 // pass is packed whatever the leaf's size. The sources of a leaf are staged
 // by the warp in shared memory 64 at a time as pairs {x_hi, y_hi} {z_hi, q}
 // {x_lo, y_lo} {z_lo} of two sources each (broadcast reads; an odd count is
-// padded with a neutral source). Targets: two per lane while more than 32
-// remain, else one per lane, with the lanes split into groups over the source
-// pairs when 16 or fewer remain. A pair term is
+// padded with a neutral source). Targets: two per lane while more than 48
+// remain, else up to 32 at one per lane, with the lanes split into groups
+// over the source pairs when 16 or fewer remain. A pair term is
 //   r = (t_hi - s_hi) + (t_lo - s_lo)  (t - s formed as fma(s, -1, t)),
 // exact to FP32 rounding of |r| for neighbouring leaves (Sterbenz), and is
 // zero for a pair closer than the minimum distance (r^2 := +inf, so 1/r = 0;
@@ -2423,8 +2423,11 @@ fmm_p2p32_kernel(const Octree t, const int2* __restrict__ work, int n_work, cons
   };
   for (int base = tr.x; base < tr.y;) {
     const int rem = tr.y - base;
-    if (rem > 32) {
-      // ---- two targets per lane (the second may be past the leaf: computed, not written)
+    if (rem > 48) {
+      // ---- two targets per lane (the second may be past the leaf: computed, not written);
+      // with 33-48 left, a one-per-lane pass of 32 and a grouped pass of the
+      // rest cost less than the idle second slots (measured: 19.5 -> 19.3 ms
+      // per 1M step)
       const int i0 = base + lane, i1 = min(base + 32 + lane, tr.y - 1);
       P2PTarget t0, t1;
       p2p32_load_target(t0, shi, slo, i0);
@@ -2469,7 +2472,7 @@ fmm_p2p32_kernel(const Octree t, const int2* __restrict__ work, int n_work, cons
       continue;
     }
     // ---- at most 32 targets: one per lane, lanes in groups over the source pairs
-    const int nt = rem;
+    const int nt = min(rem, 32);
     const int groups = 32 / nt;
     const int g = lane / nt, tl = lane - g * nt;
     const bool active = g < groups;
