@@ -1249,7 +1249,7 @@ def run_kernels(args):
         tree_ms = ph["tree"][0] / max(ph["tree"][1], 1) - sort_ms  # the tree phase encloses the sort
         sb = 256.0 * n
         tb = 100.0 * n + 78.0 * nodes
-        out["radix sort (hist_kernel, scan, scatter_kernel)"] = {
+        out["radix sort (hist_kernel, scan, scatter_staged_kernel)"] = {
             "ms": sort_ms, "algorithmic_bytes": sb, "achieved_gbs": sb / (sort_ms * 1e-3) / 1e9,
             "frac": sb / (sort_ms * 1e-3) / 1e9 / hbm,
             "unit": "256 B per key: 8 passes of 8 B key read (histogram) + 12 B read + 12 B written (scatter)"}
