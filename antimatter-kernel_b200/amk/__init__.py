@@ -506,12 +506,13 @@ class Simulation:
 
     def autotune(self, error_budget=1e-5, samples=1024, flags=0):
         """Runs the autotuner; returns (candidates, chosen index)."""
-        out = (TuneCandidate * 128)()
+        cap = 256
+        out = (TuneCandidate * cap)()
         n, ch = C.c_int(0), C.c_int(-1)
-        rc = lib().amk_autotune(self._h, float(error_budget), int(samples), int(flags), out, 128, C.byref(n),
+        rc = lib().amk_autotune(self._h, float(error_budget), int(samples), int(flags), out, cap, C.byref(n),
                                 C.byref(ch))
         cands = [{"method": out[k].method, "order": out[k].order, "theta": out[k].theta, "leaf": out[k].leaf,
-                  "ms": out[k].ms, "rms": out[k].rms, "meets": bool(out[k].meets)} for k in range(n.value)]
+                  "ms": out[k].ms, "rms": out[k].rms, "meets": bool(out[k].meets)} for k in range(min(n.value, cap))]
         check(rc, "amk_autotune")
         return cands, ch.value
 
