@@ -47,3 +47,51 @@ def test_default_workload_is_the_1m_tree_solver_comparison():
     assert 'default="tree1m"' in src
     cfg = bench.tree_config(1 << 20, 2)
     assert cfg["n_particles"] == 1 << 20 and cfg["error_budget"] == 1e-5 and "replicas x2" in cfg["parallelism"]
+
+
+class _FakeSim:
+    """Stands in for amk.Simulation in tree_roofline: phase times, FMM
+    statistics and the FFMA probe of a tensor-mode p = 7 step."""
+
+    def __init__(self, near_ms, products_ms):
+        self.near_ms, self.products_ms = near_ms, products_ms
+
+    def set_profiling(self, on):
+        pass
+
+    def reset_phase_times(self):
+        pass
+
+    def step(self, n):
+        pass
+
+    def synchronize(self):
+        pass
+
+    def phase_times(self):
+        return {"fmm_m2l_products": (self.products_ms, 1), "fmm_m2l": (2 * self.products_ms, 1),
+                "fmm_near": (self.near_ms, 1)}
+
+    def fmm_stats(self):
+        return {"order": 7, "m2l_class_pairs": 13_000_000, "m2l_pairs": 13_100_000, "m2l_classes": 29_000,
+                "p2p_particle_pairs": 5_000_000_000}
+
+    def measure_fp32_peak(self):
+        return 72.0
+
+
+@pytest.mark.parametrize("near_ms,products_ms,kernel", [(6.7, 3.7, "fmm_p2p32_kernel"),
+                                                         (2.0, 3.7, "m2l_class_tc_kernel<7>")])
+def test_tree_roofline_reports_the_dominant_kernel(near_ms, products_ms, kernel):
+    # the roofline object describes whichever of the near-field pairs and the
+    # M2L class products takes longer per launch, and carries the other one
+    sys.path.insert(0, ROOT)
+    import bench
+    over = {"coulomb_method": "fast-multipole", "fast_multipole_order": 7, "precision": "tensor"}
+    r = bench.tree_roofline(_FakeSim(near_ms, products_ms), over, 1 << 20)
+    assert r["kernel"] == kernel and r["other_kernel"]["kernel"] != kernel
+    near = r if kernel == "fmm_p2p32_kernel" else r["other_kernel"]
+    assert near["achieved"] == pytest.approx(20.0 * 5e9 / (near_ms * 1e-3) / 1e12)
+    assert near["frac"] == pytest.approx(near["achieved"] / 72.0)
+    prod = r["other_kernel"] if kernel == "fmm_p2p32_kernel" else r
+    assert prod["achieved"] == pytest.approx(2.0 * 120 * 120 * 13e6 / (products_ms * 1e-3) / 1e12)
