@@ -2809,7 +2809,8 @@ int fmm_run(amk_ctx* c, const View& v, int order, double theta, long leaf_capaci
   AMK_TRY(phase_end(c, AMK_PHASE_FMM_LISTS));
 
   // ---- near-field set-up: work items (a target leaf and up to kP2PChunk
-  // source leaves of its list) and the per-item partial sums' layout
+  // source leaves of its list, kP2P32Chunk in the FP32 near field) and the
+  // per-item partial sums' layout
   double4* ef = slot<double4>(c, kSlotFmmWork4, t.m, &rc);
   AMK_TRY(rc);
   const double min_sq = kMinSquaredDistance / (hf.length * hf.length);
