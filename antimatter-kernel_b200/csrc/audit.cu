@@ -176,7 +176,7 @@ extern "C" int amk_autotune(amk_ctx* c, double error_budget, long samples, int f
   std::vector<amk_tune_candidate> cand;
   if (!(flags & AMK_TUNE_NO_ALLPAIRS)) cand.push_back({AMK_METHOD_ALLPAIRS, 0, 0.0, 0, 0.0, 0.0, 0});
   if (!(flags & AMK_TUNE_NO_FMM))
-    for (double theta : {0.6, 0.55, 0.525, 0.5, 0.475, 0.45, 0.4})
+    for (double theta : {0.6, 0.55, 0.5375, 0.525, 0.5, 0.475, 0.45, 0.4})
       for (int leaf : {16, 32, 64, 128, 256})
         for (int order : {4, 5, 6, 7, 8}) cand.push_back({AMK_METHOD_FAST_MULTIPOLE, order, theta, leaf, 0.0, 0.0, 0});
   if (!(flags & AMK_TUNE_NO_BARNES_HUT))

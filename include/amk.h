@@ -393,9 +393,9 @@ typedef struct amk_tune_candidate {
 #define AMK_TUNE_NO_BARNES_HUT 4
 /* Autotuner: on the context's own particles, times (CUDA events, median of
  * 3 after a warm call) and audits (amk_force_error with `samples`) the
- * all-pairs solver, the FMM for orders 4..8 x theta 0.6/0.55/0.525/0.5/
- * 0.475/0.45/0.4 x leaf 16/32/64/128/256 (higher orders skipped once a lower
- * one meets the budget; up to 179 candidates with the others) and
+ * all-pairs solver, the FMM for orders 4..8 x theta 0.6/0.55/0.5375/0.525/
+ * 0.5/0.475/0.45/0.4 x leaf 16/32/64/128/256 (higher orders skipped once a
+ * lower one meets the budget; up to 204 candidates with the others) and
  * Barnes-Hut for theta 0.5/0.3/0.2, then sets the context's Coulomb method,
  * order, theta and leaf size to the fastest candidate whose RMS error is
  * <= error_budget. out (max_out entries, may be NULL) receives every
